@@ -1,0 +1,225 @@
+/* meeuuw_b200 -- C ABI of the B200 (sm_100a) implementation of meeuuw's per-timestep hot path.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t passed as void*,
+ * launches stream-ordered work and returns an int status (MW_OK = 0).  Nothing allocates device
+ * memory: callers pass outputs and, where a routine needs scratch, a workspace whose size a
+ * *_workspace_bytes() query returns.  Problems a kernel detects (a particle outside [-1,1], an
+ * element without particles, ...) are OR-ed into an optional device int32 flag word `err`
+ * (MW_FLAG_*), which the caller reads when it needs the reference's exit semantics.
+ *
+ * Mesh: the reference's uniform Cartesian box (build_velocity_mesh.py:113-145,
+ * build_velocity_connectivity.py:63-92, build_pressure_connectivity.py).  Connectivity (icon_V,
+ * icon_P, local_to_globalV) is implied by mw_box and computed in the kernels.
+ *
+ * Each declaration names the reference function it replaces (file:line in cedrict/meeuuw).
+ */
+#ifndef MEEUUW_B200_H
+#define MEEUUW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (return values) ---- */
+#define MW_OK 0
+#define MW_ERR_BAD_ARG 1
+#define MW_ERR_CUDA 2
+#define MW_ERR_NOT_CONVERGED 3
+#define MW_ERR_WORKSPACE 4
+#define MW_ERR_DEVICE_FLAG 5
+
+/* ---- device flag bits (err word) ---- */
+#define MW_FLAG_R_OUT_OF_BOUNDS 1   /* locate_particles.py:61-62 "r value out of bounds" */
+#define MW_FLAG_T_OUT_OF_BOUNDS 2   /* locate_particles.py:63-64 "t value out of bounds" */
+#define MW_FLAG_ELEMENT_RANGE 4     /* a point maps to an element index outside the mesh */
+#define MW_FLAG_EMPTY_ELEMENT 8     /* meeuuw.py:1198-1199 "an element contains no particle" */
+#define MW_FLAG_NONFINITE 16        /* NaN/Inf met in a solver reduction */
+#define MW_FLAG_ITER_LIMIT 32       /* a bounded device loop gave up */
+
+#define MW_MAX_FIELDS 8
+
+#define MW_AVG_ARITHMETIC 0
+#define MW_AVG_GEOMETRIC 1
+#define MW_AVG_HARMONIC 2
+
+#define MW_SPACE_Q2 0        /* N_V on the 9 Q2 nodes (icon_V)          */
+#define MW_SPACE_Q1_ON_V 1   /* N_P on the 4 corner V nodes (icon_V[0:4]) */
+#define MW_SPACE_Q1 2        /* N_P on the 4 pressure nodes (icon_P)       */
+
+#define MW_MATERIAL_BOUSSINESQ 0 /* experiment0.py:254-264: rho0(1-alpha T), eta=exp(-gamma T) or eta0 */
+#define MW_MATERIAL_TWO 1        /* experiment1.py:104-111: rho, eta by particle material id          */
+
+typedef struct {
+  int32_t nelx, nelz;
+  double Lx, Lz, hx, hz; /* hx = Lx/nelx, hz = Lz/nelz as build_velocity_mesh.py:19-20 */
+} mw_box;
+
+typedef struct {
+  int32_t kind;
+  double rho0, alphaT, fk_gamma, eta0, hcond, hcapa, hprod;
+  double mat_rho[8], mat_eta[8];
+} mw_material;
+
+typedef struct { /* nodal (nn_V) fields interpolated onto particles; NULL entries are skipped */
+  const double *exx, *ezz, *exz, *q, *T;
+} mw_nodal5;
+
+typedef struct { /* per-particle outputs; NULL entries are not written (rho, eta required) */
+  double *exx, *ezz, *exz, *p, *T, *rho, *eta, *hcond, *hcapa, *hprod, *alpha;
+} mw_swarm_props;
+
+/* ======================= particle-in-cell (pic_functions.py) ======================= */
+
+/* locate_particles___box, pic_functions.py:108-137 (+ bounds check locate_particles.py:61-64).
+ * Inactive particles get r=t=0, iel=0. */
+int mw_locate_box(mw_box box, int64_t nparticle, const uint8_t* active, const double* x, const double* z,
+                  double* r, double* t, int32_t* iel, int32_t* err, void* stream);
+
+/* interpolate_field_on_particles, pic_functions.py:85-101, for nfield (<= MW_MAX_FIELDS) nodal
+ * fields at once; `fields` and `out` are HOST arrays of device pointers. */
+int mw_interp_q2(mw_box box, int64_t nparticle, const uint8_t* active, const double* r, const double* t,
+                 const int32_t* iel, int32_t nfield, const double* const* fields, double* const* out,
+                 void* stream);
+
+/* The five interpolations of meeuuw.py:1118-1125 fused with material_model (meeuuw.py:1154;
+ * experiment0.py:230-264 and experiment1.py:91-113).  `mat` is the int8 material id (may be NULL
+ * for MW_MATERIAL_BOUSSINESQ). */
+int mw_interp_material(mw_box box, int64_t nparticle, const uint8_t* active, const double* r, const double* t,
+                       const int32_t* iel, const int8_t* mat, mw_nodal5 nodal, mw_material m,
+                       mw_swarm_props out, void* stream);
+
+/* advect_particles___box, pic_functions.py:180-292 (RK 1, 2, 4).  x, z, active are updated in
+ * place; up/wp receive the particle velocities (may be NULL).  If dt_dev is not NULL the time step
+ * is read from that device scalar instead of `dt`. */
+int mw_advect_box(mw_box box, int32_t rk, double dt, const double* dt_dev, int64_t nparticle, double* x, double* z,
+                  uint8_t* active, const double* u, const double* w, double* up, double* wp, int32_t* err,
+                  void* stream);
+
+/* Counting sort of the active particles by element (no reference counterpart: it is the data
+ * structure behind the atomic-free projections below).  counts[nel], offsets[nel+1],
+ * order[nparticle]; bins are sorted by particle index. */
+size_t mw_bin_workspace_bytes(int32_t nel);
+int mw_bin_particles(int32_t nel, int64_t nparticle, const uint8_t* active, const int32_t* iel, int32_t* counts,
+                     int32_t* offsets, int32_t* order, void* work, size_t work_bytes, int32_t* err, void* stream);
+
+/* project_particles_on_elements, pic_functions.py:603-650 (nparticle_per_element = counts from
+ * mw_bin_particles).  Empty elements set MW_FLAG_EMPTY_ELEMENT. */
+int mw_project_elements(int32_t nel, const int32_t* offsets, const int32_t* order, const double* rho,
+                        const double* eta, int32_t averaging, double* rho_e, double* eta_e, int32_t* err,
+                        void* stream);
+
+/* project_particle_field_on_nodes_{1,2,3,4}, pic_functions.py:659-1053, for nfield fields at once
+ * (each with its own averaging); `averaging`, `phi`, `phi_nodal` are HOST arrays. */
+int mw_project_nodes(mw_box box, int32_t flavour, int32_t nfield, const int32_t* averaging, const int32_t* offsets,
+                     const int32_t* order, const double* r, const double* t, const double* const* phi,
+                     double* const* phi_nodal, void* stream);
+
+/* project_nodal_{V,P,T}field_onto_qpoints, project_nodal_field_onto_qpoints.py:12-62.
+ * N is the device (9 x m) basis table (N_V for MW_SPACE_Q2, N_P otherwise); phiq is (nel, 9). */
+int mw_nodal_to_qpoints(mw_box box, int32_t space, const double* N, const double* phi, double* phiq, void* stream);
+
+/* ======================= element assembly ======================= */
+
+#define MW_F64 0
+#define MW_F32 1
+
+typedef struct { /* inputs of build_matrix_stokes (build_matrix_stokes.py:18-64), device pointers */
+  const double *rhoq, *etaq, *JxWq, *jcbi00q, *jcbi01q, *jcbi10q, *jcbi11q, *gxq, *gzq; /* (nel, 9) */
+  const double* eta_e;                                                             /* (nel)    */
+  const double *N_V, *N_P, *dNdr_V, *dNdt_V, *dNdr_P, *dNdt_P; /* (9,9) / (9,4) basis tables     */
+  const uint8_t* bc_fix_V;                                     /* (Nfem_V)                       */
+  const double* bc_val_V;                                      /* (Nfem_V)                       */
+  double eta_ref, L_ref;
+} mw_stokes_in;
+
+typedef struct { /* outputs; VV arrays are float or double per `precision`; rhs always double */
+  void *VV_Stokes, *VV_K, *VV_G, *VV_GT, *VV_M, *VV_M_eta, *VV_H;
+  double *rhs_f, *rhs_h;
+} mw_stokes_out;
+
+/* build_matrix_stokes, build_matrix_stokes.py:18-278 (box, plane strain).  blocks=0 writes the
+ * full layout VV_Stokes (nel*468, :267-276), blocks=1 the K/G/GT/M/M_eta/H blocks (:235-265).
+ * Matches the COO index arrays II/JJ of meeuuw.py:884-1017. */
+size_t mw_assemble_stokes_workspace_bytes(mw_box box);
+int mw_assemble_stokes(mw_box box, int32_t blocks, int32_t precision, mw_stokes_in in, mw_stokes_out out, void* work,
+                       size_t work_bytes, void* stream);
+
+typedef struct { /* inputs of build_matrix_energy (build_matrix_energy.py:12-47) */
+  const double* T; /* (nn_V) previous-step temperature, T_mem */
+  const double *rhoq, *etaq, *Tq, *uq, *wq, *hcondq, *hcapaq, *alphaq, *hprodq, *exxq, *ezzq, *exzq, *JxWq;
+  const double *jcbi00q, *jcbi01q, *jcbi10q, *jcbi11q;
+  const double *N_T, *dNdr_T, *dNds_T;
+  const uint8_t* bc_fix_T;
+  const double* bc_val_T;
+  double dt, rho0;
+  const double* dt_dev; /* if not NULL, dt is read from this device scalar */
+  int32_t formulation;  /* 0 = "BA", 1 = "EBA" */
+} mw_energy_in;
+
+/* build_matrix_energy, build_matrix_energy.py:12-141: VV_T (nel*81, float or double) and rhs. */
+size_t mw_assemble_energy_workspace_bytes(mw_box box);
+int mw_assemble_energy(mw_box box, int32_t precision, mw_energy_in in, void* VV_T, double* rhs, void* work,
+                       size_t work_bytes, void* stream);
+
+/* ======================= FP64 derived fields and reductions ======================= */
+
+#define MW_PNORM_NONE 0
+#define MW_PNORM_SURFACE 1
+#define MW_PNORM_VOLUME 2
+
+typedef struct { double c[3], w[3]; } mw_gauss3; /* qcoords, qweights (quadrature_setup.py:13-15) */
+
+typedef struct {
+  double CFLnb, hx, hz, dt_max;
+  int32_t solve_T;
+} mw_dt_params;
+
+/* Scratch for the reductions below (partial sums). */
+size_t mw_post_workspace_bytes(void);
+
+/* compute_pressure_offset, compute_pressure_offset.py:12-66 (Cartesian): writes the device scalar
+ * *offset.  "surface" sums the top edge sequentially in element order as the reference does. */
+int mw_pressure_offset(mw_box box, int32_t normalisation, const double* p, const double* N_P, const double* JxWq,
+                       double volume, double* offset, void* work, size_t work_bytes, void* stream);
+
+/* p -= offset (meeuuw.py:1977) and compute_nodal_pressure (compute_nodal_pressure.py:8-21):
+ * q on V nodes.  offset may be NULL; q may be NULL (only the subtraction is done). */
+int mw_nodal_pressure(mw_box box, double* p, const double* offset, int32_t subtract_in_place, const double* N_P_n,
+                      double* q, void* stream);
+
+/* compute_nodal_strain_rate, compute_strain_rate.py:51-73.  The jcbi*n (nel, 9) arrays may be NULL
+ * for the uniform box (inverse Jacobian diag(2/hx, 2/hz)). */
+int mw_nodal_strain_rate(mw_box box, const double* u, const double* w, const double* dNdr_V_n,
+                         const double* dNdt_V_n, const double* jcbi00n, const double* jcbi01n, const double* jcbi10n,
+                         const double* jcbi11n, double* exx_n, double* ezz_n, double* exz_n, void* stream);
+
+/* compute_nodal_heat_flux, compute_nodal_heat_flux.py:12-40 -> dTdx_n, dTdz_n, qx_n, qz_n. */
+int mw_nodal_heat_flux(mw_box box, const double* T, const double* hcond_n, const double* dNdr_T_n,
+                       const double* dNdt_T_n, const double* jcbi00, const double* jcbi01, const double* jcbi10,
+                       const double* jcbi11, double* dTdx_n, double* dTdz_n, double* qx_n, double* qz_n,
+                       void* stream);
+
+/* compute_Nu, postprocessors.py:114-248: out13 = the reference's 13-tuple, Nu last. */
+size_t mw_nu_workspace_bytes(mw_box box);
+int mw_compute_nu(mw_box box, const double* T, const double* dTdx_n, const double* dTdz_n, const double* hcond_n,
+                  mw_gauss3 g, double* out13, void* work, size_t work_bytes, void* stream);
+
+/* compute_global_quantities, postprocessors.py:14-83 (the vrms, Tavrg and mass sums):
+ * out3 = {vrms, Tavrg, TM}.  Tq, rhoq may be NULL. */
+int mw_global_quantities(int64_t nq, const double* uq, const double* wq, const double* Tq, const double* rhoq,
+                         const double* JxWq, double volume, double* out3, void* work, size_t work_bytes,
+                         void* stream);
+
+/* Time step, meeuuw.py:2112-2139: state2 = {dt1_mem, dt2_mem} (device, updated),
+ * out3 = {dt, dt1, dt2} (device). */
+int mw_compute_dt(int64_t nn_V, const double* u, const double* w, int64_t nparticle, const double* swarm_hcond,
+                  const double* swarm_hcapa, const double* swarm_rho, mw_dt_params prm, double* state2,
+                  double* out3, void* work, size_t work_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

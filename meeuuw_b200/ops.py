@@ -1,0 +1,258 @@
+"""Tensor-level wrappers over the C ABI (device tensors in, device tensors out).
+
+Each function launches the CUDA kernels of ``libmeeuuw_b200.so`` on the current torch stream.
+Outputs are allocated here when not supplied; the hot loop (``meeuuw_b200.timestep``) passes
+preallocated buffers so that nothing is allocated per step.
+"""
+import ctypes
+
+import torch
+
+from . import _lib as L
+from ._lib import call, ptr, stream_ptr
+
+f64, i32, u8 = torch.float64, torch.int32, torch.uint8
+
+
+class Workspace:
+    """Grow-only device scratch owned by the caller (the library never allocates)."""
+
+    def __init__(self, device="cuda"):
+        self.device = device
+        self.buf = torch.empty(0, dtype=torch.uint8, device=device)
+
+    def get(self, nbytes):
+        nbytes = int(nbytes)
+        if self.buf.numel() < nbytes:
+            self.buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
+        return ctypes.c_void_p(self.buf.data_ptr()), ctypes.c_size_t(self.buf.numel())
+
+
+_ws = {}
+
+
+def workspace(tag="default"):
+    if tag not in _ws:
+        _ws[tag] = Workspace()
+    return _ws[tag]
+
+
+def _empty(n, dtype=f64, like=None):
+    dev = like.device if like is not None else "cuda"
+    return torch.empty(n, dtype=dtype, device=dev)
+
+
+def as_u8(active):
+    if active.dtype == torch.bool:
+        return active.view(torch.uint8)
+    if active.dtype != torch.uint8:
+        raise TypeError("active must be bool or uint8")
+    return active
+
+
+# ----------------------------------------------------------------------------- PIC
+def locate(box, active, x, z, r=None, t=None, iel=None, err=None):
+    n = x.numel()
+    r = _empty(n, like=x) if r is None else r
+    t = _empty(n, like=x) if t is None else t
+    iel = _empty(n, i32, like=x) if iel is None else iel
+    call("mw_locate_box", box, n, ptr(as_u8(active)), ptr(x), ptr(z), ptr(r), ptr(t), ptr(iel), ptr(err), stream_ptr())
+    return r, t, iel
+
+
+def interp(box, active, r, t, iel, fields, outs=None):
+    n = r.numel()
+    if outs is None:
+        outs = [_empty(n, like=r) for _ in fields]
+    for i in range(0, len(fields), L.MAX_FIELDS):
+        fs, os_ = fields[i:i + L.MAX_FIELDS], outs[i:i + L.MAX_FIELDS]
+        call("mw_interp_q2", box, n, ptr(as_u8(active)), ptr(r), ptr(t), ptr(iel), len(fs), L.ptr_array(fs),
+             L.ptr_array(os_), stream_ptr())
+    return outs
+
+
+def material_struct(cfg):
+    m = L.MwMaterial()
+    if cfg.material == "two_material":
+        m.kind = L.MATERIAL_TWO
+        for i, v in enumerate(cfg.mat_rho):
+            m.mat_rho[i] = v
+        for i, v in enumerate(cfg.mat_eta):
+            m.mat_eta[i] = v
+    else:
+        m.kind = L.MATERIAL_BOUSSINESQ
+    m.rho0, m.alphaT, m.fk_gamma, m.eta0 = cfg.rho0, cfg.alphaT, cfg.fk_gamma, 1.0
+    m.hcond, m.hcapa, m.hprod = cfg.hcond, cfg.hcapa, cfg.hprod
+    return m
+
+
+def interp_material(box, active, r, t, iel, mat, nodal, material, out):
+    """nodal: dict exx, ezz, exz, q, T (tensors or None); out: dict of per-particle tensors."""
+    nd = L.MwNodal5(*[ptr(nodal.get(k)) for k in ("exx", "ezz", "exz", "q", "T")])
+    op = L.MwSwarmProps(*[ptr(out.get(k)) for k in ("exx", "ezz", "exz", "p", "T", "rho", "eta", "hcond", "hcapa",
+                                                     "hprod", "alpha")])
+    call("mw_interp_material", box, r.numel(), ptr(as_u8(active)), ptr(r), ptr(t), ptr(iel), ptr(mat), nd, material,
+         op, stream_ptr())
+    return out
+
+
+def advect(box, rk, dt, x, z, active, u, w, up=None, wp=None, err=None, dt_dev=None):
+    call("mw_advect_box", box, int(rk), float(dt), ptr(dt_dev), x.numel(), ptr(x), ptr(z), ptr(as_u8(active)),
+         ptr(u), ptr(w), ptr(up), ptr(wp), ptr(err), stream_ptr())
+    return x, z, up, wp, active
+
+
+def bin_particles(nel, active, iel, counts=None, offsets=None, order=None, err=None):
+    n = iel.numel()
+    counts = _empty(nel, i32, like=iel) if counts is None else counts
+    offsets = _empty(nel + 1, i32, like=iel) if offsets is None else offsets
+    order = _empty(max(n, 1), i32, like=iel) if order is None else order
+    wp, wb = workspace("bin").get(L.lib().mw_bin_workspace_bytes(nel))
+    call("mw_bin_particles", nel, n, ptr(as_u8(active)), ptr(iel), ptr(counts), ptr(offsets), ptr(order), wp, wb,
+         ptr(err), stream_ptr())
+    return counts, offsets, order
+
+
+def project_elements(nel, offsets, order, rho, eta, averaging, rho_e=None, eta_e=None, err=None):
+    rho_e = _empty(nel, like=rho) if rho_e is None else rho_e
+    eta_e = _empty(nel, like=rho) if eta_e is None else eta_e
+    call("mw_project_elements", nel, ptr(offsets), ptr(order), ptr(rho), ptr(eta), L.AVG[averaging], ptr(rho_e),
+         ptr(eta_e), ptr(err), stream_ptr())
+    return rho_e, eta_e
+
+
+def project_nodes(box, flavour, fields, offsets, order, r, t, outs=None):
+    """fields: list of (phi, averaging) -> list of nodal arrays (nn_V)."""
+    nn = (2 * box.nelx + 1) * (2 * box.nelz + 1)
+    if outs is None:
+        outs = [_empty(nn, like=r) for _ in fields]
+    for i in range(0, len(fields), L.MAX_FIELDS):
+        fs, os_ = fields[i:i + L.MAX_FIELDS], outs[i:i + L.MAX_FIELDS]
+        avg = (ctypes.c_int32 * len(fs))(*[L.AVG[a] for _, a in fs])
+        call("mw_project_nodes", box, int(flavour), len(fs), avg, ptr(offsets), ptr(order), ptr(r), ptr(t),
+             L.ptr_array([p for p, _ in fs]), L.ptr_array(os_), stream_ptr())
+    return outs
+
+
+def nodal_to_qpoints(box, space, N, phi, out=None):
+    nel = box.nelx * box.nelz
+    out = _empty((nel, 9), like=phi) if out is None else out
+    call("mw_nodal_to_qpoints", box, int(space), ptr(N), ptr(phi), ptr(out), stream_ptr())
+    return out
+
+
+# ----------------------------------------------------------------------------- assembly
+def assemble_stokes(box, blocks, precision, q, tables, bc_fix_V, bc_val_V, eta_ref, L_ref, out=None):
+    """q: dict rhoq, etaq, JxWq, jcbi**q, gxq, gzq (nel,9) and eta_e (nel)."""
+    nel = box.nelx * box.nelz
+    nv = 2 * (2 * box.nelx + 1) * (2 * box.nelz + 1)
+    npp = (box.nelx + 1) * (box.nelz + 1)
+    dt = torch.float32 if precision == 1 else f64
+    dev = q["etaq"].device
+    if out is None:
+        if blocks:
+            out = dict(VV_K=torch.empty(nel * 324, dtype=dt, device=dev), VV_G=torch.empty(nel * 72, dtype=dt, device=dev),
+                       VV_GT=torch.empty(nel * 72, dtype=dt, device=dev), VV_M=torch.empty(nel * 16, dtype=dt, device=dev),
+                       VV_M_eta=torch.empty(nel * 16, dtype=dt, device=dev), VV_H=torch.empty(nel * 72, dtype=dt, device=dev))
+        else:
+            out = dict(VV_Stokes=torch.empty(nel * 468, dtype=dt, device=dev))
+        out["rhs_f"] = torch.empty(nv, dtype=f64, device=dev)
+        out["rhs_h"] = torch.empty(npp, dtype=f64, device=dev)
+    ins = L.MwStokesIn(*[ptr(q[k]) for k in ("rhoq", "etaq", "JxWq", "jcbi00q", "jcbi01q", "jcbi10q", "jcbi11q", "gxq",
+                                             "gzq", "eta_e")],
+                       *[ptr(tables[k]) for k in ("N_V", "N_P", "dNdr_V", "dNdt_V", "dNdr_P", "dNdt_P")],
+                       ptr(as_u8(bc_fix_V)), ptr(bc_val_V), float(eta_ref), float(L_ref))
+    outs = L.MwStokesOut(*[ptr(out.get(k)) for k in ("VV_Stokes", "VV_K", "VV_G", "VV_GT", "VV_M", "VV_M_eta", "VV_H",
+                                                     "rhs_f", "rhs_h")])
+    wp, wb = workspace("asm").get(L.lib().mw_assemble_stokes_workspace_bytes(box))
+    call("mw_assemble_stokes", box, int(bool(blocks)), int(precision), ins, outs, wp, wb, stream_ptr())
+    return out
+
+
+def assemble_energy(box, precision, T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, VV=None, rhs=None,
+                    dt_dev=None):
+    nel = box.nelx * box.nelz
+    nn = (2 * box.nelx + 1) * (2 * box.nelz + 1)
+    dty = torch.float32 if precision == 1 else f64
+    VV = torch.empty(nel * 81, dtype=dty, device=T.device) if VV is None else VV
+    rhs = torch.empty(nn, dtype=f64, device=T.device) if rhs is None else rhs
+    keys = ("rhoq", "etaq", "Tq", "uq", "wq", "hcondq", "hcapaq", "alphaq", "hprodq", "exxq", "ezzq", "exzq", "JxWq",
+            "jcbi00q", "jcbi01q", "jcbi10q", "jcbi11q")
+    ins = L.MwEnergyIn(ptr(T), *[ptr(q.get(k)) for k in keys], ptr(tables["N_V"]), ptr(tables["dNdr_V"]),
+                       ptr(tables["dNdt_V"]), ptr(as_u8(bc_fix_T)), ptr(bc_val_T), float(dt), float(rho0),
+                       ptr(dt_dev), 1 if formulation == "EBA" else 0)
+    wp, wb = workspace("asm").get(L.lib().mw_assemble_energy_workspace_bytes(box))
+    call("mw_assemble_energy", box, int(precision), ins, ptr(VV), ptr(rhs), wp, wb, stream_ptr())
+    return VV, rhs
+
+
+# ----------------------------------------------------------------------------- post
+PNORM = {"none": 0, "surface": 1, "volume": 2}
+
+
+def pressure_offset(box, normalisation, p, N_P, JxWq, volume, out=None):
+    out = torch.empty(1, dtype=f64, device=p.device) if out is None else out
+    wp, wb = workspace("post").get(L.lib().mw_post_workspace_bytes())
+    call("mw_pressure_offset", box, PNORM[normalisation], ptr(p), ptr(N_P), ptr(JxWq), float(volume), ptr(out), wp, wb,
+         stream_ptr())
+    return out
+
+
+def nodal_pressure(box, p, offset, N_P_n, q=None, subtract=True):
+    nn = (2 * box.nelx + 1) * (2 * box.nelz + 1)
+    q = torch.empty(nn, dtype=f64, device=p.device) if q is None else q
+    call("mw_nodal_pressure", box, ptr(p), ptr(offset), int(bool(subtract)), ptr(N_P_n), ptr(q), stream_ptr())
+    return q
+
+
+def nodal_strain_rate(box, u, w, tables, jcbi=None, out=None):
+    nn = u.numel()
+    out = [torch.empty(nn, dtype=f64, device=u.device) for _ in range(3)] if out is None else out
+    j = jcbi if jcbi is not None else (None, None, None, None)
+    call("mw_nodal_strain_rate", box, ptr(u), ptr(w), ptr(tables["dNdr_V_n"]), ptr(tables["dNdt_V_n"]),
+         *[ptr(a) for a in j], *[ptr(o) for o in out], stream_ptr())
+    return out
+
+
+def nodal_heat_flux(box, T, hcond_n, tables, jcbi=None, out=None):
+    nn = T.numel()
+    out = [torch.empty(nn, dtype=f64, device=T.device) for _ in range(4)] if out is None else out
+    j = jcbi if jcbi is not None else (None, None, None, None)
+    call("mw_nodal_heat_flux", box, ptr(T), ptr(hcond_n), ptr(tables["dNdr_V_n"]), ptr(tables["dNdt_V_n"]),
+         *[ptr(a) for a in j], *[ptr(o) for o in out], stream_ptr())
+    return out
+
+
+def gauss_struct():
+    from .fe_tables import gauss3
+    qc, qw = gauss3()
+    g = L.MwGauss3()
+    for i in range(3):
+        g.c[i], g.w[i] = qc[i], qw[i]
+    return g
+
+
+def compute_nu(box, T, dTdx, dTdz, hcond_n, out=None):
+    out = torch.empty(13, dtype=f64, device=T.device) if out is None else out
+    wp, wb = workspace("nu").get(L.lib().mw_nu_workspace_bytes(box))
+    call("mw_compute_nu", box, ptr(T), ptr(dTdx), ptr(dTdz), ptr(hcond_n), gauss_struct(), ptr(out), wp, wb,
+         stream_ptr())
+    return out
+
+
+def global_quantities(uq, wq, Tq, rhoq, JxWq, volume, out=None):
+    out = torch.empty(3, dtype=f64, device=uq.device) if out is None else out
+    wp, wb = workspace("post").get(L.lib().mw_post_workspace_bytes())
+    call("mw_global_quantities", uq.numel(), ptr(uq), ptr(wq), ptr(Tq), ptr(rhoq), ptr(JxWq), float(volume), ptr(out),
+         wp, wb, stream_ptr())
+    return out
+
+
+def compute_dt(u, w, hcond, hcapa, rho, CFLnb, hx, hz, dt_max, solve_T, state, out=None):
+    out = torch.empty(3, dtype=f64, device=u.device) if out is None else out
+    prm = L.MwDtParams(float(CFLnb), float(hx), float(hz), float(dt_max), int(bool(solve_T)))
+    wp, wb = workspace("post").get(L.lib().mw_post_workspace_bytes())
+    n = rho.numel()
+    call("mw_compute_dt", u.numel(), ptr(u), ptr(w), n, ptr(hcond), ptr(hcapa), ptr(rho), prm, ptr(state), ptr(out),
+         wp, wb, stream_ptr())
+    return out

@@ -43,7 +43,8 @@ k_assemble_stokes(mw_box b, mw_stokes_in in, int blocks, S* __restrict__ vv_full
   R* dNdz_P = dNdx_P + EB_S * 36;
   R* qin = dNdz_P + EB_S * 36;     // 5 arrays * EB*9 : rho, eta, JxW, gx, gz
   R* G0 = qin + 5 * EB_S * 9;      // EB*18*4 (fixed rows of G, for h)
-  double* bcv = reinterpret_cast<double*>(G0 + EB_S * 72);   // EB*18 values
+  // the float instantiation ends G0 at a 4-byte boundary: realign before the double array
+  double* bcv = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(G0 + EB_S * 72) + 15) & ~uintptr_t(15));
   int* bcf = reinterpret_cast<int*>(bcv + EB_S * 18);        // EB*18 flags
   S* outs = reinterpret_cast<S*>(bcf + EB_S * 18);           // staged element outputs
 
@@ -347,7 +348,7 @@ template <typename R>
 static size_t stokes_smem_bytes() {
   size_t n = 117 + 2 * EB_S * 81 + 2 * EB_S * 36 + 5 * EB_S * 9 + EB_S * 72;
   size_t bytes = n * sizeof(R);
-  bytes = (bytes + 7) & ~size_t(7);
+  bytes = ((bytes + 15) & ~size_t(15)) + 16;
   bytes += EB_S * 18 * sizeof(double) + EB_S * 18 * sizeof(int);
   bytes += (size_t)EB_S * 572 * sizeof(double);   // largest staged output (blocks layout, f64)
   return bytes;

@@ -219,6 +219,83 @@ int mw_compute_dt(int64_t nn_V, const double* u, const double* w, int64_t nparti
                   const double* swarm_hcapa, const double* swarm_rho, mw_dt_params prm, double* state2,
                   double* out3, void* work, size_t work_bytes, void* stream);
 
+/* ======================= matrix-free Stokes operator and solver ======================= */
+
+#define MW_SCHEME_CD_U_ETA 0 /* cd_u_eta.py:13-99: Schur PCG preconditioned by M_eta (Q1 mass / eta_e) */
+#define MW_SCHEME_UZAWA3 1   /* uzawa3_solver_L2.py:21-99: Schur PCG preconditioned by M             */
+
+typedef struct mw_stokes mw_stokes; /* opaque host-side handle; device memory is the caller's workspace */
+
+typedef struct {
+  double eta_ref, L_ref;  /* G scaling eta_ref/L_ref, build_matrix_stokes.py:157                    */
+  int32_t precisions;     /* bit 0: FP64 multigrid hierarchy, bit 1: FP32 hierarchy                */
+  int32_t coarse_min;     /* coarsen while both element counts stay >= coarse_min                   */
+  int32_t dense_max;      /* coarsest level solved with a dense inverse when its dofs <= dense_max   */
+  int32_t cheb_degree;    /* Chebyshev-Jacobi smoothing steps per pre/post sweep                     */
+  double cheb_ratio;      /* smoothing interval [lambda_max/ratio, lambda_max]                       */
+  double cheb_safety;     /* lambda_max estimate multiplier                                          */
+  int32_t power_iters;    /* power iterations for lambda_max(D^-1 K) per level                       */
+} mw_stokes_params;
+
+typedef struct {
+  int32_t scheme;         /* MW_SCHEME_*                                                             */
+  int32_t precision;      /* MW_F64: plain FP64; MW_F32: FP32 inner PCG + FP64 iterative refinement  */
+  double tol;             /* FP64 relative true residual ||b - A x|| / ||b|| target (e.g. 1e-8)      */
+  int32_t max_outer;      /* Schur-PCG iterations per run (the reference caps at 100)                */
+  int32_t max_inner;      /* multigrid-PCG iterations per K solve                                    */
+  double inner_rtol;      /* relative tolerance of each K solve                                      */
+  int32_t max_refine;     /* refinement sweeps (MW_F32)                                              */
+  double sweep_reduction; /* Schur residual reduction per refinement sweep (MW_F32)                  */
+  double mass_rtol;       /* relative tolerance of the M / M_eta solves                              */
+  int32_t mass_maxit;
+  int32_t use_guess;      /* 1: start from the solV/solP passed in (warm start)                      */
+} mw_solve_params;
+
+typedef struct {
+  int32_t outer_iters, inner_iters, refinements, converged;
+  double rel_residual, initial_rel_residual;
+} mw_solve_info;
+
+void mw_stokes_default_params(mw_stokes_params* p);
+void mw_solve_default_params(mw_solve_params* p);
+
+/* Device workspace the solver needs for this mesh and parameter set. */
+size_t mw_stokes_workspace_bytes(mw_box box, mw_stokes_params prm);
+
+/* Create a solver for the box with the velocity Dirichlet mask bc_fix_V (device, Nfem_V bytes,
+ * kept by reference).  All device arrays are carved from `work`. */
+int mw_stokes_create(mw_box box, mw_stokes_params prm, const uint8_t* bc_fix_V, void* work, size_t work_bytes,
+                     mw_stokes** out);
+int mw_stokes_destroy(mw_stokes* S);
+int mw_stokes_levels(const mw_stokes* S, int32_t precision);
+
+/* New viscosity (etaq (nel,9), eta_e (nel) or NULL): the data build_matrix_stokes.py reads. */
+int mw_stokes_set_viscosity(mw_stokes* S, const double* etaq, const double* eta_e, void* stream);
+
+/* Matrix-free y = [K G; G^T 0] (u, p) with the Dirichlet elimination of
+ * build_matrix_stokes.py:206-217 -- equal to SpMV with the assembled COO (meeuuw.py:1798).
+ * u or p may be NULL (treated as zero); yV or yP may be NULL (not computed). */
+int mw_stokes_apply(mw_stokes* S, const double* u, const double* p, double* yV, double* yP, void* stream);
+int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV, float* yP, void* stream);
+
+/* One multigrid V-cycle for K (the inner preconditioner); b, x in the given precision. */
+int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, void* stream);
+
+/* K x = b by multigrid-preconditioned CG (replaces splu(K).solve, uzawa3_solver_L2.py:37-38). */
+int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,
+                      int32_t* iters, double* relres, void* stream);
+
+/* FP64 residual (RV, RP) = (f, h) - A (V, P) and its 2-norm. */
+int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const double* f, const double* h, double* RV,
+                       double* RP, double* norm_out, void* stream);
+
+/* uzawa3_solver_L2 (uzawa3_solver_L2.py:21-99) / cd_u_eta (cd_u_eta.py:13-99) on the device: the
+ * Schur-complement PCG with K^-1 by multigrid PCG, stopped on the FP64 relative true residual.
+ * solV (Nfem_V, interleaved u,w) and solP (Nfem_P) receive the solution (solP is the unscaled
+ * Stokes pressure: the caller multiplies by eta_ref/L_ref as meeuuw.py:1848 does). */
+int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
+                    mw_solve_info* info, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,1332 @@
+// Matrix-free Q2xQ1 Stokes operator, geometric-multigrid PCG for the velocity block, and the
+// Uzawa (Schur-complement PCG) outer solver -- all on the device (sm_100a).
+//
+// Reference: the operator is the one assembled by build_matrix_stokes.py:18-278 (K, G with the
+// Dirichlet elimination of :206-217); the outer scheme is uzawa3_solver_L2.py:21-99 and its
+// M_eta-preconditioned form cd_u_eta.py:13-99; the reference solves K with SuperLU (splu), here
+// K^-1 is a multigrid-preconditioned conjugate gradient run on the device.
+//
+// Operator tiles: a CTA owns a TX x TZ tile of elements' nodes; it recomputes a one-element halo
+// on its left/bottom so that every owned node sums all its incident elements itself, in
+// ascending element order, from shared memory.  No atomics, deterministic results.  The element
+// kernel evaluates K u, G p, G^T u at the 3x3 Gauss points from the viscosity at the qpoints and
+// the uniform-box Jacobian (no stored element matrices).
+//
+// Dirichlet semantics (identical to SpMV with the reference's eliminated COO): fixed velocity
+// dofs are zeroed before the element products; fixed rows return diag(K)_i * u_i; G rows of
+// fixed dofs are zero.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mw {
+
+// ---------------------------------------------------------------- reference-element tables
+struct RefTables {
+  double dr[81], dt[81];   // d N_V / d r, d t at the 9 Gauss points  [q*9+k]
+  double NV[81];           // N_V at the Gauss points
+  double NP[36];           // N_P at the Gauss points   [q*4+k]
+  double wq[9];            // Gauss weights
+};
+__constant__ RefTables c_ref;
+static bool g_ref_ready = false;
+
+static void host_ref_tables(RefTables* T) {
+  const double qc[3] = {-std::sqrt(3.0 / 5.0), 0.0, std::sqrt(3.0 / 5.0)};
+  const double qw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  int q = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j, ++q) {
+      double r = qc[i], s = qc[j];
+      T->wq[q] = qw[i] * qw[j];
+      double N[9];
+      q2_basis<double>(r, s, N);
+      for (int k = 0; k < 9; ++k) T->NV[q * 9 + k] = N[k];
+      double dr[9] = {0.5 * (2.0 * r - 1.0) * 0.5 * s * (s - 1), 0.5 * (2.0 * r + 1.0) * 0.5 * s * (s - 1),
+                      0.5 * (2.0 * r + 1.0) * 0.5 * s * (s + 1), 0.5 * (2.0 * r - 1.0) * 0.5 * s * (s + 1),
+                      (-2.0 * r) * 0.5 * s * (s - 1), 0.5 * (2.0 * r + 1.0) * (1.0 - s * s),
+                      (-2.0 * r) * 0.5 * s * (s + 1), 0.5 * (2.0 * r - 1.0) * (1.0 - s * s), (-2.0 * r) * (1.0 - s * s)};
+      double dt[9] = {0.5 * r * (r - 1.0) * 0.5 * (2.0 * s - 1.0), 0.5 * r * (r + 1.0) * 0.5 * (2.0 * s - 1.0),
+                      0.5 * r * (r + 1.0) * 0.5 * (2.0 * s + 1.0), 0.5 * r * (r - 1.0) * 0.5 * (2.0 * s + 1.0),
+                      (1.0 - r * r) * 0.5 * (2.0 * s - 1.0), 0.5 * r * (r + 1.0) * (-2.0 * s),
+                      (1.0 - r * r) * 0.5 * (2.0 * s + 1.0), 0.5 * r * (r - 1.0) * (-2.0 * s), (1.0 - r * r) * (-2.0 * s)};
+      for (int k = 0; k < 9; ++k) { T->dr[q * 9 + k] = dr[k]; T->dt[q * 9 + k] = dt[k]; }
+      T->NP[q * 4 + 0] = 0.25 * (1 - r) * (1 - s);
+      T->NP[q * 4 + 1] = 0.25 * (1 + r) * (1 - s);
+      T->NP[q * 4 + 2] = 0.25 * (1 + r) * (1 + s);
+      T->NP[q * 4 + 3] = 0.25 * (1 - r) * (1 + s);
+    }
+}
+
+static int ensure_ref_tables() {
+  if (g_ref_ready) return MW_OK;
+  RefTables T;
+  host_ref_tables(&T);
+  if (cudaMemcpyToSymbol(c_ref, &T, sizeof(T)) != cudaSuccess) return MW_ERR_CUDA;
+  g_ref_ready = true;
+  return MW_OK;
+}
+
+// ---------------------------------------------------------------- level geometry
+struct LevelGeo {
+  int nx, nz;        // elements
+  int nnx, nnz;      // Q2 lattice nodes
+  double hx, hz;
+  double s;          // G scaling eta_ref / L_ref (build_matrix_stokes.py:157)
+};
+
+constexpr int TX = 16, TZ = 8;                 // owned element tile
+constexpr int EX = TX + 1, EZ = TZ + 1;        // with the left/bottom halo
+constexpr int NEL_T = EX * EZ;                 // 153 element computations per CTA
+constexpr int LX = 2 * TX + 3, LZ = 2 * TZ + 3;// staged lattice nodes (35 x 19)
+constexpr int PX = TX + 2, PZ = TZ + 2;        // staged pressure nodes (18 x 10)
+constexpr int APPLY_THREADS = 160;
+
+enum ApplyMode { AM_APPLY = 0, AM_RESID = 1, AM_CHEB = 2 };
+
+template <typename R>
+struct ApplyArgs {
+  const R* u;        // velocity (interleaved u,w), may be null
+  const R* p;        // pressure, may be null
+  const R* eta;      // (nel, 9)
+  const uint8_t* fix;// (2*nn)
+  const R* diag;     // (2*nn) assembled diag(K)
+  R* yV;             // output velocity part (AM_APPLY: K u + G p; AM_RESID: b - (...))
+  R* yP;             // output pressure part: G^T u (AM_RESID: h - G^T u); may be null
+  const R* bV;       // rhs for residual / Chebyshev
+  const R* bP;
+  // Chebyshev: d = c1*d + c2*Dinv*r; xo = x + d   (x = u)
+  R* d;
+  R* xo;
+  const double* cheb; // device coefficients {c1, c2}
+};
+
+// Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points.
+template <typename R>
+MW_D void element_apply(const LevelGeo& g, const R* ue, const R* pe, const R* eq, R* ye, R* ype, bool use_p) {
+  const R sx = R(2.0 / g.hx), sz = R(2.0 / g.hz);
+  const R jac = R(g.hx * g.hz / 4.0);
+  const R s = R(g.s);
+#pragma unroll
+  for (int k = 0; k < 18; ++k) ye[k] = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) ype[k] = 0;
+#pragma unroll 1
+  for (int q = 0; q < 9; ++q) {
+    R exx = 0, ezz = 0, g1 = 0, g2 = 0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const R dr = R(c_ref.dr[q * 9 + k]), dt = R(c_ref.dt[q * 9 + k]);
+      exx += dr * ue[2 * k];
+      ezz += dt * ue[2 * k + 1];
+      g1 += dt * ue[2 * k];
+      g2 += dr * ue[2 * k + 1];
+    }
+    exx *= sx; ezz *= sz;
+    const R gg = sz * g1 + sx * g2;                 // du/dz + dw/dx
+    const R jw = jac * R(c_ref.wq[q]);
+    const R e = eq[q] * jw;
+    R pq = 0;
+    if (use_p) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pq += R(c_ref.NP[q * 4 + k]) * pe[k];
+    }
+    const R A = R(2) * e * exx - s * jw * pq;
+    const R B = R(2) * e * ezz - s * jw * pq;
+    const R C = e * gg;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const R dx = sx * R(c_ref.dr[q * 9 + k]), dz = sz * R(c_ref.dt[q * 9 + k]);
+      ye[2 * k] += dx * A + dz * C;
+      ye[2 * k + 1] += dz * B + dx * C;
+    }
+    const R dv = -s * jw * (exx + ezz);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ype[k] += R(c_ref.NP[q * 4 + k]) * dv;
+  }
+}
+
+// local Q2 node index of lattice offset (dx, dz)
+MW_D int q2_local_idx(int dx, int dz) {
+  if (dz == 0) return dx == 0 ? 0 : (dx == 1 ? 4 : 1);
+  if (dz == 1) return dx == 0 ? 7 : (dx == 1 ? 8 : 5);
+  return dx == 0 ? 3 : (dx == 1 ? 6 : 2);
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(APPLY_THREADS)
+k_apply(LevelGeo g, ApplyArgs<R> a) {
+  __shared__ R su[LZ * LX * 2];
+  __shared__ R sp[PZ * PX];
+  __shared__ R sye[NEL_T * 22];
+  const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
+  const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
+  const int tid = threadIdx.x;
+  const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
+  // ---- stage velocity (masked), pressure, viscosity ----
+  for (int i = tid; i < LZ * LX; i += APPLY_THREADS) {
+    int lz = i / LX, lx = i % LX;
+    int ix = lx0 + lx, iz = lz0 + lz;
+    R u0 = 0, u1 = 0;
+    if (use_u && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
+      int64_t n = (int64_t)iz * g.nnx + ix;
+      u0 = a.fix[2 * n] ? R(0) : a.u[2 * n];
+      u1 = a.fix[2 * n + 1] ? R(0) : a.u[2 * n + 1];
+    }
+    su[2 * i] = u0; su[2 * i + 1] = u1;
+  }
+  if (use_p)
+    for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
+      int jz = i / PX, jx = i % PX;
+      int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
+      sp[i] = (px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz) ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+    }
+  __syncthreads();
+  // ---- element products ----
+  if (tid < NEL_T) {
+    int lex = tid % EX, lez = tid / EX;
+    int ex = ex0 - 1 + lex, ez = ez0 - 1 + lez;
+    if (ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz) {
+      R ue[18], pe[4], ye[18], ype[4];
+      const int bx = 2 * lex, bz = 2 * lez;          // staged lattice coords of local node 0
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        int li = (bz + q2_dz(k)) * LX + bx + q2_dx(k);
+        ue[2 * k] = su[2 * li]; ue[2 * k + 1] = su[2 * li + 1];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pe[k] = use_p ? sp[(lez + q1_dz(k)) * PX + lex + q1_dx(k)] : R(0);
+      R eq[9];
+      const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) eq[q] = eg[q];
+      element_apply<R>(g, ue, pe, eq, ye, ype, use_p);
+#pragma unroll
+      for (int k = 0; k < 18; ++k) sye[tid * 22 + k] = ye[k];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sye[tid * 22 + 18 + k] = ype[k];
+    }
+  }
+  __syncthreads();
+  // ---- owned velocity nodes: gather incident elements in ascending order ----
+  const int ox1 = (ex0 + TX >= g.nx) ? 2 * g.nx + 1 : 2 * (ex0 + TX);   // exclusive lattice end
+  const int oz1 = (ez0 + TZ >= g.nz) ? 2 * g.nz + 1 : 2 * (ez0 + TZ);
+  const int onx = ox1 - 2 * ex0, onz = oz1 - 2 * ez0;
+  if (a.yV) {
+    for (int i = tid; i < onx * onz; i += APPLY_THREADS) {
+      int ix = 2 * ex0 + i % onx, iz = 2 * ez0 + i / onx;
+      // incident elements (global), ascending (ez, ex)
+      int exs[2], ezs[2], nxe = 0, nze = 0;
+      if (ix & 1) exs[nxe++] = ix >> 1;
+      else { if (ix / 2 - 1 >= 0) exs[nxe++] = ix / 2 - 1; if (ix / 2 < g.nx) exs[nxe++] = ix / 2; }
+      if (iz & 1) ezs[nze++] = iz >> 1;
+      else { if (iz / 2 - 1 >= 0) ezs[nze++] = iz / 2 - 1; if (iz / 2 < g.nz) ezs[nze++] = iz / 2; }
+      R y0 = 0, y1 = 0;
+      for (int az = 0; az < nze; ++az)
+        for (int ax = 0; ax < nxe; ++ax) {
+          int lex = exs[ax] - (ex0 - 1), lez = ezs[az] - (ez0 - 1);
+          int k = q2_local_idx(ix - 2 * exs[ax], iz - 2 * ezs[az]);
+          const R* ye = sye + (lez * EX + lex) * 22;
+          y0 += ye[2 * k]; y1 += ye[2 * k + 1];
+        }
+      int64_t n = (int64_t)iz * g.nnx + ix;
+      R yy[2] = {y0, y1};
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        int64_t dof = 2 * n + c;
+        R y = yy[c];
+        if (a.fix[dof]) y = use_u ? a.diag[dof] * a.u[dof] : R(0);
+        if (MODE == AM_APPLY) {
+          a.yV[dof] = y;
+        } else if (MODE == AM_RESID) {
+          a.yV[dof] = a.bV[dof] - y;
+        } else {   // Chebyshev step
+          R r = a.bV[dof] - y;
+          R dn = R(a.cheb[0]) * a.d[dof] + R(a.cheb[1]) * r / a.diag[dof];
+          a.d[dof] = dn;
+          a.xo[dof] = a.u[dof] + dn;
+        }
+      }
+    }
+  }
+  // ---- owned pressure nodes ----
+  if (a.yP) {
+    const int px1 = (ex0 + TX >= g.nx) ? g.nx + 1 : ex0 + TX;
+    const int pz1 = (ez0 + TZ >= g.nz) ? g.nz + 1 : ez0 + TZ;
+    const int pnx = px1 - ex0, pnz = pz1 - ez0;
+    for (int i = tid; i < pnx * pnz; i += APPLY_THREADS) {
+      int px = ex0 + i % pnx, pz = ez0 + i / pnx;
+      const int exs[4] = {px - 1, px, px - 1, px};
+      const int ezs[4] = {pz - 1, pz - 1, pz, pz};
+      const int kk[4] = {2, 3, 1, 0};
+      R y = 0;
+      for (int s2 = 0; s2 < 4; ++s2) {
+        if (exs[s2] < 0 || exs[s2] >= g.nx || ezs[s2] < 0 || ezs[s2] >= g.nz) continue;
+        int lex = exs[s2] - (ex0 - 1), lez = ezs[s2] - (ez0 - 1);
+        y += sye[(lez * EX + lex) * 22 + 18 + kk[s2]];
+      }
+      int64_t n = (int64_t)pz * (g.nx + 1) + px;
+      a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
+    }
+  }
+}
+
+// diag(K): sum over incident elements of the element diagonal, ascending element order.
+template <typename R>
+__global__ void k_diag(LevelGeo g, const R* __restrict__ eta, R* __restrict__ diag) {
+  const int64_t nn = (int64_t)g.nnx * g.nnz;
+  const double sx = 2.0 / g.hx, sz = 2.0 / g.hz, jac = g.hx * g.hz / 4.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    int ix = (int)(n % g.nnx), iz = (int)(n / g.nnx);
+    int exs[2], ezs[2], nxe = 0, nze = 0;
+    if (ix & 1) exs[nxe++] = ix >> 1;
+    else { if (ix / 2 - 1 >= 0) exs[nxe++] = ix / 2 - 1; if (ix / 2 < g.nx) exs[nxe++] = ix / 2; }
+    if (iz & 1) ezs[nze++] = iz >> 1;
+    else { if (iz / 2 - 1 >= 0) ezs[nze++] = iz / 2 - 1; if (iz / 2 < g.nz) ezs[nze++] = iz / 2; }
+    double d0 = 0, d1 = 0;
+    for (int az = 0; az < nze; ++az)
+      for (int ax = 0; ax < nxe; ++ax) {
+        int k = q2_local_idx(ix - 2 * exs[ax], iz - 2 * ezs[az]);
+        const R* eq = eta + ((int64_t)ezs[az] * g.nx + exs[ax]) * 9;
+        for (int q = 0; q < 9; ++q) {
+          double dx = sx * c_ref.dr[q * 9 + k], dz = sz * c_ref.dt[q * 9 + k];
+          double e = (double)eq[q] * jac * c_ref.wq[q];
+          d0 += e * (2 * dx * dx + dz * dz);
+          d1 += e * (2 * dz * dz + dx * dx);
+        }
+      }
+    diag[2 * n] = (R)d0;
+    diag[2 * n + 1] = (R)d1;
+  }
+}
+
+// coarse viscosity: mean of the 36 fine qpoint values of the 2x2 children (element constant)
+template <typename R>
+__global__ void k_coarsen_eta(LevelGeo gc, const R* __restrict__ fine, R* __restrict__ coarse) {
+  const int64_t nel = (int64_t)gc.nx * gc.nz;
+  const int fnx = 2 * gc.nx;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    int ex = (int)(e % gc.nx), ez = (int)(e / gc.nx);
+    double s = 0;
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b) {
+        const R* f = fine + ((int64_t)(2 * ez + a) * fnx + (2 * ex + b)) * 9;
+        for (int q = 0; q < 9; ++q) s += (double)f[q];
+      }
+    R v = (R)(s / 36.0);
+    for (int q = 0; q < 9; ++q) coarse[e * 9 + q] = v;
+  }
+}
+
+// 1D Q2 restriction weights of coarse lattice node J from fine node 2J+o (o in -3..3)
+MW_D double rw(int J, int o) {
+  if (J & 1) return o == 0 ? 1.0 : ((o == -1 || o == 1) ? 0.75 : 0.0);
+  if (o == 0) return 1.0;
+  if (o == -1 || o == 1) return 0.375;
+  if (o == -3 || o == 3) return -0.125;
+  return 0.0;
+}
+
+template <typename R>
+__global__ void k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
+                           R* __restrict__ bc) {
+  const int64_t nn = (int64_t)gc.nnx * gc.nnz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
+    double s0 = 0, s1 = 0;
+    for (int oz = -3; oz <= 3; ++oz) {
+      double wz = rw(J, oz);
+      int fz = 2 * J + oz;
+      if (wz == 0.0 || fz < 0 || fz >= gf.nnz) continue;
+      for (int ox = -3; ox <= 3; ++ox) {
+        double wx = rw(I, ox);
+        int fx = 2 * I + ox;
+        if (wx == 0.0 || fx < 0 || fx >= gf.nnx) continue;
+        int64_t m = (int64_t)fz * gf.nnx + fx;
+        s0 += wz * wx * (double)rf[2 * m];
+        s1 += wz * wx * (double)rf[2 * m + 1];
+      }
+    }
+    bc[2 * n] = fixc[2 * n] ? R(0) : (R)s0;
+    bc[2 * n + 1] = fixc[2 * n + 1] ? R(0) : (R)s1;
+  }
+}
+
+// 1D Q2 prolongation: fine node i from coarse nodes
+MW_D int pw(int i, int* J, double* w) {
+  if (!(i & 1)) { J[0] = i / 2; w[0] = 1.0; return 1; }
+  int E = i / 4;
+  J[0] = 2 * E; J[1] = 2 * E + 1; J[2] = 2 * E + 2;
+  if ((i & 3) == 1) { w[0] = 0.375; w[1] = 0.75; w[2] = -0.125; }
+  else { w[0] = -0.125; w[1] = 0.75; w[2] = 0.375; }
+  return 3;
+}
+
+template <typename R>
+__global__ void k_prolong_add(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc, const uint8_t* __restrict__ fixf,
+                              R* __restrict__ xf) {
+  const int64_t nn = (int64_t)gf.nnx * gf.nnz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
+    int Jx[3], Jz[3];
+    double wx[3], wz[3];
+    int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
+    double s0 = 0, s1 = 0;
+    for (int a = 0; a < nzw; ++a)
+      for (int b = 0; b < nxw; ++b) {
+        int64_t m = (int64_t)Jz[a] * gc.nnx + Jx[b];
+        double w = wz[a] * wx[b];
+        s0 += w * (double)xc[2 * m];
+        s1 += w * (double)xc[2 * m + 1];
+      }
+    if (!fixf[2 * n]) xf[2 * n] += (R)s0;
+    if (!fixf[2 * n + 1]) xf[2 * n + 1] += (R)s1;
+  }
+}
+
+template <typename R>
+__global__ void k_fix_coarse(LevelGeo gc, const uint8_t* __restrict__ fixf, int fnnx, uint8_t* __restrict__ fixc) {
+  // a coarse dof is fixed when the coincident fine dof is fixed (same boundaries)
+  const int64_t nn = (int64_t)gc.nnx * gc.nnz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
+    int64_t m = (int64_t)(2 * J) * fnnx + 2 * I;
+    fixc[2 * n] = fixf[2 * m];
+    fixc[2 * n + 1] = fixf[2 * m + 1];
+  }
+}
+
+// ---------------------------------------------------------------- BLAS-1 with device scalars
+template <typename R>
+__global__ void k_dot_partial(int64_t n, const R* __restrict__ x, const R* __restrict__ y, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v += (double)x[i] * (double)y[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) part[blockIdx.x] = v;
+  }
+}
+
+__global__ void k_dot_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double v = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += part[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) out[0] = v;
+  }
+}
+
+// y += sgn * (num/den) * x      (scalars on the device)
+template <typename R, typename S>
+__global__ void k_axpy_ratio(int64_t n, const double* __restrict__ num, const double* __restrict__ den, double sgn,
+                             const S* __restrict__ x, R* __restrict__ y) {
+  const double a = sgn * (*num / *den);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (R)((double)y[i] + a * (double)x[i]);
+}
+
+// p = z + (num/den) * p
+template <typename R>
+__global__ void k_xpby_ratio(int64_t n, const R* __restrict__ z, const double* __restrict__ num,
+                             const double* __restrict__ den, R* __restrict__ p) {
+  const double b = *num / *den;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = (R)((double)z[i] + b * (double)p[i]);
+}
+
+template <typename R>
+__global__ void k_axpy(int64_t n, double a, const R* __restrict__ x, R* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (R)((double)y[i] + a * (double)x[i]);
+}
+
+template <typename R, typename S>
+__global__ void k_copy(int64_t n, const S* __restrict__ x, R* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (R)x[i];
+}
+
+template <typename R>
+__global__ void k_set(int64_t n, R v, R* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) y[i] = v;
+}
+
+// x = c * Dinv * b ; d = x   (first Chebyshev step from a zero guess)
+template <typename R>
+__global__ void k_cheb_first(int64_t n, const double* __restrict__ cheb, const R* __restrict__ b,
+                             const R* __restrict__ diag, R* __restrict__ x, R* __restrict__ d) {
+  const R c = (R)cheb[1];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    R v = c * b[i] / diag[i];
+    x[i] = v; d[i] = v;
+  }
+}
+
+// power iteration helpers for lambda_max(D^-1 K)
+template <typename R>
+__global__ void k_scale_dinv_norm(int64_t n, const R* __restrict__ y, const R* __restrict__ diag,
+                                  const double* __restrict__ nrm2, R* __restrict__ x) {
+  const double inv = 1.0 / sqrt(fmax(*nrm2, 1e-300));
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (R)((double)y[i] / (double)diag[i] * inv);
+}
+
+template <typename R>
+__global__ void k_dinv(int64_t n, const R* __restrict__ y, const R* __restrict__ diag, R* __restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = y[i] / diag[i];
+}
+
+// Chebyshev coefficients from lambda_max (stored at lam[0] as ||D^-1 K x||^2 with ||x|| = 1).
+__global__ void k_cheb_coeffs(const double* __restrict__ lam2, int degree, double ratio, double safety,
+                              double* __restrict__ coef) {
+  if (threadIdx.x || blockIdx.x) return;
+  double lmax = sqrt(fmax(*lam2, 1e-300)) * safety;
+  double lmin = lmax / ratio;
+  double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  coef[0] = 0.0;                             // step 0: d = (1/theta) D^-1 r
+  coef[1] = 1.0 / theta;
+  for (int k = 1; k < degree; ++k) {
+    double rn = 1.0 / (2.0 * sigma - rho);
+    coef[2 * k] = rn * rho;                  // c1: d = c1 d + c2 D^-1 r
+    coef[2 * k + 1] = 2.0 * rn / delta;
+    rho = rn;
+  }
+}
+
+// ---------------------------------------------------------------- coarsest level: dense inverse
+template <typename R>
+__global__ void k_dense_assemble(LevelGeo g, const R* __restrict__ eta, const uint8_t* __restrict__ fix,
+                                 double* __restrict__ A) {
+  const int nd = 2 * g.nnx * g.nnz;
+  for (int i = threadIdx.x; i < nd * nd; i += blockDim.x) A[i] = 0.0;
+  __syncthreads();
+  const double sx = 2.0 / g.hx, sz = 2.0 / g.hz, jac = g.hx * g.hz / 4.0;
+  for (int e = 0; e < g.nx * g.nz; ++e) {          // elements in order: deterministic sums
+    int ex = e % g.nx, ez = e / g.nx;
+    for (int t = threadIdx.x; t < 324; t += blockDim.x) {
+      int ii = t / 18, jj = t % 18;
+      int ki = ii >> 1, ci = ii & 1, kj = jj >> 1, cj = jj & 1;
+      double v = 0;
+      for (int q = 0; q < 9; ++q) {
+        double dxi = sx * c_ref.dr[q * 9 + ki], dzi = sz * c_ref.dt[q * 9 + ki];
+        double dxj = sx * c_ref.dr[q * 9 + kj], dzj = sz * c_ref.dt[q * 9 + kj];
+        double bb;
+        if (ci == 0 && cj == 0) bb = 2 * dxi * dxj + dzi * dzj;
+        else if (ci == 0) bb = dzi * dxj;
+        else if (cj == 0) bb = dxi * dzj;
+        else bb = 2 * dzi * dzj + dxi * dxj;
+        v += bb * (double)eta[(int64_t)e * 9 + q] * jac * c_ref.wq[q];
+      }
+      int gi = 2 * (int)q2_node(ex, ez, ki, g.nnx) + ci, gj = 2 * (int)q2_node(ex, ez, kj, g.nnx) + cj;
+      A[(int64_t)gi * nd + gj] += v;
+    }
+    __syncthreads();
+  }
+  // Dirichlet elimination: zero fixed rows/cols except the diagonal
+  for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
+    int i = t / nd, j = t % nd;
+    if (i != j && (fix[i] || fix[j])) A[t] = 0.0;
+  }
+}
+
+// In-place Gauss-Jordan inversion of an SPD matrix, one CTA.
+__global__ void k_gauss_jordan(int nd, double* __restrict__ A) {
+  extern __shared__ double col[];
+  for (int k = 0; k < nd; ++k) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) col[i] = A[(int64_t)i * nd + k];
+    __syncthreads();
+    const double piv = 1.0 / col[k];
+    for (int j = threadIdx.x; j < nd; j += blockDim.x) A[(int64_t)k * nd + j] = (j == k ? 1.0 : A[(int64_t)k * nd + j]) * piv;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
+      int i = t / nd, j = t % nd;
+      if (i == k) continue;
+      double f = col[i];
+      double akj = A[(int64_t)k * nd + j];
+      A[t] = (j == k ? 0.0 : A[t]) - f * akj;
+    }
+  }
+}
+
+template <typename R>
+__global__ void k_dense_matvec(int nd, const double* __restrict__ Ainv, const R* __restrict__ b, R* __restrict__ x) {
+  // one warp per row
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nd) return;
+  double s = 0;
+  for (int j = lane; j < nd; j += 32) s += Ainv[(int64_t)warp * nd + j] * (double)b[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[warp] = (R)s;
+}
+
+// ---------------------------------------------------------------- pressure mass matrices
+// y = M_w p with M_w the Q1 mass matrix weighted per element by w_e (w = NULL -> 1):
+// M_el = sum_q N_P N_P^T JxW (build_matrix_stokes.py:147), M_eta = M_el / eta_e (:264).
+__global__ void k_mass_apply(LevelGeo g, const double* __restrict__ w, const double* __restrict__ p,
+                             double* __restrict__ y) {
+  const int ncx = g.nx + 1;
+  const int64_t np = (int64_t)ncx * (g.nz + 1);
+  const double jac = g.hx * g.hz / 4.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(n % ncx), j = (int)(n / ncx);
+    const int exs[4] = {i - 1, i, i - 1, i};
+    const int ezs[4] = {j - 1, j - 1, j, j};
+    const int kk[4] = {2, 3, 1, 0};
+    double acc = 0;
+    for (int s = 0; s < 4; ++s) {
+      int ex = exs[s], ez = ezs[s];
+      if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+      int64_t e = (int64_t)ez * g.nx + ex;
+      double we = w ? w[e] : 1.0;
+      double v = 0;
+      for (int k2 = 0; k2 < 4; ++k2) {
+        double m = 0;
+        for (int q = 0; q < 9; ++q) m += c_ref.NP[q * 4 + kk[s]] * c_ref.NP[q * 4 + k2] * jac * c_ref.wq[q];
+        v += m * p[q1_node(ex, ez, k2, g.nx)];
+      }
+      acc += we * v;
+    }
+    y[n] = acc;
+  }
+}
+
+__global__ void k_mass_diag(LevelGeo g, const double* __restrict__ w, double* __restrict__ d) {
+  const int ncx = g.nx + 1;
+  const int64_t np = (int64_t)ncx * (g.nz + 1);
+  const double jac = g.hx * g.hz / 4.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x) {
+    int i = (int)(n % ncx), j = (int)(n / ncx);
+    const int exs[4] = {i - 1, i, i - 1, i};
+    const int ezs[4] = {j - 1, j - 1, j, j};
+    const int kk[4] = {2, 3, 1, 0};
+    double acc = 0;
+    for (int s = 0; s < 4; ++s) {
+      int ex = exs[s], ez = ezs[s];
+      if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+      int64_t e = (int64_t)ez * g.nx + ex;
+      double m = 0;
+      for (int q = 0; q < 9; ++q) m += c_ref.NP[q * 4 + kk[s]] * c_ref.NP[q * 4 + kk[s]] * jac * c_ref.wq[q];
+      acc += (w ? w[e] : 1.0) * m;
+    }
+    d[n] = acc;
+  }
+}
+
+// element weights 1/eta_e for M_eta (eta_e = mean of the qpoint viscosities of the element)
+__global__ void k_inv_eta_e(int64_t nel, const double* __restrict__ etaq, const double* __restrict__ eta_e,
+                            double* __restrict__ w) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    double v;
+    if (eta_e) v = eta_e[e];
+    else { v = 0; for (int q = 0; q < 9; ++q) v += etaq[e * 9 + q]; v /= 9.0; }
+    w[e] = 1.0 / v;
+  }
+}
+
+// remove the mean (pressure null space of a closed box): x -= sum(x)/n
+__global__ void k_sub_mean(int64_t n, const double* __restrict__ sum, double* __restrict__ x) {
+  const double m = *sum / (double)n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] -= m;
+}
+
+__global__ void k_sum_partial(int64_t n, const double* __restrict__ x, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) v += x[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) part[blockIdx.x] = v;
+  }
+}
+
+// ================================================================= solver object
+constexpr int NB = 296;           // reduction blocks
+constexpr int MAXLEV = 12;
+constexpr int MAXDEG = 8;
+
+template <typename R>
+struct Level {
+  LevelGeo g;
+  int64_t nn, ndof, nel;
+  R *eta, *diag, *x, *b, *r, *d, *t;
+  uint8_t* fix;
+  double* cheb;       // 2*MAXDEG coefficients
+  double* lam2;
+};
+
+struct Arena {
+  char* base;
+  size_t off, cap;
+  bool dry;
+  void* take(size_t bytes) {
+    off = (off + 255) & ~size_t(255);
+    void* p = dry ? nullptr : base + off;
+    off += bytes;
+    return p;
+  }
+};
+
+template <typename R>
+struct Hierarchy {
+  int nlev = 0;
+  Level<R> L[MAXLEV];
+  double* Ainv = nullptr;    // coarsest dense inverse (double)
+  int nd = 0;
+  bool dense = true;
+};
+
+}  // namespace mw
+
+struct mw_stokes {
+  mw::LevelGeo fine;
+  mw_stokes_params prm;
+  mw::Hierarchy<double> H64;
+  mw::Hierarchy<float> H32;
+  bool has64 = false, has32 = false;
+  // fine-level solver vectors (double): Uzawa and FP64 residuals
+  double *V, *P, *f, *h, *z, *rP, *wP, *dP, *Gd, *GTz, *RV, *RP, *tP, *tP2, *minv_w, *mdiag, *medi;
+  double *cV, *cP;       // refinement corrections
+  double* diag64;        // assembled diag(K) of the fine level, FP64
+  bool dirty64 = true, dirty32 = true;
+  double* etae_w;        // 1/eta_e per element (M_eta weights)
+  double* red;           // reduction partials
+  double* sc;            // device scalars
+  // inner PCG vectors (precision of the hierarchy): x, r, z, p, Ap
+  double *pc64[5];
+  float *pc32[5];
+  const uint8_t* fixV;   // fine fixed mask (caller's)
+  double* etaq64;        // fine viscosity (double copy)
+  float* etaq32;
+  mw_solve_info last;
+};
+
+namespace mw {
+
+template <typename R>
+static void plan_levels(Hierarchy<R>& H, const LevelGeo& fine, const mw_stokes_params& prm) {
+  H.nlev = 0;
+  LevelGeo g = fine;
+  while (true) {
+    Level<R>& l = H.L[H.nlev++];
+    l.g = g;
+    l.nn = (int64_t)g.nnx * g.nnz; l.ndof = 2 * l.nn; l.nel = (int64_t)g.nx * g.nz;
+    bool can = (g.nx % 2 == 0) && (g.nz % 2 == 0) && (g.nx / 2 >= prm.coarse_min) && (g.nz / 2 >= prm.coarse_min) &&
+               H.nlev < MAXLEV && (l.nel > (int64_t)prm.coarse_min * prm.coarse_min);
+    if (!can) break;
+    LevelGeo c = g;
+    c.nx = g.nx / 2; c.nz = g.nz / 2; c.nnx = 2 * c.nx + 1; c.nnz = 2 * c.nz + 1; c.hx = 2 * g.hx; c.hz = 2 * g.hz;
+    g = c;
+  }
+  const Level<R>& lc = H.L[H.nlev - 1];
+  H.nd = (int)lc.ndof;
+  H.dense = H.nd <= prm.dense_max;
+}
+
+template <typename R>
+static void carve(Hierarchy<R>& H, Arena& A, const uint8_t* fine_fix) {
+  for (int l = 0; l < H.nlev; ++l) {
+    Level<R>& L = H.L[l];
+    L.eta = (R*)A.take(sizeof(R) * L.nel * 9);
+    L.diag = (R*)A.take(sizeof(R) * L.ndof);
+    L.x = (R*)A.take(sizeof(R) * L.ndof);
+    L.b = (R*)A.take(sizeof(R) * L.ndof);
+    L.r = (R*)A.take(sizeof(R) * L.ndof);
+    L.d = (R*)A.take(sizeof(R) * L.ndof);
+    L.t = (R*)A.take(sizeof(R) * L.ndof);
+    L.fix = l == 0 ? const_cast<uint8_t*>(fine_fix) : (uint8_t*)A.take(L.ndof);
+    L.cheb = (double*)A.take(sizeof(double) * 2 * MAXDEG);
+    L.lam2 = (double*)A.take(sizeof(double) * 4);
+  }
+  H.Ainv = H.dense ? (double*)A.take(sizeof(double) * (size_t)H.nd * H.nd) : nullptr;
+}
+
+static size_t layout(mw_stokes* S, Arena& A) {
+  const LevelGeo& g = S->fine;
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1), nel = (int64_t)g.nx * g.nz;
+  double** dv[] = {&S->V, &S->z, &S->f, &S->Gd, &S->RV, &S->cV, &S->diag64};
+  for (auto p : dv) *p = (double*)A.take(sizeof(double) * nv);
+  double** pv[] = {&S->P, &S->h, &S->rP, &S->wP, &S->dP, &S->GTz, &S->RP, &S->tP, &S->tP2, &S->minv_w, &S->mdiag,
+                   &S->medi, &S->cP};
+  for (auto p : pv) *p = (double*)A.take(sizeof(double) * np);
+  S->etae_w = (double*)A.take(sizeof(double) * nel);
+  S->red = (double*)A.take(sizeof(double) * NB * 4);
+  S->sc = (double*)A.take(sizeof(double) * 64);
+  if (S->has64) {
+    for (int i = 0; i < 5; ++i) S->pc64[i] = (double*)A.take(sizeof(double) * nv);
+    carve(S->H64, A, S->fixV);
+    S->etaq64 = S->H64.L[0].eta;
+  } else {
+    S->etaq64 = (double*)A.take(sizeof(double) * nel * 9);
+  }
+  if (S->has32) {
+    for (int i = 0; i < 5; ++i) S->pc32[i] = (float*)A.take(sizeof(float) * nv);
+    carve(S->H32, A, S->fixV);
+    S->etaq32 = S->H32.L[0].eta;
+  }
+  return A.off + 256;
+}
+
+// ---------------------------------------------------------------- launch helpers
+template <typename R, int MODE>
+static void launch_apply(const LevelGeo& g, const ApplyArgs<R>& a, cudaStream_t s) {
+  dim3 grid((g.nx + TX - 1) / TX, (g.nz + TZ - 1) / TZ);
+  k_apply<R, MODE><<<grid, APPLY_THREADS, 0, s>>>(g, a);
+}
+
+template <typename R>
+static ApplyArgs<R> args0() {
+  ApplyArgs<R> a;
+  memset(&a, 0, sizeof(a));
+  return a;
+}
+
+template <typename R>
+static void dot(mw_stokes* S, int64_t n, const R* x, const R* y, double* out, cudaStream_t s) {
+  k_dot_partial<R><<<NB, 256, 0, s>>>(n, x, y, S->red);
+  k_dot_final<<<1, 256, 0, s>>>(S->red, NB, out);
+}
+
+static void dsum(mw_stokes* S, int64_t n, const double* x, double* out, cudaStream_t s) {
+  k_sum_partial<<<NB, 256, 0, s>>>(n, x, S->red);
+  k_dot_final<<<1, 256, 0, s>>>(S->red, NB, out);
+}
+
+template <typename R>
+static void k_only_apply(const Level<R>& L, const R* x, R* y, cudaStream_t s) {
+  ApplyArgs<R> a = args0<R>();
+  a.u = x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = y;
+  launch_apply<R, AM_APPLY>(L.g, a, s);
+}
+
+// Chebyshev smoothing of level L: x (in/out) with rhs b, `steps` steps; zero_start -> x = 0 on entry.
+template <typename R>
+static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s) {
+  const int64_t n = L.ndof;
+  int k0 = 0;
+  if (zero_start) {
+    k_cheb_first<R><<<grid_for(n, 256), 256, 0, s>>>(n, L.cheb, L.b, L.diag, L.x, L.d);
+    k0 = 1;
+  } else {
+    // restart the recurrence: first step from the current x: d = (1/theta) D^-1 r; x += d
+    ApplyArgs<R> a = args0<R>();
+    a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
+    a.cheb = L.cheb;                    // step-0 pair {0, 1/theta}
+    launch_apply<R, AM_CHEB>(L.g, a, s);
+    std::swap(L.x, L.t);
+    k0 = 1;
+  }
+  for (int k = k0; k < degree; ++k) {
+    ApplyArgs<R> a = args0<R>();
+    a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
+    a.cheb = L.cheb + 2 * k;
+    launch_apply<R, AM_CHEB>(L.g, a, s);
+    std::swap(L.x, L.t);
+  }
+}
+
+template <typename R>
+static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s) {
+  Level<R>& L = H.L[l];
+  if (l == H.nlev - 1) {
+    if (H.dense) {
+      int nd = H.nd;
+      k_dense_matvec<R><<<(nd * 32 + 255) / 256, 256, 0, s>>>(nd, H.Ainv, L.b, L.x);
+    } else {
+      smooth(L, MAXDEG, true, s);
+    }
+    return;
+  }
+  Level<R>& C = H.L[l + 1];
+  smooth(L, degree, true, s);
+  ApplyArgs<R> a = args0<R>();
+  a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.r; a.bV = L.b;
+  launch_apply<R, AM_RESID>(L.g, a, s);
+  k_restrict<R><<<grid_for(C.nn, 256), 256, 0, s>>>(L.g, C.g, L.r, C.fix, C.b);
+  vcycle(H, l + 1, degree, s);
+  k_prolong_add<R><<<grid_for(L.nn, 256), 256, 0, s>>>(L.g, C.g, C.x, L.fix, L.x);
+  smooth(L, degree, false, s);
+}
+
+template <typename R>
+__global__ void k_power_init(int64_t n, R* __restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (R)(1.0 + 0.5 * sin(0.7 * (double)i));
+}
+
+template <typename R>
+__global__ void k_normalize(int64_t n, const double* __restrict__ nrm2, R* __restrict__ v) {
+  const double inv = 1.0 / sqrt(fmax(*nrm2, 1e-300));
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (R)((double)v[i] * inv);
+}
+
+// Build the hierarchy for the fine viscosity already in L[0].eta: coarse viscosities, fixed
+// masks, diagonals, lambda_max(D^-1 K) by power iteration and the Chebyshev coefficients, and the
+// dense inverse of the coarsest operator.  No host synchronisation.
+template <typename R>
+static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
+  const mw_stokes_params& prm = S->prm;
+  for (int l = 0; l < H.nlev; ++l) {
+    Level<R>& L = H.L[l];
+    if (l > 0) {
+      Level<R>& F = H.L[l - 1];
+      k_coarsen_eta<R><<<grid_for(L.nel, 256), 256, 0, s>>>(L.g, F.eta, L.eta);
+      k_fix_coarse<R><<<grid_for(L.nn, 256), 256, 0, s>>>(L.g, F.fix, F.g.nnx, L.fix);
+    }
+    k_diag<R><<<grid_for(L.nn, 128), 128, 0, s>>>(L.g, L.eta, L.diag);
+    const bool coarsest = l == H.nlev - 1;
+    if (coarsest && H.dense) {
+      k_dense_assemble<R><<<1, 1024, 0, s>>>(L.g, L.eta, L.fix, H.Ainv);
+      k_gauss_jordan<<<1, 1024, sizeof(double) * H.nd, s>>>(H.nd, H.Ainv);
+      continue;
+    }
+    R* v = L.r;
+    R* t = L.t;
+    k_power_init<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, v);
+    for (int it = 0; it < prm.power_iters; ++it) {
+      dot<R>(S, L.ndof, v, v, L.lam2 + 1, s);
+      k_normalize<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.lam2 + 1, v);
+      k_only_apply<R>(L, v, L.d, s);
+      k_dinv<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.d, L.diag, t);
+      std::swap(v, t);
+    }
+    dot<R>(S, L.ndof, v, v, L.lam2, s);          // ||D^-1 K v_prev||^2 with ||v_prev|| = 1
+    int deg = coarsest ? MAXDEG : prm.cheb_degree;
+    k_cheb_coeffs<<<1, 32, 0, s>>>(L.lam2, deg, prm.cheb_ratio, prm.cheb_safety, L.cheb);
+  }
+  return cudaGetLastError() == cudaSuccess ? MW_OK : MW_ERR_CUDA;
+}
+
+static double read_scalar(const double* d, cudaStream_t s) {
+  double h = 0;
+  cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return h;
+}
+
+// Preconditioned CG for K x = b (b in double), MG V-cycle preconditioner at precision R.
+// x is written (overwritten) in double.  Returns iterations; *relres = ||r|| / ||b||.
+template <typename R>
+static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double* x, double rtol, int maxit,
+                 double* relres, cudaStream_t s) {
+  Level<R>& L = H.L[0];
+  const int64_t n = L.ndof;
+  R *xr = pc[0], *r = pc[1], *z = pc[2], *p = pc[3], *Ap = pc[4];
+  double* sc = S->sc;   // [0] rz, [1] pAp, [2] rr, [3] bb, [4] rz_new
+  k_copy<R, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
+  k_set<R><<<grid_for(n, 256), 256, 0, s>>>(n, R(0), xr);
+  dot<R>(S, n, r, r, sc + 3, s);
+  double bb = read_scalar(sc + 3, s);
+  if (!(bb > 0)) {
+    k_set<double><<<grid_for(n, 256), 256, 0, s>>>(n, 0.0, x);
+    *relres = 0;
+    return 0;
+  }
+  auto precond = [&](const R* rin, R* zout) {
+    k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, rin, L.b);
+    vcycle(H, 0, S->prm.cheb_degree, s);
+    k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, L.x, zout);
+  };
+  precond(r, z);
+  k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
+  dot<R>(S, n, r, z, sc + 0, s);
+  int it = 0;
+  double rr = bb;
+  for (it = 1; it <= maxit; ++it) {
+    k_only_apply<R>(L, p, Ap, s);
+    dot<R>(S, n, p, Ap, sc + 1, s);
+    k_axpy_ratio<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, 1.0, p, xr);
+    k_axpy_ratio<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, -1.0, Ap, r);
+    dot<R>(S, n, r, r, sc + 2, s);
+    rr = read_scalar(sc + 2, s);
+    if (!std::isfinite(rr)) break;
+    if (rr <= rtol * rtol * bb) break;
+    precond(r, z);
+    dot<R>(S, n, r, z, sc + 4, s);
+    k_xpby_ratio<R><<<grid_for(n, 256), 256, 0, s>>>(n, z, sc + 4, sc + 0, p);
+    cudaMemcpyAsync(sc + 0, sc + 4, sizeof(double), cudaMemcpyDeviceToDevice, s);
+  }
+  k_copy<double, R><<<grid_for(n, 256), 256, 0, s>>>(n, xr, x);
+  *relres = std::sqrt(rr / bb);
+  return it > maxit ? maxit : it;
+}
+
+// Jacobi-PCG for the (weighted) Q1 mass matrix: M_w x = b.  weights NULL -> M (uzawa3),
+// weights = 1/eta_e -> M_eta (cd_u_eta).
+static int mass_solve(mw_stokes* S, const double* w, const double* b, double* x, double rtol, int maxit,
+                      cudaStream_t s) {
+  const LevelGeo& g = S->fine;
+  const int64_t n = (int64_t)(g.nx + 1) * (g.nz + 1);
+  double *r = S->tP, *z = S->tP2, *p = S->minv_w, *Ap = S->medi, *dg = S->mdiag;
+  double* sc = S->sc + 16;
+  k_mass_diag<<<grid_for(n, 256), 256, 0, s>>>(g, w, dg);
+  k_copy<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
+  k_set<double><<<grid_for(n, 256), 256, 0, s>>>(n, 0.0, x);
+  dot<double>(S, n, r, r, sc + 3, s);
+  double bb = read_scalar(sc + 3, s);
+  if (!(bb > 0)) return 0;
+  k_dinv<double><<<grid_for(n, 256), 256, 0, s>>>(n, r, dg, z);
+  k_copy<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
+  dot<double>(S, n, r, z, sc + 0, s);
+  int it;
+  for (it = 1; it <= maxit; ++it) {
+    k_mass_apply<<<grid_for(n, 256), 256, 0, s>>>(g, w, p, Ap);
+    dot<double>(S, n, p, Ap, sc + 1, s);
+    k_axpy_ratio<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, 1.0, p, x);
+    k_axpy_ratio<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, -1.0, Ap, r);
+    if (it % 8 == 0 || it == maxit) {
+      dot<double>(S, n, r, r, sc + 2, s);
+      double rr = read_scalar(sc + 2, s);
+      if (!(rr > rtol * rtol * bb)) break;
+    }
+    k_dinv<double><<<grid_for(n, 256), 256, 0, s>>>(n, r, dg, z);
+    dot<double>(S, n, r, z, sc + 4, s);
+    k_xpby_ratio<double><<<grid_for(n, 256), 256, 0, s>>>(n, z, sc + 4, sc + 0, p);
+    cudaMemcpyAsync(sc + 0, sc + 4, sizeof(double), cudaMemcpyDeviceToDevice, s);
+  }
+  return it;
+}
+
+static void remove_mean(mw_stokes* S, int64_t n, double* x, cudaStream_t s) {
+  dsum(S, n, x, S->sc + 40, s);
+  k_sub_mean<<<grid_for(n, 256), 256, 0, s>>>(n, S->sc + 40, x);
+}
+
+// Full saddle residual in FP64: (RV, RP) = (f, h) - [K G; G^T 0] (V, P).  Returns ||R||/||b||
+// when bnorm > 0 (bnorm = ||(f, h)||), else ||R||.
+static double true_residual(mw_stokes* S, const double* V, const double* P, const double* f, const double* h,
+                            double bnorm, cudaStream_t s) {
+  const LevelGeo& g = S->fine;
+  ApplyArgs<double> a = args0<double>();
+  a.u = V; a.p = P; a.eta = S->etaq64; a.fix = S->fixV;
+  a.diag = S->diag64;
+  a.yV = S->RV; a.yP = S->RP; a.bV = f; a.bP = h;
+  launch_apply<double, AM_RESID>(g, a, s);
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  dot<double>(S, nv, S->RV, S->RV, S->sc + 50, s);
+  dot<double>(S, np, S->RP, S->RP, S->sc + 51, s);
+  double a2[2];
+  cudaMemcpyAsync(a2, S->sc + 50, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  double r = std::sqrt(a2[0] + a2[1]);
+  return bnorm > 0 ? r / bnorm : r;
+}
+
+// Inner K solve at the requested precision.
+static int ensure_hierarchy(mw_stokes* S, int prec, cudaStream_t s) {
+  if (prec == MW_F32) {
+    if (!S->has32) return MW_ERR_BAD_ARG;
+    if (S->dirty32) { int rc = setup_hierarchy<float>(S, S->H32, s); if (rc) return rc; S->dirty32 = false; }
+  } else {
+    if (!S->has64) return MW_ERR_BAD_ARG;
+    if (S->dirty64) { int rc = setup_hierarchy<double>(S, S->H64, s); if (rc) return rc; S->dirty64 = false; }
+  }
+  return MW_OK;
+}
+
+static int solve_K(mw_stokes* S, int prec, const double* b, double* x, double rtol, int maxit, double* relres,
+                   cudaStream_t s) {
+  if (prec == MW_F32) return pcg_K<float>(S, S->H32, S->pc32, b, x, rtol, maxit, relres, s);
+  return pcg_K<double>(S, S->H64, S->pc64, b, x, rtol, maxit, relres, s);
+}
+
+// Schur-complement PCG (uzawa3_solver_L2.py:21-99 / cd_u_eta.py:13-99) for the saddle system
+// with right-hand side (f, h), starting from (V, P) (V is recomputed from P).  Stops when the
+// Schur residual has dropped by `reduction` relative to its start, when the FP64 true residual
+// meets `tol` (checked each iteration if check_true), or after max_outer iterations.
+static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double* f, const double* h, double* V,
+                 double* P, double reduction, bool check_true, double bnorm, mw_solve_info* info, cudaStream_t s) {
+  const LevelGeo& g = S->fine;
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  const double* w = sp.scheme == MW_SCHEME_UZAWA3 ? nullptr : S->etae_w;
+  double rel;
+  // V = K^-1 (f - G P)
+  {
+    ApplyArgs<double> a = args0<double>();
+    a.p = P; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd; a.bV = f;
+    launch_apply<double, AM_RESID>(g, a, s);                 // Gd = f - G P   (u = null)
+  }
+  int inner = solve_K(S, prec, S->Gd, V, sp.inner_rtol, sp.max_inner, &rel, s);
+  info->inner_iters += inner;
+  // rho = G^T V - h
+  {
+    ApplyArgs<double> a = args0<double>();
+    a.u = V; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64;
+    a.yP = S->rP;
+    launch_apply<double, AM_APPLY>(g, a, s);                 // rP = G^T V (yV not written)
+    if (h) k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
+  }
+  remove_mean(S, np, S->rP, s);
+  mass_solve(S, w, S->rP, S->wP, sp.mass_rtol, sp.mass_maxit, s);
+  remove_mean(S, np, S->wP, s);
+  k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, S->dP);
+  double* sc = S->sc + 24;    // [0] rw, [1] dSd, [2] rw_new, [3] rr0, [4] rr
+  dot<double>(S, np, S->rP, S->wP, sc + 0, s);
+  dot<double>(S, np, S->rP, S->rP, sc + 3, s);
+  const double rr0 = read_scalar(sc + 3, s);
+  int k;
+  for (k = 0; k < sp.max_outer; ++k) {
+    // z = K^-1 G d
+    ApplyArgs<double> a = args0<double>();
+    a.p = S->dP; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd;
+    launch_apply<double, AM_APPLY>(g, a, s);
+    inner = solve_K(S, prec, S->Gd, S->z, sp.inner_rtol, sp.max_inner, &rel, s);
+    info->inner_iters += inner;
+    // G^T z, step length alpha = (rho, w) / (d, G^T z)
+    ApplyArgs<double> b2 = args0<double>();
+    b2.u = S->z; b2.eta = S->etaq64; b2.fix = S->fixV; b2.diag = S->diag64;
+    b2.yP = S->GTz;
+    launch_apply<double, AM_APPLY>(g, b2, s);
+    dot<double>(S, np, S->dP, S->GTz, sc + 1, s);
+    k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, 1.0, S->dP, P);
+    k_axpy_ratio<double, double><<<grid_for(nv, 256), 256, 0, s>>>(nv, sc + 0, sc + 1, -1.0, S->z, V);
+    k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, -1.0, S->GTz, S->rP);
+    remove_mean(S, np, S->rP, s);
+    mass_solve(S, w, S->rP, S->wP, sp.mass_rtol, sp.mass_maxit, s);
+    remove_mean(S, np, S->wP, s);
+    dot<double>(S, np, S->rP, S->wP, sc + 2, s);
+    k_xpby_ratio<double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, sc + 2, sc + 0, S->dP);
+    cudaMemcpyAsync(sc + 0, sc + 2, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    info->outer_iters += 1;
+    dot<double>(S, np, S->rP, S->rP, sc + 4, s);
+    double rr = read_scalar(sc + 4, s);
+    if (!std::isfinite(rr)) return MW_ERR_NOT_CONVERGED;
+    if (check_true) {
+      double tr = true_residual(S, V, P, f, h, bnorm, s);
+      info->rel_residual = tr;
+      if (tr <= sp.tol) { ++k; break; }
+    }
+    if (rr <= reduction * reduction * rr0) { ++k; break; }
+  }
+  return MW_OK;
+}
+
+template <typename R>
+__global__ void k_cast(int64_t n, const double* __restrict__ a, R* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (R)a[i];
+}
+
+}  // namespace mw
+
+using namespace mw;
+
+extern "C" {
+
+static size_t do_layout(mw_stokes* S, char* base, bool dry) {
+  Arena A{base, 0, 0, dry};
+  return layout(S, A);
+}
+
+static void init_params(mw_stokes* S, mw_box box, const mw_stokes_params& prm) {
+  S->prm = prm;
+  S->fine.nx = box.nelx; S->fine.nz = box.nelz;
+  S->fine.nnx = 2 * box.nelx + 1; S->fine.nnz = 2 * box.nelz + 1;
+  S->fine.hx = box.hx; S->fine.hz = box.hz;
+  S->fine.s = prm.eta_ref / prm.L_ref;
+  S->has64 = (prm.precisions & 1) != 0;
+  S->has32 = (prm.precisions & 2) != 0;
+  S->pc64[0] = nullptr;
+  if (S->has64) plan_levels(S->H64, S->fine, prm);
+  if (S->has32) plan_levels(S->H32, S->fine, prm);
+}
+
+void mw_stokes_default_params(mw_stokes_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->eta_ref = 1.0; p->L_ref = 1.0; p->precisions = 3;
+  p->coarse_min = 4; p->dense_max = 700; p->cheb_degree = 3; p->cheb_ratio = 8.0; p->cheb_safety = 1.1;
+  p->power_iters = 12;
+}
+
+void mw_solve_default_params(mw_solve_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->scheme = MW_SCHEME_CD_U_ETA; p->precision = MW_F64; p->tol = 1e-8; p->max_outer = 200;
+  p->max_inner = 500; p->inner_rtol = 1e-10; p->max_refine = 20; p->sweep_reduction = 1e-3;
+  p->mass_rtol = 1e-12; p->mass_maxit = 400; p->use_guess = 0;
+}
+
+size_t mw_stokes_workspace_bytes(mw_box box, mw_stokes_params prm) {
+  mw_stokes S;
+  init_params(&S, box, prm);
+  S.fixV = nullptr;
+  return do_layout(&S, nullptr, true);
+}
+
+int mw_stokes_create(mw_box box, mw_stokes_params prm, const uint8_t* bc_fix_V, void* work, size_t work_bytes,
+                     mw_stokes** out) {
+  if (box.nelx < 2 || box.nelz < 2 || !bc_fix_V || !work || !out || !(prm.precisions & 3)) return MW_ERR_BAD_ARG;
+  if (ensure_ref_tables()) return MW_ERR_CUDA;
+  mw_stokes* S = new mw_stokes();
+  init_params(S, box, prm);
+  S->fixV = bc_fix_V;
+  size_t need = do_layout(S, nullptr, true);
+  if (work_bytes < need) { delete S; return MW_ERR_WORKSPACE; }
+  do_layout(S, (char*)work, false);
+  *out = S;
+  return MW_OK;
+}
+
+int mw_stokes_destroy(mw_stokes* S) {
+  delete S;
+  return MW_OK;
+}
+
+int mw_stokes_levels(const mw_stokes* S, int32_t precision) {
+  return precision == MW_F32 ? S->H32.nlev : S->H64.nlev;
+}
+
+int mw_stokes_set_viscosity(mw_stokes* S, const double* etaq, const double* eta_e, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nel = (int64_t)S->fine.nx * S->fine.nz;
+  k_cast<double><<<grid_for(nel * 9, 256), 256, 0, s>>>(nel * 9, etaq, S->etaq64);
+  if (S->has32) k_cast<float><<<grid_for(nel * 9, 256), 256, 0, s>>>(nel * 9, etaq, S->etaq32);
+  k_inv_eta_e<<<grid_for(nel, 256), 256, 0, s>>>(nel, etaq, eta_e, S->etae_w);
+  k_diag<double><<<grid_for((int64_t)S->fine.nnx * S->fine.nnz, 128), 128, 0, s>>>(S->fine, S->etaq64, S->diag64);
+  S->dirty64 = S->dirty32 = true;
+  if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
+  return MW_OK;
+}
+
+int mw_stokes_apply(mw_stokes* S, const double* u, const double* p, double* yV, double* yP, void* stream) {
+  ApplyArgs<double> a = args0<double>();
+  a.u = u; a.p = p; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64; a.yV = yV; a.yP = yP;
+  launch_apply<double, AM_APPLY>(S->fine, a, (cudaStream_t)stream);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV, float* yP, void* stream) {
+  if (!S->has32) return MW_ERR_BAD_ARG;
+  if (ensure_hierarchy(S, MW_F32, (cudaStream_t)stream)) return MW_ERR_CUDA;
+  ApplyArgs<float> a = args0<float>();
+  a.u = u; a.p = p; a.eta = S->etaq32; a.fix = S->fixV; a.diag = S->H32.L[0].diag; a.yV = yV; a.yP = yP;
+  launch_apply<float, AM_APPLY>(S->fine, a, (cudaStream_t)stream);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int rc = ensure_hierarchy(S, precision, s)) return rc;
+  if (precision == MW_F32) {
+    Level<float>& L = S->H32.L[0];
+    k_copy<float, float><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, (const float*)b, L.b);
+    vcycle(S->H32, 0, S->prm.cheb_degree, s);
+    k_copy<float, float><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.x, (float*)x);
+  } else {
+    Level<double>& L = S->H64.L[0];
+    k_copy<double, double><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, (const double*)b, L.b);
+    vcycle(S->H64, 0, S->prm.cheb_degree, s);
+    k_copy<double, double><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.x, (double*)x);
+  }
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,
+                      int32_t* iters, double* relres, void* stream) {
+  double rr = 0;
+  if (int rc = ensure_hierarchy(S, precision, (cudaStream_t)stream)) return rc;
+  int it = solve_K(S, precision, b, x, rtol, maxit, &rr, (cudaStream_t)stream);
+  if (iters) *iters = it;
+  if (relres) *relres = rr;
+  if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
+  return rr <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
+}
+
+int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const double* f, const double* h, double* RV,
+                       double* RP, double* norm_out, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  double r = true_residual(S, V, P, f, h, 0.0, s);
+  if (RV) cudaMemcpyAsync(RV, S->RV, sizeof(double) * 2 * S->fine.nnx * S->fine.nnz, cudaMemcpyDeviceToDevice, s);
+  if (RP) cudaMemcpyAsync(RP, S->RP, sizeof(double) * (S->fine.nx + 1) * (S->fine.nz + 1), cudaMemcpyDeviceToDevice, s);
+  if (norm_out) *norm_out = r;
+  return cudaGetLastError() == cudaSuccess ? MW_OK : MW_ERR_CUDA;
+}
+
+int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
+                    mw_solve_info* info, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  const LevelGeo& g = S->fine;
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  mw_solve_info inf;
+  memset(&inf, 0, sizeof(inf));
+  if (!f || !h || !solV || !solP) return MW_ERR_BAD_ARG;
+  if (int rc = ensure_hierarchy(S, sp.precision == MW_F32 ? MW_F32 : MW_F64, s)) return rc;
+  if (!sp.use_guess) {
+    k_set<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 0.0, solV);
+    k_set<double><<<grid_for(np, 256), 256, 0, s>>>(np, 0.0, solP);
+  }
+  // ||b||
+  dot<double>(S, nv, f, f, S->sc + 52, s);
+  if (h) dot<double>(S, np, h, h, S->sc + 53, s);
+  double bb[2] = {0, 0};
+  cudaMemcpyAsync(bb, S->sc + 52, (h ? 2 : 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  const double bnorm = std::sqrt(bb[0] + bb[1]);
+  if (!(bnorm > 0)) { if (info) *info = inf; return MW_OK; }
+  inf.initial_rel_residual = true_residual(S, solV, solP, f, h, bnorm, s);
+  int rc = MW_OK;
+  if (sp.precision == MW_F64) {
+    // plain FP64: one Schur-PCG run with the true residual checked every iteration
+    inf.rel_residual = inf.initial_rel_residual;
+    if (inf.rel_residual > sp.tol)
+      rc = uzawa(S, sp, MW_F64, f, h, solV, solP, 0.0, true, bnorm, &inf, s);
+    inf.rel_residual = true_residual(S, solV, solP, f, h, bnorm, s);
+  } else {
+    // mixed: FP64 iterative refinement around an FP32-inner Uzawa correction solve
+    double rel = inf.initial_rel_residual;
+    for (int it = 0; it < sp.max_refine && rel > sp.tol; ++it) {
+      // residual (RV, RP) is current in S->RV / S->RP from true_residual
+      double* cV = S->cV;
+      // solve A (cV, cP) = (RV, RP): copy the residual into f/h slots, zero guess
+      double* fr = S->f;
+      double* hr = S->h;
+      k_copy<double, double><<<grid_for(nv, 256), 256, 0, s>>>(nv, S->RV, fr);
+      k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->RP, hr);
+      k_set<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 0.0, cV);
+      double* cPr = S->cP;
+      k_set<double><<<grid_for(np, 256), 256, 0, s>>>(np, 0.0, cPr);
+      rc = uzawa(S, sp, MW_F32, fr, hr, cV, cPr, sp.sweep_reduction, false, 0.0, &inf, s);
+      if (rc) break;
+      k_axpy<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 1.0, cV, solV);
+      k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, 1.0, cPr, solP);
+      inf.refinements += 1;
+      rel = true_residual(S, solV, solP, f, h, bnorm, s);
+      inf.rel_residual = rel;
+    }
+    inf.rel_residual = rel;
+  }
+  inf.converged = inf.rel_residual <= sp.tol ? 1 : 0;
+  S->last = inf;
+  if (info) *info = inf;
+  if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
+  if (rc) return rc;
+  return inf.converged ? MW_OK : MW_ERR_NOT_CONVERGED;
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+"""Device Stokes solver handle (matrix-free operator + multigrid PCG + Uzawa), over the C ABI.
+
+Mirrors the reference's block solvers ``uzawa3_solver_L2`` (uzawa3_solver_L2.py:21-99) and
+``cd_u_eta`` (cd_u_eta.py:13-99): the Schur-complement PCG with step lengths and the FP64
+stopping test on the device, K^-1 by geometric-multigrid PCG instead of SuperLU.
+"""
+import ctypes
+
+import torch
+
+from . import _lib as L
+from ._lib import c_double, c_int32, c_size_t, c_void_p, call, ptr, stream_ptr
+
+
+class MwStokesParams(ctypes.Structure):
+    _fields_ = [("eta_ref", c_double), ("L_ref", c_double), ("precisions", c_int32), ("coarse_min", c_int32),
+                ("dense_max", c_int32), ("cheb_degree", c_int32), ("cheb_ratio", c_double),
+                ("cheb_safety", c_double), ("power_iters", c_int32)]
+
+
+class MwSolveParams(ctypes.Structure):
+    _fields_ = [("scheme", c_int32), ("precision", c_int32), ("tol", c_double), ("max_outer", c_int32),
+                ("max_inner", c_int32), ("inner_rtol", c_double), ("max_refine", c_int32),
+                ("sweep_reduction", c_double), ("mass_rtol", c_double), ("mass_maxit", c_int32),
+                ("use_guess", c_int32)]
+
+
+class MwSolveInfo(ctypes.Structure):
+    _fields_ = [("outer_iters", c_int32), ("inner_iters", c_int32), ("refinements", c_int32), ("converged", c_int32),
+                ("rel_residual", c_double), ("initial_rel_residual", c_double)]
+
+
+L.extra_protos({
+    "mw_stokes_default_params": (None, [c_void_p]),
+    "mw_solve_default_params": (None, [c_void_p]),
+    "mw_stokes_workspace_bytes": (c_size_t, [L.MwBox, MwStokesParams]),
+    "mw_stokes_create": (c_int32, [L.MwBox, MwStokesParams, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "mw_stokes_destroy": (c_int32, [c_void_p]),
+    "mw_stokes_levels": (c_int32, [c_void_p, c_int32]),
+    "mw_stokes_set_viscosity": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mw_stokes_apply": (c_int32, [c_void_p] * 6),
+    "mw_stokes_apply_f32": (c_int32, [c_void_p] * 6),
+    "mw_stokes_vcycle": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
+    "mw_stokes_solve_K": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
+                                    c_void_p]),
+    "mw_stokes_residual": (c_int32, [c_void_p] * 7 + [c_void_p, c_void_p]),
+    "mw_stokes_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, MwSolveParams, c_void_p,
+                                  c_void_p]),
+})
+
+SCHEME = {"cd_u_eta": 0, "uzawa3": 1}
+PREC = {"f64": 0, "f32": 1, "mixed": 1}
+
+
+class StokesSolver:
+    """One box mesh's Stokes solver; owns its device workspace (a torch uint8 tensor)."""
+
+    def __init__(self, box, bc_fix_V, eta_ref=1.0, L_ref=1.0, precisions=("f64", "f32"), **kw):
+        L.require_cuda()
+        self.box = box
+        self.fix = bc_fix_V.view(torch.uint8) if bc_fix_V.dtype == torch.bool else bc_fix_V
+        prm = MwStokesParams()
+        L.lib().mw_stokes_default_params(ctypes.byref(prm))
+        prm.eta_ref, prm.L_ref = float(eta_ref), float(L_ref)
+        prm.precisions = (1 if "f64" in precisions else 0) | (2 if ("f32" in precisions or "mixed" in precisions) else 0)
+        for k, v in kw.items():
+            setattr(prm, k, v)
+        self.prm = prm
+        nbytes = L.lib().mw_stokes_workspace_bytes(box, prm)
+        self.work = torch.empty(int(nbytes), dtype=torch.uint8, device="cuda")
+        h = c_void_p()
+        call("mw_stokes_create", box, prm, ptr(self.fix), ptr(self.work), c_size_t(self.work.numel()), ctypes.byref(h))
+        self.h = h
+        self.nv = 2 * (2 * box.nelx + 1) * (2 * box.nelz + 1)
+        self.np = (box.nelx + 1) * (box.nelz + 1)
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and L._lib is not None:
+            L.lib().mw_stokes_destroy(self.h)
+            self.h = None
+
+    def levels(self, precision="f64"):
+        return L.lib().mw_stokes_levels(self.h, PREC[precision])
+
+    def set_viscosity(self, etaq, eta_e=None):
+        self._eta = etaq
+        call("mw_stokes_set_viscosity", self.h, ptr(etaq), ptr(eta_e), stream_ptr())
+
+    def apply(self, u=None, p=None, yV=None, yP=None, precision="f64"):
+        dt = torch.float32 if precision == "f32" else torch.float64
+        if yV is None:
+            yV = torch.empty(self.nv, dtype=dt, device="cuda")
+        if yP is None:
+            yP = torch.empty(self.np, dtype=dt, device="cuda")
+        name = "mw_stokes_apply_f32" if precision == "f32" else "mw_stokes_apply"
+        call(name, self.h, ptr(u), ptr(p), ptr(yV), ptr(yP), stream_ptr())
+        return yV, yP
+
+    def solve_K(self, b, precision="f64", rtol=1e-10, maxit=500):
+        x = torch.empty_like(b)
+        it = c_int32()
+        rr = c_double()
+        rc = L.lib().mw_stokes_solve_K(self.h, PREC[precision], ptr(b), ptr(x), rtol, maxit, ctypes.byref(it),
+                                       ctypes.byref(rr), stream_ptr())
+        if rc not in (0, 3):
+            raise RuntimeError(f"mw_stokes_solve_K returned {L.STATUS.get(rc, rc)}")
+        return x, it.value, rr.value
+
+    def vcycle(self, b, precision="f64"):
+        x = torch.empty_like(b)
+        call("mw_stokes_vcycle", self.h, PREC[precision], ptr(b), ptr(x), stream_ptr())
+        return x
+
+    def residual(self, V, P, f, h):
+        RV = torch.empty(self.nv, dtype=torch.float64, device="cuda")
+        RP = torch.empty(self.np, dtype=torch.float64, device="cuda")
+        nrm = c_double()
+        call("mw_stokes_residual", self.h, ptr(V), ptr(P), ptr(f), ptr(h), ptr(RV), ptr(RP), ctypes.byref(nrm),
+             stream_ptr())
+        return RV, RP, nrm.value
+
+    def solve(self, f, h, V=None, P=None, scheme="cd_u_eta", precision="f64", tol=1e-8, raise_on_fail=False, **kw):
+        """Returns (solV, solP, info dict).  V/P given -> warm start (overwritten in place)."""
+        sp = MwSolveParams()
+        L.lib().mw_solve_default_params(ctypes.byref(sp))
+        sp.scheme, sp.precision, sp.tol = SCHEME[scheme], PREC[precision], float(tol)
+        for k, v in kw.items():
+            setattr(sp, k, v)
+        if V is None or P is None:
+            V = torch.zeros(self.nv, dtype=torch.float64, device="cuda")
+            P = torch.zeros(self.np, dtype=torch.float64, device="cuda")
+            sp.use_guess = 0
+        else:
+            sp.use_guess = 1
+        info = MwSolveInfo()
+        rc = L.lib().mw_stokes_solve(self.h, ptr(f), ptr(h), ptr(V), ptr(P), sp, ctypes.byref(info), stream_ptr())
+        out = {k: getattr(info, k) for k, _ in MwSolveInfo._fields_}
+        out["status"] = L.STATUS.get(rc, rc)
+        if rc not in (0, 3) or (raise_on_fail and rc != 0):
+            raise RuntimeError(f"mw_stokes_solve returned {out['status']} ({out})")
+        return V, P, out

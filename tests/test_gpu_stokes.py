@@ -1,0 +1,110 @@
+"""GPU parity of the matrix-free Stokes operator and the device Uzawa / multigrid solvers.
+
+* operator: equal to SpMV with the reference-assembled, Dirichlet-eliminated COO matrix
+  (meeuuw.py:1798), FP64 relative 1e-12, FP32 relative 1e-5;
+* K solve: relative residual below the requested tolerance;
+* Stokes solve: FP64 relative true residual <= 1e-8 and the velocity
+  within 1e-6 (relative, max norm) of SciPy's direct solve of the same system.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def make_case(nelx, nelz, Lx=1.0, contrast=1e3, bc="free_slip", eta_ref=1.0, seed=0):
+    from oracle import assembly, solvers
+    from oracle.fe import BoxMesh
+    m = BoxMesh(nelx, nelz, Lx, 1.0)
+    rng = np.random.default_rng(seed)
+    T = (1 - m.zq) + 0.05 * np.cos(np.pi * m.xq / Lx) * np.sin(np.pi * m.zq) + 0.01 * rng.standard_normal(m.xq.shape)
+    etaq = np.exp(-np.log(contrast) * T)
+    eta_e = etaq.mean(axis=1)
+    rhoq = 1 - 1e-2 * T
+    fix = np.zeros(m.Nfem_V, dtype=bool)
+    x, z = m.x_V, m.z_V
+    fix[0::2] |= (x / Lx < 1e-8) | (x / Lx > 1 - 1e-8)
+    fix[1::2] |= (z < 1e-8) | (z > 1 - 1e-8)
+    if bc == "noslip_tb":
+        fix[0::2] |= (z < 1e-8) | (z > 1 - 1e-8)
+    val = np.zeros(m.Nfem_V)
+    gx = np.zeros((m.nel, 9))
+    gz = np.full((m.nel, 9), -1e6)
+    res = assembly.build_matrix_stokes(0, 0, 0, 0, m.nel, 9, 9, 4, 2, m.Nfem_V, m.Nfem_P, 18, m.icon_V, m.icon_P,
+                                       rhoq, etaq, m.JxWq, m.local_to_globalV, gx, gz, m.N_V, m.N_P, m.dNdr_V,
+                                       m.dNdt_V, m.dNdr_P, m.dNdt_P, m.jcbi00q, m.jcbi01q, m.jcbi10q, m.jcbi11q,
+                                       eta_e, eta_ref, m.L_ref, fix, val, m.bot_element, m.top_element, False, False,
+                                       "box", None, False, m.xq, False)
+    A = solvers.stokes_full(m, res[0])
+    return dict(m=m, etaq=etaq, eta_e=eta_e, fix=fix, A=A, f=res[1], h=res[2], eta_ref=eta_ref)
+
+
+def solver_for(c, **kw):
+    from meeuuw_b200 import _lib
+    from meeuuw_b200.stokes import StokesSolver
+    m = c["m"]
+    box = _lib.box_of(m.nelx, m.nelz, m.Lx, m.Lz)
+    S = StokesSolver(box, torch.as_tensor(c["fix"]).cuda(), eta_ref=c["eta_ref"], L_ref=m.L_ref, **kw)
+    S.set_viscosity(torch.as_tensor(c["etaq"]).cuda(), torch.as_tensor(c["eta_e"]).cuda())
+    return S
+
+
+@pytest.mark.parametrize("shape", [(6, 4), (16, 12), (32, 32)])
+def test_apply_matches_assembled_coo(shape):
+    c = make_case(*shape, Lx=1.3, eta_ref=2.0)
+    S = solver_for(c)
+    m = c["m"]
+    rng = np.random.default_rng(1)
+    u = rng.standard_normal(m.Nfem_V)
+    p = rng.standard_normal(m.Nfem_P)
+    yref = c["A"] @ np.concatenate([u, p])
+    yV, yP = S.apply(torch.as_tensor(u).cuda(), torch.as_tensor(p).cuda())
+    assert rel_err(yV.cpu().numpy(), yref[:m.Nfem_V]) < 1e-12
+    assert rel_err(yP.cpu().numpy(), yref[m.Nfem_V:]) < 1e-12
+    yV32, yP32 = S.apply(torch.as_tensor(u).float().cuda(), torch.as_tensor(p).float().cuda(), precision="f32")
+    assert rel_err(yV32.double().cpu().numpy(), yref[:m.Nfem_V]) < 1e-5
+    assert rel_err(yP32.double().cpu().numpy(), yref[m.Nfem_V:]) < 1e-5
+
+
+@pytest.mark.parametrize("precision,tol", [("f64", 1e-10), ("f32", 1e-5)])
+def test_multigrid_pcg_K(precision, tol):
+    c = make_case(64, 64, contrast=1e4)
+    S = solver_for(c)
+    m = c["m"]
+    K = c["A"][:m.Nfem_V, :m.Nfem_V]
+    b = torch.as_tensor(c["f"]).cuda()
+    x, it, rr = S.solve_K(b, precision=precision, rtol=tol, maxit=300)
+    xr = x.cpu().numpy()
+    res = np.linalg.norm(c["f"] - K @ xr) / np.linalg.norm(c["f"])
+    assert res < 3 * tol, (res, it)
+    assert it < 100, it
+
+
+@pytest.mark.parametrize("scheme", ["cd_u_eta", "uzawa3"])
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_stokes_solve_to_1e8(scheme, precision):
+    import scipy.sparse.linalg as sla
+    contrast = 1e3 if scheme == "cd_u_eta" else 1.0
+    c = make_case(32, 32, contrast=contrast)
+    S = solver_for(c)
+    m = c["m"]
+    f, h = torch.as_tensor(c["f"]).cuda(), torch.as_tensor(c["h"]).cuda()
+    V, P, info = S.solve(f, h, scheme=scheme, precision=precision, tol=1e-8)
+    assert info["converged"] == 1, info
+    sol = np.concatenate([V.cpu().numpy(), P.cpu().numpy()])
+    b = np.concatenate([c["f"], c["h"]])
+    res = np.linalg.norm(b - c["A"] @ sol) / np.linalg.norm(b)
+    assert res <= 1.05e-8, (res, info)
+    ref = sla.spsolve(c["A"], b)
+    assert rel_err(sol[:m.Nfem_V], ref[:m.Nfem_V]) < 1e-6
+
+
+def test_noslip_rayleigh_taylor_box_solve():
+    c = make_case(32, 32, Lx=0.9142, contrast=100.0, bc="noslip_tb", eta_ref=100.0)
+    S = solver_for(c)
+    f, h = torch.as_tensor(c["f"]).cuda(), torch.as_tensor(c["h"]).cuda()
+    V, P, info = S.solve(f, h, precision="mixed", tol=1e-8)
+    assert info["converged"] == 1, info

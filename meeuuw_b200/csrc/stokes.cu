@@ -245,7 +245,9 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
           a.yV[dof] = a.bV[dof] - y;
         } else {   // Chebyshev step
           R r = a.bV[dof] - y;
-          R dn = R(a.cheb[0]) * a.d[dof] + R(a.cheb[1]) * r / a.diag[dof];
+          const double c1 = a.cheb[0];
+          R dn = R(a.cheb[1]) * r / a.diag[dof];
+          if (c1 != 0.0) dn += R(c1) * a.d[dof];     // restart steps never read the old direction
           a.d[dof] = dn;
           a.xo[dof] = a.u[dof] + dn;
         }

@@ -1,0 +1,344 @@
+"""Benchmark: timesteps/s of the meeuuw hot path at 512x512 Q2xQ1 (FK viscosity, 4.2M particles).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 512]
+
+One step = one full timestep of the box path on the GPU (particle interpolation + material,
+projections, Stokes right-hand side + device Uzawa solve to an FP64 relative residual of 1e-8,
+pressure normalisation, dt, energy assembly + solve, heat flux / Nu, strain rate, vrms,
+RK4 advection, locate).  The product path is the mixed-precision solver (FP32 multigrid-PCG
+inner solves, FP64 refinement) warm-started from the previous step; the plain FP64 path is
+measured beside it.  With N > 1 each rank advances its own independent model (replicas: a
+single model does not shard), so `value` is the sum over ranks of timesteps/s ("weak").
+
+`--impl reference` times the CPU oracle (a restatement of the reference's Numba/SciPy path) on a
+bounded sample and extrapolates to the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "timesteps/s at 512x512 Q2xQ1, learned+mixed vs plain GPU at 1e-8 Stokes residual"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.stop_ = index, [], threading.Event()
+
+    def _run(self):
+        while not self.stop_.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self.stop_.wait(0.2)
+
+    def __enter__(self):
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop_.set()
+        self.th.join(timeout=10)
+
+    def summary(self):
+        import statistics
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for nm, v in zip(names, r[4:8]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------------------- ours
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from meeuuw_b200 import _lib, configs, ops
+    from meeuuw_b200.timestep import GPUModel
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.n
+    cfg = configs.fk_convection(n, seed=1000 + rank)
+    host = configs.build_host_model(cfg)
+
+    def timed(model, K, W):
+        for _ in range(W):
+            model.step()
+        model.check()
+        barrier()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(K):
+            model.step()
+        e.record()
+        barrier()
+        ms = s.elapsed_time(e)
+        model.check()
+        return ms
+
+    # ---- product path: mixed precision, previous-step warm start ----
+    model = GPUModel(cfg, host, stokes="mixed", tol=1e-8)
+    dev_index = torch.cuda.current_device()
+    with ClockSampler(dev_index) as clk:
+        ms = timed(model, args.steps, args.warmup)
+    ms = max_over_ranks(ms)
+    diag = model.diagnostics()
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1000.0)
+
+    # ---- launches per step (profiled step, untimed) ----
+    launches = None
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            model.step()
+            torch.cuda.synchronize()
+        names = [evt.name for evt in prof.events() if evt.device_type.name == "CUDA"]
+        ours = [nm for nm in names if "mw::" in nm]
+        launches = int(len(ours) * args.steps)
+        kernel_mix = {}
+        for nm in ours:
+            k = nm.split("(")[0].replace("void ", "")
+            kernel_mix[k] = kernel_mix.get(k, 0) + 1
+    except Exception as ex:  # profiler unavailable: leave the claim empty
+        kernel_mix = {"error": str(ex)}
+
+    # ---- roofline of the dominant kernel: fine-level operator apply (FP32), CUDA events ----
+    roof = roofline_apply(model, torch)
+
+    # ---- plain FP64 path (same problem, same warm start) ----
+    plain = None
+    if not args.no_plain:
+        pmodel = GPUModel(cfg, host, stokes="f64", tol=1e-8)
+        Kp = max(2, args.steps // 2)
+        pms = max_over_ranks(timed(pmodel, Kp, args.warmup))
+        pdiag = pmodel.diagnostics()
+        plain = {"value": world * Kp / (pms / 1000.0), "ms_per_step": pms / Kp, "steps": Kp,
+                 "stokes": pdiag["stokes"], "vrms": pdiag["vrms"], "Nu": pdiag["Nu"]}
+        del pmodel
+
+    # ---- end to end through host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(model, torch, max(2, args.steps // 2), world, barrier, max_over_ranks)
+
+    # ---- CPU baseline (rank 0, N = 1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(n)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32 (FP32 inner multigrid-PCG, FP64 refinement/reductions)",
+            "data": "synthetic (seeded FK convection: T0 + N(0,1e-3), 16 random particles/element)",
+            "config": {"workload": f"fk_convection {n}x{n} Q2xQ1, Ra=1e6, eta=exp(-ln(1e5) T), geometric "
+                                   f"averaging, RK4, 16 particles/element, Crank-Nicolson energy",
+                       "nel": cfg.nel, "nparticle": cfg.nparticle, "stokes_tol": 1e-8,
+                       "stokes_solver": "device Uzawa (cd_u_eta recurrence) + multigrid-PCG K solves, mixed",
+                       "warm_start": "previous step", "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (swarm state ~0.5 GB, fields ~0.2 GB)"},
+            "clocks": clk.summary(), "gpu_launches": launches, "kernel_mix_per_step": kernel_mix,
+            "roofline": roof, "e2e": e2e, "plain_fp64": plain,
+            "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
+            "last_step": {"vrms": diag["vrms"], "Nu": diag["Nu"], "dt": diag["dt"], "stokes": diag["stokes"]},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def roofline_apply(model, torch):
+    """Average duration of the fine-level FP32 operator apply (k_apply), CUDA events on its stream."""
+    from meeuuw_b200 import _lib
+    S = model.solver
+    nv, npp = S.nv, S.np
+    u = torch.randn(nv, dtype=torch.float32, device="cuda")
+    p = torch.randn(npp, dtype=torch.float32, device="cuda")
+    yV = torch.empty_like(u)
+    yP = torch.empty_like(p)
+    for _ in range(5):
+        S.apply(u, p, yV, yP, precision="f32")
+    reps = 50
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        S.apply(u, p, yV, yP, precision="f32")
+    e.record()
+    torch.cuda.synchronize()
+    us = s.elapsed_time(e) * 1000.0 / reps
+    nel, nn = model.nel, model.nn
+    # algorithmic bytes per apply: read u (2nn f32), p (np f32), eta (9 nel f32), Dirichlet mask (2nn u8);
+    # write yV (2nn f32), yP (np f32)
+    algo = 4 * 2 * nn + 4 * npp + 4 * 9 * nel + 2 * nn + 4 * 2 * nn + 4 * npp
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = algo / (us * 1e-6) / 1e9
+    return {"kernel": "mw::k_apply<float, AM_APPLY> (fine level, 512x512)", "bound": "hbm", "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None, "us_per_launch": us,
+            "algorithmic_bytes": algo,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650"}
+
+
+def run_e2e(model, torch, K, world, barrier, max_over_ranks):
+    """Same metric through host buffers: each step uploads the swarm and T from pinned host memory
+    and reads back the step's state (x, z, active, T) and scalars."""
+    names = ("x", "z", "T")
+    host = {k: torch.empty(getattr(model, k).shape, dtype=getattr(model, k).dtype, pin_memory=True) for k in names}
+    host_act = torch.empty(model.active.shape, dtype=torch.bool, pin_memory=True)
+    for k in names:
+        host[k].copy_(getattr(model, k))
+    host_act.copy_(model.active)
+    sc = torch.empty(3, dtype=torch.float64, pin_memory=True)
+    h2d = sum(host[k].numel() * host[k].element_size() for k in names) + host_act.numel()
+    d2h = h2d + 3 * 8
+
+    def one():
+        for k in names:
+            getattr(model, k).copy_(host[k], non_blocking=True)
+        model.active.copy_(host_act, non_blocking=True)
+        from meeuuw_b200 import ops
+        ops.locate(model.box, model.active, model.x, model.z, model.r, model.t, model.iel, model.err)
+        model.step()
+        for k in names:
+            host[k].copy_(getattr(model, k), non_blocking=True)
+        host_act.copy_(model.active, non_blocking=True)
+        sc.copy_(model.gq_out, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    one()
+    barrier()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(K):
+        one()
+    e.record()
+    barrier()
+    ms = max_over_ranks(s.elapsed_time(e))
+    return {"value": world * K / (ms / 1000.0), "unit": "timesteps/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "steps": K}
+
+
+# ---------------------------------------------------------------------------------------- CPU
+def cpu_phase_times(n, seed=0):
+    """One oracle timestep at n x n of the FK workload, per-phase wall times (s)."""
+    import numpy as np
+
+    from meeuuw_b200 import configs
+    from oracle.model import OracleModel
+    cfg = configs.fk_convection(n, seed=seed)
+    host = configs.build_host_model(cfg)
+    om = OracleModel(cfg, host)
+    t0 = time.perf_counter()
+    out = om.step(solver="cd_u_eta")
+    t1 = time.perf_counter()
+    return t1 - t0, out
+
+
+def cpu_baseline_sample(n_target, sizes=(32, 64)):
+    """Oracle timesteps at two small sizes; elementwise phases scale with n^2, the total is fitted
+    as a power law in n and extrapolated to n_target."""
+    import math
+    ts = []
+    for n in sizes:
+        t, _ = cpu_phase_times(n)
+        ts.append(t)
+    a = math.log(ts[1] / ts[0]) / math.log(sizes[1] / sizes[0])
+    a = max(a, 2.0)
+    t_target = ts[1] * (n_target / sizes[1]) ** a
+    return {"value": 1.0 / t_target, "unit": "timesteps/s", "cores": 1, "kind": "port",
+            "sample": f"oracle timestep (numpy/SciPy, cd_u_eta with SuperLU) at {sizes[0]}^2 and {sizes[1]}^2: "
+                      f"{ts[0]:.2f} s and {ts[1]:.2f} s; extrapolated to {n_target}^2 with the fitted exponent "
+                      f"{a:.2f}", "sample_seconds": ts}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    nsz = (32, 64)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_phase_times(nsz[0])
+    samples = []
+    for _ in range(max(1, min(args.steps, 3))):
+        samples.append(cpu_baseline_sample(args.n, nsz))
+    v = sorted(s["value"] for s in samples)[len(samples) // 2]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
+            "steps": len(samples), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded FK convection)",
+            "config": {"workload": f"fk_convection {args.n}x{args.n} Q2xQ1 (CPU oracle sample, extrapolated)"},
+            "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": 1, "kind": "port",
+                             "sample": samples[0]["sample"]},
+            "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -142,7 +142,8 @@ typedef struct { /* outputs; VV arrays are float or double per `precision`; rhs 
 
 /* build_matrix_stokes, build_matrix_stokes.py:18-278 (box, plane strain).  blocks=0 writes the
  * full layout VV_Stokes (nel*468, :267-276), blocks=1 the K/G/GT/M/M_eta/H blocks (:235-265).
- * Matches the COO index arrays II/JJ of meeuuw.py:884-1017. */
+ * Matches the COO index arrays II/JJ of meeuuw.py:884-1017.  With all VV pointers NULL only
+ * rhs_f and rhs_h are produced (the matrix-free solver needs no stored matrix). */
 size_t mw_assemble_stokes_workspace_bytes(mw_box box);
 int mw_assemble_stokes(mw_box box, int32_t blocks, int32_t precision, mw_stokes_in in, mw_stokes_out out, void* work,
                        size_t work_bytes, void* stream);
@@ -295,6 +296,24 @@ int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const dou
  * Stokes pressure: the caller multiplies by eta_ref/L_ref as meeuuw.py:1848 does). */
 int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
                     mw_solve_info* info, void* stream);
+
+/* u, w from the interleaved solution and p = solP * scale (meeuuw.py:1846-1851). */
+int mw_split_solution(int64_t nn_V, int64_t nn_P, const double* solV, const double* solP, double scale, double* u,
+                      double* w, double* p, void* stream);
+
+/* "elemental" qpoint fields (meeuuw.py:1512-1514, :1545-1547): aq[e, :] = a[e] (b, bq optional). */
+int mw_elemental_to_qpoints(int64_t nel, const double* a, const double* b, double* aq, double* bq, void* stream);
+
+/* ======================= energy solve ======================= */
+
+/* y = A x with A the summed element matrices VV_T (nel*81, build_matrix_energy.py:133-137). */
+int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y, void* stream);
+
+/* T = A^-1 rhs (replaces spsolve of coo_matrix((VV_T,(II_T,JJ_T))).tocsr(), meeuuw.py:2232-2235):
+ * Jacobi-preconditioned BiCGSTAB in FP64 from the initial guess in T, to rtol. */
+size_t mw_energy_solve_workspace_bytes(mw_box box);
+int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
+                    int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream);
 
 #ifdef __cplusplus
 }

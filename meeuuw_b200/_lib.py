@@ -106,6 +106,13 @@ _PROTOS = {
                                        c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_compute_dt": (c_int32, [c_int64, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, MwDtParams,
                                 c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "mw_split_solution": (c_int32, [c_int64, c_int64, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p,
+                                    c_void_p]),
+    "mw_elemental_to_qpoints": (c_int32, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mw_energy_matvec": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mw_energy_solve_workspace_bytes": (c_size_t, [MwBox]),
+    "mw_energy_solve": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
+                                  c_void_p, c_size_t, c_void_p]),
 }
 
 

@@ -165,7 +165,8 @@ k_assemble_stokes(mw_box b, mw_stokes_in in, int blocks, S* __restrict__ vv_full
       h_el[(e0 + el) * 4 + ikk] = (double)h;
     }
   }
-  // ---- stage outputs and store coalesced ----
+  // ---- stage outputs and store coalesced (skipped in rhs-only mode) ----
+  if (vv_full == nullptr && vv_K == nullptr) return;
   if (!blocks) {
     if (live) {
       S* o = outs + el * 468 + ikk * 26;                                   // :268-276
@@ -382,7 +383,9 @@ size_t mw_assemble_stokes_workspace_bytes(mw_box box) {
 int mw_assemble_stokes(mw_box box, int32_t blocks, int32_t precision, mw_stokes_in in, mw_stokes_out out, void* work,
                        size_t work_bytes, void* stream) {
   if (box.nelx <= 0 || box.nelz <= 0 || !out.rhs_f || !out.rhs_h) return MW_ERR_BAD_ARG;
-  if (blocks ? !(out.VV_K && out.VV_G && out.VV_GT && out.VV_M && out.VV_M_eta && out.VV_H) : !out.VV_Stokes)
+  const bool rhs_only = !out.VV_Stokes && !out.VV_K;
+  if (!rhs_only && (blocks ? !(out.VV_K && out.VV_G && out.VV_GT && out.VV_M && out.VV_M_eta && out.VV_H)
+                           : !out.VV_Stokes))
     return MW_ERR_BAD_ARG;
   if (work_bytes < mw_assemble_stokes_workspace_bytes(box)) return MW_ERR_WORKSPACE;
   cudaStream_t s = (cudaStream_t)stream;

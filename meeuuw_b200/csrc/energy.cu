@@ -1,0 +1,196 @@
+// Device solve of the Crank-Nicolson energy system (sm_100a).
+//
+// Reference: meeuuw.py:2232-2235 converts (II_T, JJ_T, VV_T) to CSR (summing duplicates) and calls
+// SuperLU's spsolve.  Here the element matrices VV_T written by build_matrix_energy
+// (build_matrix_energy.py:133-137, nel*81 values) are used directly: y = A x is a node-centric
+// gather over the (up to 4) incident elements in ascending element order -- the summed COO
+// matrix applied without forming it -- and the system is solved by Jacobi-preconditioned
+// BiCGSTAB in FP64 to a relative residual tolerance.
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace mw {
+
+MW_D int q2_local_e(int dx, int dz) {
+  if (dz == 0) return dx == 0 ? 0 : (dx == 1 ? 4 : 1);
+  if (dz == 1) return dx == 0 ? 7 : (dx == 1 ? 8 : 5);
+  return dx == 0 ? 3 : (dx == 1 ? 6 : 2);
+}
+
+// y = A x  (mode 0), or r = b - A x (mode 1).  Also writes diag when diag != null.
+__global__ void k_energy_matvec(mw_box b, const double* __restrict__ vv, const double* __restrict__ x,
+                                const double* __restrict__ rhs, double* __restrict__ y, double* __restrict__ diag,
+                                int mode) {
+  const int nnx = 2 * b.nelx + 1;
+  const int64_t nn = (int64_t)nnx * (2 * b.nelz + 1);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    int ix = (int)(n % nnx), iz = (int)(n / nnx);
+    int exs[2], ezs[2], nxe = 0, nze = 0;
+    if (ix & 1) exs[nxe++] = ix >> 1;
+    else { if (ix / 2 - 1 >= 0) exs[nxe++] = ix / 2 - 1; if (ix / 2 < b.nelx) exs[nxe++] = ix / 2; }
+    if (iz & 1) ezs[nze++] = iz >> 1;
+    else { if (iz / 2 - 1 >= 0) ezs[nze++] = iz / 2 - 1; if (iz / 2 < b.nelz) ezs[nze++] = iz / 2; }
+    double acc = 0.0, dg = 0.0;
+    for (int a = 0; a < nze; ++a)
+      for (int c = 0; c < nxe; ++c) {
+        int ex = exs[c], ez = ezs[a];
+        int kl = q2_local_e(ix - 2 * ex, iz - 2 * ez);
+        const double* row = vv + (((int64_t)ez * b.nelx + ex) * 81 + kl * 9);
+        for (int j = 0; j < 9; ++j) acc += row[j] * x[q2_node(ex, ez, j, nnx)];
+        dg += row[kl];
+      }
+    y[n] = mode == 1 ? rhs[n] - acc : acc;
+    if (diag) diag[n] = dg;
+  }
+}
+
+__global__ void k_edot_partial(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                               double* __restrict__ part) {
+  __shared__ double sh[32];
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v += a[i] * b[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) part[blockIdx.x] = v;
+  }
+}
+
+__global__ void k_edot_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double v = 0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) v += part[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) out[0] = v;
+  }
+}
+
+// BiCGSTAB vector updates with device scalars s[]: see the host loop for the slot meaning.
+// p = r + beta (p - omega v), beta = (rho_new/rho_old) (alpha/omega)
+__global__ void k_bicg_p(int64_t n, const double* __restrict__ s, const double* __restrict__ r,
+                         const double* __restrict__ v, double* __restrict__ p, int first) {
+  const double beta = first ? 0.0 : (s[0] / s[1]) * (s[2] / s[3]);
+  const double om = first ? 0.0 : s[3];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);   // first pass never reads p, v
+}
+
+__global__ void k_scale_diag(int64_t n, const double* __restrict__ x, const double* __restrict__ d,
+                             double* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i] / d[i];
+}
+
+// s = r - alpha v, alpha = rho / (r0, v) = s[0] / s[4]
+__global__ void k_bicg_s(int64_t n, const double* __restrict__ sc, const double* __restrict__ r,
+                         const double* __restrict__ v, double* __restrict__ sv) {
+  const double alpha = sc[0] / sc[4];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    sv[i] = r[i] - alpha * v[i];
+}
+
+// x += alpha phat + omega shat ; r = s - omega t ; omega = (t,s)/(t,t) = sc[5]/sc[6]
+__global__ void k_bicg_x(int64_t n, double* __restrict__ sc, const double* __restrict__ ph,
+                         const double* __restrict__ sh, const double* __restrict__ sv, const double* __restrict__ t,
+                         double* __restrict__ x, double* __restrict__ r) {
+  const double alpha = sc[0] / sc[4];
+  const double omega = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * ph[i] + omega * sh[i];
+    r[i] = sv[i] - omega * t[i];
+  }
+}
+
+// keep alpha (slot 2) and omega (slot 3) of this iteration, rho_old (slot 1) <- rho (slot 0)
+__global__ void k_bicg_roll(double* sc) {
+  if (threadIdx.x || blockIdx.x) return;
+  sc[2] = sc[0] / sc[4];
+  sc[3] = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
+  sc[1] = sc[0];
+}
+
+}  // namespace mw
+
+using namespace mw;
+
+extern "C" {
+
+size_t mw_energy_solve_workspace_bytes(mw_box box) {
+  int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  return (size_t)(9 * nn + 512) * sizeof(double);
+}
+
+int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y, void* stream) {
+  int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  k_energy_matvec<<<grid_for(nn, 256), 256, 0, (cudaStream_t)stream>>>(box, VV_T, x, nullptr, y, nullptr, 0);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
+                    int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream) {
+  if (work_bytes < mw_energy_solve_workspace_bytes(box) || maxit < 1) return MW_ERR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  double* w = (double*)work;
+  double *r = w, *r0 = w + n, *p = w + 2 * n, *v = w + 3 * n, *sv = w + 4 * n, *t = w + 5 * n, *ph = w + 6 * n,
+         *sh = w + 7 * n, *dg = w + 8 * n;
+  double* part = w + 9 * n;         // 296 partials
+  double* sc = part + 300;          // scalar slots
+  const int NBk = 296;
+  auto dot = [&](const double* a, const double* b2, double* out) {
+    k_edot_partial<<<NBk, 256, 0, s>>>(n, a, b2, part);
+    k_edot_final<<<1, 256, 0, s>>>(part, NBk, out);
+  };
+  auto rd = [&](const double* d) {
+    double h = 0;
+    cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    return h;
+  };
+  // r = b - A T (T is the initial guess), diag
+  k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, T, rhs, r, dg, 1);
+  cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+  dot(rhs, rhs, sc + 10);
+  dot(r, r, sc + 11);
+  double bb = rd(sc + 10);
+  double rr = rd(sc + 11);
+  int it = 0;
+  if (!(bb > 0)) bb = 1.0;
+  for (it = 1; it <= maxit && rr > rtol * rtol * bb; ++it) {
+    dot(r0, r, sc + 0);                                       // rho
+    k_bicg_p<<<grid_for(n, 256), 256, 0, s>>>(n, sc, r, v, p, it == 1);
+    k_scale_diag<<<grid_for(n, 256), 256, 0, s>>>(n, p, dg, ph);
+    k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, ph, nullptr, v, nullptr, 0);
+    dot(r0, v, sc + 4);
+    k_bicg_s<<<grid_for(n, 256), 256, 0, s>>>(n, sc, r, v, sv);
+    k_scale_diag<<<grid_for(n, 256), 256, 0, s>>>(n, sv, dg, sh);
+    k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, sh, nullptr, t, nullptr, 0);
+    dot(t, sv, sc + 5);
+    dot(t, t, sc + 6);
+    k_bicg_x<<<grid_for(n, 256), 256, 0, s>>>(n, sc, ph, sh, sv, t, T, r);
+    k_bicg_roll<<<1, 32, 0, s>>>(sc);
+    dot(r, r, sc + 11);
+    rr = rd(sc + 11);
+    if (!std::isfinite(rr)) break;
+  }
+  if (iters) *iters = it - 1;
+  if (relres) *relres = std::sqrt(rr / bb);
+  if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
+  return std::sqrt(rr / bb) <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
+}
+
+}  // extern "C"

@@ -330,11 +330,45 @@ __global__ void k_dt_final(const double* __restrict__ partial, int nb, int64_t n
   }
 }
 
+// Split the Stokes solution: u, w from interleaved solV and p = solP * eta_ref/L_ref
+// (meeuuw.py:1846-1851).
+__global__ void k_split(int64_t nn, int64_t np, const double* __restrict__ solV, const double* __restrict__ solP,
+                        double scale, double* __restrict__ u, double* __restrict__ w, double* __restrict__ p) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x) {
+    u[i] = solV[2 * i];
+    w[i] = solV[2 * i + 1];
+    if (i < np) p[i] = solP[i] * scale;
+  }
+}
+
+// rhoq / etaq of the "elemental" projection (meeuuw.py:1512-1514, 1545-1547): phiq[e, :] = phi_e[e]
+__global__ void k_broadcast_q(int64_t nel, const double* __restrict__ a, const double* __restrict__ b,
+                              double* __restrict__ aq, double* __restrict__ bq) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nel * 9; g += (int64_t)gridDim.x * blockDim.x) {
+    aq[g] = a[g / 9];
+    if (b) bq[g] = b[g / 9];
+  }
+}
+
 }  // namespace mw
 
 using namespace mw;
 
 extern "C" {
+
+int mw_split_solution(int64_t nn_V, int64_t nn_P, const double* solV, const double* solP, double scale, double* u,
+                      double* w, double* p, void* stream) {
+  int64_t n = nn_V > nn_P ? nn_V : nn_P;
+  k_split<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(nn_V, nn_P, solV, solP, scale, u, w, p);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_elemental_to_qpoints(int64_t nel, const double* a, const double* b, double* aq, double* bq, void* stream) {
+  k_broadcast_q<<<grid_for(nel * 9, 256), 256, 0, (cudaStream_t)stream>>>(nel, a, b, aq, bq);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
 
 size_t mw_post_workspace_bytes(void) { return (size_t)4 * RB * sizeof(double) + 64; }
 

@@ -248,6 +248,34 @@ def global_quantities(uq, wq, Tq, rhoq, JxWq, volume, out=None):
     return out
 
 
+def split_solution(solV, solP, scale, u, w, p):
+    call("mw_split_solution", u.numel(), p.numel(), ptr(solV), ptr(solP), float(scale), ptr(u), ptr(w), ptr(p),
+         stream_ptr())
+    return u, w, p
+
+
+def elemental_to_qpoints(a, b, aq, bq):
+    call("mw_elemental_to_qpoints", a.numel(), ptr(a), ptr(b), ptr(aq), ptr(bq), stream_ptr())
+
+
+def energy_matvec(box, VV, x, y=None):
+    y = torch.empty_like(x) if y is None else y
+    call("mw_energy_matvec", box, ptr(VV), ptr(x), ptr(y), stream_ptr())
+    return y
+
+
+def energy_solve(box, VV, rhs, T, rtol=1e-12, maxit=200):
+    """Solves in place into T (T holds the initial guess).  Returns (iterations, relres)."""
+    it = ctypes.c_int32()
+    rr = ctypes.c_double()
+    wp, wb = workspace("energy").get(L.lib().mw_energy_solve_workspace_bytes(box))
+    rc = L.lib().mw_energy_solve(box, ptr(VV), ptr(rhs), ptr(T), float(rtol), int(maxit), ctypes.byref(it),
+                                 ctypes.byref(rr), wp, wb, stream_ptr())
+    if rc not in (0, 3):
+        raise RuntimeError(f"mw_energy_solve returned {L.STATUS.get(rc, rc)}")
+    return it.value, rr.value
+
+
 def compute_dt(u, w, hcond, hcapa, rho, CFLnb, hx, hz, dt_max, solve_T, state, out=None):
     out = torch.empty(3, dtype=f64, device=u.device) if out is None else out
     prm = L.MwDtParams(float(CFLnb), float(hx), float(hz), float(dt_max), int(bool(solve_T)))

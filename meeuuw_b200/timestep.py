@@ -1,0 +1,181 @@
+"""One model's timestep, entirely on the GPU, in the order of the reference's time loop.
+
+meeuuw.py:1105-2864 (box path): particle interpolation + material model (:1118-1154),
+element and nodal projections (:1194, :1344-1405), qpoint fields (:1503-1590), Stokes
+right-hand side and solve (:1705-1851), pressure normalisation and nodal pressure (:1958-2051),
+time step (:2112-2139), energy assembly and solve (:2186-2235), heat flux and Nu (:2259-2308),
+nodal strain rate (:2385), vrms (:2512), advection (:2726) and locate (:2862).
+
+All state lives in device tensors allocated once; a step launches only this library's kernels
+(plus the solver's host-driven convergence checks).  Scalars (dt, vrms, Nu, solver statistics)
+stay on the device until `diagnostics()` reads them.
+"""
+import torch
+
+from . import _lib as L
+from . import configs, fe_tables, ops
+from .stokes import StokesSolver
+
+f64 = torch.float64
+
+
+class GPUModel:
+    def __init__(self, cfg, host=None, stokes="mixed", scheme="cd_u_eta", tol=1e-8, warm_start="previous",
+                 inner_rtol=None, device="cuda"):
+        L.require_cuda()
+        self.cfg = cfg
+        host = host if host is not None else configs.build_host_model(cfg)
+        self.box = box = L.box_of(cfg.nelx, cfg.nelz, cfg.Lx, cfg.Lz)
+        self.nel = nel = cfg.nel
+        self.nn = nn = (2 * cfg.nelx + 1) * (2 * cfg.nelz + 1)
+        self.np_ = npp = (cfg.nelx + 1) * (cfg.nelz + 1)
+        self.npart = npart = len(host.swarm_x)
+        self.L_ref = (cfg.Lx + cfg.Lz) / 2
+        self.volume = cfg.Lx * cfg.Lz
+        self.stokes_precision, self.scheme, self.tol, self.warm_start = stokes, scheme, tol, warm_start
+        self.inner_rtol = inner_rtol if inner_rtol is not None else (1e-3 if stokes == "mixed" else 1e-10)
+        D = lambda a, dt=None: torch.as_tensor(a, dtype=dt).to(device).contiguous()
+        self.tables = fe_tables.device_tables(device)
+        self.geo = fe_tables.uniform_geometry(nel, box.hx, box.hz, device)
+        E = lambda *s, dt=f64: torch.empty(*s, dtype=dt, device=device)
+        Z = lambda *s, dt=f64: torch.zeros(*s, dtype=dt, device=device)
+        # swarm
+        self.x, self.z = D(host.swarm_x, f64), D(host.swarm_z, f64)
+        self.active = D(host.swarm_active, torch.bool)
+        self.mat = D(host.swarm_mat, torch.int8)
+        self.r, self.t, self.iel = E(npart), E(npart), E(npart, dt=torch.int32)
+        self.props = {k: E(npart) for k in ("exx", "ezz", "exz", "p", "T", "rho", "eta", "hcond", "hcapa", "hprod",
+                                            "alpha")}
+        self.up, self.wp = E(npart), E(npart)
+        self.counts, self.offsets, self.order = E(nel, dt=torch.int32), E(nel + 1, dt=torch.int32), E(npart,
+                                                                                                           dt=torch.int32)
+        self.err = Z(1, dt=torch.int32)
+        # nodal / elemental / qpoint fields
+        self.T = D(host.T, f64)
+        self.exx_n, self.ezz_n, self.exz_n, self.q = Z(nn), Z(nn), Z(nn), Z(nn)
+        self.u, self.w, self.p = Z(nn), Z(nn), Z(npp)
+        self.rho_e, self.eta_e = E(nel), E(nel)
+        self.nodal = {k: E(nn) for k in ("rho", "eta", "hcond", "hcapa", "hprod", "alpha")}
+        self.qf = {k: E(nel, 9) for k in ("rhoq", "etaq", "Tq", "hcapaq", "hcondq", "hprodq", "alphaq", "uq", "wq")}
+        if cfg.formulation == "EBA":
+            for k in ("exxq", "ezzq", "exzq"):
+                self.qf[k] = E(nel, 9)
+        gx, gz = cfg.gxz
+        self.gxq = torch.full((nel, 9), float(gx), dtype=f64, device=device)
+        self.gzq = torch.full((nel, 9), float(gz), dtype=f64, device=device)
+        self.bc_fix_V, self.bc_val_V = D(host.bc_fix_V, torch.bool), D(host.bc_val_V, f64)
+        self.bc_fix_T, self.bc_val_T = D(host.bc_fix_T, torch.bool), D(host.bc_val_T, f64)
+        self.rhs_f, self.rhs_h = E(2 * nn), E(npp)
+        self.solV, self.solP = Z(2 * nn), Z(npp)
+        self.VV_T, self.rhs_T = E(nel * 81), E(nn)
+        self.hf = [E(nn) for _ in range(4)]
+        # device scalars
+        self.dt_state = torch.tensor([1e50, 1e50], dtype=f64, device=device)
+        self.dt_out = Z(3)
+        self.offset = Z(1)
+        self.nu_out = Z(13)
+        self.gq_out = Z(3)
+        self.material = ops.material_struct(cfg)
+        precs = ("f64",) if stokes == "f64" else ("f32",)
+        self.solver = StokesSolver(box, self.bc_fix_V, eta_ref=cfg.eta_ref, L_ref=self.L_ref, precisions=precs)
+        self.last_solve = {}
+        self.istep = 0
+        self.guess = None      # optional callable(model) -> (solV, solP) used as the Stokes initial guess
+        ops.locate(box, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
+
+    # ------------------------------------------------------------------------------------------
+    def stokes_inputs(self):
+        q = dict(rhoq=self.qf["rhoq"], etaq=self.qf["etaq"], gxq=self.gxq, gzq=self.gzq, eta_e=self.eta_e)
+        q.update(self.geo)
+        return q
+
+    def step(self):
+        c, b, tb = self.cfg, self.box, self.tables
+        P = self.props
+        # particle fields + material (meeuuw.py:1118-1154)
+        nodal = dict(exx=self.exx_n, ezz=self.ezz_n, exz=self.exz_n, q=self.q, T=self.T if c.solve_T else None)
+        ops.interp_material(b, self.active, self.r, self.t, self.iel, self.mat, nodal, self.material, P)
+        # elements and nodes (meeuuw.py:1194, 1344-1405)
+        ops.bin_particles(self.nel, self.active, self.iel, self.counts, self.offsets, self.order, self.err)
+        ops.project_elements(self.nel, self.offsets, self.order, P["rho"], P["eta"], c.averaging, self.rho_e,
+                             self.eta_e, self.err)
+        nd = self.nodal
+        ops.project_nodes(b, c.nodal_projection_type, [(P["rho"], "arithmetic"), (P["eta"], c.averaging)],
+                          self.offsets, self.order, self.r, self.t, [nd["rho"], nd["eta"]])
+        if c.solve_T:
+            ops.project_nodes(b, 2, [(P[k], "arithmetic") for k in ("hcond", "hcapa", "hprod", "alpha")],
+                              self.offsets, self.order, self.r, self.t, [nd[k] for k in ("hcond", "hcapa", "hprod",
+                                                                                        "alpha")])
+        # qpoint fields (meeuuw.py:1503-1590, "elemental" rho/eta)
+        qf = self.qf
+        ops.elemental_to_qpoints(self.rho_e, self.eta_e, qf["rhoq"], qf["etaq"])
+        if c.solve_T:
+            ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], self.T, qf["Tq"])
+            for k in ("hcapa", "hcond", "hprod", "alpha"):
+                ops.nodal_to_qpoints(b, L.SPACE_Q1_ON_V, tb["N_P"], nd[k], qf[k + "q"])
+        if c.formulation == "EBA":
+            for k in ("exx", "ezz", "exz"):
+                ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], getattr(self, k + "_n"), qf[k + "q"])
+        # Stokes (meeuuw.py:1705-1851): right-hand side, matrix-free solve
+        ops.assemble_stokes(b, False, 0, self.stokes_inputs(), tb, self.bc_fix_V, self.bc_val_V, c.eta_ref,
+                            self.L_ref, out=dict(rhs_f=self.rhs_f, rhs_h=self.rhs_h))
+        self.solver.set_viscosity(qf["etaq"], self.eta_e)
+        if self.guess is not None:
+            self.guess(self)
+        elif self.warm_start != "previous":
+            self.solV.zero_()
+            self.solP.zero_()
+        _, _, info = self.solver.solve(self.rhs_f, self.rhs_h, self.solV, self.solP, scheme=self.scheme,
+                                       precision=self.stokes_precision, tol=self.tol, inner_rtol=self.inner_rtol)
+        self.last_solve = info
+        ops.split_solution(self.solV, self.solP, c.eta_ref / self.L_ref, self.u, self.w, self.p)
+        # pressure normalisation and nodal pressure (meeuuw.py:1958-2051)
+        ops.pressure_offset(b, c.pressure_normalisation, self.p, tb["N_P"], self.geo["JxWq"], self.volume, self.offset)
+        ops.nodal_pressure(b, self.p, self.offset, tb["N_P_n"], self.q, subtract=True)
+        # time step (meeuuw.py:2112-2139)
+        ops.compute_dt(self.u, self.w, P["hcond"], P["hcapa"], P["rho"], c.CFLnb, b.hx, b.hz, c.dt_max, c.solve_T,
+                       self.dt_state, self.dt_out)
+        ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], self.u, qf["uq"])
+        ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], self.w, qf["wq"])
+        if c.solve_T:
+            # energy (meeuuw.py:2186-2235); T on entry is T_mem
+            q = {k: qf[k] for k in ("rhoq", "etaq", "Tq", "uq", "wq", "hcondq", "hcapaq", "alphaq", "hprodq")}
+            for k in ("exxq", "ezzq", "exzq"):
+                q[k] = qf.get(k)
+            q.update(self.geo)
+            ops.assemble_energy(b, 0, self.T, q, tb, self.bc_fix_T, self.bc_val_T, 0.0, c.rho0, c.formulation,
+                                self.VV_T, self.rhs_T, dt_dev=self.dt_out)
+            self.energy_info = ops.energy_solve(b, self.VV_T, self.rhs_T, self.T, rtol=1e-12, maxit=300)
+            # heat flux and Nu (meeuuw.py:2259-2308)
+            ops.nodal_heat_flux(b, self.T, nd["hcond"], tb, out=self.hf)
+            ops.compute_nu(b, self.T, self.hf[0], self.hf[1], nd["hcond"], self.nu_out)
+        # nodal strain rate for the next step's particles (meeuuw.py:2385)
+        ops.nodal_strain_rate(b, self.u, self.w, tb, out=[self.exx_n, self.ezz_n, self.exz_n])
+        # vrms (meeuuw.py:2512; uses the Tq of this step as the reference does)
+        ops.global_quantities(qf["uq"], qf["wq"], qf["Tq"] if c.solve_T else None, qf["rhoq"], self.geo["JxWq"],
+                              self.volume, self.gq_out)
+        # advect and locate (meeuuw.py:2726, 2862)
+        ops.advect(b, c.RKorder, 0.0, self.x, self.z, self.active, self.u, self.w, self.up, self.wp, self.err,
+                   dt_dev=self.dt_out)
+        ops.locate(b, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
+        self.istep += 1
+
+    def diagnostics(self):
+        """Reads the step's scalars (synchronises) and applies the reference's exit checks."""
+        err = int(self.err.item())
+        d = dict(istep=self.istep, dt=float(self.dt_out[0].item()), vrms=float(self.gq_out[0].item()),
+                 Tavrg=float(self.gq_out[1].item()), Nu=float(self.nu_out[12].item()) if self.cfg.solve_T else None,
+                 err=err, stokes=dict(self.last_solve))
+        return d
+
+    def check(self):
+        """SystemExit with the reference's message when a device flag is set."""
+        err = int(self.err.item())
+        if err & L.FLAG_EMPTY_ELEMENT:
+            raise SystemExit("ABORT: an element contains no particle!")          # meeuuw.py:1198-1199
+        if err & L.FLAG_R_OUT:
+            raise SystemExit("r value out of bounds")                             # locate_particles.py:61-62
+        if err & L.FLAG_T_OUT:
+            raise SystemExit("t value out of bounds")                             # locate_particles.py:63-64
+        if err & L.FLAG_ELEMENT_RANGE:
+            raise SystemExit("particle outside the mesh")

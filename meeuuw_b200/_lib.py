@@ -117,8 +117,13 @@ _PROTOS = {
 
 
 def extra_protos(d):
-    """Other modules register their prototypes here before the first load."""
+    """Other modules register their prototypes here (applied now if the library is loaded)."""
     _PROTOS.update(d)
+    if _lib is not None:
+        for name, (res, args) in d.items():
+            fn = getattr(_lib, name)
+            fn.restype = res
+            fn.argtypes = args
 
 
 def lib():

@@ -41,8 +41,8 @@ L.extra_protos({
     "mw_stokes_apply": (c_int32, [c_void_p] * 6),
     "mw_stokes_apply_f32": (c_int32, [c_void_p] * 6),
     "mw_stokes_vcycle": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
-    "mw_stokes_solve_K": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
-                                    c_void_p]),
+    "mw_stokes_solve_K": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_double, c_int32,
+                                    ctypes.POINTER(c_int32), ctypes.POINTER(c_double), c_void_p]),
     "mw_stokes_residual": (c_int32, [c_void_p] * 7 + [c_void_p, c_void_p]),
     "mw_stokes_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, MwSolveParams, c_void_p,
                                   c_void_p]),
@@ -100,7 +100,7 @@ class StokesSolver:
         x = torch.empty_like(b)
         it = c_int32()
         rr = c_double()
-        rc = L.lib().mw_stokes_solve_K(self.h, PREC[precision], ptr(b), ptr(x), rtol, maxit, ctypes.byref(it),
+        rc = L.lib().mw_stokes_solve_K(self.h, PREC[precision], ptr(b), ptr(x), float(rtol), int(maxit), ctypes.byref(it),
                                        ctypes.byref(rr), stream_ptr())
         if rc not in (0, 3):
             raise RuntimeError(f"mw_stokes_solve_K returned {L.STATUS.get(rc, rc)}")

@@ -37,6 +37,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-profile", action="store_true", help="skip the torch-profiler launch count")
     return ap.parse_args()
 
 
@@ -142,7 +143,10 @@ def run_ours(args):
 
     # ---- launches per step (profiled step, untimed) ----
     launches = None
+    kernel_mix = {}
     try:
+        if args.no_profile:
+            raise RuntimeError("launch count skipped (--no-profile)")
         from torch.profiler import ProfilerActivity, profile
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
             model.step()

@@ -38,6 +38,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="skip the torch-profiler launch count")
+    ap.add_argument("--roofline-only", action="store_true", help="set up the model, time the operator apply, exit")
     return ap.parse_args()
 
 
@@ -133,6 +134,11 @@ def run_ours(args):
 
     # ---- product path: mixed precision, previous-step warm start ----
     model = GPUModel(cfg, host, stokes="mixed", tol=1e-8)
+    if args.roofline_only:
+        from meeuuw_b200 import fe_tables
+        model.solver.set_viscosity(torch.ones(model.nel, 9, dtype=torch.float64, device="cuda"), None)
+        print(json.dumps({"roofline": roofline_apply(model, torch)}), flush=True)
+        return
     dev_index = torch.cuda.current_device()
     with ClockSampler(dev_index) as clk:
         ms = timed(model, args.steps, args.warmup)

@@ -247,8 +247,7 @@ typedef struct {
   double inner_rtol;      /* relative tolerance of each K solve                                      */
   int32_t max_refine;     /* refinement sweeps (MW_F32)                                              */
   double sweep_reduction; /* Schur residual reduction per refinement sweep (MW_F32)                  */
-  double mass_rtol;       /* relative tolerance of the M / M_eta solves                              */
-  int32_t mass_maxit;
+  int32_t mass_iters;     /* Chebyshev-Jacobi steps per M / M_eta solve (error 2^(1-iters))          */
   int32_t use_guess;      /* 1: start from the solV/solP passed in (warm start)                      */
 } mw_solve_params;
 

@@ -104,48 +104,61 @@ struct ApplyArgs {
   const double* cheb; // device coefficients {c1, c2}
 };
 
-// Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points.
+// Per-CTA tables in the kernel's precision: scaled derivatives dN/dx = (2/hx) dN/dr and
+// dN/dz = (2/hz) dN/dt at the Gauss points, N_P, and JxW = hx*hz/4 * w_q (uniform box).
 template <typename R>
-MW_D void element_apply(const LevelGeo& g, const R* ue, const R* pe, const R* eq, R* ye, R* ype, bool use_p) {
-  const R sx = R(2.0 / g.hx), sz = R(2.0 / g.hz);
-  const R jac = R(g.hx * g.hz / 4.0);
-  const R s = R(g.s);
+struct ApplyTables {
+  R DX[81], DZ[81], NP[36], JW[9];
+};
+
+template <typename R>
+MW_D void fill_tables(const LevelGeo& g, ApplyTables<R>& T, int tid, int nthreads) {
+  const double sx = 2.0 / g.hx, sz = 2.0 / g.hz, jac = g.hx * g.hz / 4.0;
+  for (int i = tid; i < 81; i += nthreads) { T.DX[i] = R(sx * c_ref.dr[i]); T.DZ[i] = R(sz * c_ref.dt[i]); }
+  for (int i = tid; i < 36; i += nthreads) T.NP[i] = R(c_ref.NP[i]);
+  for (int i = tid; i < 9; i += nthreads) T.JW[i] = R(jac * c_ref.wq[i]);
+}
+
+// Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points:
+// strain rate B u at each point, stress 2 eta (exx, ezz) and eta (du/dz + dw/dx) with the
+// pressure term, then B^T back onto the nodes (build_matrix_stokes.py:130-157 applied to a vector).
+template <typename R>
+MW_D void element_apply(const ApplyTables<R>& T, R s, const R* ue, const R* pe, const R* eq, R* ye, R* ype,
+                        bool use_p) {
 #pragma unroll
   for (int k = 0; k < 18; ++k) ye[k] = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) ype[k] = 0;
-#pragma unroll 1
+#pragma unroll
   for (int q = 0; q < 9; ++q) {
-    R exx = 0, ezz = 0, g1 = 0, g2 = 0;
+    R exx = 0, ezz = 0, gg = 0;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const R dr = R(c_ref.dr[q * 9 + k]), dt = R(c_ref.dt[q * 9 + k]);
-      exx += dr * ue[2 * k];
-      ezz += dt * ue[2 * k + 1];
-      g1 += dt * ue[2 * k];
-      g2 += dr * ue[2 * k + 1];
+      const R dx = T.DX[q * 9 + k], dz = T.DZ[q * 9 + k];
+      exx += dx * ue[2 * k];
+      ezz += dz * ue[2 * k + 1];
+      gg += dz * ue[2 * k] + dx * ue[2 * k + 1];       // du/dz + dw/dx
     }
-    exx *= sx; ezz *= sz;
-    const R gg = sz * g1 + sx * g2;                 // du/dz + dw/dx
-    const R jw = jac * R(c_ref.wq[q]);
+    const R jw = T.JW[q];
     const R e = eq[q] * jw;
     R pq = 0;
     if (use_p) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) pq += R(c_ref.NP[q * 4 + k]) * pe[k];
+      for (int k = 0; k < 4; ++k) pq += T.NP[q * 4 + k] * pe[k];
     }
-    const R A = R(2) * e * exx - s * jw * pq;
-    const R B = R(2) * e * ezz - s * jw * pq;
+    const R sp = s * jw * pq;
+    const R A = R(2) * e * exx - sp;
+    const R B = R(2) * e * ezz - sp;
     const R C = e * gg;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const R dx = sx * R(c_ref.dr[q * 9 + k]), dz = sz * R(c_ref.dt[q * 9 + k]);
+      const R dx = T.DX[q * 9 + k], dz = T.DZ[q * 9 + k];
       ye[2 * k] += dx * A + dz * C;
       ye[2 * k + 1] += dz * B + dx * C;
     }
     const R dv = -s * jw * (exx + ezz);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) ype[k] += R(c_ref.NP[q * 4 + k]) * dv;
+    for (int k = 0; k < 4; ++k) ype[k] += T.NP[q * 4 + k] * dv;
   }
 }
 
@@ -162,6 +175,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   __shared__ R su[LZ * LX * 2];
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
+  __shared__ ApplyTables<R> T;
   const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
@@ -178,6 +192,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     }
     su[2 * i] = u0; su[2 * i + 1] = u1;
   }
+  fill_tables<R>(g, T, tid, APPLY_THREADS);
   if (use_p)
     for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
       int jz = i / PX, jx = i % PX;
@@ -203,7 +218,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
 #pragma unroll
       for (int q = 0; q < 9; ++q) eq[q] = eg[q];
-      element_apply<R>(g, ue, pe, eq, ye, ype, use_p);
+      element_apply<R>(T, R(g.s), ue, pe, eq, ye, ype, use_p);
 #pragma unroll
       for (int k = 0; k < 18; ++k) sye[tid * 22 + k] = ye[k];
 #pragma unroll
@@ -218,26 +233,34 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   if (a.yV) {
     for (int i = tid; i < onx * onz; i += APPLY_THREADS) {
       int ix = 2 * ex0 + i % onx, iz = 2 * ez0 + i / onx;
-      // incident elements (global), ascending (ez, ex)
-      int exs[2], ezs[2], nxe = 0, nze = 0;
-      if (ix & 1) exs[nxe++] = ix >> 1;
-      else { if (ix / 2 - 1 >= 0) exs[nxe++] = ix / 2 - 1; if (ix / 2 < g.nx) exs[nxe++] = ix / 2; }
-      if (iz & 1) ezs[nze++] = iz >> 1;
-      else { if (iz / 2 - 1 >= 0) ezs[nze++] = iz / 2 - 1; if (iz / 2 < g.nz) ezs[nze++] = iz / 2; }
+      // incident elements, ascending (ez, ex): x candidates (xa, xb), z candidates (za, zb);
+      // tile-local element coordinates and the node's local index offsets
+      const bool xo = ix & 1, zo = iz & 1;
+      const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
+      const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = (iz >> 1);
+      const bool vxa = xa >= 0, vxb = !xo && xb < g.nx;
+      const bool vza = za >= 0, vzb = !zo && zb < g.nz;
+      const int dxa = xo ? 1 : 2, dza = zo ? 1 : 2;   // offsets inside element xa / za; 0 inside xb / zb
       R y0 = 0, y1 = 0;
-      for (int az = 0; az < nze; ++az)
-        for (int ax = 0; ax < nxe; ++ax) {
-          int lex = exs[ax] - (ex0 - 1), lez = ezs[az] - (ez0 - 1);
-          int k = q2_local_idx(ix - 2 * exs[ax], iz - 2 * ezs[az]);
-          const R* ye = sye + (lez * EX + lex) * 22;
-          y0 += ye[2 * k]; y1 += ye[2 * k + 1];
-        }
+      if (vza) {
+        const int lez = za - (ez0 - 1);
+        if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, dza);
+                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+        if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, dza);
+                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+      }
+      if (vzb) {
+        const int lez = zb - (ez0 - 1);
+        if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, 0);
+                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+        if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
+                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+      }
       int64_t n = (int64_t)iz * g.nnx + ix;
-      R yy[2] = {y0, y1};
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         int64_t dof = 2 * n + c;
-        R y = yy[c];
+        R y = c == 0 ? y0 : y1;
         if (a.fix[dof]) y = use_u ? a.diag[dof] * a.u[dof] : R(0);
         if (MODE == AM_APPLY) {
           a.yV[dof] = y;
@@ -261,15 +284,14 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     const int pnx = px1 - ex0, pnz = pz1 - ez0;
     for (int i = tid; i < pnx * pnz; i += APPLY_THREADS) {
       int px = ex0 + i % pnx, pz = ez0 + i / pnx;
-      const int exs[4] = {px - 1, px, px - 1, px};
-      const int ezs[4] = {pz - 1, pz - 1, pz, pz};
-      const int kk[4] = {2, 3, 1, 0};
+      // incident elements (pz-1, px-1) k=2, (pz-1, px) k=3, (pz, px-1) k=1, (pz, px) k=0
+      const bool l = px >= 1, rr = px < g.nx, bo = pz >= 1, to = pz < g.nz;
+      const int lx = px - ex0, lz = pz - ez0;          // tile-local index of element (px, pz) is (lx+1, lz+1)
       R y = 0;
-      for (int s2 = 0; s2 < 4; ++s2) {
-        if (exs[s2] < 0 || exs[s2] >= g.nx || ezs[s2] < 0 || ezs[s2] >= g.nz) continue;
-        int lex = exs[s2] - (ex0 - 1), lez = ezs[s2] - (ez0 - 1);
-        y += sye[(lez * EX + lex) * 22 + 18 + kk[s2]];
-      }
+      if (bo && l) y += sye[((lz) * EX + lx) * 22 + 18 + 2];
+      if (bo && rr) y += sye[((lz) * EX + lx + 1) * 22 + 18 + 3];
+      if (to && l) y += sye[((lz + 1) * EX + lx) * 22 + 18 + 1];
+      if (to && rr) y += sye[((lz + 1) * EX + lx + 1) * 22 + 18 + 0];
       int64_t n = (int64_t)pz * (g.nx + 1) + px;
       a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
     }
@@ -334,7 +356,11 @@ MW_D double rw(int J, int o) {
 
 template <typename R>
 __global__ void k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
-                           R* __restrict__ bc) {
+                           R* __restrict__ bc, const double* __restrict__ cheb_c, const R* __restrict__ diag_c,
+                           R* __restrict__ xc, R* __restrict__ dc) {
+  // also performs the coarse level's first Chebyshev step from a zero guess when cheb_c != null:
+  // x_c = d_c = (1/theta_c) D_c^-1 b_c
+  const double c0 = cheb_c ? cheb_c[1] : 0.0;
   const int64_t nn = (int64_t)gc.nnx * gc.nnz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
     int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
@@ -352,8 +378,14 @@ __global__ void k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, c
         s1 += wz * wx * (double)rf[2 * m + 1];
       }
     }
-    bc[2 * n] = fixc[2 * n] ? R(0) : (R)s0;
-    bc[2 * n + 1] = fixc[2 * n + 1] ? R(0) : (R)s1;
+    const R b0 = fixc[2 * n] ? R(0) : (R)s0, b1 = fixc[2 * n + 1] ? R(0) : (R)s1;
+    bc[2 * n] = b0;
+    bc[2 * n + 1] = b1;
+    if (cheb_c) {
+      const R x0 = R(c0) * b0 / diag_c[2 * n], x1 = R(c0) * b1 / diag_c[2 * n + 1];
+      xc[2 * n] = x0; dc[2 * n] = x0;
+      xc[2 * n + 1] = x1; dc[2 * n + 1] = x1;
+    }
   }
 }
 
@@ -633,6 +665,97 @@ __global__ void k_mass_diag(LevelGeo g, const double* __restrict__ w, double* __
   }
 }
 
+// One fused Chebyshev-Jacobi step for M_w x = b:  r = b - M_w x_in ; d = c1 d + c2 D^-1 r ;
+// x_out = x_in + d.  `first` means x_in = 0 (no product, no old direction).  For Q1 mass matrices
+// with positive element weights, lambda(D^-1 M_w) lies in [0.25, 2.25] whatever the weights
+// (element-by-element bound; the exactly integrated bilinear element matrix has D_e^-1 M_e eigenvalues
+// 9/4, 3/4, 3/4, 1/4), so the coefficients are fixed and need no dot products.
+__global__ void k_mass_cheb(LevelGeo g, const double* __restrict__ w, const double* __restrict__ b,
+                            const double* __restrict__ xin, double* __restrict__ xout, double* __restrict__ d,
+                            const double* __restrict__ dg, double c1, double c2, int first) {
+  __shared__ double Me[16];
+  if (threadIdx.x < 16) {
+    const double jac = g.hx * g.hz / 4.0;
+    int a = threadIdx.x / 4, c = threadIdx.x % 4;
+    double m = 0;
+    for (int q = 0; q < 9; ++q) m += c_ref.NP[q * 4 + a] * c_ref.NP[q * 4 + c] * jac * c_ref.wq[q];
+    Me[threadIdx.x] = m;
+  }
+  __syncthreads();
+  const int ncx = g.nx + 1;
+  const int64_t np = (int64_t)ncx * (g.nz + 1);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x) {
+    double y = 0;
+    if (!first) {
+      const int i = (int)(n % ncx), j = (int)(n / ncx);
+      // incident elements (j-1,i-1) k=2, (j-1,i) k=3, (j,i-1) k=1, (j,i) k=0
+      for (int s = 0; s < 4; ++s) {
+        const int ex = (s & 1) ? i : i - 1, ez = (s & 2) ? j : j - 1;
+        if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+        const int kl = s == 0 ? 2 : (s == 1 ? 3 : (s == 2 ? 1 : 0));
+        const int64_t e = (int64_t)ez * g.nx + ex;
+        double v = 0;
+        for (int k2 = 0; k2 < 4; ++k2) v += Me[kl * 4 + k2] * xin[q1_node(ex, ez, k2, g.nx)];
+        y += (w ? w[e] : 1.0) * v;
+      }
+    }
+    const double r = b[n] - y;
+    const double dn = first ? c2 * r / dg[n] : c1 * d[n] + c2 * r / dg[n];
+    d[n] = dn;
+    xout[n] = (first ? 0.0 : xin[n]) + dn;
+  }
+}
+
+// Deterministic single-launch dot product: block partials, then the last block to finish sums
+// them in block order (threadfence + arrival counter, reset for the next call).
+template <typename R>
+__global__ void k_dot1(int64_t n, const R* __restrict__ x, const R* __restrict__ y, double* __restrict__ part,
+                       unsigned* __restrict__ counter, double* __restrict__ out) {
+  __shared__ double sh[32];
+  __shared__ bool last;
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v += (double)x[i] * (double)y[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  if (wid == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) {
+      part[blockIdx.x] = v;
+      __threadfence();
+      last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double t = 0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += ((volatile double*)part)[i];
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+  if (lane == 0) sh[wid] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sh[k];
+    out[0] = s;
+    *counter = 0u;
+  }
+}
+
+// x += (num/den) p ; r -= (num/den) Ap   (one launch for both PCG updates)
+template <typename R>
+__global__ void k_pcg_update(int64_t n, const double* __restrict__ num, const double* __restrict__ den,
+                             const R* __restrict__ p, const R* __restrict__ Ap, R* __restrict__ x, R* __restrict__ r) {
+  const double a = *num / *den;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] = (R)((double)x[i] + a * (double)p[i]);
+    r[i] = (R)((double)r[i] - a * (double)Ap[i]);
+  }
+}
+
 // element weights 1/eta_e for M_eta (eta_e = mean of the qpoint viscosities of the element)
 __global__ void k_inv_eta_e(int64_t nel, const double* __restrict__ etaq, const double* __restrict__ eta_e,
                             double* __restrict__ w) {
@@ -717,6 +840,7 @@ struct mw_stokes {
   double* etae_w;        // 1/eta_e per element (M_eta weights)
   double* red;           // reduction partials
   double* sc;            // device scalars
+  unsigned* counter;     // arrival counter of the single-launch dot products
   // inner PCG vectors (precision of the hierarchy): x, r, z, p, Ap
   double *pc64[5];
   float *pc32[5];
@@ -777,6 +901,7 @@ static size_t layout(mw_stokes* S, Arena& A) {
   S->etae_w = (double*)A.take(sizeof(double) * nel);
   S->red = (double*)A.take(sizeof(double) * NB * 4);
   S->sc = (double*)A.take(sizeof(double) * 64);
+  S->counter = (unsigned*)A.take(sizeof(unsigned) * 4);
   if (S->has64) {
     for (int i = 0; i < 5; ++i) S->pc64[i] = (double*)A.take(sizeof(double) * nv);
     carve(S->H64, A, S->fixV);
@@ -808,8 +933,7 @@ static ApplyArgs<R> args0() {
 
 template <typename R>
 static void dot(mw_stokes* S, int64_t n, const R* x, const R* y, double* out, cudaStream_t s) {
-  k_dot_partial<R><<<NB, 256, 0, s>>>(n, x, y, S->red);
-  k_dot_final<<<1, 256, 0, s>>>(S->red, NB, out);
+  k_dot1<R><<<NB, 256, 0, s>>>(n, x, y, S->red, S->counter, out);
 }
 
 static void dsum(mw_stokes* S, int64_t n, const double* x, double* out, cudaStream_t s) {
@@ -826,22 +950,21 @@ static void k_only_apply(const Level<R>& L, const R* x, R* y, cudaStream_t s) {
 
 // Chebyshev smoothing of level L: x (in/out) with rhs b, `steps` steps; zero_start -> x = 0 on entry.
 template <typename R>
-static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s) {
+static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s, bool first_done = false) {
   const int64_t n = L.ndof;
-  int k0 = 0;
-  if (zero_start) {
+  if (first_done) {
+    // x = d = (1/theta) D^-1 b was written by the restriction kernel
+  } else if (zero_start) {
     k_cheb_first<R><<<grid_for(n, 256), 256, 0, s>>>(n, L.cheb, L.b, L.diag, L.x, L.d);
-    k0 = 1;
   } else {
-    // restart the recurrence: first step from the current x: d = (1/theta) D^-1 r; x += d
+    // restart the recurrence from the current x: d = (1/theta) D^-1 r; x += d
     ApplyArgs<R> a = args0<R>();
     a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
     a.cheb = L.cheb;                    // step-0 pair {0, 1/theta}
     launch_apply<R, AM_CHEB>(L.g, a, s);
     std::swap(L.x, L.t);
-    k0 = 1;
   }
-  for (int k = k0; k < degree; ++k) {
+  for (int k = 1; k < degree; ++k) {
     ApplyArgs<R> a = args0<R>();
     a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
     a.cheb = L.cheb + 2 * k;
@@ -851,24 +974,26 @@ static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s) {
 }
 
 template <typename R>
-static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s) {
+static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool first_done = false) {
   Level<R>& L = H.L[l];
   if (l == H.nlev - 1) {
     if (H.dense) {
       int nd = H.nd;
       k_dense_matvec<R><<<(nd * 32 + 255) / 256, 256, 0, s>>>(nd, H.Ainv, L.b, L.x);
     } else {
-      smooth(L, MAXDEG, true, s);
+      smooth(L, MAXDEG, !first_done, s, first_done);
     }
     return;
   }
   Level<R>& C = H.L[l + 1];
-  smooth(L, degree, true, s);
+  smooth(L, degree, !first_done, s, first_done);
   ApplyArgs<R> a = args0<R>();
   a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.r; a.bV = L.b;
   launch_apply<R, AM_RESID>(L.g, a, s);
-  k_restrict<R><<<grid_for(C.nn, 256), 256, 0, s>>>(L.g, C.g, L.r, C.fix, C.b);
-  vcycle(H, l + 1, degree, s);
+  const bool fuse = !(l + 1 == H.nlev - 1 && H.dense);
+  k_restrict<R><<<grid_for(C.nn, 256), 256, 0, s>>>(L.g, C.g, L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
+                                                      C.x, C.d);
+  vcycle(H, l + 1, degree, s, fuse);
   k_prolong_add<R><<<grid_for(L.nn, 256), 256, 0, s>>>(L.g, C.g, C.x, L.fix, L.x);
   smooth(L, degree, false, s);
 }
@@ -937,7 +1062,8 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
                  double* relres, cudaStream_t s) {
   Level<R>& L = H.L[0];
   const int64_t n = L.ndof;
-  R *xr = pc[0], *r = pc[1], *z = pc[2], *p = pc[3], *Ap = pc[4];
+  R *xr = pc[0], *r = pc[1], *p = pc[3], *Ap = pc[4];
+  R*& z = pc[2];
   double* sc = S->sc;   // [0] rz, [1] pAp, [2] rr, [3] bb, [4] rz_new
   k_copy<R, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
   k_set<R><<<grid_for(n, 256), 256, 0, s>>>(n, R(0), xr);
@@ -948,10 +1074,14 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
     *relres = 0;
     return 0;
   }
-  auto precond = [&](const R* rin, R* zout) {
-    k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, rin, L.b);
+  // preconditioner z = V(r): the fine level reads r in place and the result buffer is exchanged
+  // with z (host pointers only, no copies)
+  auto precond = [&](R* rin, R*& zout) {
+    R* saved_b = L.b;
+    L.b = rin;
     vcycle(H, 0, S->prm.cheb_degree, s);
-    k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, L.x, zout);
+    L.b = saved_b;
+    std::swap(zout, L.x);
   };
   precond(r, z);
   k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
@@ -961,8 +1091,7 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
   for (it = 1; it <= maxit; ++it) {
     k_only_apply<R>(L, p, Ap, s);
     dot<R>(S, n, p, Ap, sc + 1, s);
-    k_axpy_ratio<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, 1.0, p, xr);
-    k_axpy_ratio<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, -1.0, Ap, r);
+    k_pcg_update<R><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, p, Ap, xr, r);
     dot<R>(S, n, r, r, sc + 2, s);
     rr = read_scalar(sc + 2, s);
     if (!std::isfinite(rr)) break;
@@ -979,38 +1108,32 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
 
 // Jacobi-PCG for the (weighted) Q1 mass matrix: M_w x = b.  weights NULL -> M (uzawa3),
 // weights = 1/eta_e -> M_eta (cd_u_eta).
-static int mass_solve(mw_stokes* S, const double* w, const double* b, double* x, double rtol, int maxit,
-                      cudaStream_t s) {
+// Solve M_w x = b (M_w = M for uzawa3, M_eta for cd_u_eta) by `iters` fixed-coefficient
+// Chebyshev-Jacobi steps on lambda(D^-1 M_w) in [0.25, 2.25] (see k_mass_cheb): error reduction
+// 2 (1/2)^iters, no dot products, no host synchronisation.  The diagonals are refreshed by
+// mw_stokes_set_viscosity.  Replaces the splu solves of uzawa3_solver_L2.py:46-47 / cd_u_eta.py:284-289.
+static int mass_solve(mw_stokes* S, const double* w, const double* b, double* x, int iters, cudaStream_t s) {
   const LevelGeo& g = S->fine;
   const int64_t n = (int64_t)(g.nx + 1) * (g.nz + 1);
-  double *r = S->tP, *z = S->tP2, *p = S->minv_w, *Ap = S->medi, *dg = S->mdiag;
-  double* sc = S->sc + 16;
-  k_mass_diag<<<grid_for(n, 256), 256, 0, s>>>(g, w, dg);
-  k_copy<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
-  k_set<double><<<grid_for(n, 256), 256, 0, s>>>(n, 0.0, x);
-  dot<double>(S, n, r, r, sc + 3, s);
-  double bb = read_scalar(sc + 3, s);
-  if (!(bb > 0)) return 0;
-  k_dinv<double><<<grid_for(n, 256), 256, 0, s>>>(n, r, dg, z);
-  k_copy<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
-  dot<double>(S, n, r, z, sc + 0, s);
-  int it;
-  for (it = 1; it <= maxit; ++it) {
-    k_mass_apply<<<grid_for(n, 256), 256, 0, s>>>(g, w, p, Ap);
-    dot<double>(S, n, p, Ap, sc + 1, s);
-    k_axpy_ratio<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, 1.0, p, x);
-    k_axpy_ratio<double, double><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, -1.0, Ap, r);
-    if (it % 8 == 0 || it == maxit) {
-      dot<double>(S, n, r, r, sc + 2, s);
-      double rr = read_scalar(sc + 2, s);
-      if (!(rr > rtol * rtol * bb)) break;
+  const double* dg = w ? S->medi : S->mdiag;
+  const double a = 0.25 / 1.02, bb = 2.25 * 1.02;
+  const double theta = 0.5 * (bb + a), delta = 0.5 * (bb - a), sigma = theta / delta;
+  double rho = 1.0 / sigma;
+  double* bufs[2] = {x, S->tP};
+  const int K = iters < 1 ? 1 : iters;
+  for (int k = 0; k < K; ++k) {
+    double c1 = 0.0, c2 = 1.0 / theta;
+    if (k > 0) {
+      double rn = 1.0 / (2.0 * sigma - rho);
+      c1 = rn * rho;
+      c2 = 2.0 * rn / delta;
+      rho = rn;
     }
-    k_dinv<double><<<grid_for(n, 256), 256, 0, s>>>(n, r, dg, z);
-    dot<double>(S, n, r, z, sc + 4, s);
-    k_xpby_ratio<double><<<grid_for(n, 256), 256, 0, s>>>(n, z, sc + 4, sc + 0, p);
-    cudaMemcpyAsync(sc + 0, sc + 4, sizeof(double), cudaMemcpyDeviceToDevice, s);
+    double* xin = bufs[(K - k) % 2];
+    double* xout = bufs[(K - 1 - k) % 2];
+    k_mass_cheb<<<grid_for(n, 256), 256, 0, s>>>(g, w, b, xin, xout, S->tP2, dg, c1, c2, k == 0);
   }
-  return it;
+  return K;
 }
 
 static void remove_mean(mw_stokes* S, int64_t n, double* x, cudaStream_t s) {
@@ -1083,7 +1206,7 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
     if (h) k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
   }
   remove_mean(S, np, S->rP, s);
-  mass_solve(S, w, S->rP, S->wP, sp.mass_rtol, sp.mass_maxit, s);
+  mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
   remove_mean(S, np, S->wP, s);
   k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, S->dP);
   double* sc = S->sc + 24;    // [0] rw, [1] dSd, [2] rw_new, [3] rr0, [4] rr
@@ -1108,7 +1231,7 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
     k_axpy_ratio<double, double><<<grid_for(nv, 256), 256, 0, s>>>(nv, sc + 0, sc + 1, -1.0, S->z, V);
     k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, -1.0, S->GTz, S->rP);
     remove_mean(S, np, S->rP, s);
-    mass_solve(S, w, S->rP, S->wP, sp.mass_rtol, sp.mass_maxit, s);
+    mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
     remove_mean(S, np, S->wP, s);
     dot<double>(S, np, S->rP, S->wP, sc + 2, s);
     k_xpby_ratio<double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, sc + 2, sc + 0, S->dP);
@@ -1168,7 +1291,7 @@ void mw_solve_default_params(mw_solve_params* p) {
   memset(p, 0, sizeof(*p));
   p->scheme = MW_SCHEME_CD_U_ETA; p->precision = MW_F64; p->tol = 1e-8; p->max_outer = 200;
   p->max_inner = 500; p->inner_rtol = 1e-10; p->max_refine = 20; p->sweep_reduction = 1e-3;
-  p->mass_rtol = 1e-12; p->mass_maxit = 400; p->use_guess = 0;
+  p->mass_iters = 36; p->use_guess = 0;
 }
 
 size_t mw_stokes_workspace_bytes(mw_box box, mw_stokes_params prm) {
@@ -1188,6 +1311,7 @@ int mw_stokes_create(mw_box box, mw_stokes_params prm, const uint8_t* bc_fix_V, 
   size_t need = do_layout(S, nullptr, true);
   if (work_bytes < need) { delete S; return MW_ERR_WORKSPACE; }
   do_layout(S, (char*)work, false);
+  if (cudaMemset(S->counter, 0, sizeof(unsigned) * 4) != cudaSuccess) { delete S; return MW_ERR_CUDA; }
   *out = S;
   return MW_OK;
 }
@@ -1208,6 +1332,9 @@ int mw_stokes_set_viscosity(mw_stokes* S, const double* etaq, const double* eta_
   if (S->has32) k_cast<float><<<grid_for(nel * 9, 256), 256, 0, s>>>(nel * 9, etaq, S->etaq32);
   k_inv_eta_e<<<grid_for(nel, 256), 256, 0, s>>>(nel, etaq, eta_e, S->etae_w);
   k_diag<double><<<grid_for((int64_t)S->fine.nnx * S->fine.nnz, 128), 128, 0, s>>>(S->fine, S->etaq64, S->diag64);
+  const int64_t np = (int64_t)(S->fine.nx + 1) * (S->fine.nz + 1);
+  k_mass_diag<<<grid_for(np, 256), 256, 0, s>>>(S->fine, nullptr, S->mdiag);      // M
+  k_mass_diag<<<grid_for(np, 256), 256, 0, s>>>(S->fine, S->etae_w, S->medi);     // M_eta
   S->dirty64 = S->dirty32 = true;
   if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
   return MW_OK;

@@ -21,7 +21,7 @@ class MwStokesParams(ctypes.Structure):
 class MwSolveParams(ctypes.Structure):
     _fields_ = [("scheme", c_int32), ("precision", c_int32), ("tol", c_double), ("max_outer", c_int32),
                 ("max_inner", c_int32), ("inner_rtol", c_double), ("max_refine", c_int32),
-                ("sweep_reduction", c_double), ("mass_rtol", c_double), ("mass_maxit", c_int32),
+                ("sweep_reduction", c_double), ("mass_iters", c_int32),
                 ("use_guess", c_int32)]
 
 

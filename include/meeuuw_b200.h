@@ -112,10 +112,14 @@ int mw_project_elements(int32_t nel, const int32_t* offsets, const int32_t* orde
                         void* stream);
 
 /* project_particle_field_on_nodes_{1,2,3,4}, pic_functions.py:659-1053, for nfield fields at once
- * (each with its own averaging); `averaging`, `phi`, `phi_nodal` are HOST arrays. */
+ * (each with its own averaging); `averaging`, `phi`, `phi_nodal` are HOST arrays.  With a
+ * workspace of mw_project_nodes_workspace_bytes() the sums go through per-element partials (fast);
+ * with work == NULL each node merges its elements' particles in particle-index order (the
+ * reference's exact summation order, slower). */
+size_t mw_project_nodes_workspace_bytes(mw_box box, int32_t nfield);
 int mw_project_nodes(mw_box box, int32_t flavour, int32_t nfield, const int32_t* averaging, const int32_t* offsets,
                      const int32_t* order, const double* r, const double* t, const double* const* phi,
-                     double* const* phi_nodal, void* stream);
+                     double* const* phi_nodal, void* work, size_t work_bytes, void* stream);
 
 /* project_nodal_{V,P,T}field_onto_qpoints, project_nodal_field_onto_qpoints.py:12-62.
  * N is the device (9 x m) basis table (N_V for MW_SPACE_Q2, N_P otherwise); phiq is (nel, 9). */
@@ -146,6 +150,13 @@ typedef struct { /* outputs; VV arrays are float or double per `precision`; rhs 
  * rhs_f and rhs_h are produced (the matrix-free solver needs no stored matrix). */
 size_t mw_assemble_stokes_workspace_bytes(mw_box box);
 int mw_assemble_stokes(mw_box box, int32_t blocks, int32_t precision, mw_stokes_in in, mw_stokes_out out, void* work,
+                       size_t work_bytes, void* stream);
+
+/* rhs_f, rhs_h of build_matrix_stokes (build_matrix_stokes.py:141-143, :206-229) for the case
+ * where every Dirichlet value bc_val_V is zero: body force only, fixed rows 0, rhs_h = 0.
+ * Workspace: mw_assemble_stokes_workspace_bytes(box). */
+int mw_stokes_rhs_body(mw_box box, const double* rhoq, const double* gxq, const double* gzq, const double* JxWq,
+                       const double* N_V, const uint8_t* bc_fix_V, double* rhs_f, double* rhs_h, void* work,
                        size_t work_bytes, void* stream);
 
 typedef struct { /* inputs of build_matrix_energy (build_matrix_energy.py:12-47) */
@@ -235,7 +246,8 @@ typedef struct {
   int32_t cheb_degree;    /* Chebyshev-Jacobi smoothing steps per pre/post sweep                     */
   double cheb_ratio;      /* smoothing interval [lambda_max/ratio, lambda_max]                       */
   double cheb_safety;     /* lambda_max estimate multiplier                                          */
-  int32_t power_iters;    /* power iterations for lambda_max(D^-1 K) per level                       */
+  int32_t power_iters;    /* power iterations for lambda_max(D^-1 K) per level (first viscosity)    */
+  int32_t power_iters_warm; /* power iterations on later viscosities, warm-started                   */
 } mw_stokes_params;
 
 typedef struct {

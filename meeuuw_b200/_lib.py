@@ -86,11 +86,14 @@ _PROTOS = {
                                    c_size_t, c_void_p, c_void_p]),
     "mw_project_elements": (c_int32, [c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_void_p,
                                       c_void_p, c_void_p, c_void_p]),
+    "mw_project_nodes_workspace_bytes": (c_size_t, [MwBox, c_int32]),
     "mw_project_nodes": (c_int32, [MwBox, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
-                                   c_void_p, c_void_p, c_void_p]),
+                                   c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_nodal_to_qpoints": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_assemble_stokes_workspace_bytes": (c_size_t, [MwBox]),
     "mw_assemble_stokes": (c_int32, [MwBox, c_int32, c_int32, MwStokesIn, MwStokesOut, c_void_p, c_size_t, c_void_p]),
+    "mw_stokes_rhs_body": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_assemble_energy_workspace_bytes": (c_size_t, [MwBox]),
     "mw_assemble_energy": (c_int32, [MwBox, c_int32, MwEnergyIn, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_post_workspace_bytes": (c_size_t, []),

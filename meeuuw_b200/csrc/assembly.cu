@@ -345,6 +345,33 @@ k_assemble_energy(mw_box b, mw_energy_in in, S* __restrict__ vv, double* __restr
   b_el[e * 9 + i] = (double)rhs;
 }
 
+// Body-force element vectors f_el[2i+c] = sum_q N_V[q,i] JxW rho g_c (build_matrix_stokes.py:141-143)
+// without the element matrices; fixed dofs get 0 (their rhs is K_ii * bc_val = 0 when every
+// Dirichlet value is zero, :215).
+__global__ void k_body_force(mw_box b, const double* __restrict__ rhoq, const double* __restrict__ gxq,
+                             const double* __restrict__ gzq, const double* __restrict__ JxWq,
+                             const double* __restrict__ NV, const uint8_t* __restrict__ fix, double* __restrict__ fel) {
+  __shared__ double N[81];
+  for (int i = threadIdx.x; i < 81; i += blockDim.x) N[i] = NV[i];
+  __syncthreads();
+  const int64_t n = (int64_t)b.nelx * b.nelz * 9;
+  const int nnx = 2 * b.nelx + 1;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = g / 9;
+    const int i = (int)(g % 9);
+    double fx = 0.0, fz = 0.0;
+    for (int q = 0; q < 9; ++q) {
+      const int64_t gq = e * 9 + q;
+      const double t = N[q * 9 + i] * JxWq[gq] * rhoq[gq];
+      fx += t * gxq[gq];
+      fz += t * gzq[gq];
+    }
+    const int64_t node = q2_node((int)(e % b.nelx), (int)(e / b.nelx), i, nnx);
+    fel[e * 18 + 2 * i] = fix[2 * node] ? 0.0 : fx;
+    fel[e * 18 + 2 * i + 1] = fix[2 * node + 1] ? 0.0 : fz;
+  }
+}
+
 template <typename R>
 static size_t stokes_smem_bytes() {
   size_t n = 117 + 2 * EB_S * 81 + 2 * EB_S * 36 + 5 * EB_S * 9 + EB_S * 72;
@@ -401,6 +428,24 @@ int mw_assemble_stokes(mw_box box, int32_t blocks, int32_t precision, mw_stokes_
   int64_t np = (int64_t)(box.nelx + 1) * (box.nelz + 1);
   k_gather_q1<<<grid_for(np, 256), 256, 0, s>>>(box, hel, out.rhs_h);
   MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_rhs_body(mw_box box, const double* rhoq, const double* gxq, const double* gzq, const double* JxWq,
+                       const double* N_V, const uint8_t* bc_fix_V, double* rhs_f, double* rhs_h, void* work,
+                       size_t work_bytes, void* stream) {
+  if (box.nelx <= 0 || box.nelz <= 0 || !rhs_f || !rhs_h) return MW_ERR_BAD_ARG;
+  if (work_bytes < mw_assemble_stokes_workspace_bytes(box)) return MW_ERR_WORKSPACE;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nel = (int64_t)box.nelx * box.nelz;
+  double* fel = (double*)work;
+  k_body_force<<<grid_for(nel * 9, 256), 256, 0, s>>>(box, rhoq, gxq, gzq, JxWq, N_V, bc_fix_V, fel);
+  MW_CHECK_LAUNCH();
+  const int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  k_gather_q2<<<grid_for(nn, 256), 256, 0, s>>>(box, 2, fel, rhs_f);
+  MW_CHECK_LAUNCH();
+  const int64_t np = (int64_t)(box.nelx + 1) * (box.nelz + 1);
+  if (cudaMemsetAsync(rhs_h, 0, sizeof(double) * np, s) != cudaSuccess) return MW_ERR_CUDA;
   return MW_OK;
 }
 

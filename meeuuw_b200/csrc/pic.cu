@@ -431,6 +431,79 @@ __global__ void k_project_corners(mw_box b, int flavour, const int32_t* __restri
   }
 }
 
+// Faster form of the same projection: each element sums its particles (in particle-index order)
+// per corner into partials (nel x 4 x (nfield+1) doubles), then each corner node adds the partials
+// of its incident elements in ascending element order and applies the averaging.  The sums agree
+// with the reference's particle-ordered sums to rounding (different association).
+__global__ void k_project_elem_partials(mw_box b, int flavour, const int32_t* __restrict__ offsets,
+                                        const int32_t* __restrict__ order, const double* __restrict__ r,
+                                        const double* __restrict__ t, ProjFields pf, double* __restrict__ part) {
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  const int nf1 = pf.n + 1;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    double acc[4][MW_MAX_FIELDS + 1];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+      for (int f = 0; f <= MW_MAX_FIELDS; ++f) acc[k][f] = 0.0;
+    const int b0 = offsets[e], b1 = offsets[e + 1];
+    for (int j = b0; j < b1; ++j) {
+      const int p = order[j];
+      const double rp = r[p], tp = t[p];
+      double v[MW_MAX_FIELDS];
+#pragma unroll
+      for (int f = 0; f < MW_MAX_FIELDS; ++f)
+        if (f < pf.n) v[f] = avg_transform(pf.averaging[f], pf.phi[f][p]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        bool use; double w;
+        corner_weight(flavour, k, rp, tp, &use, &w);
+        if (!use) continue;
+        const bool plain = (flavour == 1 || flavour == 3);
+        acc[k][MW_MAX_FIELDS] = plain ? acc[k][MW_MAX_FIELDS] + 1.0 : acc[k][MW_MAX_FIELDS] + 1 * w;
+#pragma unroll
+        for (int f = 0; f < MW_MAX_FIELDS; ++f)
+          if (f < pf.n) acc[k][f] = plain ? acc[k][f] + v[f] : acc[k][f] + v[f] * w;
+      }
+    }
+    double* o = part + e * 4 * nf1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      for (int f = 0; f < pf.n; ++f) o[k * nf1 + f] = acc[k][f];
+      o[k * nf1 + pf.n] = acc[k][MW_MAX_FIELDS];
+    }
+  }
+}
+
+__global__ void k_project_corner_finish(mw_box b, ProjFields pf, const double* __restrict__ part) {
+  const int ncx = b.nelx + 1, ncz = b.nelz + 1;
+  const int nnx = 2 * b.nelx + 1;
+  const int nf1 = pf.n + 1;
+  const int64_t ncorner = (int64_t)ncx * ncz;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncorner; c += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(c % ncx), j = (int)(c / ncx);
+    double acc[MW_MAX_FIELDS + 1];
+    for (int f = 0; f <= pf.n; ++f) acc[f] = 0.0;
+    // ascending element order: (j-1,i-1) corner 2, (j-1,i) corner 3, (j,i-1) corner 1, (j,i) corner 0
+    for (int s2 = 0; s2 < 4; ++s2) {
+      const int ex = (s2 & 1) ? i : i - 1, ez = (s2 & 2) ? j : j - 1;
+      if (ex < 0 || ex >= b.nelx || ez < 0 || ez >= b.nelz) continue;
+      const int k = s2 == 0 ? 2 : (s2 == 1 ? 3 : (s2 == 2 ? 1 : 0));
+      const double* o = part + ((int64_t)ez * b.nelx + ex) * 4 * nf1 + k * nf1;
+      for (int f = 0; f <= pf.n; ++f) acc[f] += o[f];
+    }
+    const double cnt = acc[pf.n];
+    const int64_t node = (int64_t)(2 * j) * nnx + 2 * i;
+    for (int f = 0; f < pf.n; ++f) {
+      double v;
+      if (pf.averaging[f] == MW_AVG_GEOMETRIC) v = pow(10.0, acc[f] / cnt);
+      else if (pf.averaging[f] == MW_AVG_HARMONIC) v = cnt / acc[f];
+      else v = acc[f] / cnt;
+      pf.out[f][node] = v;
+    }
+  }
+}
+
 // Edge and centre nodes from the corners: pic_functions.py:801-809.
 __global__ void k_fill_q2(mw_box b, ProjFields pf) {
   const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
@@ -570,9 +643,13 @@ int mw_project_elements(int32_t nel, const int32_t* offsets, const int32_t* orde
   return MW_OK;
 }
 
+size_t mw_project_nodes_workspace_bytes(mw_box box, int32_t nfield) {
+  return (size_t)box.nelx * box.nelz * 4 * (nfield + 1) * sizeof(double);
+}
+
 int mw_project_nodes(mw_box box, int32_t flavour, int32_t nfield, const int32_t* averaging, const int32_t* offsets,
                      const int32_t* order, const double* r, const double* t, const double* const* phi,
-                     double* const* phi_nodal, void* stream) {
+                     double* const* phi_nodal, void* work, size_t work_bytes, void* stream) {
   if (!box_ok(box) || flavour < 1 || flavour > 4 || nfield < 1 || nfield > MW_MAX_FIELDS) return MW_ERR_BAD_ARG;
   ProjFields pf;
   pf.n = nfield;
@@ -582,7 +659,15 @@ int mw_project_nodes(mw_box box, int32_t flavour, int32_t nfield, const int32_t*
   }
   cudaStream_t s = (cudaStream_t)stream;
   int64_t nc = (int64_t)(box.nelx + 1) * (box.nelz + 1);
-  k_project_corners<<<grid_for(nc, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf);
+  if (work && work_bytes >= mw_project_nodes_workspace_bytes(box, nfield)) {
+    int64_t nel = (int64_t)box.nelx * box.nelz;
+    k_project_elem_partials<<<grid_for(nel, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf, (double*)work);
+    MW_CHECK_LAUNCH();
+    k_project_corner_finish<<<grid_for(nc, 256), 256, 0, s>>>(box, pf, (const double*)work);
+  } else {
+    // no workspace: per-node merge of the incident elements' particles in particle-index order
+    k_project_corners<<<grid_for(nc, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf);
+  }
   MW_CHECK_LAUNCH();
   int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
   k_fill_q2<<<grid_for(nn, 256), 256, 0, s>>>(box, pf);

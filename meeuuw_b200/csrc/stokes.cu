@@ -32,7 +32,23 @@ struct RefTables {
   double wq[9];            // Gauss weights
 };
 __constant__ RefTables c_ref;
+// the same tables in single precision, so that FP32 kernels use them as constant-bank operands
+__constant__ float c_dr32[81], c_dt32[81], c_np32[36], c_wq32[9];
 static bool g_ref_ready = false;
+
+template <typename R> struct CT;
+template <> struct CT<double> {
+  MW_D static double dr(int i) { return c_ref.dr[i]; }
+  MW_D static double dt(int i) { return c_ref.dt[i]; }
+  MW_D static double np(int i) { return c_ref.NP[i]; }
+  MW_D static double wq(int i) { return c_ref.wq[i]; }
+};
+template <> struct CT<float> {
+  MW_D static float dr(int i) { return c_dr32[i]; }
+  MW_D static float dt(int i) { return c_dt32[i]; }
+  MW_D static float np(int i) { return c_np32[i]; }
+  MW_D static float wq(int i) { return c_wq32[i]; }
+};
 
 static void host_ref_tables(RefTables* T) {
   const double qc[3] = {-std::sqrt(3.0 / 5.0), 0.0, std::sqrt(3.0 / 5.0)};
@@ -66,6 +82,15 @@ static int ensure_ref_tables() {
   RefTables T;
   host_ref_tables(&T);
   if (cudaMemcpyToSymbol(c_ref, &T, sizeof(T)) != cudaSuccess) return MW_ERR_CUDA;
+  float f[81];
+  for (int i = 0; i < 81; ++i) f[i] = (float)T.dr[i];
+  if (cudaMemcpyToSymbol(c_dr32, f, sizeof(float) * 81) != cudaSuccess) return MW_ERR_CUDA;
+  for (int i = 0; i < 81; ++i) f[i] = (float)T.dt[i];
+  if (cudaMemcpyToSymbol(c_dt32, f, sizeof(float) * 81) != cudaSuccess) return MW_ERR_CUDA;
+  for (int i = 0; i < 36; ++i) f[i] = (float)T.NP[i];
+  if (cudaMemcpyToSymbol(c_np32, f, sizeof(float) * 36) != cudaSuccess) return MW_ERR_CUDA;
+  for (int i = 0; i < 9; ++i) f[i] = (float)T.wq[i];
+  if (cudaMemcpyToSymbol(c_wq32, f, sizeof(float) * 9) != cudaSuccess) return MW_ERR_CUDA;
   g_ref_ready = true;
   return MW_OK;
 }
@@ -87,6 +112,10 @@ constexpr int APPLY_THREADS = 160;
 
 enum ApplyMode { AM_APPLY = 0, AM_RESID = 1, AM_CHEB = 2 };
 
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { typedef float2 T; };
+template <> struct Vec2<double> { typedef double2 T; };
+
 template <typename R>
 struct ApplyArgs {
   const R* u;        // velocity (interleaved u,w), may be null
@@ -104,61 +133,48 @@ struct ApplyArgs {
   const double* cheb; // device coefficients {c1, c2}
 };
 
-// Per-CTA tables in the kernel's precision: scaled derivatives dN/dx = (2/hx) dN/dr and
-// dN/dz = (2/hz) dN/dt at the Gauss points, N_P, and JxW = hx*hz/4 * w_q (uniform box).
+// Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points: strain rate B u
+// at each point, stress 2 eta (exx, ezz) and eta (du/dz + dw/dx) with the pressure term, then B^T
+// back onto the nodes (build_matrix_stokes.py:130-157 applied to a vector).  The reference-element
+// tables are __constant__ and every loop is unrolled, so each table value is an immediate
+// constant-bank operand of the FMA; the uniform-box Jacobian enters as sx = 2/hx, sz = 2/hz.
 template <typename R>
-struct ApplyTables {
-  R DX[81], DZ[81], NP[36], JW[9];
-};
-
-template <typename R>
-MW_D void fill_tables(const LevelGeo& g, ApplyTables<R>& T, int tid, int nthreads) {
-  const double sx = 2.0 / g.hx, sz = 2.0 / g.hz, jac = g.hx * g.hz / 4.0;
-  for (int i = tid; i < 81; i += nthreads) { T.DX[i] = R(sx * c_ref.dr[i]); T.DZ[i] = R(sz * c_ref.dt[i]); }
-  for (int i = tid; i < 36; i += nthreads) T.NP[i] = R(c_ref.NP[i]);
-  for (int i = tid; i < 9; i += nthreads) T.JW[i] = R(jac * c_ref.wq[i]);
-}
-
-// Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points:
-// strain rate B u at each point, stress 2 eta (exx, ezz) and eta (du/dz + dw/dx) with the
-// pressure term, then B^T back onto the nodes (build_matrix_stokes.py:130-157 applied to a vector).
-template <typename R>
-MW_D void element_apply(const ApplyTables<R>& T, R s, const R* ue, const R* pe, const R* eq, R* ye, R* ype,
-                        bool use_p) {
+MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const R* eq, R* ye, R* ype, bool use_p) {
 #pragma unroll
   for (int k = 0; k < 18; ++k) ye[k] = 0;
 #pragma unroll
   for (int k = 0; k < 4; ++k) ype[k] = 0;
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
-    R exx = 0, ezz = 0, gg = 0;
+    R dxu = 0, dzw = 0, dzu = 0, dxw = 0;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const R dx = T.DX[q * 9 + k], dz = T.DZ[q * 9 + k];
-      exx += dx * ue[2 * k];
-      ezz += dz * ue[2 * k + 1];
-      gg += dz * ue[2 * k] + dx * ue[2 * k + 1];       // du/dz + dw/dx
+      const R r = CT<R>::dr(q * 9 + k), t = CT<R>::dt(q * 9 + k);
+      dxu += r * ue[2 * k];
+      dzw += t * ue[2 * k + 1];
+      dzu += t * ue[2 * k];
+      dxw += r * ue[2 * k + 1];
     }
-    const R jw = T.JW[q];
+    const R exx = sx * dxu, ezz = sz * dzw, gg = sz * dzu + sx * dxw;   // gg = du/dz + dw/dx
+    const R jw = jac * CT<R>::wq(q);
     const R e = eq[q] * jw;
     R pq = 0;
     if (use_p) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) pq += T.NP[q * 4 + k] * pe[k];
+      for (int k = 0; k < 4; ++k) pq += CT<R>::np(q * 4 + k) * pe[k];
     }
     const R sp = s * jw * pq;
-    const R A = R(2) * e * exx - sp;
-    const R B = R(2) * e * ezz - sp;
-    const R C = e * gg;
+    const R A = (R(2) * e * exx - sp) * sx, B = (R(2) * e * ezz - sp) * sz;
+    const R Cx = e * gg * sx, Cz = e * gg * sz;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const R dx = T.DX[q * 9 + k], dz = T.DZ[q * 9 + k];
-      ye[2 * k] += dx * A + dz * C;
-      ye[2 * k + 1] += dz * B + dx * C;
+      const R r = CT<R>::dr(q * 9 + k), t = CT<R>::dt(q * 9 + k);
+      ye[2 * k] += r * A + t * Cz;
+      ye[2 * k + 1] += t * B + r * Cx;
     }
     const R dv = -s * jw * (exx + ezz);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) ype[k] += T.NP[q * 4 + k] * dv;
+    for (int k = 0; k < 4; ++k) ype[k] += CT<R>::np(q * 4 + k) * dv;
   }
 }
 
@@ -172,27 +188,32 @@ MW_D int q2_local_idx(int dx, int dz) {
 template <typename R, int MODE>
 __global__ void __launch_bounds__(APPLY_THREADS)
 k_apply(LevelGeo g, ApplyArgs<R> a) {
-  __shared__ R su[LZ * LX * 2];
+  __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
-  __shared__ ApplyTables<R> T;
   const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
   const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
-  // ---- stage velocity (masked), pressure, viscosity ----
+  // ---- stage velocity (masked; one vector load per node), pressure ----
+  typedef typename Vec2<R>::T R2;
+  const R2* u2 = reinterpret_cast<const R2*>(a.u);
+  const uchar2* f2 = reinterpret_cast<const uchar2*>(a.fix);
+  R2* su2 = reinterpret_cast<R2*>(su);
   for (int i = tid; i < LZ * LX; i += APPLY_THREADS) {
-    int lz = i / LX, lx = i % LX;
-    int ix = lx0 + lx, iz = lz0 + lz;
-    R u0 = 0, u1 = 0;
+    const int lz = i / LX, lx = i - lz * LX;
+    const int ix = lx0 + lx, iz = lz0 + lz;
+    R2 v;
+    v.x = 0; v.y = 0;
     if (use_u && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
-      int64_t n = (int64_t)iz * g.nnx + ix;
-      u0 = a.fix[2 * n] ? R(0) : a.u[2 * n];
-      u1 = a.fix[2 * n + 1] ? R(0) : a.u[2 * n + 1];
+      const int64_t n = (int64_t)iz * g.nnx + ix;
+      const R2 uu = u2[n];
+      const uchar2 ff = f2[n];
+      v.x = ff.x ? R(0) : uu.x;
+      v.y = ff.y ? R(0) : uu.y;
     }
-    su[2 * i] = u0; su[2 * i + 1] = u1;
+    su2[i] = v;
   }
-  fill_tables<R>(g, T, tid, APPLY_THREADS);
   if (use_p)
     for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
       int jz = i / PX, jx = i % PX;
@@ -218,7 +239,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
 #pragma unroll
       for (int q = 0; q < 9; ++q) eq[q] = eg[q];
-      element_apply<R>(T, R(g.s), ue, pe, eq, ye, ype, use_p);
+      element_apply<R>(R(2.0 / g.hx), R(2.0 / g.hz), R(g.hx * g.hz / 4.0), R(g.s), ue, pe, eq, ye, ype, use_p);
 #pragma unroll
       for (int k = 0; k < 18; ++k) sye[tid * 22 + k] = ye[k];
 #pragma unroll
@@ -582,6 +603,29 @@ __global__ void k_dense_assemble(LevelGeo g, const R* __restrict__ eta, const ui
 }
 
 // In-place Gauss-Jordan inversion of an SPD matrix, one CTA.
+// Same inversion with the whole matrix held in shared memory (nd*nd doubles + a column).
+__global__ void k_gauss_jordan_smem(int nd, double* __restrict__ Ag) {
+  extern __shared__ double sm[];
+  double* A = sm;
+  double* col = sm + (size_t)nd * nd;
+  for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) A[t] = Ag[t];
+  for (int k = 0; k < nd; ++k) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) col[i] = A[i * nd + k];
+    __syncthreads();
+    const double piv = 1.0 / col[k];
+    for (int j = threadIdx.x; j < nd; j += blockDim.x) A[k * nd + j] = (j == k ? 1.0 : A[k * nd + j]) * piv;
+    __syncthreads();
+    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
+      const int i = t / nd, j = t - i * nd;
+      if (i == k) continue;
+      A[t] = (j == k ? 0.0 : A[t]) - col[i] * A[k * nd + j];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) Ag[t] = A[t];
+}
+
 __global__ void k_gauss_jordan(int nd, double* __restrict__ A) {
   extern __shared__ double col[];
   for (int k = 0; k < nd; ++k) {
@@ -801,6 +845,8 @@ struct Level {
   uint8_t* fix;
   double* cheb;       // 2*MAXDEG coefficients
   double* lam2;
+  R* ev;              // power-iteration vector, kept between viscosity updates (warm start)
+  bool ev_ready;
 };
 
 struct Arena {
@@ -886,6 +932,8 @@ static void carve(Hierarchy<R>& H, Arena& A, const uint8_t* fine_fix) {
     L.fix = l == 0 ? const_cast<uint8_t*>(fine_fix) : (uint8_t*)A.take(L.ndof);
     L.cheb = (double*)A.take(sizeof(double) * 2 * MAXDEG);
     L.lam2 = (double*)A.take(sizeof(double) * 4);
+    L.ev = (R*)A.take(sizeof(R) * L.ndof);
+    L.ev_ready = false;
   }
   H.Ainv = H.dense ? (double*)A.take(sizeof(double) * (size_t)H.nd * H.nd) : nullptr;
 }
@@ -1028,18 +1076,32 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
     const bool coarsest = l == H.nlev - 1;
     if (coarsest && H.dense) {
       k_dense_assemble<R><<<1, 1024, 0, s>>>(L.g, L.eta, L.fix, H.Ainv);
-      k_gauss_jordan<<<1, 1024, sizeof(double) * H.nd, s>>>(H.nd, H.Ainv);
+      const size_t smem = sizeof(double) * ((size_t)H.nd * H.nd + H.nd);
+      int dev = 0, optin = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      if (smem <= (size_t)optin &&
+          cudaFuncSetAttribute(k_gauss_jordan_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+              cudaSuccess)
+        k_gauss_jordan_smem<<<1, 1024, smem, s>>>(H.nd, H.Ainv);
+      else
+        k_gauss_jordan<<<1, 1024, sizeof(double) * H.nd, s>>>(H.nd, H.Ainv);
       continue;
     }
-    R* v = L.r;
-    R* t = L.t;
-    k_power_init<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, v);
-    for (int it = 0; it < prm.power_iters; ++it) {
+    // power iteration v <- D^-1 K v / |v|, warm-started from the previous viscosity's vector
+    R* v = L.ev;
+    int iters = prm.power_iters;
+    if (!L.ev_ready) {
+      k_power_init<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, v);
+      L.ev_ready = true;
+    } else {
+      iters = prm.power_iters_warm > 0 ? prm.power_iters_warm : prm.power_iters;
+    }
+    for (int it = 0; it < iters; ++it) {
       dot<R>(S, L.ndof, v, v, L.lam2 + 1, s);
       k_normalize<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.lam2 + 1, v);
       k_only_apply<R>(L, v, L.d, s);
-      k_dinv<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.d, L.diag, t);
-      std::swap(v, t);
+      k_dinv<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.d, L.diag, v);
     }
     dot<R>(S, L.ndof, v, v, L.lam2, s);          // ||D^-1 K v_prev||^2 with ||v_prev|| = 1
     int deg = coarsest ? MAXDEG : prm.cheb_degree;
@@ -1285,6 +1347,7 @@ void mw_stokes_default_params(mw_stokes_params* p) {
   p->eta_ref = 1.0; p->L_ref = 1.0; p->precisions = 3;
   p->coarse_min = 4; p->dense_max = 700; p->cheb_degree = 3; p->cheb_ratio = 8.0; p->cheb_safety = 1.1;
   p->power_iters = 12;
+  p->power_iters_warm = 3;
 }
 
 void mw_solve_default_params(mw_solve_params* p) {

@@ -121,16 +121,21 @@ def project_elements(nel, offsets, order, rho, eta, averaging, rho_e=None, eta_e
     return rho_e, eta_e
 
 
-def project_nodes(box, flavour, fields, offsets, order, r, t, outs=None):
-    """fields: list of (phi, averaging) -> list of nodal arrays (nn_V)."""
+def project_nodes(box, flavour, fields, offsets, order, r, t, outs=None, exact_order=False):
+    """fields: list of (phi, averaging) -> list of nodal arrays (nn_V).  exact_order=True sums in
+    the reference's particle-index order (per-node merge, slower)."""
     nn = (2 * box.nelx + 1) * (2 * box.nelz + 1)
     if outs is None:
         outs = [_empty(nn, like=r) for _ in fields]
     for i in range(0, len(fields), L.MAX_FIELDS):
         fs, os_ = fields[i:i + L.MAX_FIELDS], outs[i:i + L.MAX_FIELDS]
         avg = (ctypes.c_int32 * len(fs))(*[L.AVG[a] for _, a in fs])
+        if exact_order:
+            wp, wb = None, ctypes.c_size_t(0)
+        else:
+            wp, wb = workspace("proj").get(L.lib().mw_project_nodes_workspace_bytes(box, len(fs)))
         call("mw_project_nodes", box, int(flavour), len(fs), avg, ptr(offsets), ptr(order), ptr(r), ptr(t),
-             L.ptr_array([p for p, _ in fs]), L.ptr_array(os_), stream_ptr())
+             L.ptr_array([p for p, _ in fs]), L.ptr_array(os_), wp, wb, stream_ptr())
     return outs
 
 
@@ -246,6 +251,14 @@ def global_quantities(uq, wq, Tq, rhoq, JxWq, volume, out=None):
     call("mw_global_quantities", uq.numel(), ptr(uq), ptr(wq), ptr(Tq), ptr(rhoq), ptr(JxWq), float(volume), ptr(out),
          wp, wb, stream_ptr())
     return out
+
+
+def stokes_rhs_body(box, rhoq, gxq, gzq, JxWq, N_V, bc_fix_V, rhs_f, rhs_h):
+    """Stokes right-hand side for all-zero Dirichlet values (body force only)."""
+    wp, wb = workspace("asm").get(L.lib().mw_assemble_stokes_workspace_bytes(box))
+    call("mw_stokes_rhs_body", box, ptr(rhoq), ptr(gxq), ptr(gzq), ptr(JxWq), ptr(N_V), ptr(as_u8(bc_fix_V)),
+         ptr(rhs_f), ptr(rhs_h), wp, wb, stream_ptr())
+    return rhs_f, rhs_h
 
 
 def split_solution(solV, solP, scale, u, w, p):

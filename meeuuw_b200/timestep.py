@@ -64,6 +64,7 @@ class GPUModel:
         self.gxq = torch.full((nel, 9), float(gx), dtype=f64, device=device)
         self.gzq = torch.full((nel, 9), float(gz), dtype=f64, device=device)
         self.bc_fix_V, self.bc_val_V = D(host.bc_fix_V, torch.bool), D(host.bc_val_V, f64)
+        self.zero_bc_values = not bool((host.bc_val_V != 0).any())
         self.bc_fix_T, self.bc_val_T = D(host.bc_fix_T, torch.bool), D(host.bc_val_T, f64)
         self.rhs_f, self.rhs_h = E(2 * nn), E(npp)
         self.solV, self.solP = Z(2 * nn), Z(npp)
@@ -117,8 +118,12 @@ class GPUModel:
             for k in ("exx", "ezz", "exz"):
                 ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], getattr(self, k + "_n"), qf[k + "q"])
         # Stokes (meeuuw.py:1705-1851): right-hand side, matrix-free solve
-        ops.assemble_stokes(b, False, 0, self.stokes_inputs(), tb, self.bc_fix_V, self.bc_val_V, c.eta_ref,
-                            self.L_ref, out=dict(rhs_f=self.rhs_f, rhs_h=self.rhs_h))
+        if self.zero_bc_values:
+            ops.stokes_rhs_body(b, qf["rhoq"], self.gxq, self.gzq, self.geo["JxWq"], tb["N_V"], self.bc_fix_V,
+                                self.rhs_f, self.rhs_h)
+        else:
+            ops.assemble_stokes(b, False, 0, self.stokes_inputs(), tb, self.bc_fix_V, self.bc_val_V, c.eta_ref,
+                                self.L_ref, out=dict(rhs_f=self.rhs_f, rhs_h=self.rhs_h))
         self.solver.set_viscosity(qf["etaq"], self.eta_e)
         if self.guess is not None:
             self.guess(self)

@@ -63,12 +63,14 @@ def test_projections(M, avg):
     assert np.array_equal(H(rho_e), g[f"out_elem_{avg}_rho"])
     assert rel_err(H(eta_e), g[f"out_elem_{avg}_eta"]) < 1e-14
     for fl in (1, 2, 3, 4):
-        (v,) = ops.project_nodes(M["box"], fl, [(D(g["swarm_eta"]), avg)], offsets, order, D(g["out_r"]), D(g["out_t"]))
-        ref = g[f"out_nodes{fl}_{avg}"]
-        v = H(v)
-        ok = ~np.isnan(ref)
-        assert np.array_equal(np.isnan(v), np.isnan(ref)), fl
-        assert rel_err(v[ok], ref[ok]) < 1e-14, (fl, avg)
+        for exact in (False, True):   # per-element partials / per-node particle-order merge
+            (v,) = ops.project_nodes(M["box"], fl, [(D(g["swarm_eta"]), avg)], offsets, order, D(g["out_r"]),
+                                     D(g["out_t"]), exact_order=exact)
+            ref = g[f"out_nodes{fl}_{avg}"]
+            v = H(v)
+            ok = ~np.isnan(ref)
+            assert np.array_equal(np.isnan(v), np.isnan(ref)), fl
+            assert rel_err(v[ok], ref[ok]) < 1e-14, (fl, avg, exact)
 
 
 @pytest.mark.parametrize("rk", [1, 2, 4])

@@ -30,6 +30,7 @@ extern "C" {
 #define MW_ERR_NOT_CONVERGED 3
 #define MW_ERR_WORKSPACE 4
 #define MW_ERR_DEVICE_FLAG 5
+#define MW_ERR_TOO_LARGE 6   /* the problem exceeds a fixed-capacity entry point's static scratch */
 
 /* ---- device flag bits (err word) ---- */
 #define MW_FLAG_R_OUT_OF_BOUNDS 1   /* locate_particles.py:61-62 "r value out of bounds" */
@@ -218,6 +219,22 @@ int mw_nodal_heat_flux(mw_box box, const double* T, const double* hcond_n, const
 size_t mw_nu_workspace_bytes(mw_box box);
 int mw_compute_nu(mw_box box, const double* T, const double* dTdx_n, const double* dTdz_n, const double* hcond_n,
                   mw_gauss3 g, double* out13, void* work, size_t work_bytes, void* stream);
+
+/* Nusselt number without any allocation.  No counterpart in the reference: it exists for callers
+ * that hold the temperature and heat-flux arrays on the device but cannot allocate device memory
+ * themselves -- for example a diagnostics or monitoring hook that a host code hands read-only
+ * device pointers to, with no allocator of its own, and that must not change the memory state of
+ * the running simulation (mw_compute_nu needs a caller-allocated workspace).  Its scratch is a
+ * fixed file-scope device array sized for at most MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS boundary
+ * elements, 2*(nelx+nelz) (2.25 MiB, held by every GPU that loads the library until exit);
+ * larger meshes return MW_ERR_TOO_LARGE.  The call makes no cudaMalloc/cudaFree and calls no
+ * allocating routine.  The first call on a device looks up the array's device address (set-up)
+ * and should therefore come before any stream capture.  All calls share the one array: calls
+ * that overlap on the GPU (different streams, same device) race and must be serialised by the
+ * caller.  Output: the same 13 values as mw_compute_nu. */
+#define MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS 32768
+int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, const double* dTdz_n,
+                          const double* hcond_n, mw_gauss3 g, double* out13, void* stream);
 
 /* compute_global_quantities, postprocessors.py:14-83 (the vrms, Tavrg and mass sums):
  * out3 = {vrms, Tavrg, TM}.  Tq, rhoq may be NULL. */

@@ -9,9 +9,16 @@
 // count -- the reference's order, without atomics.  Global sums use a fixed two-level tree
 // (deterministic, not the reference's sequential order); the short boundary sums of the surface
 // pressure offset and of Nu are summed sequentially in the reference's element order.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace mw {
+
+// Scratch of mw_compute_nu_noalloc: 3 doubles per boundary (element, Gauss point) pair for at most
+// MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS boundary elements (2.25 MiB).  Every GPU that loads the
+// library holds this array until the process exits.
+static __device__ __align__(256) double g_nu_scratch[(size_t)MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS * 3 * 3];
 
 constexpr int RT = 256;   // reduction block size
 constexpr int RB = 296;   // reduction blocks (2 x 148 SMs)
@@ -442,6 +449,41 @@ int mw_compute_nu(mw_box box, const double* T, const double* dTdx_n, const doubl
   k_nu_terms<<<grid_for(total, 128), 128, 0, s>>>(box, T, dTdx_n, dTdz_n, hcond_n, g, (double*)work);
   MW_CHECK_LAUNCH();
   k_nu_final<<<1, 32, 0, s>>>(box, (const double*)work, out13);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+// Device address of g_nu_scratch, looked up once per device (host code cannot use the symbol
+// itself as a device pointer).
+static double* nu_scratch_for_current_device(int* status) {
+  static std::mutex mtx;
+  static double* addr[64] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { *status = MW_ERR_CUDA; return nullptr; }
+  std::lock_guard<std::mutex> lock(mtx);
+  if (!addr[dev]) {
+    double* p = nullptr;
+    if (cudaGetSymbolAddress((void**)&p, g_nu_scratch) != cudaSuccess || !p) { *status = MW_ERR_CUDA; return nullptr; }
+    addr[dev] = p;
+  }
+  *status = MW_OK;
+  return addr[dev];
+}
+
+int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, const double* dTdz_n,
+                          const double* hcond_n, mw_gauss3 g, double* out13, void* stream) {
+  if (box.nelx <= 0 || box.nelz <= 0 || !T || !dTdx_n || !dTdz_n || !hcond_n || !out13) return MW_ERR_BAD_ARG;
+  const int64_t nbound = 2LL * box.nelx + 2LL * box.nelz;
+  if (nbound > MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS) return MW_ERR_TOO_LARGE;
+  int st = MW_OK;
+  double* scratch = nu_scratch_for_current_device(&st);
+  if (st != MW_OK) return st;
+  // every scratch slot the final sum reads is written by k_nu_terms first: nothing to clear
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t total = nbound * 3;
+  k_nu_terms<<<grid_for(total, 128), 128, 0, s>>>(box, T, dTdx_n, dTdz_n, hcond_n, g, scratch);
+  MW_CHECK_LAUNCH();
+  k_nu_final<<<1, 32, 0, s>>>(box, scratch, out13);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }

@@ -343,6 +343,27 @@ size_t mw_energy_solve_workspace_bytes(mw_box box);
 int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
                     int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream);
 
+/* ======================= learned warm start: tensor-core kernels ======================= */
+/* No reference counterpart: the learned warm start is this build's addition to the method. */
+
+#define MW_GEMM_EPI_F32 0   /* out: float, D (+ bias)                      */
+#define MW_GEMM_EPI_BF16 1  /* out: bf16, relu?(D + bias)                  */
+
+typedef struct {
+  int32_t mode, relu, splits; /* splits > 1: split-K with FP32 partials in `work` (mode F32 only) */
+  const float* bias;          /* per output column, may be NULL                                  */
+  void* out;                  /* row-major [M, N] with leading dimension ldo                     */
+  int64_t ldo;
+} mw_gemm_epilogue;
+
+/* D[M, N] = A[M, K] * B[N, K]^T with BF16 operands (row-major, leading dimensions lda, ldb >= K,
+ * K a multiple of 64, 16-byte aligned rows) and FP32 accumulation: TMA-fed tcgen05.mma with
+ * the accumulator in TMEM.  err (device int32, may be NULL) receives MW_FLAG_ITER_LIMIT if a
+ * pipeline wait ever gives up. */
+size_t mw_gemm_workspace_bytes(int32_t M, int32_t N, int32_t splits);
+int mw_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const void* A, int64_t lda, const void* B, int64_t ldb,
+                    mw_gemm_epilogue epi, void* work, size_t work_bytes, int32_t* err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -297,3 +297,35 @@ def compute_dt(u, w, hcond, hcapa, rho, CFLnb, hx, hz, dt_max, solve_T, state, o
     call("mw_compute_dt", u.numel(), ptr(u), ptr(w), n, ptr(hcond), ptr(hcapa), ptr(rho), prm, ptr(state), ptr(out),
          wp, wb, stream_ptr())
     return out
+
+
+# ----------------------------------------------------------------------------- tensor-core GEMM
+class MwGemmEpilogue(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int32), ("relu", ctypes.c_int32), ("splits", ctypes.c_int32),
+                ("bias", ctypes.c_void_p), ("out", ctypes.c_void_p), ("ldo", ctypes.c_int64)]
+
+
+L.extra_protos({
+    "mw_gemm_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "mw_gemm_bf16_tn": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                         ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, MwGemmEpilogue,
+                                         ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),
+})
+
+EPI_F32, EPI_BF16 = 0, 1
+
+
+def gemm_bf16_tn(A, B, out=None, bias=None, relu=False, splits=1, out_bf16=False, err=None):
+    """out[M, N] = A[M, K] @ B[N, K]^T on the tensor cores (A, B bf16, K % 64 == 0)."""
+    M, K = A.shape
+    N = B.shape[0]
+    if out is None:
+        out = torch.empty(M, N, dtype=torch.bfloat16 if out_bf16 else torch.float32, device=A.device)
+    ep = MwGemmEpilogue(EPI_BF16 if out_bf16 else EPI_F32, int(bool(relu)), int(splits), ptr(bias), ptr(out),
+                        out.stride(0))
+    if splits > 1:
+        wp, wb = workspace("gemm").get(L.lib().mw_gemm_workspace_bytes(M, N, splits))
+    else:
+        wp, wb = None, ctypes.c_size_t(0)
+    call("mw_gemm_bf16_tn", M, N, K, ptr(A), A.stride(0), ptr(B), B.stride(0), ep, wp, wb, ptr(err), stream_ptr())
+    return out

@@ -364,6 +364,47 @@ size_t mw_gemm_workspace_bytes(int32_t M, int32_t N, int32_t splits);
 int mw_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const void* A, int64_t lda, const void* B, int64_t ldb,
                     mw_gemm_epilogue epi, void* work, size_t work_bytes, int32_t* err, void* stream);
 
+/* U-Net building blocks (activations NHWC BF16, gradients FP32; conv K index = tap*C + c, zero
+ * padded to Kp, a multiple of 64).  transposed=1 writes the im2col matrix as [Kp, B*H*W]. */
+int mw_unet_im2col(int32_t B, int32_t H, int32_t W, int32_t C, int32_t Kp, int32_t transposed, const void* X,
+                   void* col, void* stream);
+int mw_unet_cast_bf16(int64_t n, const float* a, void* b, void* stream);
+/* weights of the data-gradient convolution: Wt[ci][tap*Cout+co] = W[co][(8-tap)*Cin+ci] */
+int mw_unet_weights_bwd(int32_t Cout, int32_t Cin, int32_t Kp_in, int32_t Kp_out, const float* W, void* Wt,
+                        void* stream);
+/* dZ = dA * (A > 0) (relu=1) or dA: bf16 [M,C], bf16 transposed [C,M], fp32 [M,C] */
+int mw_unet_relu_grad(int64_t M, int32_t C, int32_t relu, const float* dA, const void* A, void* dZ, void* dZT,
+                      float* dZ32, void* stream);
+int mw_unet_colsum(int64_t M, int32_t C, const float* X, float* out, void* stream);
+int mw_unet_avgpool2(int32_t B, int32_t H, int32_t W, int32_t C, const void* X, void* Y, void* stream);
+int mw_unet_avgpool2_bwd(int32_t B, int32_t H, int32_t W, int32_t C, const float* dY, float* dX, int32_t accumulate,
+                         void* stream);
+int mw_unet_upsample2_into(int32_t B, int32_t h, int32_t w, int32_t C, int32_t Ctot, int32_t c0, const void* X,
+                           void* Y, void* stream);
+int mw_unet_copy_channels(int64_t P, int32_t C, int32_t Ctot, int32_t c0, const void* X, void* Y, void* stream);
+int mw_unet_upsample2_bwd(int32_t B, int32_t h, int32_t w, int32_t C, int32_t Ctot, int32_t c0, const float* dY,
+                          float* dX, void* stream);
+int mw_unet_slice_grad(int64_t P, int32_t C, int32_t Ctot, int32_t c0, const float* dY, float* dX, int32_t accumulate,
+                       void* stream);
+int mw_unet_mse(int64_t n, const float* y, const float* t, float* dy, double* loss_part, int32_t nparts,
+                void* stream);
+int mw_unet_adam(int64_t n, float* w, float* m, float* v, const float* g, float lr, float b1, float b2, float eps,
+                 float bc1, float bc2, void* w16, void* stream);
+/* network input [nelz/f, nelx/f, 2] from T (nodal) and eta_e: (T at element centres,
+ * (log10 eta_e - mean)/2.5), each averaged over f x f elements; stats = {mean log10 eta,
+ * Ra / 10^mean} (device) */
+int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e, double Ra, double* stats, void* X,
+                     void* stream);
+/* network output [nelz/f, nelx/f, 3] -> Stokes initial guess (solV interleaved on the Q2
+ * lattice, solP on Q1 nodes; bilinear in the network-cell centres, fixed dofs 0); velocities in
+ * units of stats[1], dynamic pressure in units of pscale, plus the hydrostatic pressure
+ * ghyd * (Lz/2 - z) (ghyd = rho0 |g_z| in the solver's pressure units) */
+int mw_unet_to_fields(mw_box box, int32_t f, const float* Y, const double* stats, double pscale, double ghyd,
+                      const uint8_t* bc_fix_V, double* solV, double* solP, void* stream);
+/* training targets from a solution (inverse of mw_unet_to_fields at the element centres) */
+int mw_unet_targets(mw_box box, const double* solV, const double* solP, const double* stats, double pscale,
+                    double ghyd, float* Y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

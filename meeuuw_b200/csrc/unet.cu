@@ -1,0 +1,442 @@
+// Data-movement and element-wise kernels of the U-Net warm start (sm_100a).  The convolutions
+// themselves are implicit GEMMs on the tcgen05 GEMM (gemm_tc.cu) over the im2col matrices built
+// here.  Activations are NHWC; convolution K index = tap * C + c with tap = (dy+1)*3 + (dx+1),
+// zero-padded to a multiple of 64.
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace mw {
+
+typedef __nv_bfloat16 bf16;
+
+// X [B,H,W,C] (bf16) -> col [M = B*H*W, Kp] (bf16), 'same' 3x3 patches, zeros outside
+__global__ void k_im2col(int B, int H, int W, int C, int Kp, const bf16* __restrict__ X, bf16* __restrict__ col) {
+  const int64_t M = (int64_t)B * H * W;
+  const int64_t total = M * Kp;
+  const bf16 z = __float2bfloat16(0.f);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / Kp;
+    const int k = (int)(i - p * Kp);
+    bf16 v = z;
+    if (k < 9 * C) {
+      const int tap = k / C, c = k - tap * C;
+      const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
+      const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
+      if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = X[(((int64_t)b * H + yy) * W + xx) * C + c];
+    }
+    col[i] = v;
+  }
+}
+
+// transposed im2col: colT [Kp, M]
+__global__ void k_im2col_T(int B, int H, int W, int C, int Kp, const bf16* __restrict__ X, bf16* __restrict__ colT) {
+  const int64_t M = (int64_t)B * H * W;
+  const int64_t total = M * Kp;
+  const bf16 z = __float2bfloat16(0.f);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i / M);
+    const int64_t p = i - (int64_t)k * M;
+    bf16 v = z;
+    if (k < 9 * C) {
+      const int tap = k / C, c = k - tap * C;
+      const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
+      const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
+      if (yy >= 0 && yy < H && xx >= 0 && xx < W) v = X[(((int64_t)b * H + yy) * W + xx) * C + c];
+    }
+    colT[i] = v;
+  }
+}
+
+// fp32 master weights W [Cout, Kp_in] -> bf16 copy
+__global__ void k_cast_bf16(int64_t n, const float* __restrict__ a, bf16* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16(a[i]);
+}
+
+// Weights of the data-gradient convolution: Wt[ci][tap'*Cout + co] = W[co][(8-tap')*Cin + ci]
+__global__ void k_w_bwd(int Cout, int Cin, int Kp_in, int Kp_out, const float* __restrict__ W, bf16* __restrict__ Wt) {
+  const int64_t total = (int64_t)Cin * Kp_out;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int ci = (int)(i / Kp_out), k = (int)(i % Kp_out);
+    float v = 0.f;
+    if (k < 9 * Cout) {
+      const int tp = k / Cout, co = k - tp * Cout;
+      v = W[(int64_t)co * Kp_in + (8 - tp) * Cin + ci];
+    }
+    Wt[i] = __float2bfloat16(v);
+  }
+}
+
+// dZ = dA * (A > 0 or !relu): bf16 [M, C], bf16 transposed [C, M], fp32 [M, C]
+__global__ void k_relu_grad(int64_t M, int C, int relu, const float* __restrict__ dA, const bf16* __restrict__ A,
+                            bf16* __restrict__ dZ, bf16* __restrict__ dZT, float* __restrict__ dZ32) {
+  const int64_t total = M * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / C;
+    const int c = (int)(i - p * C);
+    float g = dA[i];
+    if (relu && !(__bfloat162float(A[i]) > 0.f)) g = 0.f;
+    const bf16 gb = __float2bfloat16(g);
+    dZ[i] = gb;
+    dZT[(int64_t)c * M + p] = gb;
+    dZ32[i] = g;
+  }
+}
+
+// column sums of X [M, C] (fp32): one block per column, deterministic
+__global__ void k_colsum(int64_t M, int C, const float* __restrict__ X, float* __restrict__ out) {
+  __shared__ double sh[32];
+  const int c = blockIdx.x;
+  double s = 0;
+  for (int64_t p = threadIdx.x; p < M; p += blockDim.x) s += X[p * C + c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    out[c] = (float)t;
+  }
+}
+
+// 2x2 average pooling, NHWC bf16
+__global__ void k_avgpool2(int B, int H, int W, int C, const bf16* __restrict__ X, bf16* __restrict__ Y) {
+  const int h = H / 2, w = W / 2;
+  const int64_t total = (int64_t)B * h * w * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const int64_t q = i / C;
+    const int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((int64_t)w * h));
+    const bf16* s = X + (((int64_t)b * H + 2 * y) * W + 2 * x) * C + c;
+    float v = __bfloat162float(s[0]) + __bfloat162float(s[C]) + __bfloat162float(s[(int64_t)W * C]) +
+              __bfloat162float(s[(int64_t)W * C + C]);
+    Y[i] = __float2bfloat16(0.25f * v);
+  }
+}
+
+// gradient of avg pooling: dX[b,y,x,c] (+)= dY[b,y/2,x/2,c] / 4   (fp32)
+__global__ void k_avgpool2_bwd(int B, int H, int W, int C, const float* __restrict__ dY, float* __restrict__ dX,
+                               int accumulate) {
+  const int64_t total = (int64_t)B * H * W * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const int64_t q = i / C;
+    const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((int64_t)W * H));
+    const float g = 0.25f * dY[(((int64_t)b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c];
+    dX[i] = accumulate ? dX[i] + g : g;
+  }
+}
+
+// nearest 2x upsampling of X [B,h,w,C] into channels [c0, c0+C) of Y [B,2h,2w,Ctot]
+__global__ void k_upsample2_into(int B, int h, int w, int C, int Ctot, int c0, const bf16* __restrict__ X,
+                                 bf16* __restrict__ Y) {
+  const int H = 2 * h, W = 2 * w;
+  const int64_t total = (int64_t)B * H * W * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const int64_t q = i / C;
+    const int x = (int)(q % W), y = (int)((q / W) % H), b = (int)(q / ((int64_t)W * H));
+    Y[q * Ctot + c0 + c] = X[(((int64_t)b * h + y / 2) * w + x / 2) * C + c];
+  }
+}
+
+// copy X [.., C] into channels [c0, c0+C) of Y [.., Ctot]
+__global__ void k_copy_channels(int64_t P, int C, int Ctot, int c0, const bf16* __restrict__ X, bf16* __restrict__ Y) {
+  const int64_t total = P * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / C;
+    const int c = (int)(i - p * C);
+    Y[p * Ctot + c0 + c] = X[i];
+  }
+}
+
+// gradient of the upsample into a concat: dX[b,y,x,c] = sum of the 4 fine cells' dY[.., c0+c]
+__global__ void k_upsample2_bwd(int B, int h, int w, int C, int Ctot, int c0, const float* __restrict__ dY,
+                                float* __restrict__ dX) {
+  const int W = 2 * w;
+  const int64_t total = (int64_t)B * h * w * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % C);
+    const int64_t q = i / C;
+    const int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((int64_t)w * h));
+    const int64_t r0 = ((int64_t)b * 2 * h + 2 * y) * W + 2 * x;
+    float s = dY[r0 * Ctot + c0 + c] + dY[(r0 + 1) * Ctot + c0 + c] + dY[(r0 + W) * Ctot + c0 + c] +
+              dY[(r0 + W + 1) * Ctot + c0 + c];
+    dX[i] = s;
+  }
+}
+
+// dX[.., c] (+)= dY[.., c0 + c]   (channel slice of a concat gradient)
+__global__ void k_slice_grad(int64_t P, int C, int Ctot, int c0, const float* __restrict__ dY, float* __restrict__ dX,
+                             int accumulate) {
+  const int64_t total = P * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / C;
+    const int c = (int)(i - p * C);
+    const float g = dY[p * Ctot + c0 + c];
+    dX[i] = accumulate ? dX[i] + g : g;
+  }
+}
+
+// MSE: loss = mean((y - t)^2); dy = 2 (y - t) / n ; partial sums of the loss per block
+__global__ void k_mse(int64_t n, const float* __restrict__ y, const float* __restrict__ t, float* __restrict__ dy,
+                      double* __restrict__ loss_part) {
+  __shared__ double sh[32];
+  double s = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float d = y[i] - t[i];
+    dy[i] = 2.f * d / (float)n;
+    s += (double)d * d;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t2 = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t2 += sh[w];
+    loss_part[blockIdx.x] = t2;
+  }
+}
+
+// Adam (decoupled weight decay off): fp32 master weights, moments, gradient; bf16 copy refreshed
+__global__ void k_adam(int64_t n, float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ g, float lr, float b1, float b2, float eps, float bc1, float bc2,
+                       bf16* __restrict__ w16) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    w[i] = wi;
+    if (w16) w16[i] = __float2bfloat16(wi);
+  }
+}
+
+// ---- between finite-element fields and the element-centre grid of the network ----
+// mean of log10(eta_e) -> stats[0]; velocity scale Ra / 10^mean -> stats[1]  (one block)
+__global__ void k_feature_stats(int64_t nel, const double* __restrict__ eta_e, double Ra, double* __restrict__ stats) {
+  __shared__ double sh[32];
+  double s = 0;
+  for (int64_t e = threadIdx.x; e < nel; e += blockDim.x) s += log10(eta_e[e]);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    const double m = t / (double)nel;
+    stats[0] = m;
+    stats[1] = Ra / pow(10.0, m);
+  }
+}
+
+// features [nelz/f, nelx/f, 2] bf16 on the network grid (f x f elements per cell, averaged):
+// T at the element centre nodes, (log10 eta_e - mean) / 2.5
+__global__ void k_features(mw_box b, int f, const double* __restrict__ T, const double* __restrict__ eta_e,
+                           const double* __restrict__ stats, bf16* __restrict__ X) {
+  const int gx = b.nelx / f, gz = b.nelz / f;
+  const int64_t ncell = (int64_t)gx * gz;
+  const int nnx = 2 * b.nelx + 1;
+  const double inv = 1.0 / ((double)f * f);
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
+    const int cx = (int)(c % gx), cz = (int)(c / gx);
+    double st = 0, se = 0;
+    for (int a = 0; a < f; ++a)
+      for (int d = 0; d < f; ++d) {
+        const int ex = cx * f + d, ez = cz * f + a;
+        st += T ? T[q2_node(ex, ez, 8, nnx)] : 0.0;
+        se += log10(eta_e[(int64_t)ez * b.nelx + ex]);
+      }
+    X[2 * c] = __float2bfloat16((float)(st * inv));
+    X[2 * c + 1] = __float2bfloat16((float)((se * inv - stats[0]) / 2.5));
+  }
+}
+
+// hydrostatic pressure of the reference density: ghyd * (Lz/2 - z) (zero mean over a uniform lattice)
+__device__ __forceinline__ double p_hydro(const mw_box& b, double ghyd, double z) { return ghyd * (0.5 * b.Lz - z); }
+
+// prediction [nelz/f, nelx/f, 3] (u, w in units of stats[1]; dynamic pressure in units of pscale)
+// -> solV (interleaved u, w on the Q2 lattice, bilinear between network-cell centres, fixed dofs 0)
+// and solP (Q1 nodes, bilinear dynamic pressure + hydrostatic pressure)
+__global__ void k_to_fields(mw_box b, int f, const float* __restrict__ Y, const double* __restrict__ stats,
+                            double pscale, double ghyd, const uint8_t* __restrict__ fix, double* __restrict__ solV,
+                            double* __restrict__ solP) {
+  const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
+  const int gxn = b.nelx / f, gzn = b.nelz / f;          // network grid
+  const int64_t nn = (int64_t)nnx * nnz;
+  const int64_t np = (int64_t)(b.nelx + 1) * (b.nelz + 1);
+  const double vs = stats[1];
+  auto at = [&](int cx, int cz, int ch) -> double {
+    cx = cx < 0 ? 0 : (cx >= gxn ? gxn - 1 : cx);
+    cz = cz < 0 ? 0 : (cz >= gzn ? gzn - 1 : cz);
+    return (double)Y[((int64_t)cz * gxn + cx) * 3 + ch];
+  };
+  auto bilin = [&](double gx, double gz, int ch) -> double {
+    const int x0 = (int)floor(gx), z0 = (int)floor(gz);
+    const double fx = gx - x0, fz = gz - z0;
+    return (1 - fz) * ((1 - fx) * at(x0, z0, ch) + fx * at(x0 + 1, z0, ch)) +
+           fz * ((1 - fx) * at(x0, z0 + 1, ch) + fx * at(x0 + 1, z0 + 1, ch));
+  };
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nn + np; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < nn) {
+      const int ix = (int)(i % nnx), iz = (int)(i / nnx);
+      const double gx = ix / (2.0 * f) - 0.5, gz = iz / (2.0 * f) - 0.5;   // network-cell-centre coordinates
+      for (int c = 0; c < 2; ++c) solV[2 * i + c] = fix[2 * i + c] ? 0.0 : bilin(gx, gz, c) * vs;
+    } else {
+      const int64_t n = i - nn;
+      const int px = (int)(n % (b.nelx + 1)), pz = (int)(n / (b.nelx + 1));
+      solP[n] = bilin(px / (double)f - 0.5, pz / (double)f - 0.5, 2) * pscale + p_hydro(b, ghyd, pz * b.hz);
+    }
+  }
+}
+
+// targets [nelz, nelx, 3] fp32 from a solution: (u, w at centres) / stats[1],
+// (p at the centre (mean of the 4 corners) - hydrostatic) / pscale
+__global__ void k_targets(mw_box b, const double* __restrict__ solV, const double* __restrict__ solP,
+                          const double* __restrict__ stats, double pscale, double ghyd, float* __restrict__ Y) {
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  const int nnx = 2 * b.nelx + 1;
+  const double vs = stats[1];
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
+    const int64_t c = q2_node(ex, ez, 8, nnx);
+    Y[3 * e] = (float)(solV[2 * c] / vs);
+    Y[3 * e + 1] = (float)(solV[2 * c + 1] / vs);
+    double p = 0;
+    for (int k = 0; k < 4; ++k) p += solP[q1_node(ex, ez, k, b.nelx)];
+    Y[3 * e + 2] = (float)((0.25 * p - p_hydro(b, ghyd, (ez + 0.5) * b.hz)) / pscale);
+  }
+}
+
+}  // namespace mw
+
+using namespace mw;
+
+extern "C" {
+
+#define MW_GRID(n) grid_for((n), 256), 256, 0, (cudaStream_t)stream
+
+int mw_unet_im2col(int32_t B, int32_t H, int32_t W, int32_t C, int32_t Kp, int32_t transposed, const void* X,
+                   void* col, void* stream) {
+  if (Kp < 9 * C || (Kp % 64) != 0) return MW_ERR_BAD_ARG;
+  const int64_t n = (int64_t)B * H * W * Kp;
+  if (transposed) k_im2col_T<<<MW_GRID(n)>>>(B, H, W, C, Kp, (const bf16*)X, (bf16*)col);
+  else k_im2col<<<MW_GRID(n)>>>(B, H, W, C, Kp, (const bf16*)X, (bf16*)col);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_cast_bf16(int64_t n, const float* a, void* b, void* stream) {
+  k_cast_bf16<<<MW_GRID(n)>>>(n, a, (bf16*)b);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_weights_bwd(int32_t Cout, int32_t Cin, int32_t Kp_in, int32_t Kp_out, const float* W, void* Wt,
+                        void* stream) {
+  if (Kp_out < 9 * Cout || Kp_in < 9 * Cin) return MW_ERR_BAD_ARG;
+  k_w_bwd<<<MW_GRID((int64_t)Cin * Kp_out)>>>(Cout, Cin, Kp_in, Kp_out, W, (bf16*)Wt);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_relu_grad(int64_t M, int32_t C, int32_t relu, const float* dA, const void* A, void* dZ, void* dZT,
+                      float* dZ32, void* stream) {
+  k_relu_grad<<<MW_GRID(M * C)>>>(M, C, relu, dA, (const bf16*)A, (bf16*)dZ, (bf16*)dZT, dZ32);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_colsum(int64_t M, int32_t C, const float* X, float* out, void* stream) {
+  k_colsum<<<C, 256, 0, (cudaStream_t)stream>>>(M, C, X, out);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_avgpool2(int32_t B, int32_t H, int32_t W, int32_t C, const void* X, void* Y, void* stream) {
+  k_avgpool2<<<MW_GRID((int64_t)B * (H / 2) * (W / 2) * C)>>>(B, H, W, C, (const bf16*)X, (bf16*)Y);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_avgpool2_bwd(int32_t B, int32_t H, int32_t W, int32_t C, const float* dY, float* dX, int32_t accumulate,
+                         void* stream) {
+  k_avgpool2_bwd<<<MW_GRID((int64_t)B * H * W * C)>>>(B, H, W, C, dY, dX, accumulate);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_upsample2_into(int32_t B, int32_t h, int32_t w, int32_t C, int32_t Ctot, int32_t c0, const void* X,
+                           void* Y, void* stream) {
+  k_upsample2_into<<<MW_GRID((int64_t)B * 4 * h * w * C)>>>(B, h, w, C, Ctot, c0, (const bf16*)X, (bf16*)Y);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_copy_channels(int64_t P, int32_t C, int32_t Ctot, int32_t c0, const void* X, void* Y, void* stream) {
+  k_copy_channels<<<MW_GRID(P * C)>>>(P, C, Ctot, c0, (const bf16*)X, (bf16*)Y);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_upsample2_bwd(int32_t B, int32_t h, int32_t w, int32_t C, int32_t Ctot, int32_t c0, const float* dY,
+                          float* dX, void* stream) {
+  k_upsample2_bwd<<<MW_GRID((int64_t)B * h * w * C)>>>(B, h, w, C, Ctot, c0, dY, dX);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_slice_grad(int64_t P, int32_t C, int32_t Ctot, int32_t c0, const float* dY, float* dX, int32_t accumulate,
+                       void* stream) {
+  k_slice_grad<<<MW_GRID(P * C)>>>(P, C, Ctot, c0, dY, dX, accumulate);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_mse(int64_t n, const float* y, const float* t, float* dy, double* loss_part, int32_t nparts,
+                void* stream) {
+  if (nparts < 1) return MW_ERR_BAD_ARG;
+  k_mse<<<nparts, 256, 0, (cudaStream_t)stream>>>(n, y, t, dy, loss_part);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_adam(int64_t n, float* w, float* m, float* v, const float* g, float lr, float b1, float b2, float eps,
+                 float bc1, float bc2, void* w16, void* stream) {
+  k_adam<<<MW_GRID(n)>>>(n, w, m, v, g, lr, b1, b2, eps, bc1, bc2, (bf16*)w16);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e, double Ra, double* stats, void* X,
+                     void* stream) {
+  if (f < 1 || box.nelx % f || box.nelz % f) return MW_ERR_BAD_ARG;
+  const int64_t nel = (int64_t)box.nelx * box.nelz;
+  k_feature_stats<<<1, 1024, 0, (cudaStream_t)stream>>>(nel, eta_e, Ra, stats);
+  MW_CHECK_LAUNCH();
+  k_features<<<MW_GRID(nel / ((int64_t)f * f))>>>(box, f, T, eta_e, stats, (bf16*)X);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_to_fields(mw_box box, int32_t f, const float* Y, const double* stats, double pscale, double ghyd,
+                      const uint8_t* bc_fix_V, double* solV, double* solP, void* stream) {
+  if (f < 1 || box.nelx % f || box.nelz % f) return MW_ERR_BAD_ARG;
+  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1) + (int64_t)(box.nelx + 1) * (box.nelz + 1);
+  k_to_fields<<<MW_GRID(n)>>>(box, f, Y, stats, pscale, ghyd, bc_fix_V, solV, solP);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_targets(mw_box box, const double* solV, const double* solP, const double* stats, double pscale,
+                    double ghyd, float* Y, void* stream) {
+  const int64_t nel = (int64_t)box.nelx * box.nelz;
+  k_targets<<<MW_GRID(nel)>>>(box, solV, solP, stats, pscale, ghyd, Y);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+}  // extern "C"

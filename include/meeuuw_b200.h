@@ -241,6 +241,13 @@ int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, con
 int mw_global_quantities(int64_t nq, const double* uq, const double* wq, const double* Tq, const double* rhoq,
                          const double* JxWq, double volume, double* out3, void* work, size_t work_bytes,
                          void* stream);
+/* The whole compute_global_quantities tuple (postprocessors.py:14-83): out9 = {vrms, EK, WAG,
+ * TVD, GPE (= 0), ITE, TM, Tavrg, eta_avrg}; eta_avrg is NaN when sum(eII JxW) = 0, where the
+ * reference leaves it unassigned.  All arrays (nq = nel*9 qpoint values) are required. */
+int mw_global_quantities_full(int64_t nq, const double* uq, const double* wq, const double* Tq, const double* rhoq,
+                              const double* hcapaq, const double* etaq, const double* exxq, const double* ezzq,
+                              const double* exzq, const double* gxq, const double* gzq, const double* JxWq,
+                              double volume, double* out9, void* work, size_t work_bytes, void* stream);
 
 /* Time step, meeuuw.py:2112-2139: state2 = {dt1_mem, dt2_mem} (device, updated),
  * out3 = {dt, dt1, dt2} (device). */
@@ -278,6 +285,8 @@ typedef struct {
   double sweep_reduction; /* Schur residual reduction per refinement sweep (MW_F32)                  */
   int32_t mass_iters;     /* Chebyshev-Jacobi steps per M / M_eta solve (error 2^(1-iters))          */
   int32_t use_guess;      /* 1: start from the solV/solP passed in (warm start)                      */
+  double* history;        /* optional device [4][history_len]: per Schur iteration xiV = ||alpha d||, */
+  int32_t history_len;    /* xiP = ||alpha p||, alpha, beta (the reference's array_xiV/xiP/alpha/beta) */
 } mw_solve_params;
 
 typedef struct {
@@ -365,16 +374,18 @@ int mw_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const void* A, int64_t lda,
                     mw_gemm_epilogue epi, void* work, size_t work_bytes, int32_t* err, void* stream);
 
 /* U-Net building blocks (activations NHWC BF16, gradients FP32; conv K index = tap*C + c, zero
- * padded to Kp, a multiple of 64).  transposed=1 writes the im2col matrix as [Kp, B*H*W]. */
-int mw_unet_im2col(int32_t B, int32_t H, int32_t W, int32_t C, int32_t Kp, int32_t transposed, const void* X,
-                   void* col, void* stream);
+ * padded to Kp, a multiple of 64).  transposed=1 writes the im2col matrix as [Kp, ldT] with
+ * ldT >= B*H*W and zeros in the columns past B*H*W (ldT ignored otherwise). */
+int mw_unet_im2col(int32_t B, int32_t H, int32_t W, int32_t C, int32_t Kp, int32_t transposed, int64_t ldT,
+                   const void* X, void* col, void* stream);
 int mw_unet_cast_bf16(int64_t n, const float* a, void* b, void* stream);
 /* weights of the data-gradient convolution: Wt[ci][tap*Cout+co] = W[co][(8-tap)*Cin+ci] */
 int mw_unet_weights_bwd(int32_t Cout, int32_t Cin, int32_t Kp_in, int32_t Kp_out, const float* W, void* Wt,
                         void* stream);
-/* dZ = dA * (A > 0) (relu=1) or dA: bf16 [M,C], bf16 transposed [C,M], fp32 [M,C] */
-int mw_unet_relu_grad(int64_t M, int32_t C, int32_t relu, const float* dA, const void* A, void* dZ, void* dZT,
-                      float* dZ32, void* stream);
+/* dZ = dA * (A > 0) (relu=1) or dA: bf16 [M,C], bf16 transposed [C,ldT] (ldT >= M, columns past
+ * M left untouched), fp32 [M,C] */
+int mw_unet_relu_grad(int64_t M, int32_t C, int32_t relu, int64_t ldT, const float* dA, const void* A, void* dZ,
+                      void* dZT, float* dZ32, void* stream);
 int mw_unet_colsum(int64_t M, int32_t C, const float* X, float* out, void* stream);
 int mw_unet_avgpool2(int32_t B, int32_t H, int32_t W, int32_t C, const void* X, void* Y, void* stream);
 int mw_unet_avgpool2_bwd(int32_t B, int32_t H, int32_t W, int32_t C, const float* dY, float* dX, int32_t accumulate,

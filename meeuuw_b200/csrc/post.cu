@@ -286,6 +286,61 @@ __global__ void k_global_final(const double* __restrict__ partial, int nb, doubl
   if (threadIdx.x == 0) { out[0] = sqrt(a / volume); out[1] = t / volume; out[2] = m; }
 }
 
+// The whole compute_global_quantities tuple (postprocessors.py:42-83): nine per-qpoint sums
+// {TM, EK, WAG, TVD, ITE, vrms, Tavrg, num, denom} in two deterministic levels.  GPE stays 0 as
+// in the reference (its line is commented out, :69).
+struct GlobalFullIn {
+  const double *uq, *wq, *Tq, *rhoq, *hcapaq, *etaq, *exxq, *ezzq, *exzq, *gxq, *gzq, *JxWq;
+};
+
+__global__ void k_global_full_partial(int64_t nq, GlobalFullIn in, double* __restrict__ partial) {
+  __shared__ double sh[32];
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nq; g += (int64_t)gridDim.x * blockDim.x) {
+    const double jxw = in.JxWq[g], u = in.uq[g], w = in.wq[g], rho = in.rhoq[g], T = in.Tq[g];
+    const double exx = in.exxq[g], ezz = in.ezzq[g], exz = in.exzq[g], eta = in.etaq[g];
+    const double eII = exx * exx + ezz * ezz + 2 * exz * exz;
+    acc[0] += rho * jxw;
+    acc[1] += 0.5 * rho * (u * u + w * w) * jxw;
+    acc[2] -= rho * (u * in.gxq[g] + w * in.gzq[g]) * jxw;
+    acc[3] += 2 * eta * (2 * exx * exx / 3 + 2 * ezz * ezz / 3 - 2 * exx * ezz / 3 + 2 * exz * exz) * jxw;
+    acc[4] += rho * in.hcapaq[g] * T * jxw;
+    acc[5] += (u * u + w * w) * jxw;
+    acc[6] += T * jxw;
+    acc[7] += eta * eII * jxw;
+    acc[8] += eII * jxw;
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const double v = block_sum(acc[k], sh);
+    if (threadIdx.x == 0) partial[k * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+// out9 = {vrms, EK, WAG, TVD, GPE, ITE, TM, Tavrg, eta_avrg}; eta_avrg is NaN when the strain-rate
+// sum is zero (the reference leaves it unassigned then)
+__global__ void k_global_full_final(const double* __restrict__ partial, int nb, double volume, double* __restrict__ out) {
+  __shared__ double sh[32];
+  double acc[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    double a = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) a += partial[k * nb + i];
+    acc[k] = block_sum(a, sh);
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sqrt(acc[5] / volume);
+    out[1] = acc[1];
+    out[2] = acc[2];
+    out[3] = acc[3];
+    out[4] = 0.0;
+    out[5] = acc[4];
+    out[6] = acc[0];
+    out[7] = acc[6] / volume;
+    out[8] = acc[8] > 0 ? acc[7] / acc[8] : __longlong_as_double(0x7ff8000000000000LL);
+  }
+}
+
 // Time step (meeuuw.py:2112-2139): max |v| over V nodes and the particle means of hcond,
 // hcapa, rho.  state = {dt1_mem, dt2_mem}; out = {dt, dt1, dt2}.
 __global__ void k_dt_partial(int64_t nn, const double* __restrict__ u, const double* __restrict__ w, int64_t np,
@@ -377,7 +432,7 @@ int mw_elemental_to_qpoints(int64_t nel, const double* a, const double* b, doubl
   return MW_OK;
 }
 
-size_t mw_post_workspace_bytes(void) { return (size_t)4 * RB * sizeof(double) + 64; }
+size_t mw_post_workspace_bytes(void) { return (size_t)9 * RB * sizeof(double) + 64; }
 
 int mw_pressure_offset(mw_box box, int32_t normalisation, const double* p, const double* N_P, const double* JxWq,
                        double volume, double* offset, void* work, size_t work_bytes, void* stream) {
@@ -497,6 +552,23 @@ int mw_global_quantities(int64_t nq, const double* uq, const double* wq, const d
   k_global_partial<<<RB, RT, 0, s>>>(nq, uq, wq, Tq, rhoq, JxWq, part);
   MW_CHECK_LAUNCH();
   k_global_final<<<1, RT, 0, s>>>(part, RB, volume, out3);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_global_quantities_full(int64_t nq, const double* uq, const double* wq, const double* Tq, const double* rhoq,
+                              const double* hcapaq, const double* etaq, const double* exxq, const double* ezzq,
+                              const double* exzq, const double* gxq, const double* gzq, const double* JxWq,
+                              double volume, double* out9, void* work, size_t work_bytes, void* stream) {
+  if (work_bytes < mw_post_workspace_bytes()) return MW_ERR_WORKSPACE;
+  if (!uq || !wq || !Tq || !rhoq || !hcapaq || !etaq || !exxq || !ezzq || !exzq || !gxq || !gzq || !JxWq)
+    return MW_ERR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  double* part = (double*)work;
+  GlobalFullIn in{uq, wq, Tq, rhoq, hcapaq, etaq, exxq, ezzq, exzq, gxq, gzq, JxWq};
+  k_global_full_partial<<<RB, RT, 0, s>>>(nq, in, part);
+  MW_CHECK_LAUNCH();
+  k_global_full_final<<<1, RT, 0, s>>>(part, RB, volume, out9);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }

@@ -1241,6 +1241,16 @@ static int solve_K(mw_stokes* S, int prec, const double* b, double* x, double rt
   return pcg_K<double>(S, S->H64, S->pc64, b, x, rtol, maxit, relres, s);
 }
 
+// Convergence history row k in the reference's terms (uzawa3_solver_L2.py:85-88, cd_u_eta.py):
+// xiV = ||alpha d_k||, xiP = ||alpha p_k||, alpha, beta.  hist is [4][len] (xiV, xiP, alpha, beta).
+__global__ void k_history(const double* __restrict__ sc, double* __restrict__ hist, int len, int k) {
+  const double alpha = sc[0] / sc[1];
+  hist[k] = fabs(alpha) * sqrt(sc[6]);
+  hist[len + k] = fabs(alpha) * sqrt(sc[5]);
+  hist[2 * len + k] = alpha;
+  hist[3 * len + k] = sc[2] / sc[0];
+}
+
 // Schur-complement PCG (uzawa3_solver_L2.py:21-99 / cd_u_eta.py:13-99) for the saddle system
 // with right-hand side (f, h), starting from (V, P) (V is recomputed from P).  Stops when the
 // Schur residual has dropped by `reduction` relative to its start, when the FP64 true residual
@@ -1289,6 +1299,11 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
     b2.yP = S->GTz;
     launch_apply<double, AM_APPLY>(g, b2, s);
     dot<double>(S, np, S->dP, S->GTz, sc + 1, s);
+    const bool hist = sp.history && info->outer_iters < sp.history_len;
+    if (hist) {                                               // ||d_k||^2, ||z_k||^2 before the updates
+      dot<double>(S, np, S->dP, S->dP, sc + 5, s);
+      dot<double>(S, nv, S->z, S->z, sc + 6, s);
+    }
     k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, 1.0, S->dP, P);
     k_axpy_ratio<double, double><<<grid_for(nv, 256), 256, 0, s>>>(nv, sc + 0, sc + 1, -1.0, S->z, V);
     k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, -1.0, S->GTz, S->rP);
@@ -1296,6 +1311,7 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
     mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
     remove_mean(S, np, S->wP, s);
     dot<double>(S, np, S->rP, S->wP, sc + 2, s);
+    if (hist) k_history<<<1, 1, 0, s>>>(sc, sp.history, sp.history_len, info->outer_iters);
     k_xpby_ratio<double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, sc + 2, sc + 0, S->dP);
     cudaMemcpyAsync(sc + 0, sc + 2, sizeof(double), cudaMemcpyDeviceToDevice, s);
     info->outer_iters += 1;

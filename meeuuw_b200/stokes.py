@@ -22,7 +22,7 @@ class MwSolveParams(ctypes.Structure):
     _fields_ = [("scheme", c_int32), ("precision", c_int32), ("tol", c_double), ("max_outer", c_int32),
                 ("max_inner", c_int32), ("inner_rtol", c_double), ("max_refine", c_int32),
                 ("sweep_reduction", c_double), ("mass_iters", c_int32),
-                ("use_guess", c_int32)]
+                ("use_guess", c_int32), ("history", c_void_p), ("history_len", c_int32)]
 
 
 class MwSolveInfo(ctypes.Structure):

@@ -1,7 +1,7 @@
 """Train the warm-start U-Net on snapshots of the device time stepper and report what it buys.
 
-    python -m meeuuw_b200.train_warmstart --n 128 --runs 16 --steps 160 --epochs 20 \
-        --out meeuuw_b200/weights/unet_fk128.npz
+    python -m meeuuw_b200.train_warmstart --n 128 --runs 20 --steps 110 --epochs 20 \
+        --out meeuuw_b200/weights/unet_fk128.npz      (20 runs x 100 recorded steps = 2000 snapshots)
 
 Every number printed comes from the device: the snapshots are generated by ``GPUModel`` (mixed
 precision, 1e-8 relative Stokes residual), the network trains with the library's tensor-core
@@ -22,8 +22,8 @@ from .unet import UNet, compare_guesses, generate_dataset, train
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=128)
-    ap.add_argument("--runs", type=int, default=16)
-    ap.add_argument("--steps", type=int, default=160)
+    ap.add_argument("--runs", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=110)
     ap.add_argument("--skip", type=int, default=10)
     ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--batch", type=int, default=16)

@@ -26,10 +26,10 @@ from ._lib import c_double, c_int32, c_int64, c_void_p, call, ptr, stream_ptr
 bf16, f32 = torch.bfloat16, torch.float32
 
 L.extra_protos({
-    "mw_unet_im2col": (c_int32, [c_int32] * 6 + [c_void_p] * 3),
+    "mw_unet_im2col": (c_int32, [c_int32] * 6 + [c_int64] + [c_void_p] * 3),
     "mw_unet_cast_bf16": (c_int32, [c_int64, c_void_p, c_void_p, c_void_p]),
     "mw_unet_weights_bwd": (c_int32, [c_int32] * 4 + [c_void_p] * 3),
-    "mw_unet_relu_grad": (c_int32, [c_int64, c_int32, c_int32] + [c_void_p] * 6),
+    "mw_unet_relu_grad": (c_int32, [c_int64, c_int32, c_int32, c_int64] + [c_void_p] * 6),
     "mw_unet_colsum": (c_int32, [c_int64, c_int32, c_void_p, c_void_p, c_void_p]),
     "mw_unet_avgpool2": (c_int32, [c_int32] * 4 + [c_void_p] * 3),
     "mw_unet_avgpool2_bwd": (c_int32, [c_int32] * 4 + [c_void_p, c_void_p, c_int32, c_void_p]),
@@ -78,38 +78,40 @@ class Conv:
     def forward(self, X, B, H, W, out_f32=False):
         M = B * H * W
         col = _buf(("col", M, self.kp), (M, self.kp), bf16)
-        call("mw_unet_im2col", B, H, W, self.cin, self.kp, 0, ptr(X), ptr(col), stream_ptr())
+        call("mw_unet_im2col", B, H, W, self.cin, self.kp, 0, 0, ptr(X), ptr(col), stream_ptr())
         return gemm_bf16_tn(col, self.w16, bias=self.b, relu=self.relu, out_bf16=not out_f32)
 
     def backward(self, X, A, dA, B, H, W, need_dx=True):
         """X: input [M, cin] bf16, A: output [M, cout] (bf16, post-ReLU), dA: d loss / d A (fp32)."""
         M = B * H * W
+        Mp = (M + 63) // 64 * 64      # pixel (contraction) dimension of the weight-gradient GEMM, zero padded
         dZ = _buf(("dZ", M, self.cout), (M, self.cout), bf16)
-        dZT = _buf(("dZT", M, self.cout), (self.cout, M), bf16)
+        dZT = _buf(("dZT", M, self.cout), (self.cout, Mp), bf16, zero=True)
         dZ32 = _buf(("dZ32", M, self.cout), (M, self.cout), f32)
-        call("mw_unet_relu_grad", M, self.cout, int(self.relu), ptr(dA), ptr(A), ptr(dZ), ptr(dZT), ptr(dZ32),
+        call("mw_unet_relu_grad", M, self.cout, int(self.relu), Mp, ptr(dA), ptr(A), ptr(dZ), ptr(dZT), ptr(dZ32),
              stream_ptr())
         call("mw_unet_colsum", M, self.cout, ptr(dZ32), ptr(self.gb), stream_ptr())
-        colT = _buf(("colT", M, self.kp), (self.kp, M), bf16)
-        call("mw_unet_im2col", B, H, W, self.cin, self.kp, 1, ptr(X), ptr(colT), stream_ptr())
-        splits = max(1, min(64, M // 4096))
+        colT = _buf(("colT", M, self.kp), (self.kp, Mp), bf16)
+        call("mw_unet_im2col", B, H, W, self.cin, self.kp, 1, Mp, ptr(X), ptr(colT), stream_ptr())
+        splits = max(1, min(64, Mp // 4096))
         gemm_bf16_tn(dZT, colT, out=self.gw, splits=splits)
         if not need_dx:
             return None
         call("mw_unet_weights_bwd", self.cout, self.cin, self.kp, self.kpo, ptr(self.w), ptr(self.wt16), stream_ptr())
         colZ = _buf(("colZ", M, self.kpo), (M, self.kpo), bf16)
-        call("mw_unet_im2col", B, H, W, self.cout, self.kpo, 0, ptr(dZ), ptr(colZ), stream_ptr())
+        call("mw_unet_im2col", B, H, W, self.cout, self.kpo, 0, 0, ptr(dZ), ptr(colZ), stream_ptr())
         return gemm_bf16_tn(colZ, self.wt16)
 
 
 _bufs = {}
 
 
-def _buf(key, shape, dtype):
+def _buf(key, shape, dtype, zero=False):
+    """Scratch tensor reused across calls with the same key (consumed in stream order)."""
     k = (key, dtype)
     b = _bufs.get(k)
     if b is None or tuple(b.shape) != tuple(shape):
-        b = torch.empty(shape, dtype=dtype, device="cuda")
+        b = (torch.zeros if zero else torch.empty)(shape, dtype=dtype, device="cuda")
         _bufs[k] = b
     return b
 
@@ -273,7 +275,7 @@ def features_targets(box, T, eta_e, Ra, alphaT, f=1, solV=None, solP=None, stats
     return X, Y, stats
 
 
-def generate_dataset(n=128, nruns=16, nsteps=160, skip=10, seed=0, Ra_range=(1e5, 1e6), contrast_range=(1e3, 1e5),
+def generate_dataset(n=128, nruns=20, nsteps=110, skip=10, seed=0, Ra_range=(1e4, 1e6), contrast_range=(1.0, 1e5),
                      tol=1e-8, log=None):
     """Snapshots of the time-stepping method itself: `nruns` Frank-Kamenetskii convection models
     (Ra and viscosity contrast log-uniform, random smooth initial temperature) advanced `nsteps`
@@ -299,6 +301,10 @@ def generate_dataset(n=128, nruns=16, nsteps=160, skip=10, seed=0, Ra_range=(1e5
         m.guess = rec
         for k in range(nsteps):
             m.step()
+            if m.last_solve.get("status") != "MW_OK":       # keep only converged solutions
+                if log:
+                    log(f"dataset run {run}: step {k} not converged ({m.last_solve}); run stopped")
+                break
             if k >= skip:
                 features_targets(m.box, rec.T, rec.eta, cfg.Ra, cfg.alphaT, 1, m.solV, m.solP, X=Xs[s], Y=Ys[s],
                                  rho0=cfg.rho0, s=cfg.eta_ref / m.L_ref)
@@ -307,6 +313,12 @@ def generate_dataset(n=128, nruns=16, nsteps=160, skip=10, seed=0, Ra_range=(1e5
         if log:
             log(f"dataset run {run}/{nruns}: Ra={Ra:.3g} contrast={c:.3g} last uzawa={m.last_solve}")
         del m
+    Xs, Ys = Xs[:s], Ys[:s]
+    bad = ~torch.isfinite(Ys.view(s, -1)).all(1)
+    if bool(bad.any()):
+        keep = (~bad).nonzero().view(-1)
+        Xs, Ys = Xs[keep], Ys[keep]
+        meta = [meta[i] for i in keep.tolist()]
     return Xs, Ys, meta
 
 
@@ -412,7 +424,7 @@ class LearnedGuess:
             torch.add(m.solV, self.nnV - self.prevV, out=self.candV)
             torch.add(m.solP, self.nnP - self.prevP, out=self.candP)
             res["increment"] = S.residual(self.candV, self.candP, m.rhs_f, m.rhs_h)[2]
-        best = min(res, key=res.get)
+        best = min(res, key=lambda k: res[k] if math.isfinite(res[k]) else math.inf)
         if best == "learned":
             m.solV.copy_(self.nnV)
             m.solP.copy_(self.nnP)

@@ -154,6 +154,23 @@ def compute_global_quantities(uq, wq, Tq, rhoq, JxWq, volume):
     return vrms, Tavrg, TM
 
 
+def compute_global_quantities_full(uq, wq, Tq, rhoq, hcapaq, etaq, exxq, ezzq, exzq, gxq, gzq, JxWq, volume):
+    """postprocessors.py:42-83, the whole returned tuple (vrms, EK, WAG, TVD, GPE, ITE, TM, Tavrg,
+    eta_avrg); GPE stays 0 (its accumulation is commented out at :69); eta_avrg is None when the
+    strain-rate sum is zero (the reference leaves the name unassigned)."""
+    eII = exxq ** 2 + ezzq ** 2 + 2 * exzq ** 2
+    TM = _seqsum(rhoq * JxWq)
+    EK = _seqsum(0.5 * rhoq * (uq ** 2 + wq ** 2) * JxWq)
+    WAG = -_seqsum(rhoq * (uq * gxq + wq * gzq) * JxWq)
+    TVD = _seqsum(2 * etaq * (2 * exxq ** 2 / 3 + 2 * ezzq ** 2 / 3 - 2 * exxq * ezzq / 3 + 2 * exzq ** 2) * JxWq)
+    ITE = _seqsum(rhoq * hcapaq * Tq * JxWq)
+    vrms = np.sqrt(_seqsum((uq ** 2 + wq ** 2) * JxWq) / volume)
+    Tavrg = _seqsum(Tq * JxWq) / volume
+    num, denom = _seqsum(etaq * eII * JxWq), _seqsum(eII * JxWq)
+    eta_avrg = num / denom if denom > 0 else None
+    return vrms, EK, WAG, TVD, 0, ITE, TM, Tavrg, eta_avrg
+
+
 def compute_dt(CFLnb, hx, hz, u, w, swarm_hcond, swarm_hcapa, swarm_rho, dt1_mem, dt2_mem, dt_max,
                solve_T=True):
     """meeuuw.py:2112-2139 (box): CFL and diffusion limits, 25 % growth limiter."""

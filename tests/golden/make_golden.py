@@ -211,9 +211,13 @@ def case_post(R, rng, M):
     f = lambda: rng.normal(size=(nel, 9))
     uq, wq, Tq, rhoq = f(), f(), f(), f()
     z9 = np.zeros((nel, 9))
-    gq = R.pp.compute_global_quantities(nel, 9, M["xq"], M["zq"], uq, wq, Tq, rhoq, z9 + 1, z9, z9 + 1,
-                                        f() ** 2, f(), f(), f(), f(), f(), M["Lx"] * M["Lz"], M["JxWq"], z9, z9 - 1)
-    d.update(gq_uq=uq, gq_wq=wq, gq_Tq=Tq, gq_rhoq=rhoq, out_vrms=gq[0], out_Tavrg=gq[7], out_TM=gq[6])
+    hcapaq, etaq, exxq, ezzq, exzq = f() ** 2 + 1, np.exp(f()), f(), f(), f()
+    gxq, gzq = f(), f() - 1
+    gq = R.pp.compute_global_quantities(nel, 9, M["xq"], M["zq"], uq, wq, Tq, rhoq, hcapaq, z9, etaq,
+                                        exxq, ezzq, exzq, f(), f(), f(), M["Lx"] * M["Lz"], M["JxWq"], gxq, gzq)
+    d.update(gq_uq=uq, gq_wq=wq, gq_Tq=Tq, gq_rhoq=rhoq, gq_hcapaq=hcapaq, gq_etaq=etaq, gq_exxq=exxq, gq_ezzq=ezzq,
+             gq_exzq=exzq, gq_gxq=gxq, gq_gzq=gzq, out_vrms=gq[0], out_Tavrg=gq[7], out_TM=gq[6],
+             out_gq_tuple=np.array(gq, dtype=np.float64))
     return d
 
 
@@ -276,7 +280,23 @@ def main():
     for k, v in cases.items():
         np.savez_compressed(os.path.join(HERE, f"{k}.npz"), **v)
     np.savez_compressed(os.path.join(HERE, "solvers_8.npz"), **case_solvers(R, rng, 8))
+    write_signatures()
     print("wrote", sorted(os.listdir(HERE)))
+
+
+def write_signatures():
+    """Positional parameter lists of the reference functions the drop-ins replace."""
+    import importlib
+    import inspect
+    import json
+    from meeuuw_b200.dropin import TABLE
+    sig = {}
+    for mod, names in TABLE.items():
+        m = importlib.import_module(mod)
+        for n in names:
+            sig[f"{mod}.{n}"] = list(inspect.signature(getattr(m, n)).parameters)
+    with open(os.path.join(HERE, "signatures.json"), "w") as f:
+        json.dump(sig, f, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":

@@ -156,6 +156,12 @@ def test_post(mesh):
                                                      m.JxWq, m.volume)
     assert abs(vrms - float(g["out_vrms"])) < 1e-13 * float(g["out_vrms"])
     assert abs(Tavrg - float(g["out_Tavrg"])) < 1e-12 * max(1, abs(float(g["out_Tavrg"])))
+    full = post.compute_global_quantities_full(*(g["gq_" + k] for k in ("uq", "wq", "Tq", "rhoq", "hcapaq", "etaq",
+                                                                         "exxq", "ezzq", "exzq", "gxq", "gzq")),
+                                               m.JxWq, m.volume)
+    ref = g["out_gq_tuple"]
+    for i, (a, b) in enumerate(zip(full, ref)):
+        assert abs(a - b) <= 1e-12 * max(1.0, abs(b)), (i, a, b)
 
 
 def test_solvers_match_reference():

@@ -124,8 +124,10 @@ def run_ours(args):
         barrier()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
+        torch.cuda.nvtx.range_push("timed")     # lets a profiler select exactly the timed steps
         for _ in range(K):
             model.step()
+        torch.cuda.nvtx.range_pop()
         e.record()
         barrier()
         ms = s.elapsed_time(e)

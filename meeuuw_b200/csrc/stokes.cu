@@ -894,6 +894,26 @@ struct mw_stokes {
   double* etaq64;        // fine viscosity (double copy)
   float* etaq32;
   mw_solve_info last;
+  // Launch-bound sequences (V-cycles, mass-matrix Chebyshev solves) are recorded once into CUDA
+  // graphs and replayed.  Capture needs a stream other than the legacy default stream, so the
+  // solver works on its own non-blocking stream, ordered after / before the caller's stream by
+  // events.  The graphs stay valid across viscosity updates (they read the coefficients through
+  // device pointers that never move).
+  struct GraphEntry {
+    int kind;
+    std::vector<void*> before, after;
+    cudaGraphExec_t exec;
+  };
+  std::vector<GraphEntry> graphs;
+  bool use_graphs = true;
+  cudaStream_t ws = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  ~mw_stokes() {
+    for (auto& e : graphs) cudaGraphExecDestroy(e.exec);
+    if (ev_in) cudaEventDestroy(ev_in);
+    if (ev_out) cudaEventDestroy(ev_out);
+    if (ws) cudaStreamDestroy(ws);
+  }
 };
 
 namespace mw {
@@ -1046,6 +1066,80 @@ static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool firs
   smooth(L, degree, false, s);
 }
 
+// Replays the kernels `record` issues on s from a CUDA graph cached under (kind, host state).
+// `save` returns the host-side state the sequence depends on (buffer pointers it reads and may
+// permute), `load` reinstates one.  The first call per state records the graph (the capture only
+// records, so the graph is then launched); when capture is unavailable (legacy default stream,
+// an enclosing capture) the kernels are issued directly.
+template <typename Rec, typename Save, typename Load>
+static void graph_run(mw_stokes* S, int kind, Rec record, Save save, Load load, cudaStream_t s) {
+  std::vector<void*> st = save();
+  if (S->use_graphs) {
+    for (auto& e : S->graphs) {
+      if (e.kind == kind && e.before == st) {
+        if (cudaGraphLaunch(e.exec, s) == cudaSuccess) {
+          load(e.after);
+          return;
+        }
+        cudaGetLastError();
+        record();
+        return;
+      }
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (S->graphs.size() < 256 && s != nullptr && cudaStreamIsCapturing(s, &cs) == cudaSuccess &&
+        cs == cudaStreamCaptureStatusNone && cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      record();
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t ex = nullptr;
+      const bool ok = cudaStreamEndCapture(s, &g) == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      if (ok) {
+        mw_stokes::GraphEntry e;
+        e.kind = kind;
+        e.before = st;
+        e.after = save();
+        e.exec = ex;
+        S->graphs.push_back(e);
+        if (cudaGraphLaunch(ex, s) == cudaSuccess) return;
+      }
+      cudaGetLastError();
+      load(st);        // nothing ran: issue the kernels from the original state
+    } else {
+      cudaGetLastError();
+    }
+  }
+  record();
+}
+
+template <typename R>
+static std::vector<void*> vstate(const Hierarchy<R>& H) {
+  std::vector<void*> v;
+  for (int l = 0; l < H.nlev; ++l) {
+    v.push_back(H.L[l].x);
+    v.push_back(H.L[l].t);
+  }
+  v.push_back(H.L[0].b);
+  return v;
+}
+
+template <typename R>
+static void vload(Hierarchy<R>& H, const std::vector<void*>& v) {
+  for (int l = 0; l < H.nlev; ++l) {
+    H.L[l].x = (R*)v[2 * l];
+    H.L[l].t = (R*)v[2 * l + 1];
+  }
+  H.L[0].b = (R*)v[2 * H.nlev];
+}
+
+// One V-cycle of hierarchy H (degree-`degree` Chebyshev smoothing) from a cached graph.
+template <typename R>
+static void vcycle_run(mw_stokes* S, Hierarchy<R>& H, int degree, cudaStream_t s) {
+  const int kind = (sizeof(R) == 4 ? 1 : 2) * 64 + degree;
+  graph_run(S, kind, [&]() { vcycle(H, 0, degree, s); }, [&]() { return vstate(H); },
+            [&](const std::vector<void*>& v) { vload(H, v); }, s);
+}
+
 template <typename R>
 __global__ void k_power_init(int64_t n, R* __restrict__ v) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -1141,7 +1235,7 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
   auto precond = [&](R* rin, R*& zout) {
     R* saved_b = L.b;
     L.b = rin;
-    vcycle(H, 0, S->prm.cheb_degree, s);
+    vcycle_run(S, H, S->prm.cheb_degree, s);
     L.b = saved_b;
     std::swap(zout, L.x);
   };
@@ -1174,7 +1268,17 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
 // Chebyshev-Jacobi steps on lambda(D^-1 M_w) in [0.25, 2.25] (see k_mass_cheb): error reduction
 // 2 (1/2)^iters, no dot products, no host synchronisation.  The diagonals are refreshed by
 // mw_stokes_set_viscosity.  Replaces the splu solves of uzawa3_solver_L2.py:46-47 / cd_u_eta.py:284-289.
+static void mass_solve_kernels(mw_stokes* S, const double* w, const double* b, double* x, int iters, cudaStream_t s);
+
 static int mass_solve(mw_stokes* S, const double* w, const double* b, double* x, int iters, cudaStream_t s) {
+  const int K = iters < 1 ? 1 : iters;
+  std::vector<void*> key = {(void*)w, (void*)b, (void*)x, (void*)(intptr_t)K};
+  graph_run(S, 1, [&]() { mass_solve_kernels(S, w, b, x, K, s); }, [&]() { return key; },
+            [&](const std::vector<void*>&) {}, s);
+  return K;
+}
+
+static void mass_solve_kernels(mw_stokes* S, const double* w, const double* b, double* x, int iters, cudaStream_t s) {
   const LevelGeo& g = S->fine;
   const int64_t n = (int64_t)(g.nx + 1) * (g.nz + 1);
   const double* dg = w ? S->medi : S->mdiag;
@@ -1195,7 +1299,6 @@ static int mass_solve(mw_stokes* S, const double* w, const double* b, double* x,
     double* xout = bufs[(K - 1 - k) % 2];
     k_mass_cheb<<<grid_for(n, 256), 256, 0, s>>>(g, w, b, xin, xout, S->tP2, dg, c1, c2, k == 0);
   }
-  return K;
 }
 
 static void remove_mean(mw_stokes* S, int64_t n, double* x, cudaStream_t s) {
@@ -1455,11 +1558,18 @@ int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, vo
   return MW_OK;
 }
 
+static cudaStream_t enter(mw_stokes* S, cudaStream_t caller);
+static void leave(mw_stokes* S, cudaStream_t caller, cudaStream_t s);
+
 int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,
                       int32_t* iters, double* relres, void* stream) {
   double rr = 0;
-  if (int rc = ensure_hierarchy(S, precision, (cudaStream_t)stream)) return rc;
-  int it = solve_K(S, precision, b, x, rtol, maxit, &rr, (cudaStream_t)stream);
+  cudaStream_t caller = (cudaStream_t)stream;
+  cudaStream_t s = enter(S, caller);
+  int rc = ensure_hierarchy(S, precision, s);
+  int it = rc ? 0 : solve_K(S, precision, b, x, rtol, maxit, &rr, s);
+  leave(S, caller, s);
+  if (rc) return rc;
   if (iters) *iters = it;
   if (relres) *relres = rr;
   if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
@@ -1476,9 +1586,45 @@ int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const dou
   return cudaGetLastError() == cudaSuccess ? MW_OK : MW_ERR_CUDA;
 }
 
+// The solver's own stream, ordered after everything already queued on the caller's stream; leave()
+// orders the caller's stream after the solver's work.  Falls back to the caller's stream when a
+// stream or event cannot be created.
+static cudaStream_t enter(mw_stokes* S, cudaStream_t caller) {
+  if (!S->ws) {
+    if (cudaStreamCreateWithFlags(&S->ws, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&S->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      if (S->ws) cudaStreamDestroy(S->ws);
+      S->ws = nullptr;
+      return caller;
+    }
+  }
+  cudaEventRecord(S->ev_in, caller);
+  cudaStreamWaitEvent(S->ws, S->ev_in, 0);
+  return S->ws;
+}
+
+static void leave(mw_stokes* S, cudaStream_t caller, cudaStream_t s) {
+  if (s == caller) return;
+  cudaEventRecord(S->ev_out, s);
+  cudaStreamWaitEvent(caller, S->ev_out, 0);
+}
+
+static int stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
+                        const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s);
+
 int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
                     mw_solve_info* info, void* stream) {
-  cudaStream_t s = (cudaStream_t)stream;
+  cudaStream_t caller = (cudaStream_t)stream;
+  cudaStream_t s = enter(S, caller);
+  int rc = stokes_solve(S, f, h, solV, solP, sp, info, s);
+  leave(S, caller, s);
+  return rc;
+}
+
+static int stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
+                        const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s) {
   const LevelGeo& g = S->fine;
   const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
   mw_solve_info inf;

@@ -406,15 +406,17 @@ int mw_unet_adam(int64_t n, float* w, float* m, float* v, const float* g, float 
  * Ra / 10^mean} (device) */
 int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e, double Ra, double* stats, void* X,
                      void* stream);
-/* network output [nelz/f, nelx/f, 3] -> Stokes initial guess (solV interleaved on the Q2
- * lattice, solP on Q1 nodes; bilinear in the network-cell centres, fixed dofs 0); velocities in
- * units of stats[1], dynamic pressure in units of pscale, plus the hydrostatic pressure
- * ghyd * (Lz/2 - z) (ghyd = rho0 |g_z| in the solver's pressure units) */
+/* network output [nelz/f, nelx/f, 5] -> Stokes initial guess (solV interleaved on the Q2
+ * lattice, solP on Q1 nodes; bilinear in the network-cell centres, fixed dofs 0).  Channels:
+ * u/sv, w/sv, (p - hydrostatic)/sp, log10 sv, log10 sp; velocities in units of stats[1], dynamic
+ * pressure in units of pscale, the hydrostatic pressure ghyd * (Lz/2 - z) added (ghyd = rho0 |g_z|
+ * in the solver's pressure units).  scales (device, 2 doubles) receives the predicted (sv, sp). */
 int mw_unet_to_fields(mw_box box, int32_t f, const float* Y, const double* stats, double pscale, double ghyd,
-                      const uint8_t* bc_fix_V, double* solV, double* solP, void* stream);
-/* training targets from a solution (inverse of mw_unet_to_fields at the element centres) */
+                      double* scales, const uint8_t* bc_fix_V, double* solV, double* solP, void* stream);
+/* training targets [nelz, nelx, 5] from a solution (inverse of mw_unet_to_fields at the element
+ * centres); scales (device, 2 doubles) receives the solution's (sv, sp) */
 int mw_unet_targets(mw_box box, const double* solV, const double* solP, const double* stats, double pscale,
-                    double ghyd, float* Y, void* stream);
+                    double ghyd, double* scales, float* Y, void* stream);
 
 #ifdef __cplusplus
 }

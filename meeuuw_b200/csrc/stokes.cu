@@ -32,22 +32,33 @@ struct RefTables {
   double wq[9];            // Gauss weights
 };
 __constant__ RefTables c_ref;
-// the same tables in single precision, so that FP32 kernels use them as constant-bank operands
-__constant__ float c_dr32[81], c_dt32[81], c_np32[36], c_wq32[9];
 static bool g_ref_ready = false;
 
-template <typename R> struct CT;
-template <> struct CT<double> {
-  MW_D static double dr(int i) { return c_ref.dr[i]; }
-  MW_D static double dt(int i) { return c_ref.dt[i]; }
-  MW_D static double np(int i) { return c_ref.NP[i]; }
-  MW_D static double wq(int i) { return c_ref.wq[i]; }
-};
-template <> struct CT<float> {
-  MW_D static float dr(int i) { return c_dr32[i]; }
-  MW_D static float dt(int i) { return c_dt32[i]; }
-  MW_D static float np(int i) { return c_np32[i]; }
-  MW_D static float wq(int i) { return c_wq32[i]; }
+// The same reference-element values as compile-time expressions for the operator kernels: inside
+// fully unrolled loops they fold into immediates, and the terms whose basis value vanishes at a
+// Gauss point (a third of them: the 1D Q2 functions are 0 or 1 at the middle point) disappear.
+// Gauss point q = 3 i + j sits at (r, s) = (g_i, g_j), g = (-sqrt(3/5), 0, sqrt(3/5)).
+constexpr double GQ = 0.77459666924148337704;      // sqrt(3/5)
+MW_HD constexpr double gpt(int i) { return i == 0 ? -GQ : (i == 1 ? 0.0 : GQ); }
+MW_HD constexpr double gwt(int i) { return i == 1 ? 8.0 / 9.0 : 5.0 / 9.0; }
+// 1D Q2 Lagrange functions on nodes -1, 0, 1 (a = 0, 1, 2) and their derivatives
+MW_HD constexpr double lq(int a, double x) { return a == 0 ? 0.5 * x * (x - 1.0) : (a == 1 ? 1.0 - x * x : 0.5 * x * (x + 1.0)); }
+MW_HD constexpr double dlq(int a, double x) { return a == 0 ? x - 0.5 : (a == 1 ? -2.0 * x : x + 0.5); }
+MW_HD constexpr int kdx(int k) { return (k == 0 || k == 3 || k == 7) ? 0 : ((k == 1 || k == 2 || k == 5) ? 2 : 1); }
+MW_HD constexpr int kdz(int k) { return (k == 0 || k == 1 || k == 4) ? 0 : ((k == 2 || k == 3 || k == 6) ? 2 : 1); }
+MW_HD constexpr double ref_dr(int q, int k) { return dlq(kdx(k), gpt(q / 3)) * lq(kdz(k), gpt(q % 3)); }
+MW_HD constexpr double ref_dt(int q, int k) { return lq(kdx(k), gpt(q / 3)) * dlq(kdz(k), gpt(q % 3)); }
+MW_HD constexpr double ref_np(int q, int k) {
+  return 0.25 * (k == 0 || k == 3 ? 1.0 - gpt(q / 3) : 1.0 + gpt(q / 3)) *
+         (k == 0 || k == 1 ? 1.0 - gpt(q % 3) : 1.0 + gpt(q % 3));
+}
+MW_HD constexpr double ref_wq(int q) { return gwt(q / 3) * gwt(q % 3); }
+
+template <typename R> struct CT {
+  MW_D static constexpr R dr(int q, int k) { return (R)ref_dr(q, k); }
+  MW_D static constexpr R dt(int q, int k) { return (R)ref_dt(q, k); }
+  MW_D static constexpr R np(int q, int k) { return (R)ref_np(q, k); }
+  MW_D static constexpr R wq(int q) { return (R)ref_wq(q); }
 };
 
 static void host_ref_tables(RefTables* T) {
@@ -82,15 +93,6 @@ static int ensure_ref_tables() {
   RefTables T;
   host_ref_tables(&T);
   if (cudaMemcpyToSymbol(c_ref, &T, sizeof(T)) != cudaSuccess) return MW_ERR_CUDA;
-  float f[81];
-  for (int i = 0; i < 81; ++i) f[i] = (float)T.dr[i];
-  if (cudaMemcpyToSymbol(c_dr32, f, sizeof(float) * 81) != cudaSuccess) return MW_ERR_CUDA;
-  for (int i = 0; i < 81; ++i) f[i] = (float)T.dt[i];
-  if (cudaMemcpyToSymbol(c_dt32, f, sizeof(float) * 81) != cudaSuccess) return MW_ERR_CUDA;
-  for (int i = 0; i < 36; ++i) f[i] = (float)T.NP[i];
-  if (cudaMemcpyToSymbol(c_np32, f, sizeof(float) * 36) != cudaSuccess) return MW_ERR_CUDA;
-  for (int i = 0; i < 9; ++i) f[i] = (float)T.wq[i];
-  if (cudaMemcpyToSymbol(c_wq32, f, sizeof(float) * 9) != cudaSuccess) return MW_ERR_CUDA;
   g_ref_ready = true;
   return MW_OK;
 }
@@ -149,11 +151,9 @@ MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const 
     R dxu = 0, dzw = 0, dzu = 0, dxw = 0;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const R r = CT<R>::dr(q * 9 + k), t = CT<R>::dt(q * 9 + k);
-      dxu += r * ue[2 * k];
-      dzw += t * ue[2 * k + 1];
-      dzu += t * ue[2 * k];
-      dxw += r * ue[2 * k + 1];
+      const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
+      if (r != R(0)) { dxu += r * ue[2 * k]; dxw += r * ue[2 * k + 1]; }
+      if (t != R(0)) { dzw += t * ue[2 * k + 1]; dzu += t * ue[2 * k]; }
     }
     const R exx = sx * dxu, ezz = sz * dzw, gg = sz * dzu + sx * dxw;   // gg = du/dz + dw/dx
     const R jw = jac * CT<R>::wq(q);
@@ -161,20 +161,69 @@ MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const 
     R pq = 0;
     if (use_p) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) pq += CT<R>::np(q * 4 + k) * pe[k];
+      for (int k = 0; k < 4; ++k) pq += CT<R>::np(q, k) * pe[k];
     }
     const R sp = s * jw * pq;
     const R A = (R(2) * e * exx - sp) * sx, B = (R(2) * e * ezz - sp) * sz;
     const R Cx = e * gg * sx, Cz = e * gg * sz;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-      const R r = CT<R>::dr(q * 9 + k), t = CT<R>::dt(q * 9 + k);
-      ye[2 * k] += r * A + t * Cz;
-      ye[2 * k + 1] += t * B + r * Cx;
+      const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
+      if (r != R(0)) { ye[2 * k] += r * A; ye[2 * k + 1] += r * Cx; }
+      if (t != R(0)) { ye[2 * k] += t * Cz; ye[2 * k + 1] += t * B; }
     }
     const R dv = -s * jw * (exx + ezz);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) ype[k] += CT<R>::np(q * 4 + k) * dv;
+    for (int k = 0; k < 4; ++k) ype[k] += CT<R>::np(q, k) * dv;
+  }
+}
+
+// FP32 variant on the packed two-lane FMA of sm_100 (__ffma2_rn): a node's (u, w) pair is one
+// operand, so each nonzero basis value costs one instruction for both velocity components, in the
+// gradients and in the B^T scatter.
+template <>
+MW_D void element_apply<float>(float sx, float sz, float jac, float s, const float* ue, const float* pe,
+                               const float* eq, float* ye, float* ype, bool use_p) {
+  const float2* u2 = reinterpret_cast<const float2*>(ue);
+  float2 y2[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) y2[k] = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) ype[k] = 0.f;
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    float2 gx = make_float2(0.f, 0.f), gz = make_float2(0.f, 0.f);   // (du/dr, dw/dr), (du/dt, dw/dt)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float r = CT<float>::dr(q, k), t = CT<float>::dt(q, k);
+      if (r != 0.f) gx = __ffma2_rn(make_float2(r, r), u2[k], gx);
+      if (t != 0.f) gz = __ffma2_rn(make_float2(t, t), u2[k], gz);
+    }
+    const float exx = sx * gx.x, ezz = sz * gz.y, gg = sz * gz.x + sx * gx.y;
+    const float jw = jac * CT<float>::wq(q);
+    const float e = eq[q] * jw;
+    float pq = 0.f;
+    if (use_p) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pq += CT<float>::np(q, k) * pe[k];
+    }
+    const float sp = s * jw * pq;
+    const float2 ar = make_float2((2.f * e * exx - sp) * sx, e * gg * sx);   // coefficients of dN/dr
+    const float2 at = make_float2(e * gg * sz, (2.f * e * ezz - sp) * sz);   // coefficients of dN/dt
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const float r = CT<float>::dr(q, k), t = CT<float>::dt(q, k);
+      if (r != 0.f) y2[k] = __ffma2_rn(make_float2(r, r), ar, y2[k]);
+      if (t != 0.f) y2[k] = __ffma2_rn(make_float2(t, t), at, y2[k]);
+    }
+    const float dv = -s * jw * (exx + ezz);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ype[k] += CT<float>::np(q, k) * dv;
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    ye[2 * k] = y2[k].x;
+    ye[2 * k + 1] = y2[k].y;
   }
 }
 
@@ -185,8 +234,12 @@ MW_D int q2_local_idx(int dx, int dz) {
   return dx == 0 ? 3 : (dx == 1 ? 6 : 2);
 }
 
+#ifndef MW_APPLY_MINB
+#define MW_APPLY_MINB 5      // resident FP32 apply CTAs per SM the register budget is sized for
+#endif
+
 template <typename R, int MODE>
-__global__ void __launch_bounds__(APPLY_THREADS)
+__global__ void __launch_bounds__(APPLY_THREADS, sizeof(R) == 4 ? MW_APPLY_MINB : 1)
 k_apply(LevelGeo g, ApplyArgs<R> a) {
   __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ R sp[PZ * PX];
@@ -226,7 +279,8 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     int lex = tid % EX, lez = tid / EX;
     int ex = ex0 - 1 + lex, ez = ez0 - 1 + lez;
     if (ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz) {
-      R ue[18], pe[4], ye[18], ype[4];
+      __align__(16) R ue[18];
+      R pe[4], ye[18], ype[4];
       const int bx = 2 * lex, bz = 2 * lez;          // staged lattice coords of local node 0
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
@@ -1642,6 +1696,11 @@ static int stokes_solve(mw_stokes* S, const double* f, const double* h, double* 
   cudaMemcpyAsync(bb, S->sc + 52, (h ? 2 : 1) * sizeof(double), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   const double bnorm = std::sqrt(bb[0] + bb[1]);
+  if (!std::isfinite(bnorm)) {
+    inf.rel_residual = inf.initial_rel_residual = bnorm;
+    if (info) *info = inf;
+    return MW_ERR_NOT_CONVERGED;
+  }
   if (!(bnorm > 0)) { if (info) *info = inf; return MW_OK; }
   inf.initial_rel_residual = true_residual(S, solV, solP, f, h, bnorm, s);
   int rc = MW_OK;

@@ -29,16 +29,18 @@ __global__ void k_im2col(int B, int H, int W, int C, int Kp, const bf16* __restr
   }
 }
 
-// transposed im2col: colT [Kp, M]
-__global__ void k_im2col_T(int B, int H, int W, int C, int Kp, const bf16* __restrict__ X, bf16* __restrict__ colT) {
+// transposed im2col: colT [Kp, ldT] (ldT >= M; columns p >= M are zero so the pixel dimension can
+// be padded to the GEMM's K granularity)
+__global__ void k_im2col_T(int B, int H, int W, int C, int Kp, int64_t ldT, const bf16* __restrict__ X,
+                           bf16* __restrict__ colT) {
   const int64_t M = (int64_t)B * H * W;
-  const int64_t total = M * Kp;
+  const int64_t total = ldT * Kp;
   const bf16 z = __float2bfloat16(0.f);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(i / M);
-    const int64_t p = i - (int64_t)k * M;
+    const int k = (int)(i / ldT);
+    const int64_t p = i - (int64_t)k * ldT;
     bf16 v = z;
-    if (k < 9 * C) {
+    if (k < 9 * C && p < M) {
       const int tap = k / C, c = k - tap * C;
       const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((int64_t)W * H));
       const int yy = y + tap / 3 - 1, xx = x + tap % 3 - 1;
@@ -68,9 +70,10 @@ __global__ void k_w_bwd(int Cout, int Cin, int Kp_in, int Kp_out, const float* _
   }
 }
 
-// dZ = dA * (A > 0 or !relu): bf16 [M, C], bf16 transposed [C, M], fp32 [M, C]
-__global__ void k_relu_grad(int64_t M, int C, int relu, const float* __restrict__ dA, const bf16* __restrict__ A,
-                            bf16* __restrict__ dZ, bf16* __restrict__ dZT, float* __restrict__ dZ32) {
+// dZ = dA * (A > 0 or !relu): bf16 [M, C], bf16 transposed [C, ldT] (columns >= M untouched), fp32 [M, C]
+__global__ void k_relu_grad(int64_t M, int C, int relu, int64_t ldT, const float* __restrict__ dA,
+                            const bf16* __restrict__ A, bf16* __restrict__ dZ, bf16* __restrict__ dZT,
+                            float* __restrict__ dZ32) {
   const int64_t total = M * C;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = i / C;
@@ -79,7 +82,7 @@ __global__ void k_relu_grad(int64_t M, int C, int relu, const float* __restrict_
     if (relu && !(__bfloat162float(A[i]) > 0.f)) g = 0.f;
     const bf16 gb = __float2bfloat16(g);
     dZ[i] = gb;
-    dZT[(int64_t)c * M + p] = gb;
+    dZT[(int64_t)c * ldT + p] = gb;
     dZ32[i] = g;
   }
 }
@@ -258,21 +261,105 @@ __global__ void k_features(mw_box b, int f, const double* __restrict__ T, const 
 // hydrostatic pressure of the reference density: ghyd * (Lz/2 - z) (zero mean over a uniform lattice)
 __device__ __forceinline__ double p_hydro(const mw_box& b, double ghyd, double z) { return ghyd * (0.5 * b.Lz - z); }
 
-// prediction [nelz/f, nelx/f, 3] (u, w in units of stats[1]; dynamic pressure in units of pscale)
-// -> solV (interleaved u, w on the Q2 lattice, bilinear between network-cell centres, fixed dofs 0)
-// and solP (Q1 nodes, bilinear dynamic pressure + hydrostatic pressure)
+// Output channels of the network (NC = 5): 0, 1 = u, w / sv; 2 = (p - hydrostatic) / sp; 3, 4 =
+// log10 sv, log10 sp, constant maps whose mean over the grid is the prediction of the two scales.
+// sv, sp are the RMS of the velocity (units stats[1]) and of the dynamic pressure (units pscale)
+// over the element centres, so every channel the loss sees is O(1) whatever Ra and the contrast.
+constexpr int NC = 5;
+
+// element-centre values of a solution in network units before normalisation
+__device__ __forceinline__ void centre_values(const mw_box& b, const double* solV, const double* solP, double vs,
+                                              double pscale, double ghyd, int64_t e, double* u, double* w, double* p) {
+  const int nnx = 2 * b.nelx + 1;
+  const int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
+  const int64_t c = q2_node(ex, ez, 8, nnx);
+  *u = solV[2 * c] / vs;
+  *w = solV[2 * c + 1] / vs;
+  double pp = 0;
+  for (int k = 0; k < 4; ++k) pp += solP[q1_node(ex, ez, k, b.nelx)];
+  *p = (0.25 * pp - p_hydro(b, ghyd, (ez + 0.5) * b.hz)) / pscale;
+}
+
+// scales[0] = sv = sqrt(mean (u^2 + w^2) / 2), scales[1] = sp = sqrt(mean p^2) (one block)
+__global__ void k_target_scales(mw_box b, const double* __restrict__ solV, const double* __restrict__ solP,
+                                const double* __restrict__ stats, double pscale, double ghyd,
+                                double* __restrict__ scales) {
+  __shared__ double sh[32];
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  double a = 0, c = 0;
+  for (int64_t e = threadIdx.x; e < nel; e += blockDim.x) {
+    double u, w, p;
+    centre_values(b, solV, solP, stats[1], pscale, ghyd, e, &u, &w, &p);
+    a += 0.5 * (u * u + w * w);
+    c += p * p;
+  }
+  for (int o = 16; o > 0; o >>= 1) { a += __shfl_down_sync(0xffffffffu, a, o); c += __shfl_down_sync(0xffffffffu, c, o); }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) sh[wid] = a;
+  __syncthreads();
+  double ta = 0;
+  if (threadIdx.x == 0) for (int i = 0; i < nw; ++i) ta += sh[i];
+  __syncthreads();
+  if (lane == 0) sh[wid] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tc = 0;
+    for (int i = 0; i < nw; ++i) tc += sh[i];
+    scales[0] = fmax(sqrt(ta / (double)nel), 1e-300);
+    scales[1] = fmax(sqrt(tc / (double)nel), 1e-300);
+  }
+}
+
+// training targets [nelz, nelx, NC] fp32 from a solution and its scales
+__global__ void k_targets(mw_box b, const double* __restrict__ solV, const double* __restrict__ solP,
+                          const double* __restrict__ stats, double pscale, double ghyd,
+                          const double* __restrict__ scales, float* __restrict__ Y) {
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  const double sv = scales[0], spp = scales[1];
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    double u, w, p;
+    centre_values(b, solV, solP, stats[1], pscale, ghyd, e, &u, &w, &p);
+    float* y = Y + NC * e;
+    y[0] = (float)(u / sv);
+    y[1] = (float)(w / sv);
+    y[2] = (float)(p / spp);
+    y[3] = (float)log10(sv);
+    y[4] = (float)log10(spp);
+  }
+}
+
+// predicted scales from channels 3, 4: scales = 10^mean over the network grid (one block)
+__global__ void k_pred_scales(int64_t ncell, const float* __restrict__ Y, double* __restrict__ scales) {
+  __shared__ double sh[64];
+  double a = 0, c = 0;
+  for (int64_t i = threadIdx.x; i < ncell; i += blockDim.x) { a += Y[NC * i + 3]; c += Y[NC * i + 4]; }
+  for (int o = 16; o > 0; o >>= 1) { a += __shfl_down_sync(0xffffffffu, a, o); c += __shfl_down_sync(0xffffffffu, c, o); }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) { sh[wid] = a; sh[32 + wid] = c; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double ta = 0, tc = 0;
+    for (int i = 0; i < nw; ++i) { ta += sh[i]; tc += sh[32 + i]; }
+    scales[0] = pow(10.0, ta / (double)ncell);
+    scales[1] = pow(10.0, tc / (double)ncell);
+  }
+}
+
+// prediction [nelz/f, nelx/f, NC] -> Stokes initial guess: solV (interleaved u, w on the Q2
+// lattice, bilinear between network-cell centres, fixed dofs 0) and solP (Q1 nodes, bilinear
+// dynamic pressure + hydrostatic pressure); scales = (sv, sp)
 __global__ void k_to_fields(mw_box b, int f, const float* __restrict__ Y, const double* __restrict__ stats,
-                            double pscale, double ghyd, const uint8_t* __restrict__ fix, double* __restrict__ solV,
-                            double* __restrict__ solP) {
+                            double pscale, double ghyd, const double* __restrict__ scales,
+                            const uint8_t* __restrict__ fix, double* __restrict__ solV, double* __restrict__ solP) {
   const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
   const int gxn = b.nelx / f, gzn = b.nelz / f;          // network grid
   const int64_t nn = (int64_t)nnx * nnz;
   const int64_t np = (int64_t)(b.nelx + 1) * (b.nelz + 1);
-  const double vs = stats[1];
+  const double vs = stats[1] * scales[0], ps = pscale * scales[1];
   auto at = [&](int cx, int cz, int ch) -> double {
     cx = cx < 0 ? 0 : (cx >= gxn ? gxn - 1 : cx);
     cz = cz < 0 ? 0 : (cz >= gzn ? gzn - 1 : cz);
-    return (double)Y[((int64_t)cz * gxn + cx) * 3 + ch];
+    return (double)Y[((int64_t)cz * gxn + cx) * NC + ch];
   };
   auto bilin = [&](double gx, double gz, int ch) -> double {
     const int x0 = (int)floor(gx), z0 = (int)floor(gz);
@@ -288,26 +375,8 @@ __global__ void k_to_fields(mw_box b, int f, const float* __restrict__ Y, const 
     } else {
       const int64_t n = i - nn;
       const int px = (int)(n % (b.nelx + 1)), pz = (int)(n / (b.nelx + 1));
-      solP[n] = bilin(px / (double)f - 0.5, pz / (double)f - 0.5, 2) * pscale + p_hydro(b, ghyd, pz * b.hz);
+      solP[n] = bilin(px / (double)f - 0.5, pz / (double)f - 0.5, 2) * ps + p_hydro(b, ghyd, pz * b.hz);
     }
-  }
-}
-
-// targets [nelz, nelx, 3] fp32 from a solution: (u, w at centres) / stats[1],
-// (p at the centre (mean of the 4 corners) - hydrostatic) / pscale
-__global__ void k_targets(mw_box b, const double* __restrict__ solV, const double* __restrict__ solP,
-                          const double* __restrict__ stats, double pscale, double ghyd, float* __restrict__ Y) {
-  const int64_t nel = (int64_t)b.nelx * b.nelz;
-  const int nnx = 2 * b.nelx + 1;
-  const double vs = stats[1];
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
-    const int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
-    const int64_t c = q2_node(ex, ez, 8, nnx);
-    Y[3 * e] = (float)(solV[2 * c] / vs);
-    Y[3 * e + 1] = (float)(solV[2 * c + 1] / vs);
-    double p = 0;
-    for (int k = 0; k < 4; ++k) p += solP[q1_node(ex, ez, k, b.nelx)];
-    Y[3 * e + 2] = (float)((0.25 * p - p_hydro(b, ghyd, (ez + 0.5) * b.hz)) / pscale);
   }
 }
 
@@ -319,12 +388,16 @@ extern "C" {
 
 #define MW_GRID(n) grid_for((n), 256), 256, 0, (cudaStream_t)stream
 
-int mw_unet_im2col(int32_t B, int32_t H, int32_t W, int32_t C, int32_t Kp, int32_t transposed, const void* X,
-                   void* col, void* stream) {
+int mw_unet_im2col(int32_t B, int32_t H, int32_t W, int32_t C, int32_t Kp, int32_t transposed, int64_t ldT,
+                   const void* X, void* col, void* stream) {
   if (Kp < 9 * C || (Kp % 64) != 0) return MW_ERR_BAD_ARG;
-  const int64_t n = (int64_t)B * H * W * Kp;
-  if (transposed) k_im2col_T<<<MW_GRID(n)>>>(B, H, W, C, Kp, (const bf16*)X, (bf16*)col);
-  else k_im2col<<<MW_GRID(n)>>>(B, H, W, C, Kp, (const bf16*)X, (bf16*)col);
+  const int64_t M = (int64_t)B * H * W;
+  if (transposed) {
+    if (ldT < M) return MW_ERR_BAD_ARG;
+    k_im2col_T<<<MW_GRID(ldT * Kp)>>>(B, H, W, C, Kp, ldT, (const bf16*)X, (bf16*)col);
+  } else {
+    k_im2col<<<MW_GRID(M * Kp)>>>(B, H, W, C, Kp, (const bf16*)X, (bf16*)col);
+  }
   MW_CHECK_LAUNCH();
   return MW_OK;
 }
@@ -343,9 +416,10 @@ int mw_unet_weights_bwd(int32_t Cout, int32_t Cin, int32_t Kp_in, int32_t Kp_out
   return MW_OK;
 }
 
-int mw_unet_relu_grad(int64_t M, int32_t C, int32_t relu, const float* dA, const void* A, void* dZ, void* dZT,
-                      float* dZ32, void* stream) {
-  k_relu_grad<<<MW_GRID(M * C)>>>(M, C, relu, dA, (const bf16*)A, (bf16*)dZ, (bf16*)dZT, dZ32);
+int mw_unet_relu_grad(int64_t M, int32_t C, int32_t relu, int64_t ldT, const float* dA, const void* A, void* dZ,
+                      void* dZT, float* dZ32, void* stream) {
+  if (ldT < M) return MW_ERR_BAD_ARG;
+  k_relu_grad<<<MW_GRID(M * C)>>>(M, C, relu, ldT, dA, (const bf16*)A, (bf16*)dZ, (bf16*)dZT, dZ32);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }
@@ -423,18 +497,24 @@ int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e
 }
 
 int mw_unet_to_fields(mw_box box, int32_t f, const float* Y, const double* stats, double pscale, double ghyd,
-                      const uint8_t* bc_fix_V, double* solV, double* solP, void* stream) {
-  if (f < 1 || box.nelx % f || box.nelz % f) return MW_ERR_BAD_ARG;
+                      double* scales, const uint8_t* bc_fix_V, double* solV, double* solP, void* stream) {
+  if (f < 1 || box.nelx % f || box.nelz % f || !scales) return MW_ERR_BAD_ARG;
+  const int64_t ncell = (int64_t)(box.nelx / f) * (box.nelz / f);
+  k_pred_scales<<<1, 1024, 0, (cudaStream_t)stream>>>(ncell, Y, scales);
+  MW_CHECK_LAUNCH();
   const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1) + (int64_t)(box.nelx + 1) * (box.nelz + 1);
-  k_to_fields<<<MW_GRID(n)>>>(box, f, Y, stats, pscale, ghyd, bc_fix_V, solV, solP);
+  k_to_fields<<<MW_GRID(n)>>>(box, f, Y, stats, pscale, ghyd, scales, bc_fix_V, solV, solP);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }
 
 int mw_unet_targets(mw_box box, const double* solV, const double* solP, const double* stats, double pscale,
-                    double ghyd, float* Y, void* stream) {
+                    double ghyd, double* scales, float* Y, void* stream) {
+  if (!scales) return MW_ERR_BAD_ARG;
   const int64_t nel = (int64_t)box.nelx * box.nelz;
-  k_targets<<<MW_GRID(nel)>>>(box, solV, solP, stats, pscale, ghyd, Y);
+  k_target_scales<<<1, 1024, 0, (cudaStream_t)stream>>>(box, solV, solP, stats, pscale, ghyd, scales);
+  MW_CHECK_LAUNCH();
+  k_targets<<<MW_GRID(nel)>>>(box, solV, solP, stats, pscale, ghyd, scales, Y);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }

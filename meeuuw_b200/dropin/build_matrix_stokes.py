@@ -18,14 +18,17 @@ _geometry_checked = {}
 
 
 def _uniform_spacing(jcbi00q, jcbi01q, jcbi10q, jcbi11q):
-    """hx, hz of an axis-aligned uniform mesh (jcbi = diag(2/hx, 2/hz) everywhere), else raise."""
+    """hx, hz of an axis-aligned uniform mesh (jcbi = diag(2/hx, 2/hz) everywhere, to 1e-10
+    relative), else raise."""
     key = tuple(int(t.data_ptr()) for t in (jcbi00q, jcbi01q, jcbi10q, jcbi11q))
     hit = _geometry_checked.get(key)
     if hit is not None:
         return hit
-    a, b = float(jcbi00q.reshape(-1)[0].item()), float(jcbi11q.reshape(-1)[0].item())
-    ok = bool((jcbi00q == a).all().item()) and bool((jcbi11q == b).all().item()) and \
-        not bool(jcbi01q.any().item()) and not bool(jcbi10q.any().item())
+    # the reference computes the Jacobian numerically: off-diagonal terms carry rounding noise
+    a, b = float(jcbi00q.mean().item()), float(jcbi11q.mean().item())
+    tol = 1e-10 * max(abs(a), abs(b))
+    ok = float((jcbi00q - a).abs().max().item()) <= tol and float((jcbi11q - b).abs().max().item()) <= tol and \
+        float(jcbi01q.abs().max().item()) <= tol and float(jcbi10q.abs().max().item()) <= tol
     if not ok:
         raise NotImplementedError("the device path covers uniform axis-aligned box meshes")
     hit = (2.0 / a, 2.0 / b)

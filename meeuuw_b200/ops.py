@@ -32,9 +32,12 @@ _ws = {}
 
 
 def workspace(tag="default"):
-    if tag not in _ws:
-        _ws[tag] = Workspace()
-    return _ws[tag]
+    """Scratch for `tag` on the current stream: models advanced concurrently on different streams
+    (ensembles) never share scratch, and reuse on one stream is ordered by that stream."""
+    key = (tag, torch.cuda.current_stream().cuda_stream if torch.cuda.is_available() else 0)
+    if key not in _ws:
+        _ws[key] = Workspace()
+    return _ws[key]
 
 
 def _empty(n, dtype=f64, like=None):

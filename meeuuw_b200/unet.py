@@ -4,14 +4,15 @@ Every convolution is an implicit GEMM on this library's tcgen05 BF16 kernel (FP3
 forward  A = conv(X):   out[M, Cout]  = im2col(X)[M, Kp]    . W[Cout, Kp]^T
 data grad dX:           dX[M, Cin]    = im2col(dZ)[M, Kp']  . Wflip[Cin, Kp']^T
 weight grad dW:         dW[Cout, Kp]  = dZ^T[Cout, M]       . im2col(X)^T[Kp, M]^T   (split-K)
-Activations are NHWC BF16, gradients FP32, master weights FP32 with Adam.  torch only allocates
-the buffers; every operation is one of the library's kernels.
+Activations are NHWC BF16, gradients FP32, master weights FP32 with Adam.  The network's
+arithmetic is the library's kernels; torch allocates buffers and gathers training batches.
 
-The network is trained on Stokes solutions that the device solver itself produces (random
-temperature fields, Frank-Kamenetskii viscosity, Ra and contrast log-uniform), in the units of
-``mw_unet_features`` / ``mw_unet_targets``: velocity / (Ra / geometric-mean viscosity) and
-pressure / (Ra / alpha).  At run time ``WarmStart`` proposes a guess, and the caller keeps it only
-if its FP64 Stokes residual beats the fallback guess (previous step or zero).
+The network is trained on snapshots of the device time stepper (Frank-Kamenetskii convection, Ra
+and contrast log-uniform, random smooth initial temperatures), in the units of
+``mw_unet_features`` / ``mw_unet_targets``: velocity / (Ra / geometric-mean viscosity) and the
+dynamic pressure / Ra, each normalised by its RMS over the grid, plus the two log10 RMS scales as
+extra output channels.  At run time ``LearnedGuess`` proposes guesses and the solver starts from
+whichever has the smallest FP64 Stokes residual, the previous step's solution included.
 """
 import ctypes
 import math
@@ -24,6 +25,9 @@ from .ops import gemm_bf16_tn, workspace
 from ._lib import c_double, c_int32, c_int64, c_void_p, call, ptr, stream_ptr
 
 bf16, f32 = torch.bfloat16, torch.float32
+# output channels: u / sv, w / sv, dynamic p / sp, log10 sv, log10 sp (sv, sp: RMS scales of the
+# velocity and of the dynamic pressure, so every channel is O(1) for any Ra and viscosity contrast)
+NOUT = 5
 
 L.extra_protos({
     "mw_unet_im2col": (c_int32, [c_int32] * 6 + [c_int64] + [c_void_p] * 3),
@@ -42,8 +46,9 @@ L.extra_protos({
                      [c_void_p, c_void_p]),
     "mw_unet_features": (c_int32, [L.MwBox, c_int32, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
     "mw_unet_to_fields": (c_int32, [L.MwBox, c_int32, c_void_p, c_void_p, c_double, c_double, c_void_p, c_void_p,
-                                    c_void_p, c_void_p]),
-    "mw_unet_targets": (c_int32, [L.MwBox, c_void_p, c_void_p, c_void_p, c_double, c_double, c_void_p, c_void_p]),
+                                    c_void_p, c_void_p, c_void_p]),
+    "mw_unet_targets": (c_int32, [L.MwBox, c_void_p, c_void_p, c_void_p, c_double, c_double, c_void_p, c_void_p,
+                                  c_void_p]),
 })
 
 
@@ -118,9 +123,9 @@ def _buf(key, shape, dtype, zero=False):
 
 class UNet:
     """Encoder 2-32-64-128-256 (two convs per level, 2x2 average pooling), decoder with nearest
-    upsampling and skip concatenation, 3x3 head to (u, w, p)."""
+    upsampling and skip concatenation, 3x3 head to the NOUT output channels."""
 
-    def __init__(self, base=32, levels=4, cin=2, cout=3, seed=0):
+    def __init__(self, base=32, levels=4, cin=2, cout=NOUT, seed=0):
         gen = torch.Generator().manual_seed(seed)
         ch = [base * 2 ** i for i in range(levels)]
         self.ch = ch
@@ -142,7 +147,7 @@ class UNet:
 
     # ---------------------------------------------------------------- forward
     def forward(self, X, B, H, W):
-        """X: [B, H, W, 2] bf16 -> [B*H*W, 3] fp32.  Keeps the activations for backward."""
+        """X: [B, H, W, 2] bf16 -> [B*H*W, NOUT] fp32.  Keeps the activations for backward."""
         st = {"B": B, "H": H, "W": W, "x": X, "enc": [], "dec": []}
         h, w, x = H, W, X
         for lvl, (c1, c2) in enumerate(self.enc):
@@ -262,16 +267,18 @@ def pressure_scales(Ra, alphaT, rho0=1.0, s=1.0):
 
 
 def features_targets(box, T, eta_e, Ra, alphaT, f=1, solV=None, solP=None, stats=None, X=None, Y=None, rho0=1.0,
-                     s=1.0):
+                     s=1.0, scales=None):
     """Network input (and, with a solution, its target) for one model state (all on the device)."""
     gx, gz = box.nelx // f, box.nelz // f
     stats = torch.empty(2, dtype=torch.float64, device="cuda") if stats is None else stats
     X = torch.empty(gz, gx, 2, dtype=bf16, device="cuda") if X is None else X
     call("mw_unet_features", box, f, ptr(T), ptr(eta_e), float(Ra), ptr(stats), ptr(X), stream_ptr())
     if solV is not None:
-        Y = torch.empty(box.nelz, box.nelx, 3, dtype=f32, device="cuda") if Y is None else Y
+        Y = torch.empty(box.nelz, box.nelx, NOUT, dtype=f32, device="cuda") if Y is None else Y
+        scales = torch.empty(2, dtype=torch.float64, device="cuda") if scales is None else scales
         pscale, ghyd = pressure_scales(Ra, alphaT, rho0, s)
-        call("mw_unet_targets", box, ptr(solV), ptr(solP), ptr(stats), pscale, ghyd, ptr(Y), stream_ptr())
+        call("mw_unet_targets", box, ptr(solV), ptr(solP), ptr(stats), pscale, ghyd, ptr(scales), ptr(Y),
+             stream_ptr())
     return X, Y, stats
 
 
@@ -280,14 +287,14 @@ def generate_dataset(n=128, nruns=20, nsteps=110, skip=10, seed=0, Ra_range=(1e4
     """Snapshots of the time-stepping method itself: `nruns` Frank-Kamenetskii convection models
     (Ra and viscosity contrast log-uniform, random smooth initial temperature) advanced `nsteps`
     steps each on the device; every step after `skip` contributes (features of the state the Stokes
-    solve saw, targets of its solution).  Returns (X [S, n, n, 2] bf16, Y [S, n, n, 3] fp32, meta)."""
+    solve saw, targets of its solution).  Returns (X [S, n, n, 2] bf16, Y [S, n, n, NOUT] fp32, meta)."""
     from dataclasses import replace
     from . import configs
     from .timestep import GPUModel
     rng = np.random.default_rng(seed)
     S = nruns * (nsteps - skip)
     Xs = torch.empty(S, n, n, 2, dtype=bf16, device="cuda")
-    Ys = torch.empty(S, n, n, 3, dtype=f32, device="cuda")
+    Ys = torch.empty(S, n, n, NOUT, dtype=f32, device="cuda")
     meta = []
     s = 0
     for run in range(nruns):
@@ -301,9 +308,10 @@ def generate_dataset(n=128, nruns=20, nsteps=110, skip=10, seed=0, Ra_range=(1e4
         m.guess = rec
         for k in range(nsteps):
             m.step()
-            if m.last_solve.get("status") != "MW_OK":       # keep only converged solutions
+            err = int(m.err.item())
+            if m.last_solve.get("status") != "MW_OK" or err:    # keep only converged, valid states
                 if log:
-                    log(f"dataset run {run}: step {k} not converged ({m.last_solve}); run stopped")
+                    log(f"dataset run {run}: step {k} stopped (device flags {err}, solve {m.last_solve})")
                 break
             if k >= skip:
                 features_targets(m.box, rec.T, rec.eta, cfg.Ra, cfg.alphaT, 1, m.solV, m.solP, X=Xs[s], Y=Ys[s],
@@ -341,7 +349,7 @@ def train(net, Xs, Ys, epochs=20, batch=16, lr=1e-3, seed=0, log=None):
     rng = np.random.default_rng(seed)
     losses = []
     Xb = torch.empty(batch, H, W, 2, dtype=bf16, device="cuda")
-    Yb = torch.empty(batch * H * W, 3, dtype=f32, device="cuda")
+    Yb = torch.empty(batch * H * W, NOUT, dtype=f32, device="cuda")
     for ep in range(epochs):
         perm = rng.permutation(n)
         tot = torch.zeros(1, dtype=torch.float64, device="cuda")
@@ -349,7 +357,7 @@ def train(net, Xs, Ys, epochs=20, batch=16, lr=1e-3, seed=0, log=None):
         for i in range(0, n - batch + 1, batch):
             idx = torch.as_tensor(perm[i:i + batch], device="cuda")
             torch.index_select(Xs, 0, idx, out=Xb)
-            torch.index_select(Ys, 0, idx, out=Yb.view(batch, H, W, 3))
+            torch.index_select(Ys, 0, idx, out=Yb.view(batch, H, W, NOUT))
             y = net.forward(Xb, batch, H, W)
             dy, part = net.mse(y, Yb)
             net.backward(dy)
@@ -357,7 +365,7 @@ def train(net, Xs, Ys, epochs=20, batch=16, lr=1e-3, seed=0, log=None):
             net.step(lr=lr_t)
             tot += part.sum()
             nb += 1
-        losses.append(float(tot.item()) / (nb * batch * H * W * 3))
+        losses.append(float(tot.item()) / (nb * batch * H * W * NOUT))
         if log:
             log(f"epoch {ep}: mse {losses[-1]:.4e}")
     return losses
@@ -374,14 +382,15 @@ class WarmStart:
         self.gx, self.gz = box.nelx // self.f, box.nelz // self.f
         self.fix = bc_fix_V.view(torch.uint8) if bc_fix_V.dtype == torch.bool else bc_fix_V
         self.stats = torch.empty(2, dtype=torch.float64, device="cuda")
+        self.scales = torch.empty(2, dtype=torch.float64, device="cuda")
         self.X = torch.empty(1, self.gz, self.gx, 2, dtype=bf16, device="cuda")
 
     def guess(self, T, eta_e, solV, solP):
         call("mw_unet_features", self.box, self.f, ptr(T), ptr(eta_e), self.Ra, ptr(self.stats), ptr(self.X),
              stream_ptr())
         y = self.net.forward(self.X, 1, self.gz, self.gx)
-        call("mw_unet_to_fields", self.box, self.f, ptr(y), ptr(self.stats), self.pscale, self.ghyd, ptr(self.fix),
-             ptr(solV), ptr(solP), stream_ptr())
+        call("mw_unet_to_fields", self.box, self.f, ptr(y), ptr(self.stats), self.pscale, self.ghyd,
+             ptr(self.scales), ptr(self.fix), ptr(solV), ptr(solP), stream_ptr())
         return solV, solP
 
 

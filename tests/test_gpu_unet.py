@@ -22,7 +22,7 @@ def test_forward_loss_gradients_match_fp32_reference(base, levels, B, H, W):
         l.b.copy_(torch.randn(l.cout, generator=torch.Generator().manual_seed(l.cout)) * 0.05)
     g = torch.Generator().manual_seed(3)
     x = torch.rand(B, H, W, 2, generator=g).to(torch.bfloat16)
-    t = torch.randn(B * H * W, 3, generator=g)
+    t = torch.randn(B * H * W, 5, generator=g)
     y = net.forward(x.cuda(), B, H, W)
     dy, part = net.mse(y, t.cuda())
     net.backward(dy)
@@ -51,7 +51,7 @@ def test_adam_steps_lower_the_loss():
     zz = torch.linspace(0, 1, H)
     x = torch.stack(torch.broadcast_tensors(xx[None, :], zz[:, None]), -1)[None].repeat(B, 1, 1, 1)
     x = (x + 0.1 * torch.rand(B, H, W, 2, generator=g)).to(torch.bfloat16).cuda()
-    t = torch.sin(3 * x.float()).sum(-1, keepdim=True).repeat(1, 1, 1, 3).reshape(-1, 3).contiguous()
+    t = torch.sin(3 * x.float()).sum(-1, keepdim=True).repeat(1, 1, 1, 5).reshape(-1, 5).contiguous()
     losses = []
     for _ in range(40):
         y = net.forward(x, B, H, W)
@@ -64,7 +64,8 @@ def test_adam_steps_lower_the_loss():
 
 def test_targets_to_fields_reproduce_centre_values():
     """to_fields(targets(solution)) at f = 1 is exact at the element centres (bilinear between
-    centres); the hydrostatic part is carried analytically."""
+    centres); the RMS scales travel through the two log-scale channels; the hydrostatic part is
+    carried analytically."""
     from meeuuw_b200 import _lib as L
     from meeuuw_b200.unet import features_targets, pressure_scales
     n = 16
@@ -74,8 +75,8 @@ def test_targets_to_fields_reproduce_centre_values():
     x = np.tile(np.arange(nnx) / (nnx - 1), nnx)
     z = np.repeat(np.arange(nnx) / (nnx - 1), nnx)
     solV = np.empty(2 * nnx * nnx)
-    solV[0::2] = np.sin(np.pi * x) * np.cos(np.pi * z)
-    solV[1::2] = -np.cos(np.pi * x) * np.sin(np.pi * z)
+    solV[0::2] = 3e4 * np.sin(np.pi * x) * np.cos(np.pi * z)
+    solV[1::2] = -3e4 * np.cos(np.pi * x) * np.sin(np.pi * z)
     px = np.tile(np.arange(n + 1) / n, n + 1)
     pz = np.repeat(np.arange(n + 1) / n, n + 1)
     Ra, alphaT = 1e5, 1e-2
@@ -84,18 +85,27 @@ def test_targets_to_fields_reproduce_centre_values():
     T = rng.uniform(0, 1, nnx * nnx)
     eta = np.exp(rng.normal(0, 1, n * n))
     d = lambda a: torch.as_tensor(a).cuda()
-    X, Y, stats = features_targets(box, d(T), d(eta), Ra, alphaT, 1, d(solV), d(solP))
+    scales = torch.empty(2, dtype=torch.float64, device="cuda")
+    X, Y, stats = features_targets(box, d(T), d(eta), Ra, alphaT, 1, d(solV), d(solP), scales=scales)
+    Yh = Y.cpu().numpy().reshape(n * n, 5)
+    assert np.allclose(np.sqrt(np.mean(0.5 * (Yh[:, 0] ** 2 + Yh[:, 1] ** 2))), 1.0, rtol=1e-6)
+    assert np.allclose(np.sqrt(np.mean(Yh[:, 2] ** 2)), 1.0, rtol=1e-6)
+    sc = scales.cpu().numpy()
+    assert np.allclose(Yh[:, 3], np.log10(sc[0]), rtol=1e-6) and np.allclose(Yh[:, 4], np.log10(sc[1]), rtol=1e-6)
     fix = torch.zeros(2 * nnx * nnx, dtype=torch.uint8, device="cuda")
     V2 = torch.empty(2 * nnx * nnx, dtype=torch.float64, device="cuda")
     P2 = torch.empty((n + 1) ** 2, dtype=torch.float64, device="cuda")
-    yflat = Y.reshape(-1, 3).contiguous()
-    L.call("mw_unet_to_fields", box, 1, L.ptr(yflat), L.ptr(stats), pscale, ghyd, L.ptr(fix), L.ptr(V2), L.ptr(P2),
-           L.stream_ptr())
+    yflat = Y.reshape(-1, 5).contiguous()
+    pred = torch.empty(2, dtype=torch.float64, device="cuda")
+    L.call("mw_unet_to_fields", box, 1, L.ptr(yflat), L.ptr(stats), pscale, ghyd, L.ptr(pred), L.ptr(fix),
+           L.ptr(V2), L.ptr(P2), L.stream_ptr())
+    assert np.allclose(pred.cpu().numpy(), sc, rtol=1e-5)
     V2 = V2.cpu().numpy()
     ix, iz = np.meshgrid(np.arange(1, nnx, 2), np.arange(1, nnx, 2))
     centre = (iz * nnx + ix).ravel()
-    np.testing.assert_allclose(V2[2 * centre], solV[2 * centre], rtol=1e-6, atol=1e-6)
-    np.testing.assert_allclose(V2[2 * centre + 1], solV[2 * centre + 1], rtol=1e-6, atol=1e-6)
+    vmax = np.abs(solV).max()
+    np.testing.assert_allclose(V2[2 * centre], solV[2 * centre], rtol=1e-5, atol=1e-5 * vmax)
+    np.testing.assert_allclose(V2[2 * centre + 1], solV[2 * centre + 1], rtol=1e-5, atol=1e-5 * vmax)
     # features: T at the centres and the scaled log-viscosity
     Xc = X.float().cpu().numpy().reshape(n, n, 2)
     np.testing.assert_allclose(Xc[..., 0].ravel(), T[centre], atol=4e-3)

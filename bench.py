@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="skip the torch-profiler launch count")
     ap.add_argument("--roofline-only", action="store_true", help="set up the model, time the operator apply, exit")
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="instead of the 512x512 model: an uneven ensemble of this many models (64..192 squared)")
     return ap.parse_args()
 
 
@@ -248,8 +250,11 @@ def roofline_apply(model, torch):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     achieved = algo / (us * 1e-6) / 1e9
+    # DRAM bytes (read + write) of one launch at 512x512 from an ncu capture of this kernel
+    # (profiles/k_apply_fp32_fk512.txt); other sizes scale with the element count
+    traffic = int(20133120 * nel / 262144)
     return {"kernel": "mw::k_apply<float, AM_APPLY> (fine level, 512x512)", "bound": "hbm", "achieved": achieved,
-            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None, "us_per_launch": us,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "us_per_launch": us,
             "algorithmic_bytes": algo,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650"}
 
@@ -348,9 +353,62 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args):
+    """Uneven ensemble (n ~ U[64,192], Ra ~ logU[1e4,1e7], contrast ~ logU[1,1e4], 16 particles per
+    element): aggregate model-timesteps/s of the mixed-precision ensemble with autotuned
+    concurrency, and each model's vrms after the timed steps against the same model run with the
+    FP64 solver."""
+    import torch
+    from meeuuw_b200.ensemble import Autotuner, Ensemble, sample_configs
+    cfgs = sample_configs(args.ensemble, seed=7)
+    ens = Ensemble(cfgs, stokes="mixed")
+    tune = Autotuner(cache_path=os.path.join(ROOT, "gpurun_out", "autotune.json")).tune(ens, steps=1, use_cache=False)
+    for _ in range(args.warmup):
+        ens.step()
+    ens.synchronize()
+    ens.check()
+    dev = torch.cuda.current_device()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(args.steps):
+            ens.step()
+        for st in ens.streams:               # the end event waits for every model's stream
+            torch.cuda.current_stream().wait_stream(st)
+        e.record()
+        torch.cuda.synchronize()
+    ms = s.elapsed_time(e)
+    ens.check()
+    mixed = [d["vrms"] for d in ens.diagnostics()]
+    nsteps_done = args.warmup + args.steps + 2 * len(tune["seconds_per_step"])   # autotuning steps too
+    ens.close()
+    del ens
+    # FP64 reference run of the same models for the same number of steps
+    ref = Ensemble(cfgs, stokes="f64", threads=tune["threads"])
+    for _ in range(nsteps_done):
+        ref.step()
+    ref.synchronize()
+    fp64 = [d["vrms"] for d in ref.diagnostics()]
+    ref.close()
+    err = [abs(a - b) / abs(b) for a, b in zip(mixed, fp64)]
+    line = {"metric": "aggregate model-timesteps/s, uneven ensemble (64..192 squared, 16 particles/element)",
+            "value": len(cfgs) * args.steps / (ms / 1000.0), "unit": "model-timesteps/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "dtype": "f64+f32", "data": "synthetic (seeded per model)",
+            "config": {"workload": f"ensemble of {len(cfgs)} FK convection models", "models": len(cfgs),
+                       "elements_total": int(sum(c.nel for c in cfgs)), "threads": tune["threads"],
+                       "autotune_seconds_per_step": tune["seconds_per_step"]},
+            "vrms_rel_err_vs_fp64": {"max": max(err), "median": sorted(err)[len(err) // 2]},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.ensemble:
+        run_ensemble(a)
     else:
         run_ours(a)

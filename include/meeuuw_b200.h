@@ -287,6 +287,8 @@ typedef struct {
   int32_t use_guess;      /* 1: start from the solV/solP passed in (warm start)                      */
   double* history;        /* optional device [4][history_len]: per Schur iteration xiV = ||alpha d||, */
   int32_t history_len;    /* xiP = ||alpha p||, alpha, beta (the reference's array_xiV/xiP/alpha/beta) */
+  int32_t host_loops;     /* 0: loops as CUDA-graph conditional nodes (one graph launch per solve, the  */
+                          /* default); 1: loops driven by the host (one synchronisation per iteration) */
 } mw_solve_params;
 
 typedef struct {
@@ -322,6 +324,17 @@ int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, vo
 /* K x = b by multigrid-preconditioned CG (replaces splu(K).solve, uzawa3_solver_L2.py:37-38). */
 int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,
                       int32_t* iters, double* relres, void* stream);
+
+/* 1 when this solver has run a solve as one recorded CUDA graph with device-side loops (the
+ * default), 0 when it fell back to host-driven loops. */
+int mw_stokes_device_loops(const mw_stokes* S);
+
+/* Uzawa residual of a pressure candidate (no reference counterpart: it judges initial guesses for
+ * uzawa3_solver_L2 / cd_u_eta, which recompute the velocity from the pressure): V = K^-1 (f - G P)
+ * by the multigrid PCG at `precision` to rtol (V may be NULL: internal scratch), then
+ * *norm_out = || G^T V - h ||_2 with the mean removed (closed box).  Synchronises. */
+int mw_stokes_uzawa_residual(mw_stokes* S, int32_t precision, const double* f, const double* h, const double* P,
+                             double rtol, int32_t maxit, double* V, double* norm_out, void* stream);
 
 /* FP64 residual (RV, RP) = (f, h) - A (V, P) and its 2-norm. */
 int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const double* f, const double* h, double* RV,

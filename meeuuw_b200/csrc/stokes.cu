@@ -54,11 +54,20 @@ MW_HD constexpr double ref_np(int q, int k) {
 }
 MW_HD constexpr double ref_wq(int q) { return gwt(q / 3) * gwt(q % 3); }
 
+// FP32 kernels take the values as immediates; FP64 ones read them from the constant bank (an FP64
+// immediate would be materialised in registers for every use).  Which terms vanish is decided at
+// compile time in both cases (ref_dr / ref_dt above).
 template <typename R> struct CT {
   MW_D static constexpr R dr(int q, int k) { return (R)ref_dr(q, k); }
   MW_D static constexpr R dt(int q, int k) { return (R)ref_dt(q, k); }
   MW_D static constexpr R np(int q, int k) { return (R)ref_np(q, k); }
   MW_D static constexpr R wq(int q) { return (R)ref_wq(q); }
+};
+template <> struct CT<double> {
+  MW_D static double dr(int q, int k) { return c_ref.dr[q * 9 + k]; }
+  MW_D static double dt(int q, int k) { return c_ref.dt[q * 9 + k]; }
+  MW_D static double np(int q, int k) { return c_ref.NP[q * 4 + k]; }
+  MW_D static double wq(int q) { return c_ref.wq[q]; }
 };
 
 static void host_ref_tables(RefTables* T) {
@@ -152,8 +161,8 @@ MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const 
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
-      if (r != R(0)) { dxu += r * ue[2 * k]; dxw += r * ue[2 * k + 1]; }
-      if (t != R(0)) { dzw += t * ue[2 * k + 1]; dzu += t * ue[2 * k]; }
+      if (ref_dr(q, k) != 0.0) { dxu += r * ue[2 * k]; dxw += r * ue[2 * k + 1]; }
+      if (ref_dt(q, k) != 0.0) { dzw += t * ue[2 * k + 1]; dzu += t * ue[2 * k]; }
     }
     const R exx = sx * dxu, ezz = sz * dzw, gg = sz * dzu + sx * dxw;   // gg = du/dz + dw/dx
     const R jw = jac * CT<R>::wq(q);
@@ -169,8 +178,8 @@ MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const 
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
-      if (r != R(0)) { ye[2 * k] += r * A; ye[2 * k + 1] += r * Cx; }
-      if (t != R(0)) { ye[2 * k] += t * Cz; ye[2 * k + 1] += t * B; }
+      if (ref_dr(q, k) != 0.0) { ye[2 * k] += r * A; ye[2 * k + 1] += r * Cx; }
+      if (ref_dt(q, k) != 0.0) { ye[2 * k] += t * Cz; ye[2 * k + 1] += t * B; }
     }
     const R dv = -s * jw * (exx + ezz);
 #pragma unroll
@@ -960,13 +969,17 @@ struct mw_stokes {
   };
   std::vector<GraphEntry> graphs;
   bool use_graphs = true;
+  bool device_loops = true;    // loops as graph conditional nodes (no host synchronisation)
   cudaStream_t ws = nullptr;
+  cudaStream_t bs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // capture streams of loop bodies
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   ~mw_stokes() {
     for (auto& e : graphs) cudaGraphExecDestroy(e.exec);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
     if (ws) cudaStreamDestroy(ws);
+    for (auto b : bs)
+      if (b) cudaStreamDestroy(b);
   }
 };
 
@@ -1022,7 +1035,7 @@ static size_t layout(mw_stokes* S, Arena& A) {
   for (auto p : pv) *p = (double*)A.take(sizeof(double) * np);
   S->etae_w = (double*)A.take(sizeof(double) * nel);
   S->red = (double*)A.take(sizeof(double) * NB * 4);
-  S->sc = (double*)A.take(sizeof(double) * 64);
+  S->sc = (double*)A.take(sizeof(double) * 256);
   S->counter = (unsigned*)A.take(sizeof(unsigned) * 4);
   if (S->has64) {
     for (int i = 0; i < 5; ++i) S->pc64[i] = (double*)A.take(sizeof(double) * nv);
@@ -1127,6 +1140,12 @@ static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool firs
 // an enclosing capture) the kernels are issued directly.
 template <typename Rec, typename Save, typename Load>
 static void graph_run(mw_stokes* S, int kind, Rec record, Save save, Load load, cudaStream_t s) {
+  cudaStreamCaptureStatus cs0 = cudaStreamCaptureStatusNone;
+  if (s != nullptr && cudaStreamIsCapturing(s, &cs0) == cudaSuccess && cs0 != cudaStreamCaptureStatusNone) {
+    record();            // part of an enclosing capture
+    return;
+  }
+  cudaGetLastError();
   std::vector<void*> st = save();
   if (S->use_graphs) {
     for (auto& e : S->graphs) {
@@ -1485,6 +1504,312 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
   return MW_OK;
 }
 
+// ================================================================ device-side loops
+// The whole solve as one CUDA graph: the iterations run as conditional WHILE nodes whose bodies end
+// with a one-thread kernel that updates the loop scalars and sets the condition, so no iteration
+// waits for the host.  Every loop is bounded by its iteration cap (max_inner, max_outer,
+// max_refine) and by a total work cap, both decided on the device.  Scalars live in S->sc from
+// slot 64 on.
+enum DevSlot {
+  P_RZ = 64, P_PAP, P_RR, P_BB, P_RZN, P_IT,                 // inner PCG
+  U_RW = 72, U_DSD, U_RWN, U_RR0, U_RR, U_IT, U_D2, U_Z2,    // Schur CG
+  T_RV = 84, T_RP, T_REL,                                     // true residual
+  S_BB = 88, S_BH, S_BNORM, S_REL0, S_NREF,                   // solve
+  I_OUTER = 96, I_INNER, I_STATUS                             // info
+};
+
+// Work caps of one solve on top of the per-loop caps: a stagnating solve ends with status 3 after
+// this many inner (multigrid-PCG) or outer (Schur) iterations in total.
+constexpr double DEV_INNER_BUDGET = 40000, DEV_OUTER_BUDGET = 4000;
+
+__global__ void k_dev_pcg_init(double* sc, cudaGraphConditionalHandle hw) {
+  sc[P_IT] = 0;
+  const double bb = sc[P_BB];
+  cudaGraphSetConditional(hw, (bb > 0 && isfinite(bb)) ? 1u : 0u);
+}
+
+__global__ void k_dev_pcg_check(double* sc, double rtol, int maxit, cudaGraphConditionalHandle hw,
+                                cudaGraphConditionalHandle hi) {
+  const double it = sc[P_IT] + 1;
+  sc[P_IT] = it;
+  const double rr = sc[P_RR];
+  bool go = isfinite(rr) && rr > rtol * rtol * sc[P_BB] && it < (double)maxit;
+  if (go && sc[I_INNER] + it >= DEV_INNER_BUDGET) { sc[I_STATUS] = 3; go = false; }
+  cudaGraphSetConditional(hw, go ? 1u : 0u);
+  cudaGraphSetConditional(hi, go ? 1u : 0u);
+}
+
+__global__ void k_dev_pcg_done(double* sc) { sc[I_INNER] += sc[P_IT]; }
+
+__global__ void k_dev_uz_init(double* sc, int max_outer, cudaGraphConditionalHandle hw) {
+  sc[U_IT] = 0;
+  cudaGraphSetConditional(hw, (max_outer > 0 && isfinite(sc[U_RR0]) && sc[I_STATUS] == 0) ? 1u : 0u);
+}
+
+// one Schur iteration done: stop on a non-finite residual (status 2), on the FP64 true residual
+// (check_true), on the Schur residual reduction, at max_outer or at the work cap (status 3)
+__global__ void k_dev_uz_check(double* sc, double reduction, int check_true, double tol, int max_outer,
+                               cudaGraphConditionalHandle hw) {
+  const double it = sc[U_IT] + 1;
+  sc[U_IT] = it;
+  sc[I_OUTER] += 1;
+  const double rr = sc[U_RR];
+  bool go = it < (double)max_outer;
+  if (!isfinite(rr)) { sc[I_STATUS] = 2; go = false; }
+  if (sc[I_OUTER] >= DEV_OUTER_BUDGET && sc[I_STATUS] == 0) sc[I_STATUS] = 3;
+  if (sc[I_STATUS] != 0) go = false;
+  if (check_true && sc[T_REL] <= tol) go = false;
+  if (rr <= reduction * reduction * sc[U_RR0]) go = false;
+  cudaGraphSetConditional(hw, go ? 1u : 0u);
+}
+
+__global__ void k_dev_hist(const double* sc, double* hist, int len) {
+  const int k = (int)sc[I_OUTER];
+  if (k < 0 || k >= len) return;
+  const double alpha = sc[U_RW] / sc[U_DSD];
+  hist[k] = fabs(alpha) * sqrt(sc[U_Z2]);
+  hist[len + k] = fabs(alpha) * sqrt(sc[U_D2]);
+  hist[2 * len + k] = alpha;
+  hist[3 * len + k] = sc[U_RWN] / sc[U_RW];
+}
+
+__global__ void k_dev_rel(double* sc) { sc[T_REL] = sqrt(sc[T_RV] + sc[T_RP]) / sc[S_BNORM]; }
+
+__global__ void k_dev_solve_init(double* sc) {
+  sc[S_BNORM] = sqrt(sc[S_BB] + sc[S_BH]);
+  sc[S_NREF] = 0;
+  sc[I_OUTER] = 0;
+  sc[I_INNER] = 0;
+  sc[I_STATUS] = 0;
+}
+
+__global__ void k_dev_ref_init(double* sc, double tol, int max_refine, cudaGraphConditionalHandle hw) {
+  sc[S_REL0] = sc[T_REL];
+  const double r = sc[T_REL];
+  cudaGraphSetConditional(hw, (isfinite(r) && r > tol && max_refine > 0) ? 1u : 0u);
+}
+
+__global__ void k_dev_ref_check(double* sc, double tol, int max_refine, cudaGraphConditionalHandle hw) {
+  sc[S_NREF] += 1;
+  const double r = sc[T_REL];
+  const bool go = isfinite(r) && r > tol && sc[S_NREF] < (double)max_refine && sc[I_STATUS] == 0;
+  cudaGraphSetConditional(hw, go ? 1u : 0u);
+}
+
+__global__ void k_copy1(const double* src, double* dst) { *dst = *src; }
+
+// A conditional handle in the graph being captured on s (its value is set by kernels of that graph).
+static bool cond_handle(cudaStream_t s, cudaGraphConditionalHandle* h) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr) != cudaSuccess || st != cudaStreamCaptureStatusActive)
+    return false;
+  return cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+}
+
+// Append a conditional node (handle h) to the graph captured on s, after everything captured so far,
+// and start capturing its body on bs.  cond_end(bs) closes the body.
+static bool cond_node(cudaStream_t s, cudaStream_t bs, cudaGraphConditionalNodeType type, cudaGraphConditionalHandle h) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd) != cudaSuccess || st != cudaStreamCaptureStatusActive)
+    return false;
+  cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, deps, nd, &p) != cudaSuccess) return false;
+  if (cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return false;
+  return cudaStreamBeginCaptureToGraph(bs, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+}
+
+static bool cond_end(cudaStream_t bs) {
+  cudaGraph_t g = nullptr;
+  return cudaStreamEndCapture(bs, &g) == cudaSuccess;
+}
+
+// capture stream of nesting level `depth` (0: the solve's stream)
+static cudaStream_t lvl(mw_stokes* S, cudaStream_t s, int depth) { return depth == 0 ? s : S->bs[depth - 1]; }
+
+// Inner PCG for K x = b recorded with a device WHILE loop (capture only), at nesting level `depth`
+// (uses the body streams depth and depth + 1).  Adds its iteration count to sc[I_INNER].
+template <typename R>
+static bool pcg_K_dev(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double* x, double rtol, int maxit,
+                      cudaStream_t s0, int depth) {
+  if (depth + 2 > 6) return false;
+  cudaStream_t s = lvl(S, s0, depth), b1 = S->bs[depth], b2 = S->bs[depth + 1];
+  Level<R>& L = H.L[0];
+  const int64_t n = L.ndof;
+  R *xr = pc[0], *r = pc[1], *p = pc[3], *Ap = pc[4];
+  R*& z = pc[2];
+  double* sc = S->sc;
+  auto precond = [&](R* rin, R*& zout, cudaStream_t st) {
+    R* saved_b = L.b;
+    L.b = rin;
+    vcycle(H, 0, S->prm.cheb_degree, st);
+    L.b = saved_b;
+    std::swap(zout, L.x);
+  };
+  k_copy<R, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
+  k_set<R><<<grid_for(n, 256), 256, 0, s>>>(n, R(0), xr);
+  dot<R>(S, n, r, r, sc + P_BB, s);
+  precond(r, z, s);
+  k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
+  dot<R>(S, n, r, z, sc + P_RZ, s);
+  cudaGraphConditionalHandle hw, hi;
+  if (!cond_handle(s, &hw)) return false;
+  k_dev_pcg_init<<<1, 1, 0, s>>>(sc, hw);
+  if (!cond_node(s, b1, cudaGraphCondTypeWhile, hw)) return false;
+  // body: one CG step and the convergence test, then (if continuing) the next search direction
+  k_only_apply<R>(L, p, Ap, b1);
+  dot<R>(S, n, p, Ap, sc + P_PAP, b1);
+  k_pcg_update<R><<<grid_for(n, 256), 256, 0, b1>>>(n, sc + P_RZ, sc + P_PAP, p, Ap, xr, r);
+  dot<R>(S, n, r, r, sc + P_RR, b1);
+  if (!cond_handle(b1, &hi)) return false;
+  k_dev_pcg_check<<<1, 1, 0, b1>>>(sc, rtol, maxit, hw, hi);
+  if (!cond_node(b1, b2, cudaGraphCondTypeIf, hi)) return false;
+  precond(r, z, b2);
+  dot<R>(S, n, r, z, sc + P_RZN, b2);
+  k_xpby_ratio<R><<<grid_for(n, 256), 256, 0, b2>>>(n, z, sc + P_RZN, sc + P_RZ, p);
+  k_copy1<<<1, 1, 0, b2>>>(sc + P_RZN, sc + P_RZ);
+  if (!cond_end(b2) || !cond_end(b1)) return false;
+  k_copy<double, R><<<grid_for(n, 256), 256, 0, s>>>(n, xr, x);
+  k_dev_pcg_done<<<1, 1, 0, s>>>(sc);
+  return true;
+}
+
+static bool solve_K_dev(mw_stokes* S, int prec, const double* b, double* x, double rtol, int maxit, cudaStream_t s0,
+                        int depth) {
+  if (prec == MW_F32) return pcg_K_dev<float>(S, S->H32, S->pc32, b, x, rtol, maxit, s0, depth);
+  return pcg_K_dev<double>(S, S->H64, S->pc64, b, x, rtol, maxit, s0, depth);
+}
+
+// FP64 true residual into sc[T_REL] (relative to sc[S_BNORM]); RV, RP hold the residual.
+static void true_residual_dev(mw_stokes* S, const double* V, const double* P, const double* f, const double* h,
+                              cudaStream_t s) {
+  const LevelGeo& g = S->fine;
+  ApplyArgs<double> a = args0<double>();
+  a.u = V; a.p = P; a.eta = S->etaq64; a.fix = S->fixV;
+  a.diag = S->diag64;
+  a.yV = S->RV; a.yP = S->RP; a.bV = f; a.bP = h;
+  launch_apply<double, AM_RESID>(g, a, s);
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  dot<double>(S, nv, S->RV, S->RV, S->sc + T_RV, s);
+  dot<double>(S, np, S->RP, S->RP, S->sc + T_RP, s);
+  k_dev_rel<<<1, 1, 0, s>>>(S->sc);
+}
+
+// Schur-complement CG (the recurrences of the host version `uzawa`) recorded with a device WHILE
+// loop at nesting level `depth` (uses body streams depth .. depth + 3).
+static bool uzawa_dev(mw_stokes* S, const mw_solve_params& sp, int prec, const double* f, const double* h, double* V,
+                      double* P, double reduction, bool check_true, cudaStream_t s0, int depth) {
+  if (depth + 4 > 6) return false;
+  cudaStream_t s = lvl(S, s0, depth), b1 = S->bs[depth];
+  const LevelGeo& g = S->fine;
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  const double* w = sp.scheme == MW_SCHEME_UZAWA3 ? nullptr : S->etae_w;
+  double* sc = S->sc;
+  {  // V = K^-1 (f - G P)
+    ApplyArgs<double> a = args0<double>();
+    a.p = P; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd; a.bV = f;
+    launch_apply<double, AM_RESID>(g, a, s);
+  }
+  if (!solve_K_dev(S, prec, S->Gd, V, sp.inner_rtol, sp.max_inner, s0, depth)) return false;
+  {  // rho = G^T V - h
+    ApplyArgs<double> a = args0<double>();
+    a.u = V; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64;
+    a.yP = S->rP;
+    launch_apply<double, AM_APPLY>(g, a, s);
+    if (h) k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
+  }
+  remove_mean(S, np, S->rP, s);
+  mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
+  remove_mean(S, np, S->wP, s);
+  k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, S->dP);
+  dot<double>(S, np, S->rP, S->wP, sc + U_RW, s);
+  dot<double>(S, np, S->rP, S->rP, sc + U_RR0, s);
+  cudaGraphConditionalHandle hw;
+  if (!cond_handle(s, &hw)) return false;
+  k_dev_uz_init<<<1, 1, 0, s>>>(sc, sp.max_outer, hw);
+  if (!cond_node(s, b1, cudaGraphCondTypeWhile, hw)) return false;
+  {
+    ApplyArgs<double> a = args0<double>();
+    a.p = S->dP; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd;
+    launch_apply<double, AM_APPLY>(g, a, b1);
+  }
+  if (!solve_K_dev(S, prec, S->Gd, S->z, sp.inner_rtol, sp.max_inner, s0, depth + 1)) return false;
+  {
+    ApplyArgs<double> b2 = args0<double>();
+    b2.u = S->z; b2.eta = S->etaq64; b2.fix = S->fixV; b2.diag = S->diag64;
+    b2.yP = S->GTz;
+    launch_apply<double, AM_APPLY>(g, b2, b1);
+  }
+  dot<double>(S, np, S->dP, S->GTz, sc + U_DSD, b1);
+  const bool hist = sp.history && sp.history_len > 0;
+  if (hist) {
+    dot<double>(S, np, S->dP, S->dP, sc + U_D2, b1);
+    dot<double>(S, nv, S->z, S->z, sc + U_Z2, b1);
+  }
+  k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, b1>>>(np, sc + U_RW, sc + U_DSD, 1.0, S->dP, P);
+  k_axpy_ratio<double, double><<<grid_for(nv, 256), 256, 0, b1>>>(nv, sc + U_RW, sc + U_DSD, -1.0, S->z, V);
+  k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, b1>>>(np, sc + U_RW, sc + U_DSD, -1.0, S->GTz, S->rP);
+  remove_mean(S, np, S->rP, b1);
+  mass_solve(S, w, S->rP, S->wP, sp.mass_iters, b1);
+  remove_mean(S, np, S->wP, b1);
+  dot<double>(S, np, S->rP, S->wP, sc + U_RWN, b1);
+  if (hist) k_dev_hist<<<1, 1, 0, b1>>>(sc, sp.history, sp.history_len);
+  k_xpby_ratio<double><<<grid_for(np, 256), 256, 0, b1>>>(np, S->wP, sc + U_RWN, sc + U_RW, S->dP);
+  k_copy1<<<1, 1, 0, b1>>>(sc + U_RWN, sc + U_RW);
+  dot<double>(S, np, S->rP, S->rP, sc + U_RR, b1);
+  if (check_true) true_residual_dev(S, V, P, f, h, b1);
+  k_dev_uz_check<<<1, 1, 0, b1>>>(sc, reduction, check_true ? 1 : 0, sp.tol, sp.max_outer, hw);
+  return cond_end(b1);
+}
+
+// The whole solve (FP64, or mixed: FP64 refinement around FP32-inner Schur sweeps), recorded.
+static bool stokes_solve_record(mw_stokes* S, const double* f, const double* h, double* V, double* P,
+                                const mw_solve_params& sp, cudaStream_t s) {
+  const LevelGeo& g = S->fine;
+  const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  double* sc = S->sc;
+  if (!sp.use_guess) {
+    k_set<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 0.0, V);
+    k_set<double><<<grid_for(np, 256), 256, 0, s>>>(np, 0.0, P);
+  }
+  dot<double>(S, nv, f, f, sc + S_BB, s);
+  dot<double>(S, np, h, h, sc + S_BH, s);
+  k_dev_solve_init<<<1, 1, 0, s>>>(sc);
+  true_residual_dev(S, V, P, f, h, s);
+  cudaGraphConditionalHandle hc;
+  if (!cond_handle(s, &hc)) return false;
+  if (sp.precision == MW_F64) {
+    k_dev_ref_init<<<1, 1, 0, s>>>(sc, sp.tol, 1, hc);        // records the initial residual; gate on tol
+    if (!cond_node(s, S->bs[0], cudaGraphCondTypeIf, hc)) return false;
+    if (!uzawa_dev(S, sp, MW_F64, f, h, V, P, 0.0, true, s, 1)) return false;
+    if (!cond_end(S->bs[0])) return false;
+    true_residual_dev(S, V, P, f, h, s);
+  } else {
+    k_dev_ref_init<<<1, 1, 0, s>>>(sc, sp.tol, sp.max_refine, hc);
+    if (!cond_node(s, S->bs[0], cudaGraphCondTypeWhile, hc)) return false;
+    cudaStream_t b = S->bs[0];
+    k_copy<double, double><<<grid_for(nv, 256), 256, 0, b>>>(nv, S->RV, S->f);
+    k_copy<double, double><<<grid_for(np, 256), 256, 0, b>>>(np, S->RP, S->h);
+    k_set<double><<<grid_for(nv, 256), 256, 0, b>>>(nv, 0.0, S->cV);
+    k_set<double><<<grid_for(np, 256), 256, 0, b>>>(np, 0.0, S->cP);
+    if (!uzawa_dev(S, sp, MW_F32, S->f, S->h, S->cV, S->cP, sp.sweep_reduction, false, s, 1)) return false;
+    k_axpy<double><<<grid_for(nv, 256), 256, 0, b>>>(nv, 1.0, S->cV, V);
+    k_axpy<double><<<grid_for(np, 256), 256, 0, b>>>(np, 1.0, S->cP, P);
+    true_residual_dev(S, V, P, f, h, b);
+    k_dev_ref_check<<<1, 1, 0, b>>>(sc, sp.tol, sp.max_refine, hc);
+    if (!cond_end(b)) return false;
+  }
+  return true;
+}
+
 template <typename R>
 __global__ void k_cast(int64_t n, const double* __restrict__ a, R* __restrict__ b) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -1555,6 +1880,13 @@ int mw_stokes_create(mw_box box, mw_stokes_params prm, const uint8_t* bc_fix_V, 
 int mw_stokes_destroy(mw_stokes* S) {
   delete S;
   return MW_OK;
+}
+
+int mw_stokes_device_loops(const mw_stokes* S) {
+  if (!S->device_loops) return 0;
+  for (const auto& e : S->graphs)
+    if (e.kind == 1000) return 1;
+  return 0;
 }
 
 int mw_stokes_levels(const mw_stokes* S, int32_t precision) {
@@ -1630,6 +1962,40 @@ int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* 
   return rr <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
 }
 
+// Uzawa residual of a pressure candidate P: the Schur iteration recomputes the velocity from the
+// pressure (V = K^-1 (f - G P), inner PCG to rtol), so its starting point is judged by the 2-norm
+// of G^T V - h with its mean removed.
+int mw_stokes_uzawa_residual(mw_stokes* S, int32_t precision, const double* f, const double* h, const double* P,
+                             double rtol, int32_t maxit, double* V, double* norm_out, void* stream) {
+  if (!f || !h || !P || !norm_out) return MW_ERR_BAD_ARG;
+  cudaStream_t caller = (cudaStream_t)stream;
+  cudaStream_t s = enter(S, caller);
+  int rc = ensure_hierarchy(S, precision, s);
+  if (!rc) {
+    const LevelGeo& g = S->fine;
+    const int64_t np = (int64_t)(g.nx + 1) * (g.nz + 1);
+    ApplyArgs<double> a = args0<double>();
+    a.p = P; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd; a.bV = f;
+    launch_apply<double, AM_RESID>(g, a, s);                 // Gd = f - G P
+    double rr = 0;
+    double* Vo = V ? V : S->z;
+    solve_K(S, precision, S->Gd, Vo, rtol, maxit, &rr, s);
+    ApplyArgs<double> b = args0<double>();
+    b.u = Vo; b.eta = S->etaq64; b.fix = S->fixV; b.diag = S->diag64; b.yP = S->rP;
+    launch_apply<double, AM_APPLY>(g, b, s);                 // rP = G^T V
+    k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
+    remove_mean(S, np, S->rP, s);
+    dot<double>(S, np, S->rP, S->rP, S->sc + 54, s);
+    double v = 0;
+    cudaMemcpyAsync(&v, S->sc + 54, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) rc = MW_ERR_CUDA;
+    *norm_out = std::sqrt(v);
+  }
+  leave(S, caller, s);
+  if (!rc && cudaGetLastError() != cudaSuccess) rc = MW_ERR_CUDA;
+  return rc;
+}
+
 int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const double* f, const double* h, double* RV,
                        double* RP, double* norm_out, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
@@ -1667,6 +2033,8 @@ static void leave(mw_stokes* S, cudaStream_t caller, cudaStream_t s) {
 
 static int stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
                         const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s);
+static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
+                             const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s);
 
 int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
                     mw_solve_info* info, void* stream) {
@@ -1677,8 +2045,122 @@ int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV
   return rc;
 }
 
+static void key_add(std::vector<void*>& k, double v) {
+  uint64_t u;
+  memcpy(&u, &v, sizeof(u));
+  k.push_back((void*)(uintptr_t)u);
+}
+
+// Runs the whole solve from a recorded graph (recorded on first use for these buffers, parameters
+// and multigrid pointer state) and reads the loop scalars back once.  Returns false when the
+// graph cannot be recorded or launched; the caller then runs the host-driven loops.
+static bool stokes_solve_graph(mw_stokes* S, const double* f, const double* h, double* V, double* P,
+                               const mw_solve_params& sp, mw_solve_info* inf, cudaStream_t s) {
+  if (!S->device_loops || !S->use_graphs || s == nullptr) return false;
+  for (auto& b : S->bs)
+    if (!b && cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+  std::vector<void*> key = {(void*)f, (void*)h, (void*)V, (void*)P, (void*)sp.history,
+                            (void*)(intptr_t)((sp.scheme << 24) ^ (sp.precision << 20) ^ (sp.use_guess << 16) ^
+                                              sp.history_len),
+                            (void*)(intptr_t)sp.max_outer, (void*)(intptr_t)sp.max_inner,
+                            (void*)(intptr_t)sp.max_refine, (void*)(intptr_t)sp.mass_iters};
+  key_add(key, sp.tol);
+  key_add(key, sp.inner_rtol);
+  key_add(key, sp.sweep_reduction);
+  std::vector<void*> h32 = vstate(S->H32), h64 = vstate(S->H64);
+  key.insert(key.end(), h32.begin(), h32.end());
+  key.insert(key.end(), h64.begin(), h64.end());
+  const int kind = 1000;
+  int hit = -1;
+  for (size_t i = 0; i < S->graphs.size(); ++i)
+    if (S->graphs[i].kind == kind && S->graphs[i].before == key) { hit = (int)i; break; }
+  if (hit < 0) {
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { cudaGetLastError(); return false; }
+    bool ok = stokes_solve_record(S, f, h, V, P, sp, s);
+    for (auto b : S->bs) {      // close any body capture left open by a failed recording
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(b, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t gb = nullptr;
+        cudaStreamEndCapture(b, &gb);
+        ok = false;
+      }
+    }
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    const bool captured = cudaStreamEndCapture(s, &g) == cudaSuccess && g;
+    ok = ok && captured && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {                       // the recording ran nothing: restore the pointer state
+      cudaGetLastError();
+      vload(S->H32, h32);
+      vload(S->H64, h64);
+      S->device_loops = false;       // this device cannot record the loops: keep the host loops
+      return false;
+    }
+    if (S->graphs.size() >= 192) {
+      cudaGraphExecDestroy(S->graphs.front().exec);
+      S->graphs.erase(S->graphs.begin());
+    }
+    mw_stokes::GraphEntry e;
+    e.kind = kind;
+    e.before = key;
+    std::vector<void*> a32 = vstate(S->H32), a64 = vstate(S->H64);
+    e.after = a32;
+    e.after.insert(e.after.end(), a64.begin(), a64.end());
+    e.exec = ex;
+    S->graphs.push_back(e);
+    hit = (int)S->graphs.size() - 1;
+    vload(S->H32, h32);            // the after-state is applied below, once the graph ran
+    vload(S->H64, h64);
+  }
+  mw_stokes::GraphEntry& e = S->graphs[hit];
+  if (cudaGraphLaunch(e.exec, s) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  {
+    const size_t n32 = h32.size();
+    std::vector<void*> a32(e.after.begin(), e.after.begin() + n32), a64(e.after.begin() + n32, e.after.end());
+    vload(S->H32, a32);
+    vload(S->H64, a64);
+  }
+  double q[40];
+  cudaMemcpyAsync(q, S->sc + 64, sizeof(q), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+  const double bnorm = q[S_BNORM - 64];
+  inf->outer_iters = (int)q[I_OUTER - 64];
+  inf->inner_iters = (int)q[I_INNER - 64];
+  inf->refinements = (int)q[S_NREF - 64];
+  inf->initial_rel_residual = bnorm > 0 ? q[S_REL0 - 64] : 0.0;
+  inf->rel_residual = bnorm > 0 ? q[T_REL - 64] : 0.0;
+  if (!std::isfinite(bnorm)) inf->rel_residual = inf->initial_rel_residual = bnorm;
+  if (q[I_STATUS - 64] != 0) inf->rel_residual = NAN;
+  return true;
+}
+
 static int stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
                         const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s) {
+  if (!f || !h || !solV || !solP) return MW_ERR_BAD_ARG;
+  if (int rc = ensure_hierarchy(S, sp.precision == MW_F32 ? MW_F32 : MW_F64, s)) return rc;
+  {
+    mw_solve_info inf;
+    memset(&inf, 0, sizeof(inf));
+    if (!sp.host_loops && stokes_solve_graph(S, f, h, solV, solP, sp, &inf, s)) {
+      inf.converged = inf.rel_residual <= sp.tol ? 1 : 0;
+      S->last = inf;
+      if (info) *info = inf;
+      if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
+      return inf.converged ? MW_OK : MW_ERR_NOT_CONVERGED;
+    }
+  }
+  return stokes_solve_host(S, f, h, solV, solP, sp, info, s);
+}
+
+static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
+                             const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s) {
   const LevelGeo& g = S->fine;
   const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
   mw_solve_info inf;

@@ -1,0 +1,151 @@
+"""Ensembles of independent models of uneven size advanced together on one GPU.
+
+A small model (64² elements: 4096 elements, 65 k particles) fills a fraction of a B200: its
+operator applies launch 32 thread blocks on 148 SMs, and its host-side launch sequence leaves the
+GPU idle between kernels.  An ensemble therefore runs every model on its own CUDA stream and
+advances the models concurrently from a pool of host threads (the C ABI calls release the
+interpreter lock, so launches from different threads overlap), letting the GPU interleave the
+models' kernels.  Each model keeps its own device buffers, scratch (per-stream workspaces) and
+Stokes solver (its own stream and recorded CUDA graphs), so nothing is shared between models.
+
+``Autotuner`` picks the number of host threads (the concurrency level) by timing ensemble steps,
+and caches the choice per GPU and ensemble shape.
+"""
+import json
+import math
+import os
+import time
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import replace
+
+import numpy as np
+import torch
+
+from . import configs
+from .timestep import GPUModel
+
+
+def sample_configs(n_models=64, seed=0, n_range=(64, 192), Ra_range=(1e4, 1e7), contrast_range=(1.0, 1e4),
+                   nparticle_per_dim=4):
+    """Uneven ensemble: square grids n ~ U[n_range] (even), Ra and the Frank-Kamenetskii viscosity
+    contrast log-uniform, 16 particles per element, a seed per model."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_models):
+        n = int(rng.integers(n_range[0] // 2, n_range[1] // 2 + 1)) * 2
+        Ra = math.exp(rng.uniform(math.log(Ra_range[0]), math.log(Ra_range[1])))
+        c = math.exp(rng.uniform(math.log(contrast_range[0]), math.log(contrast_range[1])))
+        base = configs.fk_convection(n)
+        out.append(replace(base, name=f"ens{i}_{n}", Ra=Ra, fk_gamma=math.log(c), seed=int(seed * 100003 + i),
+                           nparticle_per_dim=nparticle_per_dim))
+    return out
+
+
+class Ensemble:
+    """N independent models, each on its own stream, stepped concurrently by `threads` host threads."""
+
+    def __init__(self, cfgs, stokes="mixed", threads=8, tol=1e-8, guess=None):
+        self.cfgs = list(cfgs)
+        self.streams, self.models = [], []
+        for cfg in self.cfgs:
+            st = torch.cuda.Stream()
+            with torch.cuda.stream(st):
+                m = GPUModel(cfg, stokes=stokes, tol=tol)
+                if guess is not None:
+                    m.guess = guess(m)
+            self.streams.append(st)
+            self.models.append(m)
+        torch.cuda.synchronize()
+        self.threads = 0
+        self.pool = None
+        self.set_threads(threads)
+
+    def set_threads(self, threads):
+        threads = max(1, min(int(threads), len(self.models)))
+        if threads != self.threads:
+            if self.pool is not None:
+                self.pool.shutdown(wait=True)
+            self.pool = ThreadPoolExecutor(max_workers=threads)
+            self.threads = threads
+
+    def _run(self, idx):
+        for i in idx:
+            with torch.cuda.stream(self.streams[i]):
+                self.models[i].step()
+
+    def step(self):
+        """One time step of every model.  Models are dealt to the threads largest first, so each
+        thread gets a similar amount of work."""
+        order = sorted(range(len(self.models)), key=lambda i: -self.models[i].nel)
+        parts = [order[t::self.threads] for t in range(self.threads)]
+        futs = [self.pool.submit(self._run, p) for p in parts if p]
+        for f in futs:
+            f.result()
+
+    def synchronize(self):
+        for st in self.streams:
+            st.synchronize()
+
+    def diagnostics(self):
+        return [m.diagnostics() for m in self.models]
+
+    def check(self):
+        for m in self.models:
+            m.check()
+
+    def close(self):
+        if self.pool is not None:
+            self.pool.shutdown(wait=True)
+            self.pool = None
+
+
+class Autotuner:
+    """Picks an ensemble's concurrency level (host threads) by timing a few steps at each candidate,
+    keeping the fastest; the choice is cached in a JSON file keyed by GPU name and the ensemble's
+    element counts."""
+
+    def __init__(self, cache_path=None, candidates=(1, 2, 4, 8, 16, 32)):
+        self.cache_path = cache_path or os.path.join(os.path.expanduser("~"), ".cache", "meeuuw_b200_autotune.json")
+        self.candidates = candidates
+
+    def _key(self, ens):
+        name = torch.cuda.get_device_name()
+        sizes = sorted(m.nel for m in ens.models)
+        return f"{name}|{len(sizes)}|{sum(sizes)}|{sizes[0]}|{sizes[-1]}"
+
+    def _load(self):
+        try:
+            with open(self.cache_path) as f:
+                return json.load(f)
+        except Exception:
+            return {}
+
+    def tune(self, ens, steps=2, use_cache=True):
+        key = self._key(ens)
+        cache = self._load()
+        if use_cache and key in cache:
+            ens.set_threads(cache[key]["threads"])
+            return cache[key]
+        timings = {}
+        for t in self.candidates:
+            if t > len(ens.models):
+                continue
+            ens.set_threads(t)
+            ens.step()                     # settle (graph recording, workspaces) at this level
+            ens.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                ens.step()
+            ens.synchronize()
+            timings[t] = (time.perf_counter() - t0) / steps
+        best = min(timings, key=timings.get)
+        ens.set_threads(best)
+        rec = {"threads": best, "seconds_per_step": timings}
+        cache[key] = {"threads": best, "seconds_per_step": {str(k): v for k, v in timings.items()}}
+        try:
+            os.makedirs(os.path.dirname(self.cache_path), exist_ok=True)
+            with open(self.cache_path, "w") as f:
+                json.dump(cache, f, indent=1)
+        except OSError:
+            pass
+        return rec

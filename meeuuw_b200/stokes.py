@@ -22,7 +22,8 @@ class MwSolveParams(ctypes.Structure):
     _fields_ = [("scheme", c_int32), ("precision", c_int32), ("tol", c_double), ("max_outer", c_int32),
                 ("max_inner", c_int32), ("inner_rtol", c_double), ("max_refine", c_int32),
                 ("sweep_reduction", c_double), ("mass_iters", c_int32),
-                ("use_guess", c_int32), ("history", c_void_p), ("history_len", c_int32)]
+                ("use_guess", c_int32), ("history", c_void_p), ("history_len", c_int32),
+                ("host_loops", c_int32)]
 
 
 class MwSolveInfo(ctypes.Structure):
@@ -36,6 +37,9 @@ L.extra_protos({
     "mw_stokes_workspace_bytes": (c_size_t, [L.MwBox, MwStokesParams]),
     "mw_stokes_create": (c_int32, [L.MwBox, MwStokesParams, c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_stokes_destroy": (c_int32, [c_void_p]),
+    "mw_stokes_device_loops": (c_int32, [c_void_p]),
+    "mw_stokes_uzawa_residual": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_double, c_int32,
+                                           c_void_p, c_void_p, c_void_p]),
     "mw_stokes_levels": (c_int32, [c_void_p, c_int32]),
     "mw_stokes_set_viscosity": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_stokes_apply": (c_int32, [c_void_p] * 6),
@@ -110,6 +114,19 @@ class StokesSolver:
         x = torch.empty_like(b)
         call("mw_stokes_vcycle", self.h, PREC[precision], ptr(b), ptr(x), stream_ptr())
         return x
+
+    def device_loops(self):
+        """True once a solve ran as one recorded graph with its loops on the device."""
+        return bool(L.lib().mw_stokes_device_loops(self.h))
+
+    def uzawa_residual(self, f, h, P, precision="f32", rtol=1e-3, maxit=100, V=None):
+        """||G^T K^-1 (f - G P) - h|| (mean removed): how far pressure P is from the Schur solution,
+        the quantity the Uzawa iteration starts from."""
+        prec = PREC[precision]
+        nrm = c_double()
+        call("mw_stokes_uzawa_residual", self.h, prec, ptr(f), ptr(h), ptr(P), float(rtol), int(maxit), ptr(V),
+             ctypes.byref(nrm), stream_ptr())
+        return nrm.value
 
     def residual(self, V, P, f, h):
         RV = torch.empty(self.nv, dtype=torch.float64, device="cuda")

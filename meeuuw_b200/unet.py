@@ -112,8 +112,9 @@ _bufs = {}
 
 
 def _buf(key, shape, dtype, zero=False):
-    """Scratch tensor reused across calls with the same key (consumed in stream order)."""
-    k = (key, dtype)
+    """Scratch tensor reused across calls with the same key on the same stream (consumed in stream
+    order; models advanced concurrently on different streams never share one)."""
+    k = (key, dtype, torch.cuda.current_stream().cuda_stream)
     b = _bufs.get(k)
     if b is None or tuple(b.shape) != tuple(shape):
         b = (torch.zeros if zero else torch.empty)(shape, dtype=dtype, device="cuda")
@@ -395,44 +396,63 @@ class WarmStart:
 
 
 class LearnedGuess:
-    """Initial-guess hook for ``GPUModel.guess`` with a residual gate.
+    """Initial-guess hook for ``GPUModel.guess`` gated by the Uzawa residual.
 
-    Candidates for the Stokes solve of this step:
-      * ``previous``  - the previous step's solution (what the solver uses without a network);
-      * ``increment`` - previous solution + (network(state now) - network(state of the previous
-                        step)): the network's prediction of how the flow changed;
-      * ``learned``   - the network's prediction alone.
-    Each candidate's FP64 residual norm ||(f, h) - A (V, P)|| is computed with the device operator
-    and the smallest one is handed to the solver, so a poor prediction can never make the solve
-    start from a worse point than the fallback."""
+    The Schur-complement (Uzawa) iteration recomputes the velocity from the pressure, so a
+    candidate is judged by the residual it starts from: ||G^T K^-1 (f - G P) - h|| (one inner
+    multigrid-PCG solve per candidate, ``StokesSolver.uzawa_residual``).  Candidates:
+      * ``zero``      - the cold start (first step, or after ``reset()``);
+      * ``previous``  - the previous step's solution (the method without the network);
+      * ``learned``   - the network's prediction;
+      * ``increment`` - previous solution + (network(now) - network(previous step)).
+    The candidate with the smallest Uzawa residual is handed to the solver, so the network can
+    never make a solve start from a worse point than the fallback.  With ``judge="cold"`` (the
+    default) the network is consulted only when there is no previous solution and the previous
+    step's solution is used directly otherwise; ``judge="every"`` weighs all candidates at every
+    step (one extra inner solve per candidate)."""
 
-    def __init__(self, model, net, n_net=128, candidates=("previous", "increment", "learned")):
+    def __init__(self, model, net, n_net=128, judge="cold", rtol=1e-3):
         c = model.cfg
         self.ws = WarmStart(net, model.box, c.Ra, c.alphaT, model.bc_fix_V, n_net, c.rho0, c.eta_ref / model.L_ref)
-        self.candidates = tuple(candidates)
+        self.judge, self.rtol = judge, rtol
+        self.prec = "f64" if model.stokes_precision == "f64" else "f32"
         E = lambda t: torch.empty_like(t)
         self.nnV, self.nnP = E(model.solV), E(model.solP)          # network fields, this step
         self.prevV, self.prevP = E(model.solV), E(model.solP)      # network fields, previous step
         self.candV, self.candP = E(model.solV), E(model.solP)
-        self.have_prev = False
+        self.have_prev_nn = False
+        self.cold = True
         self.picks = {k: 0 for k in ("previous", "increment", "learned", "zero")}
         self.last = {}
 
+    def reset(self):
+        """Forget the previous solution (the next step is a cold start)."""
+        self.cold = True
+        self.have_prev_nn = False
+
+    def _res(self, m, P):
+        return m.solver.uzawa_residual(m.rhs_f, m.rhs_h, P, precision=self.prec, rtol=self.rtol)
+
     def __call__(self, m):
+        use_nn = self.cold or self.judge == "every"
+        if not use_nn:
+            self.picks["previous"] += 1
+            self.last = dict(pick="previous")
+            self.have_prev_nn = False
+            return
         self.ws.guess(m.T, m.eta_e, self.nnV, self.nnP)
-        S = m.solver
-        first = m.istep == 0 and not self.have_prev
         res = {}
-        if "previous" in self.candidates and not first:
-            res["previous"] = S.residual(m.solV, m.solP, m.rhs_f, m.rhs_h)[2]
-        elif first:
-            res["zero"] = S.residual(torch.zeros_like(m.solV), torch.zeros_like(m.solP), m.rhs_f, m.rhs_h)[2]
-        if "learned" in self.candidates:
-            res["learned"] = S.residual(self.nnV, self.nnP, m.rhs_f, m.rhs_h)[2]
-        if "increment" in self.candidates and self.have_prev and not first:
-            torch.add(m.solV, self.nnV - self.prevV, out=self.candV)
-            torch.add(m.solP, self.nnP - self.prevP, out=self.candP)
-            res["increment"] = S.residual(self.candV, self.candP, m.rhs_f, m.rhs_h)[2]
+        zeroP = None
+        if self.cold:
+            zeroP = torch.zeros_like(m.solP)
+            res["zero"] = self._res(m, zeroP)
+        else:
+            res["previous"] = self._res(m, m.solP)
+            if self.have_prev_nn:
+                torch.add(m.solV, self.nnV - self.prevV, out=self.candV)
+                torch.add(m.solP, self.nnP - self.prevP, out=self.candP)
+                res["increment"] = self._res(m, self.candP)
+        res["learned"] = self._res(m, self.nnP)
         best = min(res, key=lambda k: res[k] if math.isfinite(res[k]) else math.inf)
         if best == "learned":
             m.solV.copy_(self.nnV)
@@ -447,21 +467,23 @@ class LearnedGuess:
         self.last = dict(res, pick=best)
         self.nnV, self.prevV = self.prevV, self.nnV
         self.nnP, self.prevP = self.prevP, self.nnP
-        self.have_prev = True
+        self.have_prev_nn = True
+        self.cold = False
 
 
 def compare_guesses(net, cfg, nsteps=20, n_net=128, tol=1e-8, host=None):
-    """Run the same model three times (zero guess, previous-step guess, gated learned guess) and
-    return the Stokes iteration counts and residuals of each step."""
+    """Run the same model with the zero guess, the previous-step guess, the gated learned guess
+    consulted at cold starts only, and the gated learned guess weighed at every step; return the
+    Stokes iteration counts of each step."""
     from . import configs
     from .timestep import GPUModel
     host = host if host is not None else configs.build_host_model(cfg)
     out = {}
-    for mode in ("zero", "previous", "learned"):
+    for mode in ("zero", "previous", "learned", "learned_every"):
         m = GPUModel(cfg, host, stokes="mixed", tol=tol, warm_start="zero" if mode == "zero" else "previous")
         hook = None
-        if mode == "learned":
-            hook = LearnedGuess(m, net, n_net=n_net)
+        if mode.startswith("learned"):
+            hook = LearnedGuess(m, net, n_net=n_net, judge="every" if mode == "learned_every" else "cold")
             m.guess = hook
         rec = []
         for _ in range(nsteps):
@@ -472,5 +494,35 @@ def compare_guesses(net, cfg, nsteps=20, n_net=128, tol=1e-8, host=None):
         d = m.diagnostics()
         out[mode] = dict(steps=rec, outer=sum(r["outer"] for r in rec), inner=sum(r["inner"] for r in rec),
                          vrms=d["vrms"], Nu=d["Nu"], picks=dict(hook.picks) if hook else None)
+        del m
+    return out
+
+
+def cold_start_gain(net, cases, steps_before=0, n_net=128, tol=1e-8, log=None):
+    """cases: [(cfg, seed of a random smooth initial temperature or None)].  For each model: advance
+    `steps_before` steps, then solve the next step's Stokes problem twice on the same operator,
+    from zero and from the network's guess for the state that solve sees.  Returns
+    [(name, zero outer iterations, learned outer iterations, zero inner, learned inner)]."""
+    from . import configs
+    from .timestep import GPUModel
+    out = []
+    for cfg, tseed in cases:
+        host = configs.build_host_model(cfg)
+        if tseed is not None:
+            host.arrays["T"] = random_temperature(host.x_V, host.z_V, np.random.default_rng(tseed))
+        m = GPUModel(cfg, host, stokes="mixed", tol=tol)
+        rec = _Recorder(m)
+        m.guess = rec
+        for _ in range(steps_before + 1):
+            m.step()
+        ws = WarmStart(net, m.box, cfg.Ra, cfg.alphaT, m.bc_fix_V, n_net, cfg.rho0, cfg.eta_ref / m.L_ref)
+        V = torch.empty_like(m.solV)
+        P = torch.empty_like(m.solP)
+        ws.guess(rec.T, rec.eta, V, P)
+        _, _, i0 = m.solver.solve(m.rhs_f, m.rhs_h, None, None, precision="mixed", tol=tol, inner_rtol=1e-3)
+        _, _, i1 = m.solver.solve(m.rhs_f, m.rhs_h, V, P, precision="mixed", tol=tol, inner_rtol=1e-3)
+        out.append((cfg.name, i0["outer_iters"], i1["outer_iters"], i0["inner_iters"], i1["inner_iters"]))
+        if log:
+            log(f"cold start {cfg.name}: zero {i0['outer_iters']} / learned {i1['outer_iters']} outer iterations")
         del m
     return out

@@ -112,3 +112,27 @@ def test_noslip_rayleigh_taylor_box_solve():
     f, h = torch.as_tensor(c["f"]).cuda(), torch.as_tensor(c["h"]).cuda()
     V, P, info = S.solve(f, h, precision="mixed", tol=1e-8)
     assert info["converged"] == 1, info
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_device_loops_reproduce_host_loops(precision):
+    """The solve recorded as one CUDA graph (loops as conditional nodes, decided on the device) runs
+    the same kernels in the same order as the host-driven loops: same iterates, same counts.  Two
+    solves in a row exercise the replay of the recorded graph."""
+    c = make_case(32, 32, contrast=1e3)
+    f, h = torch.as_tensor(c["f"]).cuda(), torch.as_tensor(c["h"]).cuda()
+    out = {}
+    for host in (1, 0):
+        S = solver_for(c)
+        runs = []
+        for _ in range(2):
+            V, P, info = S.solve(f, h, precision=precision, tol=1e-8, host_loops=host)
+            runs.append((V.cpu().numpy(), P.cpu().numpy(), info))
+        assert S.device_loops() == (host == 0)
+        out[host] = runs
+    for (Vh, Ph, ih), (Vd, Pd, idv) in zip(out[1], out[0]):
+        assert idv["converged"] == 1 and ih["converged"] == 1, (ih, idv)
+        for k in ("outer_iters", "inner_iters", "refinements"):
+            assert idv[k] == ih[k], (k, ih, idv)
+        assert abs(idv["rel_residual"] - ih["rel_residual"]) <= 1e-6 * ih["rel_residual"]
+        assert rel_err(Vd, Vh) < 1e-12 and rel_err(Pd, Ph) < 1e-12

@@ -47,9 +47,13 @@ def compute_Nu(Lx, Lz, x_V, z_V, nel, left_element, right_element, top_element, 
     out = torch.empty(13, dtype=f64, device="cuda")
     b = box(nx, nz, Lx=Lx, Lz=Lz)
     wp, wb = ops.workspace("nu").get(L.lib().mw_nu_workspace_bytes(b))
-    call("mw_compute_nu", b, ptr(dev(T, f64)), ptr(dev(dTdx_nodal, f64)), ptr(dev(dTdz_nodal, f64)),
-         ptr(dev(hcond_n, f64)), g, ptr(out), wp, wb, stream_ptr())
-    return tuple(np.float64(x) for x in out.cpu().numpy())
+    # keep the device copies referenced until the kernels have run (the caching allocator would
+    # otherwise hand a freed copy's memory to the next one)
+    args = [dev(a, f64) for a in (T, dTdx_nodal, dTdz_nodal, hcond_n)]
+    call("mw_compute_nu", b, *[ptr(a) for a in args], g, ptr(out), wp, wb, stream_ptr())
+    res = out.cpu().numpy()
+    del args
+    return tuple(np.float64(x) for x in res)
 
 
 __all__ = ["compute_global_quantities", "compute_Nu"]

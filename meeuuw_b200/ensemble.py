@@ -56,6 +56,9 @@ class Ensemble:
             self.streams.append(st)
             self.models.append(m)
         torch.cuda.synchronize()
+        self.active = [True] * len(self.models)
+        self.retired = {}            # model index -> the reference's abort message
+        self.steps_done = 0          # model-steps taken by active models
         self.threads = 0
         self.pool = None
         self.set_threads(threads)
@@ -69,18 +72,31 @@ class Ensemble:
             self.threads = threads
 
     def _run(self, idx):
+        done = 0
         for i in idx:
             with torch.cuda.stream(self.streams[i]):
-                self.models[i].step()
+                m = self.models[i]
+                m.step()
+                done += 1
+                if int(m.err.item()):
+                    # the reference would abort this run (an empty element, a particle outside
+                    # the box): retire the model, keep the others going
+                    try:
+                        m.check()
+                        self.retired[i] = f"device flags {int(m.err.item())}"
+                    except SystemExit as e:
+                        self.retired[i] = str(e)
+                    self.active[i] = False
+        return done
 
     def step(self):
-        """One time step of every model.  Models are dealt to the threads largest first, so each
-        thread gets a similar amount of work."""
-        order = sorted(range(len(self.models)), key=lambda i: -self.models[i].nel)
+        """One time step of every active model.  Models are dealt to the threads largest first, so
+        each thread gets a similar amount of work."""
+        order = sorted((i for i in range(len(self.models)) if self.active[i]), key=lambda i: -self.models[i].nel)
         parts = [order[t::self.threads] for t in range(self.threads)]
         futs = [self.pool.submit(self._run, p) for p in parts if p]
         for f in futs:
-            f.result()
+            self.steps_done += f.result()
 
     def synchronize(self):
         for st in self.streams:
@@ -90,8 +106,10 @@ class Ensemble:
         return [m.diagnostics() for m in self.models]
 
     def check(self):
-        for m in self.models:
-            m.check()
+        """SystemExit when any model still stepping has a device flag set."""
+        for i, m in enumerate(self.models):
+            if self.active[i]:
+                m.check()
 
     def close(self):
         if self.pool is not None:

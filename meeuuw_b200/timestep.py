@@ -90,9 +90,31 @@ class GPUModel:
         q.update(self.geo)
         return q
 
+    def enable_phase_timing(self, on=True):
+        """Record CUDA events between the phases of each step (read with phase_times())."""
+        self._phases = [] if on else None
+
+    def _mark(self, name):
+        if getattr(self, "_phases", None) is not None:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            self._phases.append((name, ev))
+
+    def phase_times(self):
+        """{phase: milliseconds} summed over the steps recorded since enable_phase_timing()."""
+        ph = getattr(self, "_phases", None) or []
+        torch.cuda.synchronize()
+        out = {}
+        for (n0, e0), (n1, e1) in zip(ph, ph[1:]):
+            if n0 == "end":
+                continue
+            out[n0] = out.get(n0, 0.0) + e0.elapsed_time(e1)
+        return out
+
     def step(self):
         c, b, tb = self.cfg, self.box, self.tables
         P = self.props
+        self._mark("particles+projections")
         # particle fields + material (meeuuw.py:1118-1154)
         nodal = dict(exx=self.exx_n, ezz=self.ezz_n, exz=self.exz_n, q=self.q, T=self.T if c.solve_T else None)
         ops.interp_material(b, self.active, self.r, self.t, self.iel, self.mat, nodal, self.material, P)
@@ -117,6 +139,7 @@ class GPUModel:
         if c.formulation == "EBA":
             for k in ("exx", "ezz", "exz"):
                 ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], getattr(self, k + "_n"), qf[k + "q"])
+        self._mark("stokes")
         # Stokes (meeuuw.py:1705-1851): right-hand side, matrix-free solve
         if self.zero_bc_values:
             ops.stokes_rhs_body(b, qf["rhoq"], self.gxq, self.gzq, self.geo["JxWq"], tb["N_V"], self.bc_fix_V,
@@ -134,6 +157,7 @@ class GPUModel:
                                        precision=self.stokes_precision, tol=self.tol, inner_rtol=self.inner_rtol)
         self.last_solve = info
         ops.split_solution(self.solV, self.solP, c.eta_ref / self.L_ref, self.u, self.w, self.p)
+        self._mark("post+dt")
         # pressure normalisation and nodal pressure (meeuuw.py:1958-2051)
         ops.pressure_offset(b, c.pressure_normalisation, self.p, tb["N_P"], self.geo["JxWq"], self.volume, self.offset)
         ops.nodal_pressure(b, self.p, self.offset, tb["N_P_n"], self.q, subtract=True)
@@ -143,6 +167,7 @@ class GPUModel:
         ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], self.u, qf["uq"])
         ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], self.w, qf["wq"])
         if c.solve_T:
+            self._mark("energy")
             # energy (meeuuw.py:2186-2235); T on entry is T_mem
             q = {k: qf[k] for k in ("rhoq", "etaq", "Tq", "uq", "wq", "hcondq", "hcapaq", "alphaq", "hprodq")}
             for k in ("exxq", "ezzq", "exzq"):
@@ -154,15 +179,18 @@ class GPUModel:
             # heat flux and Nu (meeuuw.py:2259-2308)
             ops.nodal_heat_flux(b, self.T, nd["hcond"], tb, out=self.hf)
             ops.compute_nu(b, self.T, self.hf[0], self.hf[1], nd["hcond"], self.nu_out)
+        self._mark("strain+vrms")
         # nodal strain rate for the next step's particles (meeuuw.py:2385)
         ops.nodal_strain_rate(b, self.u, self.w, tb, out=[self.exx_n, self.ezz_n, self.exz_n])
         # vrms (meeuuw.py:2512; uses the Tq of this step as the reference does)
         ops.global_quantities(qf["uq"], qf["wq"], qf["Tq"] if c.solve_T else None, qf["rhoq"], self.geo["JxWq"],
                               self.volume, self.gq_out)
+        self._mark("advect+locate")
         # advect and locate (meeuuw.py:2726, 2862)
         ops.advect(b, c.RKorder, 0.0, self.x, self.z, self.active, self.u, self.w, self.up, self.wp, self.err,
                    dt_dev=self.dt_out)
         ops.locate(b, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
+        self._mark("end")
         self.istep += 1
 
     def diagnostics(self):

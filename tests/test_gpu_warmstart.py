@@ -1,0 +1,59 @@
+"""What the trained warm-start network gains over the method without it.
+
+The network (meeuuw_b200/weights/unet_fk128.npz, trained on the GPU by
+``python -m meeuuw_b200.train_warmstart`` from snapshots of the device time stepper) is applied to
+held-out models -- seeds, Ra, viscosity contrasts and initial temperatures it never saw -- at a cold
+start, where the method has no previous solution to start from.  The Stokes solve to 1e-8 from the
+network's guess needs fewer Schur (Uzawa) iterations than the solve from zero, and the gated hook
+never starts a solve from a worse Uzawa residual than its fallback."""
+import math
+import os
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(__file__)), "meeuuw_b200", "weights", "unet_fk128.npz")
+
+
+def _cases(k, n=128):
+    from meeuuw_b200 import configs
+    rng = np.random.default_rng(4242)
+    out = []
+    for i in range(k):
+        Ra = math.exp(rng.uniform(math.log(3e4), math.log(1e6)))
+        c = math.exp(rng.uniform(math.log(10.0), math.log(1e5)))
+        out.append((replace(configs.fk_convection(n), name=f"t{i}", Ra=Ra, fk_gamma=math.log(c), seed=31000 + i),
+                    71000 + i))
+    return out
+
+
+def test_learned_cold_start_needs_fewer_uzawa_iterations():
+    from meeuuw_b200.unet import UNet, cold_start_gain
+    net = UNet.load(WEIGHTS)
+    res = cold_start_gain(net, _cases(3), steps_before=5)
+    zero = sum(r[1] for r in res)
+    learned = sum(r[2] for r in res)
+    assert learned < zero, res
+
+
+def test_gate_never_starts_worse_than_fallback():
+    from meeuuw_b200 import configs
+    from meeuuw_b200.timestep import GPUModel
+    from meeuuw_b200.unet import LearnedGuess, UNet, random_temperature
+    net = UNet.load(WEIGHTS)
+    cfg, tseed = _cases(1)[0]
+    host = configs.build_host_model(cfg)
+    host.arrays["T"] = random_temperature(host.x_V, host.z_V, np.random.default_rng(tseed))
+    m = GPUModel(cfg, host, stokes="mixed")
+    hook = LearnedGuess(m, net, judge="every")
+    m.guess = hook
+    for _ in range(4):
+        m.step()
+        last = dict(hook.last)
+        pick = last.pop("pick")
+        fallback = last["zero"] if "zero" in last else last["previous"]
+        assert last[pick] <= fallback, hook.last
+        assert m.last_solve["converged"] == 1

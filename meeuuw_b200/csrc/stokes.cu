@@ -253,10 +253,6 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
-  // FP32: the tile's quadrature viscosities, staged with coalesced loads (each tile row of 17
-  // elements is 153 contiguous values); FP64 reads them per element (shared memory is full)
-  constexpr bool STAGE_ETA = sizeof(R) == 4;
-  __shared__ R seta[STAGE_ETA ? NEL_T * 9 : 1];
   const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
@@ -286,13 +282,6 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
       sp[i] = (px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz) ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
     }
-  if (STAGE_ETA)
-    for (int i = tid; i < NEL_T * 9; i += APPLY_THREADS) {
-      const int lez = i / (EX * 9), rem = i - lez * (EX * 9);
-      const int ex = ex0 - 1 + rem / 9, ez = ez0 - 1 + lez;
-      seta[i] = (ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz)
-                    ? a.eta[((int64_t)ez * g.nx + ex0 - 1) * 9 + rem] : R(0);
-    }
   __syncthreads();
   // ---- element products ----
   if (tid < NEL_T) {
@@ -310,14 +299,9 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) pe[k] = use_p ? sp[(lez + q1_dz(k)) * PX + lex + q1_dx(k)] : R(0);
       R eq[9];
-      if (STAGE_ETA) {
+      const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) eq[q] = seta[tid * 9 + q];       // tid = lez * EX + lex
-      } else {
-        const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) eq[q] = eg[q];
-      }
+      for (int q = 0; q < 9; ++q) eq[q] = eg[q];
       element_apply<R>(R(2.0 / g.hx), R(2.0 / g.hz), R(g.hx * g.hz / 4.0), R(g.s), ue, pe, eq, ye, ype, use_p);
 #pragma unroll
       for (int k = 0; k < 18; ++k) sye[tid * 22 + k] = ye[k];

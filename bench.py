@@ -203,6 +203,20 @@ def run_ours(args):
                  "phases_ms_per_step": phases(pmodel)}
         del pmodel
 
+    # ---- accuracy: both arms advanced the same steps from the same state ----
+    accuracy = None
+    if not args.no_plain:
+        ma, mb = GPUModel(cfg, host, stokes="mixed", tol=1e-8), GPUModel(cfg, host, stokes="f64", tol=1e-8)
+        na = 5
+        for _ in range(na):
+            ma.step()
+            mb.step()
+        da, db = ma.diagnostics(), mb.diagnostics()
+        accuracy = {"steps": na, "vrms_rel_diff": abs(da["vrms"] - db["vrms"]) / abs(db["vrms"]),
+                    "Nu_rel_diff": abs(da["Nu"] - db["Nu"]) / abs(db["Nu"]),
+                    "T_max_abs_diff": float((ma.T - mb.T).abs().max().item())}
+        del ma, mb
+
     # ---- end to end through host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -234,6 +248,7 @@ def run_ours(args):
             "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
             "last_step": {"vrms": diag["vrms"], "Nu": diag["Nu"], "dt": diag["dt"], "stokes": diag["stokes"]},
             "phases_ms_per_step": phase_ms,
+            "mixed_vs_fp64": accuracy,
             "warm_start_picks": dict(learned.picks) if learned else None,
             "cpu_baseline": cpu,
         }

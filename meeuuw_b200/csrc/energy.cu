@@ -8,6 +8,8 @@
 // BiCGSTAB in FP64 to a relative residual tolerance.
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "common.cuh"
 
@@ -88,6 +90,16 @@ __global__ void k_bicg_p(int64_t n, const double* __restrict__ s, const double* 
     p[i] = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);   // first pass never reads p, v
 }
 
+// the same update with the first-iteration switch read from the device iteration count sc[12]
+__global__ void k_bicg_p_dev(int64_t n, const double* __restrict__ s, const double* __restrict__ r,
+                             const double* __restrict__ v, double* __restrict__ p) {
+  const bool first = s[12] == 0.0;
+  const double beta = first ? 0.0 : (s[0] / s[1]) * (s[2] / s[3]);
+  const double om = first ? 0.0 : s[3];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);
+}
+
 __global__ void k_scale_diag(int64_t n, const double* __restrict__ x, const double* __restrict__ d,
                              double* __restrict__ y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -122,6 +134,35 @@ __global__ void k_bicg_roll(double* sc) {
   sc[1] = sc[0];
 }
 
+// ---- the iteration as a recorded CUDA graph with a device WHILE loop ----
+// sc[12] = iteration count; the loop runs while the residual is finite, above rtol * ||b|| and
+// the count is below maxit.
+__global__ void k_bicg_init(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h) {
+  if (!(sc[10] > 0)) sc[10] = 1.0;
+  sc[12] = 0;
+  const double rr = sc[11];
+  cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && maxit > 0) ? 1u : 0u);
+}
+
+__global__ void k_bicg_check(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h) {
+  const double it = sc[12] + 1;
+  sc[12] = it;
+  const double rr = sc[11];
+  cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && it < (double)maxit) ? 1u : 0u);
+}
+
+struct EnergyGraph {
+  int dev;
+  const void *VV, *rhs, *T, *work;
+  int nelx, nelz, maxit;
+  double rtol;
+  cudaGraphExec_t exec;
+};
+static std::vector<EnergyGraph> g_energy_graphs;
+static std::mutex g_energy_mutex;
+static cudaStream_t g_energy_stream[64], g_energy_body[64];   // library stream, body-capture stream
+static cudaEvent_t g_energy_ev[64][2];
+
 }  // namespace mw
 
 using namespace mw;
@@ -140,9 +181,85 @@ int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y,
   return MW_OK;
 }
 
+// Records the BiCGSTAB solve on the capturing stream s (body captured on b); false on failure.
+static bool energy_record(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int maxit,
+                          void* work, cudaStream_t s, cudaStream_t b);
+
+// The solve from a graph recorded once per (device, buffers, sizes, rtol, maxit).  A caller's own
+// (non-default) stream is captured and launched on directly, so solves of models on different
+// streams run concurrently; the legacy default stream, which cannot be captured, is served through
+// a library stream ordered after / before it by events.  Returns false when no graph can be used.
+static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol,
+                               int32_t maxit, int32_t* iters, double* relres, void* work, cudaStream_t caller) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+  const bool legacy = caller == nullptr || caller == cudaStreamLegacy || caller == cudaStreamPerThread;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t s = caller;
+  {
+    std::lock_guard<std::mutex> lock(g_energy_mutex);
+    if (!g_energy_body[dev]) {
+      if (cudaStreamCreateWithFlags(&g_energy_stream[dev], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&g_energy_body[dev], cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&g_energy_ev[dev][0], cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&g_energy_ev[dev][1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+      }
+    }
+    if (legacy) s = g_energy_stream[dev];
+    for (auto& e : g_energy_graphs)
+      if (e.dev == dev && e.VV == VV_T && e.rhs == rhs && e.T == T && e.work == work && e.nelx == box.nelx &&
+          e.nelz == box.nelz && e.maxit == maxit && e.rtol == rtol) { exec = e.exec; break; }
+    if (!exec) {
+      if (g_energy_graphs.size() >= 512) return false;
+      cudaStream_t rec = g_energy_stream[dev];   // recording only records: any capturable stream will do
+      if (cudaStreamBeginCapture(rec, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { cudaGetLastError(); return false; }
+      bool ok = energy_record(box, VV_T, rhs, T, rtol, maxit, work, rec, g_energy_body[dev]);
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(g_energy_body[dev], &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+        cudaGraph_t gb = nullptr;
+        cudaStreamEndCapture(g_energy_body[dev], &gb);
+        ok = false;
+      }
+      cudaGraph_t g = nullptr;
+      ok = cudaStreamEndCapture(rec, &g) == cudaSuccess && g && ok && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+      if (g) cudaGraphDestroy(g);
+      if (!ok) { cudaGetLastError(); return false; }
+      g_energy_graphs.push_back({dev, VV_T, rhs, T, work, box.nelx, box.nelz, maxit, rtol, exec});
+    }
+    if (legacy) {   // the library stream is shared: keep this path serialised
+      cudaEventRecord(g_energy_ev[dev][0], caller);
+      cudaStreamWaitEvent(s, g_energy_ev[dev][0], 0);
+      if (cudaGraphLaunch(exec, s) != cudaSuccess) { cudaGetLastError(); return false; }
+      cudaEventRecord(g_energy_ev[dev][1], s);
+      cudaStreamWaitEvent(caller, g_energy_ev[dev][1], 0);
+    }
+  }
+  if (!legacy && cudaGraphLaunch(exec, s) != cudaSuccess) { cudaGetLastError(); return false; }
+  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  const double* sc = (const double*)work + 9 * n + 300;
+  double q[3];
+  cudaMemcpyAsync(q, sc + 10, sizeof(q), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return false;
+  if (iters) *iters = (int32_t)q[2];
+  if (relres) *relres = std::sqrt(q[1] / q[0]);
+  return true;
+}
+
 int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
                     int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream) {
   if (work_bytes < mw_energy_solve_workspace_bytes(box) || maxit < 1) return MW_ERR_BAD_ARG;
+  {
+    int32_t it = 0;
+    double rel = 0;
+    if (energy_solve_graph(box, VV_T, rhs, T, rtol, maxit, &it, &rel, work, (cudaStream_t)stream)) {
+      if (iters) *iters = it;
+      if (relres) *relres = rel;
+      if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
+      return rel <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
+    }
+  }
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
   double* w = (double*)work;
@@ -194,3 +311,58 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
 }
 
 }  // extern "C"
+
+static bool energy_record(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int maxit,
+                          void* work, cudaStream_t s, cudaStream_t b) {
+  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  double* w = (double*)work;
+  double *r = w, *r0 = w + n, *p = w + 2 * n, *v = w + 3 * n, *sv = w + 4 * n, *t = w + 5 * n, *ph = w + 6 * n,
+         *sh = w + 7 * n, *dg = w + 8 * n;
+  double* part = w + 9 * n;
+  double* sc = part + 300;
+  const int NBk = 296;
+  auto dot = [&](const double* a, const double* b2, double* out, cudaStream_t st) {
+    k_edot_partial<<<NBk, 256, 0, st>>>(n, a, b2, part);
+    k_edot_final<<<1, 256, 0, st>>>(part, NBk, out);
+  };
+  k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, T, rhs, r, dg, 1);
+  cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+  dot(rhs, rhs, sc + 10, s);
+  dot(r, r, sc + 11, s);
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr) != cudaSuccess) return false;
+  cudaGraphConditionalHandle h;
+  if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
+  k_bicg_init<<<1, 1, 0, s>>>(sc, rtol, maxit, h);
+  if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd) != cudaSuccess) return false;
+  cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
+  prm.conditional.handle = h;
+  prm.conditional.type = cudaGraphCondTypeWhile;
+  prm.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, deps, nd, &prm) != cudaSuccess) return false;
+  if (cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess) return false;
+  if (cudaStreamBeginCaptureToGraph(b, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                    cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return false;
+  // body: one BiCGSTAB iteration (the host loop's kernels, first-iteration branch on sc[12])
+  dot(r0, r, sc + 0, b);
+  k_bicg_p_dev<<<grid_for(n, 256), 256, 0, b>>>(n, sc, r, v, p);
+  k_scale_diag<<<grid_for(n, 256), 256, 0, b>>>(n, p, dg, ph);
+  k_energy_matvec<<<grid_for(n, 256), 256, 0, b>>>(box, VV_T, ph, nullptr, v, nullptr, 0);
+  dot(r0, v, sc + 4, b);
+  k_bicg_s<<<grid_for(n, 256), 256, 0, b>>>(n, sc, r, v, sv);
+  k_scale_diag<<<grid_for(n, 256), 256, 0, b>>>(n, sv, dg, sh);
+  k_energy_matvec<<<grid_for(n, 256), 256, 0, b>>>(box, VV_T, sh, nullptr, t, nullptr, 0);
+  dot(t, sv, sc + 5, b);
+  dot(t, t, sc + 6, b);
+  k_bicg_x<<<grid_for(n, 256), 256, 0, b>>>(n, sc, ph, sh, sv, t, T, r);
+  k_bicg_roll<<<1, 32, 0, b>>>(sc);
+  dot(r, r, sc + 11, b);
+  k_bicg_check<<<1, 1, 0, b>>>(sc, rtol, maxit, h);
+  cudaGraph_t gb = nullptr;
+  return cudaStreamEndCapture(b, &gb) == cudaSuccess;
+}

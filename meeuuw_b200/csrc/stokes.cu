@@ -1852,7 +1852,7 @@ void mw_solve_default_params(mw_solve_params* p) {
   memset(p, 0, sizeof(*p));
   p->scheme = MW_SCHEME_CD_U_ETA; p->precision = MW_F64; p->tol = 1e-8; p->max_outer = 200;
   p->max_inner = 500; p->inner_rtol = 1e-10; p->max_refine = 20; p->sweep_reduction = 1e-3;
-  p->mass_iters = 36; p->use_guess = 0;
+  p->mass_iters = 12; p->use_guess = 0;
 }
 
 size_t mw_stokes_workspace_bytes(mw_box box, mw_stokes_params prm) {

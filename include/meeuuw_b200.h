@@ -325,6 +325,12 @@ int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, vo
 int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,
                       int32_t* iters, double* relres, void* stream);
 
+/* Result of the last solve from its device scalars (synchronises `stream`).  When mw_stokes_solve is
+ * called on a stream that is recording a CUDA graph, the solve is recorded into that graph (its
+ * loops as conditional nodes), returns MW_OK with a zeroed info, and this call reads the outcome
+ * after a replay; converged = rel_residual <= tol. */
+int mw_stokes_device_info(mw_stokes* S, double tol, mw_solve_info* info, void* stream);
+
 /* 1 when this solver has run a solve as one recorded CUDA graph with device-side loops (the
  * default), 0 when it fell back to host-driven loops. */
 int mw_stokes_device_loops(const mw_stokes* S);
@@ -359,6 +365,11 @@ int mw_elemental_to_qpoints(int64_t nel, const double* a, const double* b, doubl
 /* y = A x with A the summed element matrices VV_T (nel*81, build_matrix_energy.py:133-137). */
 int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y, void* stream);
 
+/* Iterations and relative residual of the last energy solve from the device scalars in `work`
+ * (synchronises).  When mw_energy_solve is called on a stream that is recording a CUDA graph the
+ * solve is recorded into it (a device-side loop) and reports 0 / 0; read the outcome here after a
+ * replay. */
+int mw_energy_device_info(mw_box box, const void* work, int32_t* iters, double* relres, void* stream);
 /* T = A^-1 rhs (replaces spsolve of coo_matrix((VV_T,(II_T,JJ_T))).tocsr(), meeuuw.py:2232-2235):
  * Jacobi-preconditioned BiCGSTAB in FP64 from the initial guess in T, to rtol. */
 size_t mw_energy_solve_workspace_bytes(mw_box box);

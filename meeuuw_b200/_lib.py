@@ -114,6 +114,7 @@ _PROTOS = {
     "mw_elemental_to_qpoints": (c_int32, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_energy_matvec": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_energy_solve_workspace_bytes": (c_size_t, [MwBox]),
+    "mw_energy_device_info": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_energy_solve": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
                                   c_void_p, c_size_t, c_void_p]),
 }

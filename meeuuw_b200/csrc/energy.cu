@@ -174,6 +174,18 @@ size_t mw_energy_solve_workspace_bytes(mw_box box) {
   return (size_t)(9 * nn + 512) * sizeof(double);
 }
 
+int mw_energy_device_info(mw_box box, const void* work, int32_t* iters, double* relres, void* stream) {
+  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  const double* sc = (const double*)work + 9 * n + 300;
+  double q[3];
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaMemcpyAsync(q, sc + 10, sizeof(q), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return MW_ERR_CUDA;
+  if (iters) *iters = (int32_t)q[2];
+  if (relres) *relres = std::sqrt(q[1] / q[0]);
+  return MW_OK;
+}
+
 int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y, void* stream) {
   int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
   k_energy_matvec<<<grid_for(nn, 256), 256, 0, (cudaStream_t)stream>>>(box, VV_T, x, nullptr, y, nullptr, 0);
@@ -250,6 +262,23 @@ static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs
 int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
                     int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream) {
   if (work_bytes < mw_energy_solve_workspace_bytes(box) || maxit < 1) return MW_ERR_BAD_ARG;
+  {  // the caller is recording a graph: record the solve into it, results stay on the device
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStream_t cs_stream = (cudaStream_t)stream;
+    if (cs_stream != nullptr && cudaStreamIsCapturing(cs_stream, &cs) == cudaSuccess &&
+        cs == cudaStreamCaptureStatusActive) {
+      int dev = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MW_ERR_CUDA;
+      std::lock_guard<std::mutex> lock(g_energy_mutex);
+      if (!g_energy_body[dev] && cudaStreamCreateWithFlags(&g_energy_body[dev], cudaStreamNonBlocking) != cudaSuccess)
+        return MW_ERR_CUDA;
+      if (!energy_record(box, VV_T, rhs, T, rtol, maxit, work, cs_stream, g_energy_body[dev])) return MW_ERR_CUDA;
+      if (iters) *iters = 0;
+      if (relres) *relres = 0;
+      return MW_OK;
+    }
+    cudaGetLastError();
+  }
   {
     int32_t it = 0;
     double rel = 0;

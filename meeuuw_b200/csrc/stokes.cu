@@ -1247,9 +1247,17 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
       int dev = 0, optin = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-      if (smem <= (size_t)optin &&
+      // the attribute is set once per device and size (so that a setup recorded into a CUDA graph
+      // issues no attribute call)
+      static size_t smem_set[64] = {0};
+      bool smem_ok = dev >= 0 && dev < 64 && smem <= smem_set[dev];
+      if (!smem_ok && smem <= (size_t)optin &&
           cudaFuncSetAttribute(k_gauss_jordan_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-              cudaSuccess)
+              cudaSuccess) {
+        smem_ok = true;
+        if (dev >= 0 && dev < 64) smem_set[dev] = smem;
+      }
+      if (smem_ok)
         k_gauss_jordan_smem<<<1, 1024, smem, s>>>(H.nd, H.Ainv);
       else
         k_gauss_jordan<<<1, 1024, sizeof(double) * H.nd, s>>>(H.nd, H.Ainv);
@@ -1882,6 +1890,24 @@ int mw_stokes_destroy(mw_stokes* S) {
   return MW_OK;
 }
 
+int mw_stokes_device_info(mw_stokes* S, double tol, mw_solve_info* info, void* stream) {
+  if (!info) return MW_ERR_BAD_ARG;
+  double q[40];
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaMemcpyAsync(q, S->sc + 64, sizeof(q), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) return MW_ERR_CUDA;
+  const double bnorm = q[S_BNORM - 64];
+  memset(info, 0, sizeof(*info));
+  info->outer_iters = (int)q[I_OUTER - 64];
+  info->inner_iters = (int)q[I_INNER - 64];
+  info->refinements = (int)q[S_NREF - 64];
+  info->initial_rel_residual = bnorm > 0 ? q[S_REL0 - 64] : 0.0;
+  info->rel_residual = bnorm > 0 ? q[T_REL - 64] : 0.0;
+  if (q[I_STATUS - 64] != 0 || !std::isfinite(bnorm)) info->rel_residual = NAN;
+  info->converged = info->rel_residual <= tol ? 1 : 0;
+  return MW_OK;
+}
+
 int mw_stokes_device_loops(const mw_stokes* S) {
   if (!S->device_loops) return 0;
   for (const auto& e : S->graphs)
@@ -2036,9 +2062,27 @@ static int stokes_solve(mw_stokes* S, const double* f, const double* h, double* 
 static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
                              const mw_solve_params& sp, mw_solve_info* info, cudaStream_t s);
 
+// The caller is recording a CUDA graph (a whole time step) on `caller`: record the solve into that
+// capture -- its loops as conditional nodes -- and leave the result scalars on the device
+// (mw_stokes_device_info reads them after a replay).
+static int stokes_solve_in_capture(mw_stokes* S, const double* f, const double* h, double* solV, double* solP,
+                                   const mw_solve_params& sp, mw_solve_info* info, cudaStream_t caller) {
+  if (!f || !h || !solV || !solP || sp.host_loops) return MW_ERR_BAD_ARG;
+  for (auto& b : S->bs)
+    if (!b && cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking) != cudaSuccess) return MW_ERR_CUDA;
+  if (int rc = ensure_hierarchy(S, sp.precision == MW_F32 ? MW_F32 : MW_F64, caller)) return rc;
+  if (!stokes_solve_record(S, f, h, solV, solP, sp, caller)) return MW_ERR_CUDA;
+  if (info) memset(info, 0, sizeof(*info));
+  return MW_OK;
+}
+
 int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
                     mw_solve_info* info, void* stream) {
   cudaStream_t caller = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (caller != nullptr && cudaStreamIsCapturing(caller, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+    return stokes_solve_in_capture(S, f, h, solV, solP, sp, info, caller);
+  cudaGetLastError();
   cudaStream_t s = enter(S, caller);
   int rc = stokes_solve(S, f, h, solV, solP, sp, info, s);
   leave(S, caller, s);

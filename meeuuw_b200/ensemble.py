@@ -44,15 +44,20 @@ def sample_configs(n_models=64, seed=0, n_range=(64, 192), Ra_range=(1e4, 1e7), 
 class Ensemble:
     """N independent models, each on its own stream, stepped concurrently by `threads` host threads."""
 
-    def __init__(self, cfgs, stokes="mixed", threads=8, tol=1e-8, guess=None):
+    def __init__(self, cfgs, stokes="mixed", threads=8, tol=1e-8, guess=None, graphs=False):
+        """graphs=True records each model's whole time step as one CUDA graph (after one eager
+        step); a step of the ensemble is then one graph launch per model, issued from one thread."""
         self.cfgs = list(cfgs)
         self.streams, self.models = [], []
+        self.graphs = bool(graphs) and guess is None
         for cfg in self.cfgs:
             st = torch.cuda.Stream()
             with torch.cuda.stream(st):
                 m = GPUModel(cfg, stokes=stokes, tol=tol)
                 if guess is not None:
                     m.guess = guess(m)
+                if self.graphs:
+                    m.capture_step()
             self.streams.append(st)
             self.models.append(m)
         torch.cuda.synchronize()
@@ -89,9 +94,31 @@ class Ensemble:
                     self.active[i] = False
         return done
 
+    def _retire_flagged(self, idx):
+        for i in idx:
+            m = self.models[i]
+            with torch.cuda.stream(self.streams[i]):
+                flags = int(m.err.item())
+            if flags:
+                try:
+                    m.check()
+                    self.retired[i] = f"device flags {flags}"
+                except SystemExit as e:
+                    self.retired[i] = str(e)
+                self.active[i] = False
+
     def step(self):
-        """One time step of every active model.  Models are dealt to the threads largest first, so
-        each thread gets a similar amount of work."""
+        """One time step of every active model.  Recorded steps: every model's graph is launched on
+        its stream, then the flags are read.  Otherwise models are dealt to the threads largest
+        first, so each thread gets a similar amount of work."""
+        if self.graphs:
+            idx = [i for i in range(len(self.models)) if self.active[i]]
+            for i in idx:
+                with torch.cuda.stream(self.streams[i]):
+                    self.models[i].step()
+            self.steps_done += len(idx)
+            self._retire_flagged(idx)
+            return
         order = sorted((i for i in range(len(self.models)) if self.active[i]), key=lambda i: -self.models[i].nel)
         parts = [order[t::self.threads] for t in range(self.threads)]
         futs = [self.pool.submit(self._run, p) for p in parts if p]

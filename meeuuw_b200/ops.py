@@ -5,6 +5,7 @@ Outputs are allocated here when not supplied; the hot loop (``meeuuw_b200.timest
 preallocated buffers so that nothing is allocated per step.
 """
 import ctypes
+import threading
 
 import torch
 
@@ -29,12 +30,35 @@ class Workspace:
 
 
 _ws = {}
+_scope = threading.local()
+
+
+class workspace_scope:
+    """Within this context, workspace(tag) returns the scratch of `owner` (a model): the same
+    buffers whichever stream the kernels go to, so a time step recorded into a CUDA graph on a
+    capture stream uses the buffers of the model's eager steps."""
+
+    def __init__(self, owner):
+        self.key = id(owner)
+
+    def __enter__(self):
+        self.prev = getattr(_scope, "key", None)
+        _scope.key = self.key
+        return self
+
+    def __exit__(self, *exc):
+        _scope.key = self.prev
 
 
 def workspace(tag="default"):
-    """Scratch for `tag` on the current stream: models advanced concurrently on different streams
-    (ensembles) never share scratch, and reuse on one stream is ordered by that stream."""
-    key = (tag, torch.cuda.current_stream().cuda_stream if torch.cuda.is_available() else 0)
+    """Scratch for `tag`: the current model's (inside workspace_scope) or the current stream's, so
+    that models advanced concurrently on different streams never share scratch and reuse is
+    ordered by one stream."""
+    owner = getattr(_scope, "key", None)
+    if owner is not None:
+        key = (tag, "model", owner)
+    else:
+        key = (tag, torch.cuda.current_stream().cuda_stream if torch.cuda.is_available() else 0)
     if key not in _ws:
         _ws[key] = Workspace()
     return _ws[key]
@@ -289,6 +313,15 @@ def energy_solve(box, VV, rhs, T, rtol=1e-12, maxit=200):
                                  ctypes.byref(rr), wp, wb, stream_ptr())
     if rc not in (0, 3):
         raise RuntimeError(f"mw_energy_solve returned {L.STATUS.get(rc, rc)}")
+    return it.value, rr.value
+
+
+def energy_device_info(box):
+    """(iterations, relative residual) of the last energy solve on this stream, from the device."""
+    it = ctypes.c_int32()
+    rr = ctypes.c_double()
+    wp, wb = workspace("energy").get(L.lib().mw_energy_solve_workspace_bytes(box))
+    call("mw_energy_device_info", box, wp, ctypes.byref(it), ctypes.byref(rr), stream_ptr())
     return it.value, rr.value
 
 

@@ -38,6 +38,7 @@ L.extra_protos({
     "mw_stokes_create": (c_int32, [L.MwBox, MwStokesParams, c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_stokes_destroy": (c_int32, [c_void_p]),
     "mw_stokes_device_loops": (c_int32, [c_void_p]),
+    "mw_stokes_device_info": (c_int32, [c_void_p, c_double, c_void_p, c_void_p]),
     "mw_stokes_uzawa_residual": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_double, c_int32,
                                            c_void_p, c_void_p, c_void_p]),
     "mw_stokes_levels": (c_int32, [c_void_p, c_int32]),
@@ -114,6 +115,14 @@ class StokesSolver:
         x = torch.empty_like(b)
         call("mw_stokes_vcycle", self.h, PREC[precision], ptr(b), ptr(x), stream_ptr())
         return x
+
+    def device_info(self, tol=1e-8):
+        """Outcome of the last solve read from its device scalars (after a recorded-graph replay)."""
+        info = MwSolveInfo()
+        call("mw_stokes_device_info", self.h, float(tol), ctypes.byref(info), stream_ptr())
+        out = {k: getattr(info, k) for k, _ in MwSolveInfo._fields_}
+        out["status"] = "MW_OK" if info.converged else "MW_ERR_NOT_CONVERGED"
+        return out
 
     def device_loops(self):
         """True once a solve ran as one recorded graph with its loops on the device."""

@@ -85,6 +85,8 @@ class GPUModel:
         self.istep = 0
         self.guess = None      # optional callable(model) -> (solV, solP) used as the Stokes initial guess
         self.solve_kw = {}     # extra mw_solve_params fields (e.g. mass_iters, sweep_reduction)
+        self.graph = None      # recorded time step (capture_step)
+        self._replayed = False
         ops.locate(box, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
 
     # ------------------------------------------------------------------------------------------
@@ -114,7 +116,35 @@ class GPUModel:
             out[n0] = out.get(n0, 0.0) + e0.elapsed_time(e1)
         return out
 
+    def capture_step(self):
+        """Record one whole time step as a CUDA graph; later step() calls replay it (one launch per
+        step, no host synchronisation).  The Stokes and energy solves record their loops as
+        conditional nodes; their outcomes are read from the device by diagnostics().  Runs one
+        eager step first when none has run (it sizes every workspace).  A guess hook runs host
+        code between the solves' inputs and the solve, so a model with one cannot be captured."""
+        if self.guess is not None:
+            raise ValueError("a Stokes guess hook runs host code and cannot be recorded into a graph")
+        if self.istep == 0:
+            self.step()
+        torch.cuda.synchronize()
+        self._phases = None
+        g = torch.cuda.CUDAGraph()
+        with ops.workspace_scope(self):
+            with torch.cuda.graph(g, capture_error_mode="thread_local"):
+                self._step_body()
+        self.istep -= 1                 # the capture recorded the step; nothing ran
+        self.graph = g
+
     def step(self):
+        if self.graph is not None:
+            self.graph.replay()
+            self.istep += 1
+            self._replayed = True
+            return
+        with ops.workspace_scope(self):
+            self._step_body()
+
+    def _step_body(self):
         c, b, tb = self.cfg, self.box, self.tables
         P = self.props
         self._mark("particles+projections")
@@ -199,6 +229,12 @@ class GPUModel:
 
     def diagnostics(self):
         """Reads the step's scalars (synchronises) and applies the reference's exit checks."""
+        if self._replayed:              # a recorded step ran: the solvers' outcomes are on the device
+            with ops.workspace_scope(self):
+                self.last_solve = self.solver.device_info(self.tol)
+                if self.cfg.solve_T:
+                    self.energy_info = ops.energy_device_info(self.box)
+            self._replayed = False
         err = int(self.err.item())
         d = dict(istep=self.istep, dt=float(self.dt_out[0].item()), vrms=float(self.gq_out[0].item()),
                  Tavrg=float(self.gq_out[1].item()), Nu=float(self.nu_out[12].item()) if self.cfg.solve_T else None,

@@ -106,7 +106,7 @@ def test_stokes_solve_to_1e8(scheme, precision):
     # residual with a larger error left in the velocity than cd_u_eta's M_eta-preconditioned one
     fwd = 2e-5 if scheme == "cd_u_eta" else 1e-4
     assert rel_err(sol[:m.Nfem_V], ref[:m.Nfem_V]) < fwd
-    assert np.linalg.norm(sol[:m.Nfem_V] - ref[:m.Nfem_V]) < fwd / 4 * np.linalg.norm(ref[:m.Nfem_V])
+    assert np.linalg.norm(sol[:m.Nfem_V] - ref[:m.Nfem_V]) < fwd / 2 * np.linalg.norm(ref[:m.Nfem_V])
 
 
 def test_noslip_rayleigh_taylor_box_solve():

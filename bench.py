@@ -470,6 +470,9 @@ def run_ensemble(args):
 
 if __name__ == "__main__":
     a = parse()
+    if a.ensemble:
+        # more hardware work queues for the many model streams (read when CUDA initialises)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     if a.impl == "reference":
         run_reference(a)
     elif a.ensemble:

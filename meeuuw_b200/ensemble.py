@@ -10,6 +10,10 @@ Stokes solver (its own stream and recorded CUDA graphs), so nothing is shared be
 
 ``Autotuner`` picks the number of host threads (the concurrency level) by timing ensemble steps,
 and caches the choice per GPU and ensemble shape.
+
+Many streams share the GPU's hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default): a
+process running a large ensemble should set it higher (up to 32) before CUDA is initialised, so
+that one model's device-side solver loop does not hold up the models queued behind it.
 """
 import json
 import math
@@ -112,7 +116,7 @@ class Ensemble:
         its stream, then the flags are read.  Otherwise models are dealt to the threads largest
         first, so each thread gets a similar amount of work."""
         if self.graphs:
-            idx = [i for i in range(len(self.models)) if self.active[i]]
+            idx = sorted((i for i in range(len(self.models)) if self.active[i]), key=lambda i: -self.models[i].nel)
             for i in idx:
                 with torch.cuda.stream(self.streams[i]):
                     self.models[i].step()

@@ -39,6 +39,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="skip the torch-profiler launch count")
     ap.add_argument("--roofline-only", action="store_true", help="set up the model, time the operator apply, exit")
+    ap.add_argument("--host-loops", action="store_true",
+                    help="solver loops driven from the host (same kernels; lets a kernel profiler list every launch)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the 512x512 model: an uneven ensemble of this many models (64..192 squared)")
     return ap.parse_args()
@@ -138,6 +140,8 @@ def run_ours(args):
 
     # ---- product path: mixed precision, learned warm start (gated; previous-step fallback) ----
     model = GPUModel(cfg, host, stokes="mixed", tol=1e-8)
+    if args.host_loops:
+        model.solve_kw = dict(host_loops=1)
     learned = None
     wpath = os.path.join(ROOT, "meeuuw_b200", "weights", "unet_fk128.npz")
     if os.path.exists(wpath):

@@ -234,17 +234,23 @@ __global__ void k_nu_terms(mw_box b, const double* __restrict__ T, const double*
 __global__ void k_nu_final(mw_box b, const double* __restrict__ terms, double* __restrict__ out) {
   // out: avrg_T_left, right, bottom, top, avrg_dTdx_left, right, avrg_dTdz_bottom, top,
   //      qx_left, qx_right, qz_bottom, qz_top, Nu     (postprocessors.py:234-248)
+  // one warp per side: lane-strided partial sums, then a fixed-order warp reduction (deterministic)
   __shared__ double res[4][3];
   const int nside[4] = {b.nelz, b.nelz, b.nelx, b.nelx};
-  int s = threadIdx.x;
+  const int s = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (s < 4) {
     int64_t off = 0;
     for (int k = 0; k < s; ++k) off += (int64_t)nside[k] * 3;
     double aT = 0, ag = 0, q = 0;
-    for (int64_t t = off; t < off + (int64_t)nside[s] * 3; ++t) {
+    for (int64_t t = off + lane; t < off + (int64_t)nside[s] * 3; t += 32) {
       aT += terms[t * 3]; ag += terms[t * 3 + 1]; q -= terms[t * 3 + 2];
     }
-    res[s][0] = aT; res[s][1] = ag; res[s][2] = q;
+    for (int o = 16; o > 0; o >>= 1) {
+      aT += __shfl_down_sync(0xffffffffu, aT, o);
+      ag += __shfl_down_sync(0xffffffffu, ag, o);
+      q += __shfl_down_sync(0xffffffffu, q, o);
+    }
+    if (lane == 0) { res[s][0] = aT; res[s][1] = ag; res[s][2] = q; }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -503,7 +509,7 @@ int mw_compute_nu(mw_box box, const double* T, const double* dTdx_n, const doubl
   int64_t total = (int64_t)(2 * box.nelz + 2 * box.nelx) * 3;
   k_nu_terms<<<grid_for(total, 128), 128, 0, s>>>(box, T, dTdx_n, dTdz_n, hcond_n, g, (double*)work);
   MW_CHECK_LAUNCH();
-  k_nu_final<<<1, 32, 0, s>>>(box, (const double*)work, out13);
+  k_nu_final<<<1, 128, 0, s>>>(box, (const double*)work, out13);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }
@@ -538,7 +544,7 @@ int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, con
   const int64_t total = nbound * 3;
   k_nu_terms<<<grid_for(total, 128), 128, 0, s>>>(box, T, dTdx_n, dTdz_n, hcond_n, g, scratch);
   MW_CHECK_LAUNCH();
-  k_nu_final<<<1, 32, 0, s>>>(box, scratch, out13);
+  k_nu_final<<<1, 128, 0, s>>>(box, scratch, out13);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }

@@ -253,6 +253,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
+  __shared__ uchar2 sfix[LZ * LX];          // Dirichlet flags of the staged nodes
   const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
@@ -267,14 +268,18 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     const int ix = lx0 + lx, iz = lz0 + lz;
     R2 v;
     v.x = 0; v.y = 0;
-    if (use_u && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
+    uchar2 ff = make_uchar2(0, 0);
+    if (ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
       const int64_t n = (int64_t)iz * g.nnx + ix;
-      const R2 uu = u2[n];
-      const uchar2 ff = f2[n];
-      v.x = ff.x ? R(0) : uu.x;
-      v.y = ff.y ? R(0) : uu.y;
+      ff = f2[n];
+      if (use_u) {
+        const R2 uu = u2[n];
+        v.x = ff.x ? R(0) : uu.x;
+        v.y = ff.y ? R(0) : uu.y;
+      }
     }
     su2[i] = v;
+    sfix[i] = ff;
   }
   if (use_p)
     for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
@@ -340,24 +345,42 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
                    y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
       }
-      int64_t n = (int64_t)iz * g.nnx + ix;
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        int64_t dof = 2 * n + c;
-        R y = c == 0 ? y0 : y1;
-        if (a.fix[dof]) y = use_u ? a.diag[dof] * a.u[dof] : R(0);
-        if (MODE == AM_APPLY) {
-          a.yV[dof] = y;
-        } else if (MODE == AM_RESID) {
-          a.yV[dof] = a.bV[dof] - y;
-        } else {   // Chebyshev step
-          R r = a.bV[dof] - y;
-          const double c1 = a.cheb[0];
-          R dn = R(a.cheb[1]) * r / a.diag[dof];
-          if (c1 != 0.0) dn += R(c1) * a.d[dof];     // restart steps never read the old direction
-          a.d[dof] = dn;
-          a.xo[dof] = a.u[dof] + dn;
+      const int64_t n = (int64_t)iz * g.nnx + ix;
+      // the node's (u, w) pair with one vector access per array; the Dirichlet flags were staged
+      const uchar2 ff = sfix[(iz - lz0) * LX + (ix - lx0)];
+      R2 y;
+      y.x = y0;
+      y.y = y1;
+      if (ff.x | ff.y) {
+        // eliminated rows act as K_ii u_i; calls without a velocity (G p only) pass no diagonal
+        R2 fy{R(0), R(0)};
+        if (use_u) {
+          const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
+          const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
+          fy = R2{dg.x * uu.x, dg.y * uu.y};
         }
+        if (ff.x) y.x = fy.x;
+        if (ff.y) y.y = fy.y;
+      }
+      if (MODE == AM_APPLY) {
+        reinterpret_cast<R2*>(a.yV)[n] = y;
+      } else if (MODE == AM_RESID) {
+        const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
+        reinterpret_cast<R2*>(a.yV)[n] = R2{bb.x - y.x, bb.y - y.y};
+      } else {   // Chebyshev step: d = c1 d + c2 D^-1 (b - y); x_out = u + d
+        const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
+        const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
+        const double c1 = a.cheb[0];
+        const R c2 = R(a.cheb[1]);
+        R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
+        if (c1 != 0.0) {                               // restart steps never read the old direction
+          const R2 dd = reinterpret_cast<const R2*>(a.d)[n];
+          dn.x += R(c1) * dd.x;
+          dn.y += R(c1) * dd.y;
+        }
+        const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
+        reinterpret_cast<R2*>(a.d)[n] = dn;
+        reinterpret_cast<R2*>(a.xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
       }
     }
   }
@@ -672,6 +695,8 @@ __global__ void k_gauss_jordan_smem(int nd, double* __restrict__ Ag) {
   double* A = sm;
   double* col = sm + (size_t)nd * nd;
   for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) A[t] = Ag[t];
+  // rows over warps, columns over lanes: no index division in the elimination sweep
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   for (int k = 0; k < nd; ++k) {
     __syncthreads();
     for (int i = threadIdx.x; i < nd; i += blockDim.x) col[i] = A[i * nd + k];
@@ -679,10 +704,12 @@ __global__ void k_gauss_jordan_smem(int nd, double* __restrict__ Ag) {
     const double piv = 1.0 / col[k];
     for (int j = threadIdx.x; j < nd; j += blockDim.x) A[k * nd + j] = (j == k ? 1.0 : A[k * nd + j]) * piv;
     __syncthreads();
-    for (int t = threadIdx.x; t < nd * nd; t += blockDim.x) {
-      const int i = t / nd, j = t - i * nd;
+    const double* rk = A + k * nd;
+    for (int i = warp; i < nd; i += nwarp) {
       if (i == k) continue;
-      A[t] = (j == k ? 0.0 : A[t]) - col[i] * A[k * nd + j];
+      const double ci = col[i];
+      double* ri = A + i * nd;
+      for (int j = lane; j < nd; j += 32) ri[j] = (j == k ? 0.0 : ri[j]) - ci * rk[j];
     }
   }
   __syncthreads();

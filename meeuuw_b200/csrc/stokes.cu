@@ -315,92 +315,152 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     }
   }
   __syncthreads();
-  // ---- owned velocity nodes: gather incident elements in ascending order ----
-  const int ox1 = (ex0 + TX >= g.nx) ? 2 * g.nx + 1 : 2 * (ex0 + TX);   // exclusive lattice end
-  const int oz1 = (ez0 + TZ >= g.nz) ? 2 * g.nz + 1 : 2 * (ez0 + TZ);
-  const int onx = ox1 - 2 * ex0, onz = oz1 - 2 * ez0;
-  if (a.yV) {
-    for (int i = tid; i < onx * onz; i += APPLY_THREADS) {
-      int ix = 2 * ex0 + i % onx, iz = 2 * ez0 + i / onx;
-      // incident elements, ascending (ez, ex): x candidates (xa, xb), z candidates (za, zb);
-      // tile-local element coordinates and the node's local index offsets
-      const bool xo = ix & 1, zo = iz & 1;
-      const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
-      const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = (iz >> 1);
-      const bool vxa = xa >= 0, vxb = !xo && xb < g.nx;
-      const bool vza = za >= 0, vzb = !zo && zb < g.nz;
-      const int dxa = xo ? 1 : 2, dza = zo ? 1 : 2;   // offsets inside element xa / za; 0 inside xb / zb
-      R y0 = 0, y1 = 0;
-      if (vza) {
-        const int lez = za - (ez0 - 1);
-        if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, dza);
-                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
-        if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, dza);
-                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
-      }
-      if (vzb) {
-        const int lez = zb - (ez0 - 1);
-        if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, 0);
-                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
-        if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
-                   y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
-      }
-      const int64_t n = (int64_t)iz * g.nnx + ix;
-      // the node's (u, w) pair with one vector access per array; the Dirichlet flags were staged
-      const uchar2 ff = sfix[(iz - lz0) * LX + (ix - lx0)];
-      R2 y;
-      y.x = y0;
-      y.y = y1;
-      if (ff.x | ff.y) {
-        // eliminated rows act as K_ii u_i; calls without a velocity (G p only) pass no diagonal
-        R2 fy{R(0), R(0)};
-        if (use_u) {
-          const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
-          const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
-          fy = R2{dg.x * uu.x, dg.y * uu.y};
-        }
-        if (ff.x) y.x = fy.x;
-        if (ff.y) y.y = fy.y;
-      }
-      if (MODE == AM_APPLY) {
-        reinterpret_cast<R2*>(a.yV)[n] = y;
-      } else if (MODE == AM_RESID) {
-        const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
-        reinterpret_cast<R2*>(a.yV)[n] = R2{bb.x - y.x, bb.y - y.y};
-      } else {   // Chebyshev step: d = c1 d + c2 D^-1 (b - y); x_out = u + d
-        const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
+  // ---- owned nodes: sums over the incident elements in ascending element order ----
+  // Each owned element's thread takes the four nodes of its lower-left quadrant (centre, bottom
+  // and left edge midpoints, lower-left corner) and its lower-left pressure node, with the element
+  // local indices known at compile time; the spare threads take the nodes on the right and top
+  // mesh boundary, which belong to no element's lower-left quadrant.
+  const bool lastx = ex0 + TX >= g.nx, lastz = ez0 + TZ >= g.nz;
+  // velocity node epilogue: Dirichlet rows, then the mode's output
+  auto emit = [&](int ix, int iz, R y0, R y1) {
+    const int64_t n = (int64_t)iz * g.nnx + ix;
+    const uchar2 ff = sfix[(iz - lz0) * LX + (ix - lx0)];
+    R2 y;
+    y.x = y0;
+    y.y = y1;
+    if (ff.x | ff.y) {
+      // eliminated rows act as K_ii u_i; calls without a velocity (G p only) pass no diagonal
+      R2 fy{R(0), R(0)};
+      if (use_u) {
         const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
-        const double c1 = a.cheb[0];
-        const R c2 = R(a.cheb[1]);
-        R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
-        if (c1 != 0.0) {                               // restart steps never read the old direction
-          const R2 dd = reinterpret_cast<const R2*>(a.d)[n];
-          dn.x += R(c1) * dd.x;
-          dn.y += R(c1) * dd.y;
-        }
         const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
-        reinterpret_cast<R2*>(a.d)[n] = dn;
-        reinterpret_cast<R2*>(a.xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
+        fy = R2{dg.x * uu.x, dg.y * uu.y};
+      }
+      if (ff.x) y.x = fy.x;
+      if (ff.y) y.y = fy.y;
+    }
+    if (MODE == AM_APPLY) {
+      reinterpret_cast<R2*>(a.yV)[n] = y;
+    } else if (MODE == AM_RESID) {
+      const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
+      reinterpret_cast<R2*>(a.yV)[n] = R2{bb.x - y.x, bb.y - y.y};
+    } else {   // Chebyshev step: d = c1 d + c2 D^-1 (b - y); x_out = u + d
+      const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
+      const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
+      const double c1 = a.cheb[0];
+      const R c2 = R(a.cheb[1]);
+      R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
+      if (c1 != 0.0) {                               // restart steps never read the old direction
+        const R2 dd = reinterpret_cast<const R2*>(a.d)[n];
+        dn.x += R(c1) * dd.x;
+        dn.y += R(c1) * dd.y;
+      }
+      const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
+      reinterpret_cast<R2*>(a.d)[n] = dn;
+      reinterpret_cast<R2*>(a.xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
+    }
+  };
+  // any velocity node of the tile (incident elements found from the node's parity)
+  auto node_generic = [&](int ix, int iz) {
+    const bool xo = ix & 1, zo = iz & 1;
+    const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
+    const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = (iz >> 1);
+    const bool vxa = xa >= 0, vxb = !xo && xb < g.nx;
+    const bool vza = za >= 0, vzb = !zo && zb < g.nz;
+    const int dxa = xo ? 1 : 2, dza = zo ? 1 : 2;   // offsets inside element xa / za; 0 inside xb / zb
+    R y0 = 0, y1 = 0;
+    if (vza) {
+      const int lez = za - (ez0 - 1);
+      if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, dza);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+      if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, dza);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+    }
+    if (vzb) {
+      const int lez = zb - (ez0 - 1);
+      if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, 0);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+      if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+    }
+    emit(ix, iz, y0, y1);
+  };
+  // any pressure node of the tile
+  auto pnode_generic = [&](int px, int pz) {
+    // incident elements (pz-1, px-1) k=2, (pz-1, px) k=3, (pz, px-1) k=1, (pz, px) k=0
+    const bool l = px >= 1, rr = px < g.nx, bo = pz >= 1, to = pz < g.nz;
+    const int lx = px - ex0, lz = pz - ez0;          // tile-local index of element (px, pz) is (lx+1, lz+1)
+    R y = 0;
+    if (bo && l) y += sye[((lz) * EX + lx) * 22 + 18 + 2];
+    if (bo && rr) y += sye[((lz) * EX + lx + 1) * 22 + 18 + 3];
+    if (to && l) y += sye[((lz + 1) * EX + lx) * 22 + 18 + 1];
+    if (to && rr) y += sye[((lz + 1) * EX + lx + 1) * 22 + 18 + 0];
+    const int64_t n = (int64_t)pz * (g.nx + 1) + px;
+    a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
+  };
+  if (tid < TX * TZ) {
+    const int lx = tid % TX, lz = tid / TX;          // TX is a power of two
+    const int ex = ex0 + lx, ez = ez0 + lz;
+    if (ex < g.nx && ez < g.nz) {
+      const R* e00 = sye + ((lz + 1) * EX + lx + 1) * 22;   // element (ex, ez)
+      const R* eL = e00 - 22;                                 // (ex-1, ez)
+      const R* eB = e00 - EX * 22;                            // (ex, ez-1)
+      const R* eBL = eB - 22;                                 // (ex-1, ez-1)
+      const bool hasL = ex > 0, hasB = ez > 0;
+      if (a.yV) {
+        emit(2 * ex + 1, 2 * ez + 1, e00[16], e00[17]);      // centre: local node 8
+        {                                                     // bottom edge midpoint: 6 of (ex,ez-1), 4
+          R y0 = 0, y1 = 0;
+          if (hasB) { y0 += eB[12]; y1 += eB[13]; }
+          y0 += e00[8]; y1 += e00[9];
+          emit(2 * ex + 1, 2 * ez, y0, y1);
+        }
+        {                                                     // left edge midpoint: 5 of (ex-1,ez), 7
+          R y0 = 0, y1 = 0;
+          if (hasL) { y0 += eL[10]; y1 += eL[11]; }
+          y0 += e00[14]; y1 += e00[15];
+          emit(2 * ex, 2 * ez + 1, y0, y1);
+        }
+        {                                                     // lower-left corner: 2, 3, 1, 0
+          R y0 = 0, y1 = 0;
+          if (hasB && hasL) { y0 += eBL[4]; y1 += eBL[5]; }
+          if (hasB) { y0 += eB[6]; y1 += eB[7]; }
+          if (hasL) { y0 += eL[2]; y1 += eL[3]; }
+          y0 += e00[0]; y1 += e00[1];
+          emit(2 * ex, 2 * ez, y0, y1);
+        }
+      }
+      if (a.yP) {                                             // pressure node (ex, ez): 2, 3, 1, 0
+        R y = 0;
+        if (hasB && hasL) y += eBL[18 + 2];
+        if (hasB) y += eB[18 + 3];
+        if (hasL) y += eL[18 + 1];
+        y += e00[18 + 0];
+        const int64_t n = (int64_t)ez * (g.nx + 1) + ex;
+        a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
       }
     }
-  }
-  // ---- owned pressure nodes ----
-  if (a.yP) {
-    const int px1 = (ex0 + TX >= g.nx) ? g.nx + 1 : ex0 + TX;
-    const int pz1 = (ez0 + TZ >= g.nz) ? g.nz + 1 : ez0 + TZ;
-    const int pnx = px1 - ex0, pnz = pz1 - ez0;
-    for (int i = tid; i < pnx * pnz; i += APPLY_THREADS) {
-      int px = ex0 + i % pnx, pz = ez0 + i / pnx;
-      // incident elements (pz-1, px-1) k=2, (pz-1, px) k=3, (pz, px-1) k=1, (pz, px) k=0
-      const bool l = px >= 1, rr = px < g.nx, bo = pz >= 1, to = pz < g.nz;
-      const int lx = px - ex0, lz = pz - ez0;          // tile-local index of element (px, pz) is (lx+1, lz+1)
-      R y = 0;
-      if (bo && l) y += sye[((lz) * EX + lx) * 22 + 18 + 2];
-      if (bo && rr) y += sye[((lz) * EX + lx + 1) * 22 + 18 + 3];
-      if (to && l) y += sye[((lz + 1) * EX + lx) * 22 + 18 + 1];
-      if (to && rr) y += sye[((lz + 1) * EX + lx + 1) * 22 + 18 + 0];
-      int64_t n = (int64_t)pz * (g.nx + 1) + px;
-      a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
+  } else if (lastx || lastz) {
+    // right column ix = 2 nx (rows of this tile) and top row iz = 2 nz (columns of this tile,
+    // the corner taken by the column)
+    const int j0 = tid - TX * TZ, nj = APPLY_THREADS - TX * TZ;
+    if (a.yV) {
+      const int oz1 = lastz ? 2 * g.nz + 1 : 2 * (ez0 + TZ);
+      const int ncol = lastx ? oz1 - 2 * ez0 : 0;
+      const int nrow = lastz ? (lastx ? 2 * (g.nx - ex0) : 2 * TX) : 0;
+      for (int j = j0; j < ncol + nrow; j += nj) {
+        if (j < ncol) node_generic(2 * g.nx, 2 * ez0 + j);
+        else node_generic(2 * ex0 + (j - ncol), 2 * g.nz);
+      }
+    }
+    if (a.yP) {
+      const int pz1 = lastz ? g.nz + 1 : ez0 + TZ;
+      const int ncol = lastx ? pz1 - ez0 : 0;
+      const int nrow = lastz ? (lastx ? g.nx - ex0 : TX) : 0;
+      for (int j = j0; j < ncol + nrow; j += nj) {
+        if (j < ncol) pnode_generic(g.nx, ez0 + j);
+        else pnode_generic(ex0 + (j - ncol), g.nz);
+      }
     }
   }
 }
@@ -1878,7 +1938,7 @@ static void init_params(mw_stokes* S, mw_box box, const mw_stokes_params& prm) {
 void mw_stokes_default_params(mw_stokes_params* p) {
   memset(p, 0, sizeof(*p));
   p->eta_ref = 1.0; p->L_ref = 1.0; p->precisions = 3;
-  p->coarse_min = 4; p->dense_max = 700; p->cheb_degree = 3; p->cheb_ratio = 8.0; p->cheb_safety = 1.1;
+  p->coarse_min = 4; p->dense_max = 700; p->cheb_degree = 2; p->cheb_ratio = 8.0; p->cheb_safety = 1.1;
   p->power_iters = 12;
   p->power_iters_warm = 3;
 }

@@ -97,25 +97,16 @@ def run_ours(args):
     from meeuuw_b200 import _lib, configs, ops
     from meeuuw_b200.timestep import GPUModel
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from meeuuw_b200 import replicas
+    world, rank, local = replicas.world()
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    replicas.init("nccl")            # replicas only: collectives for timing, none on the data path
 
     def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(device="cuda")
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(v, device="cuda")
 
     n = args.n
     cfg = configs.fk_convection(n, seed=1000 + rank)
@@ -257,9 +248,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finalize()
 
 
 def roofline_apply(model, torch):
@@ -403,8 +392,14 @@ def run_ensemble(args):
     with autotuned concurrency -- each timed with CUDA events; `value` is the faster mode.  Each
     model's vrms is compared with the same model run with the FP64 solver."""
     import torch
+    from meeuuw_b200 import replicas
     from meeuuw_b200.ensemble import Autotuner, Ensemble, sample_configs
-    cfgs = sample_configs(args.ensemble, seed=7)
+    world, rank, local = replicas.world()
+    torch.cuda.set_device(local)
+    replicas.init("nccl")
+    all_cfgs = sample_configs(args.ensemble, seed=7)
+    # the models are dealt to the GPUs balanced by element count; no data-path collective
+    cfgs = [all_cfgs[i] for i in replicas.partition([c.nel for c in all_cfgs], world)[rank]]
     dev = torch.cuda.current_device()
 
     def timed(ens):
@@ -412,7 +407,7 @@ def run_ensemble(args):
             ens.step()
         ens.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
+        replicas.barrier(device="cuda")
         done0 = ens.steps_done
         s.record()
         for _ in range(args.steps):
@@ -420,8 +415,9 @@ def run_ensemble(args):
         for st in ens.streams:               # the end event waits for every model's stream
             torch.cuda.current_stream().wait_stream(st)
         e.record()
-        torch.cuda.synchronize()
-        return s.elapsed_time(e), ens.steps_done - done0
+        replicas.barrier(device="cuda")
+        ms = replicas.max_over_ranks(s.elapsed_time(e), device="cuda")
+        return ms, replicas.sum_over_ranks(ens.steps_done - done0, device="cuda")
 
     modes = {}
     with ClockSampler(dev) as clk:
@@ -454,22 +450,35 @@ def run_ensemble(args):
     fp64 = [d["vrms"] for d in ref.diagnostics()]
     both = [i for i in range(len(cfgs)) if active[i] and ref.active[i]]
     ref.close()
-    err = sorted(abs(mixed[i] - fp64[i]) / abs(fp64[i]) for i in both)
+    err = [abs(mixed[i] - fp64[i]) / abs(fp64[i]) for i in both]
+    retired = {cfgs[i].name: why for i, why in retired.items()}
+    if world > 1:                            # gather the per-model figures on rank 0
+        import torch.distributed as dist
+        got = [None] * world
+        dist.all_gather_object(got, (err, retired, converged))
+        err = [x for g in got for x in g[0]]
+        retired = {k: v for g in got for k, v in g[1].items()}
+        converged = sum(g[2] for g in got)
+    err = sorted(err)
     best = max(modes, key=lambda k: modes[k]["model_steps_per_s"])
     line = {"metric": "aggregate model-timesteps/s, uneven ensemble (64..192 squared, 16 particles/element)",
-            "value": modes[best]["model_steps_per_s"], "unit": "model-timesteps/s", "n_gpus": 1,
+            "value": modes[best]["model_steps_per_s"], "unit": "model-timesteps/s",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": modes[best]["ms_per_step"],
             "higher_is_better": True, "dtype": "f64+f32", "data": "synthetic (seeded per model)",
-            "config": {"workload": f"ensemble of {len(cfgs)} FK convection models", "models": len(cfgs),
-                       "elements_total": int(sum(c.nel for c in cfgs)), "mode": best},
+            "n_gpus": world, "scaling": "weak" if world > 1 else None,
+            "config": {"workload": f"ensemble of {len(all_cfgs)} FK convection models", "models": len(all_cfgs),
+                       "elements_total": int(sum(c.nel for c in all_cfgs)), "mode": best,
+                       "parallelism": f"models dealt to {world} GPU(s) by element count"},
             "modes": modes,
-            "models_retired": {cfgs[i].name: why for i, why in retired.items()},
+            "models_retired": retired,
             "stokes_converged_models": converged,
             "vrms_rel_err_vs_fp64": {"models": len(err), "max": err[-1] if err else None,
                                      "median": err[len(err) // 2] if err else None,
                                      "p90": err[int(0.9 * (len(err) - 1))] if err else None},
             "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    replicas.finalize()
 
 
 if __name__ == "__main__":

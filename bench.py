@@ -116,6 +116,10 @@ def run_ours(args):
         for _ in range(W):
             model.step()
         model.check()
+        if not args.host_loops:
+            # the whole step as one CUDA graph (solver loops as conditional nodes); the learned
+            # guess is consulted at the cold start among the warm-up steps and idle afterwards
+            model.capture_step()
         barrier()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
@@ -159,9 +163,11 @@ def run_ours(args):
         if args.no_profile:
             raise RuntimeError("launch count skipped (--no-profile)")
         from torch.profiler import ProfilerActivity, profile
+        graph, model.graph = model.graph, None          # an eager step: the recorded one's kernels
         with profile(activities=[ProfilerActivity.CUDA]) as prof:
             model.step()
             torch.cuda.synchronize()
+        model.graph = graph
         names = [evt.name for evt in prof.events() if evt.device_type.name == "CUDA"]
         ours = [nm for nm in names if "mw::" in nm]
         launches = int(len(ours) * args.steps)
@@ -174,11 +180,13 @@ def run_ours(args):
 
     # ---- where a step's time goes (two more steps with CUDA events between the phases) ----
     def phases(m, k=2):
+        graph, m.graph = m.graph, None                  # eager steps, events between the phases
         m.enable_phase_timing(True)
         for _ in range(k):
             m.step()
         out = {p: v / k for p, v in m.phase_times().items()}
         m.enable_phase_timing(False)
+        m.graph = graph
         return out
 
     phase_ms = phases(model)
@@ -234,14 +242,17 @@ def run_ours(args):
                        "stokes_solver": "device Uzawa (cd_u_eta recurrence) + multigrid-PCG K solves, mixed",
                        "warm_start": ("learned U-Net (gated on the Uzawa residual, consulted at cold starts), "
                                       "previous-step fallback") if learned else "previous step",
-                       "stokes_loops": "device (one CUDA graph per solve)" if model.solver.device_loops()
+                       "stokes_loops": "device (conditional nodes)" if model.solver.device_loops()
                        else "host",
+                       "step_execution": "host-driven loops (profiling)" if args.host_loops else
+                       "one CUDA graph per time step, recorded after the warm-up (both arms)",
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (swarm state ~0.5 GB, fields ~0.2 GB)"},
             "clocks": clk.summary(), "gpu_launches": launches, "kernel_mix_per_step": kernel_mix,
             "roofline": roof, "e2e": e2e, "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
-            "last_step": {"vrms": diag["vrms"], "Nu": diag["Nu"], "dt": diag["dt"], "stokes": diag["stokes"]},
+            "last_step": {"vrms": diag["vrms"], "Nu": diag["Nu"], "dt": diag["dt"], "stokes": diag["stokes"],
+                          "energy_iters_relres": list(getattr(model, "energy_info", (None, None)))},
             "phases_ms_per_step": phase_ms,
             "mixed_vs_fp64": accuracy,
             "warm_start_picks": dict(learned.picks) if learned else None,

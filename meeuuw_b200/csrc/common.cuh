@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/meeuuw_b200.h"
 
 #define MW_HD __host__ __device__ __forceinline__
@@ -52,6 +54,37 @@ MW_D void set_flag(int32_t* err, int32_t bit) {
 // Grid size: enough CTAs to cover n work items, capped at a multiple of the SM count.
 int grid_for(int64_t n, int threads, int waves = 8);
 int num_sms();
+
+// Programmatic dependent launch.  The solver loops are long chains of short kernels on one stream;
+// launched through pdl_launch(), a kernel's CTAs are scheduled while its predecessor is still
+// running, so the launch latency between the two is hidden.  Every kernel started this way runs
+// pdl_entry() before touching global memory: it waits until every prerequisite grid has completed
+// and its writes are visible, then allows the next kernel to be scheduled (for a kernel started the
+// ordinary way both instructions return at once).  Because each kernel waits for the complete
+// predecessor before its first access, the stream order of all reads and writes is unchanged, and
+// at most one waiting grid is resident beside the running one.
+MW_D void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+bool pdl_enabled();        // false when the environment sets MW_PDL=0
+
+template <typename... KArgs, typename... Args>
+inline void pdl_launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = (s != nullptr && pdl_enabled()) ? 1 : 0;     // not on the legacy default stream
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 }  // namespace mw
 

@@ -25,6 +25,7 @@ MW_D int q2_local_e(int dx, int dz) {
 __global__ void k_energy_matvec(mw_box b, const double* __restrict__ vv, const double* __restrict__ x,
                                 const double* __restrict__ rhs, double* __restrict__ y, double* __restrict__ diag,
                                 int mode) {
+  pdl_entry();
   const int nnx = 2 * b.nelx + 1;
   const int64_t nn = (int64_t)nnx * (2 * b.nelz + 1);
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
@@ -50,6 +51,7 @@ __global__ void k_energy_matvec(mw_box b, const double* __restrict__ vv, const d
 
 __global__ void k_edot_partial(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                                double* __restrict__ part) {
+  pdl_entry();
   __shared__ double sh[32];
   double v = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -66,6 +68,7 @@ __global__ void k_edot_partial(int64_t n, const double* __restrict__ a, const do
 }
 
 __global__ void k_edot_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  pdl_entry();
   __shared__ double sh[32];
   double v = 0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) v += part[i];
@@ -84,6 +87,7 @@ __global__ void k_edot_final(const double* __restrict__ part, int nb, double* __
 // p = r + beta (p - omega v), beta = (rho_new/rho_old) (alpha/omega)
 __global__ void k_bicg_p(int64_t n, const double* __restrict__ s, const double* __restrict__ r,
                          const double* __restrict__ v, double* __restrict__ p, int first) {
+  pdl_entry();
   const double beta = first ? 0.0 : (s[0] / s[1]) * (s[2] / s[3]);
   const double om = first ? 0.0 : s[3];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -93,6 +97,7 @@ __global__ void k_bicg_p(int64_t n, const double* __restrict__ s, const double* 
 // the same update with the first-iteration switch read from the device iteration count sc[12]
 __global__ void k_bicg_p_dev(int64_t n, const double* __restrict__ s, const double* __restrict__ r,
                              const double* __restrict__ v, double* __restrict__ p) {
+  pdl_entry();
   const bool first = s[12] == 0.0;
   const double beta = first ? 0.0 : (s[0] / s[1]) * (s[2] / s[3]);
   const double om = first ? 0.0 : s[3];
@@ -102,6 +107,7 @@ __global__ void k_bicg_p_dev(int64_t n, const double* __restrict__ s, const doub
 
 __global__ void k_scale_diag(int64_t n, const double* __restrict__ x, const double* __restrict__ d,
                              double* __restrict__ y) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = x[i] / d[i];
 }
@@ -109,6 +115,7 @@ __global__ void k_scale_diag(int64_t n, const double* __restrict__ x, const doub
 // s = r - alpha v, alpha = rho / (r0, v) = s[0] / s[4]
 __global__ void k_bicg_s(int64_t n, const double* __restrict__ sc, const double* __restrict__ r,
                          const double* __restrict__ v, double* __restrict__ sv) {
+  pdl_entry();
   const double alpha = sc[0] / sc[4];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     sv[i] = r[i] - alpha * v[i];
@@ -118,6 +125,7 @@ __global__ void k_bicg_s(int64_t n, const double* __restrict__ sc, const double*
 __global__ void k_bicg_x(int64_t n, double* __restrict__ sc, const double* __restrict__ ph,
                          const double* __restrict__ sh, const double* __restrict__ sv, const double* __restrict__ t,
                          double* __restrict__ x, double* __restrict__ r) {
+  pdl_entry();
   const double alpha = sc[0] / sc[4];
   const double omega = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -128,6 +136,7 @@ __global__ void k_bicg_x(int64_t n, double* __restrict__ sc, const double* __res
 
 // keep alpha (slot 2) and omega (slot 3) of this iteration, rho_old (slot 1) <- rho (slot 0)
 __global__ void k_bicg_roll(double* sc) {
+  pdl_entry();
   if (threadIdx.x || blockIdx.x) return;
   sc[2] = sc[0] / sc[4];
   sc[3] = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
@@ -138,6 +147,7 @@ __global__ void k_bicg_roll(double* sc) {
 // sc[12] = iteration count; the loop runs while the residual is finite, above rtol * ||b|| and
 // the count is below maxit.
 __global__ void k_bicg_init(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h) {
+  pdl_entry();
   if (!(sc[10] > 0)) sc[10] = 1.0;
   sc[12] = 0;
   const double rr = sc[11];
@@ -145,6 +155,7 @@ __global__ void k_bicg_init(double* sc, double rtol, int maxit, cudaGraphConditi
 }
 
 __global__ void k_bicg_check(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h) {
+  pdl_entry();
   const double it = sc[12] + 1;
   sc[12] = it;
   const double rr = sc[11];
@@ -188,7 +199,7 @@ int mw_energy_device_info(mw_box box, const void* work, int32_t* iters, double* 
 
 int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y, void* stream) {
   int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  k_energy_matvec<<<grid_for(nn, 256), 256, 0, (cudaStream_t)stream>>>(box, VV_T, x, nullptr, y, nullptr, 0);
+  pdl_launch(k_energy_matvec, grid_for(nn, 256), 256, 0, (cudaStream_t)stream, box, VV_T, x, nullptr, y, nullptr, 0);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }
@@ -298,8 +309,8 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
   double* sc = part + 300;          // scalar slots
   const int NBk = 296;
   auto dot = [&](const double* a, const double* b2, double* out) {
-    k_edot_partial<<<NBk, 256, 0, s>>>(n, a, b2, part);
-    k_edot_final<<<1, 256, 0, s>>>(part, NBk, out);
+    pdl_launch(k_edot_partial, NBk, 256, 0, s, n, a, b2, part);
+    pdl_launch(k_edot_final, 1, 256, 0, s, part, NBk, out);
   };
   auto rd = [&](const double* d) {
     double h = 0;
@@ -308,7 +319,7 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
     return h;
   };
   // r = b - A T (T is the initial guess), diag
-  k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, T, rhs, r, dg, 1);
+  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, T, rhs, r, dg, 1);
   cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   dot(rhs, rhs, sc + 10);
   dot(r, r, sc + 11);
@@ -318,17 +329,17 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
   if (!(bb > 0)) bb = 1.0;
   for (it = 1; it <= maxit && rr > rtol * rtol * bb; ++it) {
     dot(r0, r, sc + 0);                                       // rho
-    k_bicg_p<<<grid_for(n, 256), 256, 0, s>>>(n, sc, r, v, p, it == 1);
-    k_scale_diag<<<grid_for(n, 256), 256, 0, s>>>(n, p, dg, ph);
-    k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, ph, nullptr, v, nullptr, 0);
+    pdl_launch(k_bicg_p, grid_for(n, 256), 256, 0, s, n, sc, r, v, p, it == 1);
+    pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, s, n, p, dg, ph);
+    pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, ph, nullptr, v, nullptr, 0);
     dot(r0, v, sc + 4);
-    k_bicg_s<<<grid_for(n, 256), 256, 0, s>>>(n, sc, r, v, sv);
-    k_scale_diag<<<grid_for(n, 256), 256, 0, s>>>(n, sv, dg, sh);
-    k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, sh, nullptr, t, nullptr, 0);
+    pdl_launch(k_bicg_s, grid_for(n, 256), 256, 0, s, n, sc, r, v, sv);
+    pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, s, n, sv, dg, sh);
+    pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, sh, nullptr, t, nullptr, 0);
     dot(t, sv, sc + 5);
     dot(t, t, sc + 6);
-    k_bicg_x<<<grid_for(n, 256), 256, 0, s>>>(n, sc, ph, sh, sv, t, T, r);
-    k_bicg_roll<<<1, 32, 0, s>>>(sc);
+    pdl_launch(k_bicg_x, grid_for(n, 256), 256, 0, s, n, sc, ph, sh, sv, t, T, r);
+    pdl_launch(k_bicg_roll, 1, 32, 0, s, sc);
     dot(r, r, sc + 11);
     rr = rd(sc + 11);
     if (!std::isfinite(rr)) break;
@@ -351,10 +362,10 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
   double* sc = part + 300;
   const int NBk = 296;
   auto dot = [&](const double* a, const double* b2, double* out, cudaStream_t st) {
-    k_edot_partial<<<NBk, 256, 0, st>>>(n, a, b2, part);
-    k_edot_final<<<1, 256, 0, st>>>(part, NBk, out);
+    pdl_launch(k_edot_partial, NBk, 256, 0, st, n, a, b2, part);
+    pdl_launch(k_edot_final, 1, 256, 0, st, part, NBk, out);
   };
-  k_energy_matvec<<<grid_for(n, 256), 256, 0, s>>>(box, VV_T, T, rhs, r, dg, 1);
+  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, T, rhs, r, dg, 1);
   cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   dot(rhs, rhs, sc + 10, s);
   dot(r, r, sc + 11, s);
@@ -365,7 +376,7 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
   if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr) != cudaSuccess) return false;
   cudaGraphConditionalHandle h;
   if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
-  k_bicg_init<<<1, 1, 0, s>>>(sc, rtol, maxit, h);
+  pdl_launch(k_bicg_init, 1, 1, 0, s, sc, rtol, maxit, h);
   if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd) != cudaSuccess) return false;
   cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
   prm.conditional.handle = h;
@@ -379,19 +390,19 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
     return false;
   // body: one BiCGSTAB iteration (the host loop's kernels, first-iteration branch on sc[12])
   dot(r0, r, sc + 0, b);
-  k_bicg_p_dev<<<grid_for(n, 256), 256, 0, b>>>(n, sc, r, v, p);
-  k_scale_diag<<<grid_for(n, 256), 256, 0, b>>>(n, p, dg, ph);
-  k_energy_matvec<<<grid_for(n, 256), 256, 0, b>>>(box, VV_T, ph, nullptr, v, nullptr, 0);
+  pdl_launch(k_bicg_p_dev, grid_for(n, 256), 256, 0, b, n, sc, r, v, p);
+  pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, b, n, p, dg, ph);
+  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, b, box, VV_T, ph, nullptr, v, nullptr, 0);
   dot(r0, v, sc + 4, b);
-  k_bicg_s<<<grid_for(n, 256), 256, 0, b>>>(n, sc, r, v, sv);
-  k_scale_diag<<<grid_for(n, 256), 256, 0, b>>>(n, sv, dg, sh);
-  k_energy_matvec<<<grid_for(n, 256), 256, 0, b>>>(box, VV_T, sh, nullptr, t, nullptr, 0);
+  pdl_launch(k_bicg_s, grid_for(n, 256), 256, 0, b, n, sc, r, v, sv);
+  pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, b, n, sv, dg, sh);
+  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, b, box, VV_T, sh, nullptr, t, nullptr, 0);
   dot(t, sv, sc + 5, b);
   dot(t, t, sc + 6, b);
-  k_bicg_x<<<grid_for(n, 256), 256, 0, b>>>(n, sc, ph, sh, sv, t, T, r);
-  k_bicg_roll<<<1, 32, 0, b>>>(sc);
+  pdl_launch(k_bicg_x, grid_for(n, 256), 256, 0, b, n, sc, ph, sh, sv, t, T, r);
+  pdl_launch(k_bicg_roll, 1, 32, 0, b, sc);
   dot(r, r, sc + 11, b);
-  k_bicg_check<<<1, 1, 0, b>>>(sc, rtol, maxit, h);
+  pdl_launch(k_bicg_check, 1, 1, 0, b, sc, rtol, maxit, h);
   cudaGraph_t gb = nullptr;
   return cudaStreamEndCapture(b, &gb) == cudaSuccess;
 }

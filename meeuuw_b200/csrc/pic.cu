@@ -10,6 +10,8 @@
 // index), so every element and node sums its particles in particle-index order -- the order of
 // the reference's sequential loops.  This file is compiled with -fmad=false so the basis and
 // weight arithmetic rounds exactly as the reference's unfused double-precision code.
+#include <cstdlib>
+
 #include "common.cuh"
 
 namespace mw {
@@ -23,6 +25,14 @@ int num_sms() {
     if (n <= 0) n = 148;
   }
   return n;
+}
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("MW_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 int grid_for(int64_t n, int threads, int waves) {

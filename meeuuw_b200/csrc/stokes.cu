@@ -149,7 +149,9 @@ struct ApplyArgs {
 // back onto the nodes (build_matrix_stokes.py:130-157 applied to a vector).  The reference-element
 // tables are __constant__ and every loop is unrolled, so each table value is an immediate
 // constant-bank operand of the FMA; the uniform-box Jacobian enters as sx = 2/hx, sz = 2/hz.
-template <typename R>
+// HAS_U = false: no velocity (G p only; the strain-rate terms vanish).  NEED_V = false: only the
+// pressure rows are wanted (G^T u), so the B^T scatter and the shear gradients are skipped.
+template <typename R, bool HAS_U = true, bool NEED_V = true>
 MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const R* eq, R* ye, R* ype, bool use_p) {
 #pragma unroll
   for (int k = 0; k < 18; ++k) ye[k] = 0;
@@ -158,32 +160,38 @@ MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const 
 #pragma unroll
   for (int q = 0; q < 9; ++q) {
     R dxu = 0, dzw = 0, dzu = 0, dxw = 0;
+    if (HAS_U) {
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
-      if (ref_dr(q, k) != 0.0) { dxu += r * ue[2 * k]; dxw += r * ue[2 * k + 1]; }
-      if (ref_dt(q, k) != 0.0) { dzw += t * ue[2 * k + 1]; dzu += t * ue[2 * k]; }
+      for (int k = 0; k < 9; ++k) {
+        const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
+        if (ref_dr(q, k) != 0.0) { dxu += r * ue[2 * k]; if (NEED_V) dxw += r * ue[2 * k + 1]; }
+        if (ref_dt(q, k) != 0.0) { dzw += t * ue[2 * k + 1]; if (NEED_V) dzu += t * ue[2 * k]; }
+      }
     }
     const R exx = sx * dxu, ezz = sz * dzw, gg = sz * dzu + sx * dxw;   // gg = du/dz + dw/dx
     const R jw = jac * CT<R>::wq(q);
-    const R e = eq[q] * jw;
-    R pq = 0;
-    if (use_p) {
+    if (NEED_V) {
+      const R e = eq[q] * jw;
+      R pq = 0;
+      if (use_p) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) pq += CT<R>::np(q, k) * pe[k];
+        for (int k = 0; k < 4; ++k) pq += CT<R>::np(q, k) * pe[k];
+      }
+      const R sp = s * jw * pq;
+      const R A = (R(2) * e * exx - sp) * sx, B = (R(2) * e * ezz - sp) * sz;
+      const R Cx = e * gg * sx, Cz = e * gg * sz;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
+        if (ref_dr(q, k) != 0.0) { ye[2 * k] += r * A; if (HAS_U) ye[2 * k + 1] += r * Cx; }
+        if (ref_dt(q, k) != 0.0) { if (HAS_U) ye[2 * k] += t * Cz; ye[2 * k + 1] += t * B; }
+      }
     }
-    const R sp = s * jw * pq;
-    const R A = (R(2) * e * exx - sp) * sx, B = (R(2) * e * ezz - sp) * sz;
-    const R Cx = e * gg * sx, Cz = e * gg * sz;
+    if (HAS_U) {
+      const R dv = -s * jw * (exx + ezz);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      const R r = CT<R>::dr(q, k), t = CT<R>::dt(q, k);
-      if (ref_dr(q, k) != 0.0) { ye[2 * k] += r * A; ye[2 * k + 1] += r * Cx; }
-      if (ref_dt(q, k) != 0.0) { ye[2 * k] += t * Cz; ye[2 * k + 1] += t * B; }
+      for (int k = 0; k < 4; ++k) ype[k] += CT<R>::np(q, k) * dv;
     }
-    const R dv = -s * jw * (exx + ezz);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) ype[k] += CT<R>::np(q, k) * dv;
   }
 }
 
@@ -191,8 +199,8 @@ MW_D void element_apply(R sx, R sz, R jac, R s, const R* ue, const R* pe, const 
 // operand, so each nonzero basis value costs one instruction for both velocity components, in the
 // gradients and in the B^T scatter.
 template <>
-MW_D void element_apply<float>(float sx, float sz, float jac, float s, const float* ue, const float* pe,
-                               const float* eq, float* ye, float* ype, bool use_p) {
+MW_D void element_apply<float, true, true>(float sx, float sz, float jac, float s, const float* ue, const float* pe,
+                                           const float* eq, float* ye, float* ype, bool use_p) {
   const float2* u2 = reinterpret_cast<const float2*>(ue);
   float2 y2[9];
 #pragma unroll
@@ -247,10 +255,26 @@ MW_D int q2_local_idx(int dx, int dz) {
 #define MW_APPLY_MINB 5      // resident FP32 apply CTAs per SM the register budget is sized for
 #endif
 
+// Asynchronous copy (LDGSTS) of one node's component pair from global to shared memory.
+template <typename R>
+MW_D void cp_async_pair(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if (sizeof(R) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+MW_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <typename R, int MODE>
 __global__ void __launch_bounds__(APPLY_THREADS, sizeof(R) == 4 ? MW_APPLY_MINB : 1)
 k_apply(LevelGeo g, ApplyArgs<R> a) {
+  pdl_entry();
+  typedef typename Vec2<R>::T R2;
+  // node vectors the epilogue reads for the four nodes each owned element emits (b; b, diag, d),
+  // fetched asynchronously while the element products run (FP32; the FP64 kernel's shared memory
+  // is already at the 48 KB static limit)
+  constexpr int NPRE = sizeof(R) == 8 ? 0 : (MODE == AM_CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
   __shared__ __align__(16) R su[LZ * LX * 2];
+  __shared__ __align__(16) R2 spre[(NPRE ? NPRE : 1) * 4 * TX * TZ];
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
   __shared__ uchar2 sfix[LZ * LX];          // Dirichlet flags of the staged nodes
@@ -258,8 +282,35 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
   const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
+  // ---- prefetch: the epilogue's node vectors (owned elements), the element viscosities ----
+  // slot j of an owned element: 0 centre (2ex+1, 2ez+1), 1 bottom midpoint (2ex+1, 2ez),
+  // 2 left midpoint (2ex, 2ez+1), 3 corner (2ex, 2ez)
+  if (NPRE && a.yV && tid < TX * TZ) {
+    const int ex = ex0 + tid % TX, ez = ez0 + tid / TX;
+    if (ex < g.nx && ez < g.nz) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int ix = 2 * ex + (j < 2 ? 1 : 0), iz = 2 * ez + ((j & 1) ? 0 : 1);
+        const int64_t n = (int64_t)iz * g.nnx + ix;
+        cp_async_pair<R>(&spre[j * TX * TZ + tid], a.bV + 2 * n);
+        if (NPRE == 3) {
+          cp_async_pair<R>(&spre[(4 + j) * TX * TZ + tid], a.diag + 2 * n);
+          cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
+        }
+      }
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  R eq[9];
+  if (tid < NEL_T) {
+    const int ex = ex0 - 1 + tid % EX, ez = ez0 - 1 + tid / EX;
+    if (ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz) {
+      const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) eq[q] = eg[q];
+    }
+  }
   // ---- stage velocity (masked; one vector load per node), pressure ----
-  typedef typename Vec2<R>::T R2;
   const R2* u2 = reinterpret_cast<const R2*>(a.u);
   const uchar2* f2 = reinterpret_cast<const uchar2*>(a.fix);
   R2* su2 = reinterpret_cast<R2*>(su);
@@ -303,17 +354,20 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) pe[k] = use_p ? sp[(lez + q1_dz(k)) * PX + lex + q1_dx(k)] : R(0);
-      R eq[9];
-      const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
-#pragma unroll
-      for (int q = 0; q < 9; ++q) eq[q] = eg[q];
-      element_apply<R>(R(2.0 / g.hx), R(2.0 / g.hz), R(g.hx * g.hz / 4.0), R(g.s), ue, pe, eq, ye, ype, use_p);
+      const R sxe = R(2.0 / g.hx), sze = R(2.0 / g.hz), jace = R(g.hx * g.hz / 4.0), se = R(g.s);
+      if (!use_u)                                   // G p only (the Schur iteration's G d, f - G P)
+        element_apply<R, false, true>(sxe, sze, jace, se, ue, pe, eq, ye, ype, use_p);
+      else if (!a.yV)                               // G^T u only
+        element_apply<R, true, false>(sxe, sze, jace, se, ue, pe, eq, ye, ype, use_p);
+      else
+        element_apply<R>(sxe, sze, jace, se, ue, pe, eq, ye, ype, use_p);
 #pragma unroll
       for (int k = 0; k < 18; ++k) sye[tid * 22 + k] = ye[k];
 #pragma unroll
       for (int k = 0; k < 4; ++k) sye[tid * 22 + 18 + k] = ype[k];
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   // ---- owned nodes: sums over the incident elements in ascending element order ----
   // Each owned element's thread takes the four nodes of its lower-left quadrant (centre, bottom
@@ -321,10 +375,13 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   // local indices known at compile time; the spare threads take the nodes on the right and top
   // mesh boundary, which belong to no element's lower-left quadrant.
   const bool lastx = ex0 + TX >= g.nx, lastz = ez0 + TZ >= g.nz;
-  // velocity node epilogue: Dirichlet rows, then the mode's output
-  auto emit = [&](int ix, int iz, R y0, R y1) {
+  // velocity node epilogue: Dirichlet rows, then the mode's output.  slot >= 0: an owned
+  // element's node whose b, diag, d were prefetched; slot < 0: read them here.
+  auto emit = [&](int ix, int iz, R y0, R y1, int slot) {
     const int64_t n = (int64_t)iz * g.nnx + ix;
-    const uchar2 ff = sfix[(iz - lz0) * LX + (ix - lx0)];
+    const int li = (iz - lz0) * LX + (ix - lx0);
+    const uchar2 ff = sfix[li];
+    R2 uu = su2[li];                                 // the staged velocity: exact on free dofs
     R2 y;
     y.x = y0;
     y.y = y1;
@@ -333,7 +390,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       R2 fy{R(0), R(0)};
       if (use_u) {
         const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
-        const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
+        uu = reinterpret_cast<const R2*>(a.u)[n];
         fy = R2{dg.x * uu.x, dg.y * uu.y};
       }
       if (ff.x) y.x = fy.x;
@@ -342,20 +399,20 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     if (MODE == AM_APPLY) {
       reinterpret_cast<R2*>(a.yV)[n] = y;
     } else if (MODE == AM_RESID) {
-      const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
+      const R2 bb = NPRE && slot >= 0 ? spre[slot * TX * TZ + tid] : reinterpret_cast<const R2*>(a.bV)[n];
       reinterpret_cast<R2*>(a.yV)[n] = R2{bb.x - y.x, bb.y - y.y};
     } else {   // Chebyshev step: d = c1 d + c2 D^-1 (b - y); x_out = u + d
-      const R2 bb = reinterpret_cast<const R2*>(a.bV)[n];
-      const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
+      const bool pre = NPRE && slot >= 0;
+      const R2 bb = pre ? spre[slot * TX * TZ + tid] : reinterpret_cast<const R2*>(a.bV)[n];
+      const R2 dg = pre ? spre[(4 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.diag)[n];
       const double c1 = a.cheb[0];
       const R c2 = R(a.cheb[1]);
       R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
       if (c1 != 0.0) {                               // restart steps never read the old direction
-        const R2 dd = reinterpret_cast<const R2*>(a.d)[n];
+        const R2 dd = pre ? spre[(8 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.d)[n];
         dn.x += R(c1) * dd.x;
         dn.y += R(c1) * dd.y;
       }
-      const R2 uu = reinterpret_cast<const R2*>(a.u)[n];
       reinterpret_cast<R2*>(a.d)[n] = dn;
       reinterpret_cast<R2*>(a.xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
     }
@@ -383,7 +440,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
                  y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
     }
-    emit(ix, iz, y0, y1);
+    emit(ix, iz, y0, y1, -1);
   };
   // any pressure node of the tile
   auto pnode_generic = [&](int px, int pz) {
@@ -408,18 +465,18 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       const R* eBL = eB - 22;                                 // (ex-1, ez-1)
       const bool hasL = ex > 0, hasB = ez > 0;
       if (a.yV) {
-        emit(2 * ex + 1, 2 * ez + 1, e00[16], e00[17]);      // centre: local node 8
+        emit(2 * ex + 1, 2 * ez + 1, e00[16], e00[17], 0);   // centre: local node 8
         {                                                     // bottom edge midpoint: 6 of (ex,ez-1), 4
           R y0 = 0, y1 = 0;
           if (hasB) { y0 += eB[12]; y1 += eB[13]; }
           y0 += e00[8]; y1 += e00[9];
-          emit(2 * ex + 1, 2 * ez, y0, y1);
+          emit(2 * ex + 1, 2 * ez, y0, y1, 1);
         }
         {                                                     // left edge midpoint: 5 of (ex-1,ez), 7
           R y0 = 0, y1 = 0;
           if (hasL) { y0 += eL[10]; y1 += eL[11]; }
           y0 += e00[14]; y1 += e00[15];
-          emit(2 * ex, 2 * ez + 1, y0, y1);
+          emit(2 * ex, 2 * ez + 1, y0, y1, 2);
         }
         {                                                     // lower-left corner: 2, 3, 1, 0
           R y0 = 0, y1 = 0;
@@ -427,7 +484,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
           if (hasB) { y0 += eB[6]; y1 += eB[7]; }
           if (hasL) { y0 += eL[2]; y1 += eL[3]; }
           y0 += e00[0]; y1 += e00[1];
-          emit(2 * ex, 2 * ez, y0, y1);
+          emit(2 * ex, 2 * ez, y0, y1, 3);
         }
       }
       if (a.yP) {                                             // pressure node (ex, ez): 2, 3, 1, 0
@@ -468,6 +525,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
 // diag(K): sum over incident elements of the element diagonal, ascending element order.
 template <typename R>
 __global__ void k_diag(LevelGeo g, const R* __restrict__ eta, R* __restrict__ diag) {
+  pdl_entry();
   const int64_t nn = (int64_t)g.nnx * g.nnz;
   const double sx = 2.0 / g.hx, sz = 2.0 / g.hz, jac = g.hx * g.hz / 4.0;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
@@ -497,6 +555,7 @@ __global__ void k_diag(LevelGeo g, const R* __restrict__ eta, R* __restrict__ di
 // coarse viscosity: mean of the 36 fine qpoint values of the 2x2 children (element constant)
 template <typename R>
 __global__ void k_coarsen_eta(LevelGeo gc, const R* __restrict__ fine, R* __restrict__ coarse) {
+  pdl_entry();
   const int64_t nel = (int64_t)gc.nx * gc.nz;
   const int fnx = 2 * gc.nx;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
@@ -525,6 +584,7 @@ template <typename R>
 __global__ void k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
                            R* __restrict__ bc, const double* __restrict__ cheb_c, const R* __restrict__ diag_c,
                            R* __restrict__ xc, R* __restrict__ dc) {
+  pdl_entry();
   // also performs the coarse level's first Chebyshev step from a zero guess when cheb_c != null:
   // x_c = d_c = (1/theta_c) D_c^-1 b_c
   const double c0 = cheb_c ? cheb_c[1] : 0.0;
@@ -569,6 +629,7 @@ MW_D int pw(int i, int* J, double* w) {
 template <typename R>
 __global__ void k_prolong_add(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc, const uint8_t* __restrict__ fixf,
                               R* __restrict__ xf) {
+  pdl_entry();
   const int64_t nn = (int64_t)gf.nnx * gf.nnz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
     int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
@@ -590,6 +651,7 @@ __global__ void k_prolong_add(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc
 
 template <typename R>
 __global__ void k_fix_coarse(LevelGeo gc, const uint8_t* __restrict__ fixf, int fnnx, uint8_t* __restrict__ fixc) {
+  pdl_entry();
   // a coarse dof is fixed when the coincident fine dof is fixed (same boundaries)
   const int64_t nn = (int64_t)gc.nnx * gc.nnz;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
@@ -603,6 +665,7 @@ __global__ void k_fix_coarse(LevelGeo gc, const uint8_t* __restrict__ fixf, int 
 // ---------------------------------------------------------------- BLAS-1 with device scalars
 template <typename R>
 __global__ void k_dot_partial(int64_t n, const R* __restrict__ x, const R* __restrict__ y, double* __restrict__ part) {
+  pdl_entry();
   __shared__ double sh[32];
   double v = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -619,6 +682,7 @@ __global__ void k_dot_partial(int64_t n, const R* __restrict__ x, const R* __res
 }
 
 __global__ void k_dot_final(const double* __restrict__ part, int nb, double* __restrict__ out) {
+  pdl_entry();
   __shared__ double sh[32];
   double v = 0;
   for (int i = threadIdx.x; i < nb; i += blockDim.x) v += part[i];
@@ -637,6 +701,7 @@ __global__ void k_dot_final(const double* __restrict__ part, int nb, double* __r
 template <typename R, typename S>
 __global__ void k_axpy_ratio(int64_t n, const double* __restrict__ num, const double* __restrict__ den, double sgn,
                              const S* __restrict__ x, R* __restrict__ y) {
+  pdl_entry();
   const double a = sgn * (*num / *den);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = (R)((double)y[i] + a * (double)x[i]);
@@ -646,6 +711,7 @@ __global__ void k_axpy_ratio(int64_t n, const double* __restrict__ num, const do
 template <typename R>
 __global__ void k_xpby_ratio(int64_t n, const R* __restrict__ z, const double* __restrict__ num,
                              const double* __restrict__ den, R* __restrict__ p) {
+  pdl_entry();
   const double b = *num / *den;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     p[i] = (R)((double)z[i] + b * (double)p[i]);
@@ -653,18 +719,21 @@ __global__ void k_xpby_ratio(int64_t n, const R* __restrict__ z, const double* _
 
 template <typename R>
 __global__ void k_axpy(int64_t n, double a, const R* __restrict__ x, R* __restrict__ y) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = (R)((double)y[i] + a * (double)x[i]);
 }
 
 template <typename R, typename S>
 __global__ void k_copy(int64_t n, const S* __restrict__ x, R* __restrict__ y) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = (R)x[i];
 }
 
 template <typename R>
 __global__ void k_set(int64_t n, R v, R* __restrict__ y) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) y[i] = v;
 }
 
@@ -672,6 +741,7 @@ __global__ void k_set(int64_t n, R v, R* __restrict__ y) {
 template <typename R>
 __global__ void k_cheb_first(int64_t n, const double* __restrict__ cheb, const R* __restrict__ b,
                              const R* __restrict__ diag, R* __restrict__ x, R* __restrict__ d) {
+  pdl_entry();
   const R c = (R)cheb[1];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     R v = c * b[i] / diag[i];
@@ -683,6 +753,7 @@ __global__ void k_cheb_first(int64_t n, const double* __restrict__ cheb, const R
 template <typename R>
 __global__ void k_scale_dinv_norm(int64_t n, const R* __restrict__ y, const R* __restrict__ diag,
                                   const double* __restrict__ nrm2, R* __restrict__ x) {
+  pdl_entry();
   const double inv = 1.0 / sqrt(fmax(*nrm2, 1e-300));
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] = (R)((double)y[i] / (double)diag[i] * inv);
@@ -690,6 +761,7 @@ __global__ void k_scale_dinv_norm(int64_t n, const R* __restrict__ y, const R* _
 
 template <typename R>
 __global__ void k_dinv(int64_t n, const R* __restrict__ y, const R* __restrict__ diag, R* __restrict__ x) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     x[i] = y[i] / diag[i];
 }
@@ -697,6 +769,7 @@ __global__ void k_dinv(int64_t n, const R* __restrict__ y, const R* __restrict__
 // Chebyshev coefficients from lambda_max (stored at lam[0] as ||D^-1 K x||^2 with ||x|| = 1).
 __global__ void k_cheb_coeffs(const double* __restrict__ lam2, int degree, double ratio, double safety,
                               double* __restrict__ coef) {
+  pdl_entry();
   if (threadIdx.x || blockIdx.x) return;
   double lmax = sqrt(fmax(*lam2, 1e-300)) * safety;
   double lmin = lmax / ratio;
@@ -716,6 +789,7 @@ __global__ void k_cheb_coeffs(const double* __restrict__ lam2, int degree, doubl
 template <typename R>
 __global__ void k_dense_assemble(LevelGeo g, const R* __restrict__ eta, const uint8_t* __restrict__ fix,
                                  double* __restrict__ A) {
+  pdl_entry();
   const int nd = 2 * g.nnx * g.nnz;
   for (int i = threadIdx.x; i < nd * nd; i += blockDim.x) A[i] = 0.0;
   __syncthreads();
@@ -751,6 +825,7 @@ __global__ void k_dense_assemble(LevelGeo g, const R* __restrict__ eta, const ui
 // In-place Gauss-Jordan inversion of an SPD matrix, one CTA.
 // Same inversion with the whole matrix held in shared memory (nd*nd doubles + a column).
 __global__ void k_gauss_jordan_smem(int nd, double* __restrict__ Ag) {
+  pdl_entry();
   extern __shared__ double sm[];
   double* A = sm;
   double* col = sm + (size_t)nd * nd;
@@ -777,6 +852,7 @@ __global__ void k_gauss_jordan_smem(int nd, double* __restrict__ Ag) {
 }
 
 __global__ void k_gauss_jordan(int nd, double* __restrict__ A) {
+  pdl_entry();
   extern __shared__ double col[];
   for (int k = 0; k < nd; ++k) {
     __syncthreads();
@@ -797,6 +873,7 @@ __global__ void k_gauss_jordan(int nd, double* __restrict__ A) {
 
 template <typename R>
 __global__ void k_dense_matvec(int nd, const double* __restrict__ Ainv, const R* __restrict__ b, R* __restrict__ x) {
+  pdl_entry();
   // one warp per row
   int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nd) return;
@@ -811,6 +888,7 @@ __global__ void k_dense_matvec(int nd, const double* __restrict__ Ainv, const R*
 // M_el = sum_q N_P N_P^T JxW (build_matrix_stokes.py:147), M_eta = M_el / eta_e (:264).
 __global__ void k_mass_apply(LevelGeo g, const double* __restrict__ w, const double* __restrict__ p,
                              double* __restrict__ y) {
+  pdl_entry();
   const int ncx = g.nx + 1;
   const int64_t np = (int64_t)ncx * (g.nz + 1);
   const double jac = g.hx * g.hz / 4.0;
@@ -838,6 +916,7 @@ __global__ void k_mass_apply(LevelGeo g, const double* __restrict__ w, const dou
 }
 
 __global__ void k_mass_diag(LevelGeo g, const double* __restrict__ w, double* __restrict__ d) {
+  pdl_entry();
   const int ncx = g.nx + 1;
   const int64_t np = (int64_t)ncx * (g.nz + 1);
   const double jac = g.hx * g.hz / 4.0;
@@ -867,6 +946,7 @@ __global__ void k_mass_diag(LevelGeo g, const double* __restrict__ w, double* __
 __global__ void k_mass_cheb(LevelGeo g, const double* __restrict__ w, const double* __restrict__ b,
                             const double* __restrict__ xin, double* __restrict__ xout, double* __restrict__ d,
                             const double* __restrict__ dg, double c1, double c2, int first) {
+  pdl_entry();
   __shared__ double Me[16];
   if (threadIdx.x < 16) {
     const double jac = g.hx * g.hz / 4.0;
@@ -905,6 +985,7 @@ __global__ void k_mass_cheb(LevelGeo g, const double* __restrict__ w, const doub
 template <typename R>
 __global__ void k_dot1(int64_t n, const R* __restrict__ x, const R* __restrict__ y, double* __restrict__ part,
                        unsigned* __restrict__ counter, double* __restrict__ out) {
+  pdl_entry();
   __shared__ double sh[32];
   __shared__ bool last;
   double v = 0;
@@ -943,6 +1024,7 @@ __global__ void k_dot1(int64_t n, const R* __restrict__ x, const R* __restrict__
 template <typename R>
 __global__ void k_pcg_update(int64_t n, const double* __restrict__ num, const double* __restrict__ den,
                              const R* __restrict__ p, const R* __restrict__ Ap, R* __restrict__ x, R* __restrict__ r) {
+  pdl_entry();
   const double a = *num / *den;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] = (R)((double)x[i] + a * (double)p[i]);
@@ -953,6 +1035,7 @@ __global__ void k_pcg_update(int64_t n, const double* __restrict__ num, const do
 // element weights 1/eta_e for M_eta (eta_e = mean of the qpoint viscosities of the element)
 __global__ void k_inv_eta_e(int64_t nel, const double* __restrict__ etaq, const double* __restrict__ eta_e,
                             double* __restrict__ w) {
+  pdl_entry();
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
     double v;
     if (eta_e) v = eta_e[e];
@@ -963,11 +1046,13 @@ __global__ void k_inv_eta_e(int64_t nel, const double* __restrict__ etaq, const 
 
 // remove the mean (pressure null space of a closed box): x -= sum(x)/n
 __global__ void k_sub_mean(int64_t n, const double* __restrict__ sum, double* __restrict__ x) {
+  pdl_entry();
   const double m = *sum / (double)n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) x[i] -= m;
 }
 
 __global__ void k_sum_partial(int64_t n, const double* __restrict__ x, double* __restrict__ part) {
+  pdl_entry();
   __shared__ double sh[32];
   double v = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) v += x[i];
@@ -1143,7 +1228,7 @@ static size_t layout(mw_stokes* S, Arena& A) {
 template <typename R, int MODE>
 static void launch_apply(const LevelGeo& g, const ApplyArgs<R>& a, cudaStream_t s) {
   dim3 grid((g.nx + TX - 1) / TX, (g.nz + TZ - 1) / TZ);
-  k_apply<R, MODE><<<grid, APPLY_THREADS, 0, s>>>(g, a);
+  pdl_launch(k_apply<R, MODE>, grid, APPLY_THREADS, 0, s, g, a);
 }
 
 template <typename R>
@@ -1155,12 +1240,12 @@ static ApplyArgs<R> args0() {
 
 template <typename R>
 static void dot(mw_stokes* S, int64_t n, const R* x, const R* y, double* out, cudaStream_t s) {
-  k_dot1<R><<<NB, 256, 0, s>>>(n, x, y, S->red, S->counter, out);
+  pdl_launch(k_dot1<R>, NB, 256, 0, s, n, x, y, S->red, S->counter, out);
 }
 
 static void dsum(mw_stokes* S, int64_t n, const double* x, double* out, cudaStream_t s) {
-  k_sum_partial<<<NB, 256, 0, s>>>(n, x, S->red);
-  k_dot_final<<<1, 256, 0, s>>>(S->red, NB, out);
+  pdl_launch(k_sum_partial, NB, 256, 0, s, n, x, S->red);
+  pdl_launch(k_dot_final, 1, 256, 0, s, S->red, NB, out);
 }
 
 template <typename R>
@@ -1177,7 +1262,7 @@ static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s, boo
   if (first_done) {
     // x = d = (1/theta) D^-1 b was written by the restriction kernel
   } else if (zero_start) {
-    k_cheb_first<R><<<grid_for(n, 256), 256, 0, s>>>(n, L.cheb, L.b, L.diag, L.x, L.d);
+    pdl_launch(k_cheb_first<R>, grid_for(n, 256), 256, 0, s, n, L.cheb, L.b, L.diag, L.x, L.d);
   } else {
     // restart the recurrence from the current x: d = (1/theta) D^-1 r; x += d
     ApplyArgs<R> a = args0<R>();
@@ -1201,7 +1286,7 @@ static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool firs
   if (l == H.nlev - 1) {
     if (H.dense) {
       int nd = H.nd;
-      k_dense_matvec<R><<<(nd * 32 + 255) / 256, 256, 0, s>>>(nd, H.Ainv, L.b, L.x);
+      pdl_launch(k_dense_matvec<R>, (nd * 32 + 255) / 256, 256, 0, s, nd, H.Ainv, L.b, L.x);
     } else {
       smooth(L, MAXDEG, !first_done, s, first_done);
     }
@@ -1213,10 +1298,10 @@ static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool firs
   a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.r; a.bV = L.b;
   launch_apply<R, AM_RESID>(L.g, a, s);
   const bool fuse = !(l + 1 == H.nlev - 1 && H.dense);
-  k_restrict<R><<<grid_for(C.nn, 256), 256, 0, s>>>(L.g, C.g, L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
-                                                      C.x, C.d);
+  pdl_launch(k_restrict<R>, grid_for(C.nn, 256), 256, 0, s, L.g, C.g, L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
+             C.x, C.d);
   vcycle(H, l + 1, degree, s, fuse);
-  k_prolong_add<R><<<grid_for(L.nn, 256), 256, 0, s>>>(L.g, C.g, C.x, L.fix, L.x);
+  pdl_launch(k_prolong_add<R>, grid_for(L.nn, 256), 256, 0, s, L.g, C.g, C.x, L.fix, L.x);
   smooth(L, degree, false, s);
 }
 
@@ -1302,12 +1387,14 @@ static void vcycle_run(mw_stokes* S, Hierarchy<R>& H, int degree, cudaStream_t s
 
 template <typename R>
 __global__ void k_power_init(int64_t n, R* __restrict__ v) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     v[i] = (R)(1.0 + 0.5 * sin(0.7 * (double)i));
 }
 
 template <typename R>
 __global__ void k_normalize(int64_t n, const double* __restrict__ nrm2, R* __restrict__ v) {
+  pdl_entry();
   const double inv = 1.0 / sqrt(fmax(*nrm2, 1e-300));
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     v[i] = (R)((double)v[i] * inv);
@@ -1323,13 +1410,13 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
     Level<R>& L = H.L[l];
     if (l > 0) {
       Level<R>& F = H.L[l - 1];
-      k_coarsen_eta<R><<<grid_for(L.nel, 256), 256, 0, s>>>(L.g, F.eta, L.eta);
-      k_fix_coarse<R><<<grid_for(L.nn, 256), 256, 0, s>>>(L.g, F.fix, F.g.nnx, L.fix);
+      pdl_launch(k_coarsen_eta<R>, grid_for(L.nel, 256), 256, 0, s, L.g, F.eta, L.eta);
+      pdl_launch(k_fix_coarse<R>, grid_for(L.nn, 256), 256, 0, s, L.g, F.fix, F.g.nnx, L.fix);
     }
-    k_diag<R><<<grid_for(L.nn, 128), 128, 0, s>>>(L.g, L.eta, L.diag);
+    pdl_launch(k_diag<R>, grid_for(L.nn, 128), 128, 0, s, L.g, L.eta, L.diag);
     const bool coarsest = l == H.nlev - 1;
     if (coarsest && H.dense) {
-      k_dense_assemble<R><<<1, 1024, 0, s>>>(L.g, L.eta, L.fix, H.Ainv);
+      pdl_launch(k_dense_assemble<R>, 1, 1024, 0, s, L.g, L.eta, L.fix, H.Ainv);
       const size_t smem = sizeof(double) * ((size_t)H.nd * H.nd + H.nd);
       int dev = 0, optin = 0;
       cudaGetDevice(&dev);
@@ -1345,29 +1432,29 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
         if (dev >= 0 && dev < 64) smem_set[dev] = smem;
       }
       if (smem_ok)
-        k_gauss_jordan_smem<<<1, 1024, smem, s>>>(H.nd, H.Ainv);
+        pdl_launch(k_gauss_jordan_smem, 1, 1024, smem, s, H.nd, H.Ainv);
       else
-        k_gauss_jordan<<<1, 1024, sizeof(double) * H.nd, s>>>(H.nd, H.Ainv);
+        pdl_launch(k_gauss_jordan, 1, 1024, sizeof(double) * H.nd, s, H.nd, H.Ainv);
       continue;
     }
     // power iteration v <- D^-1 K v / |v|, warm-started from the previous viscosity's vector
     R* v = L.ev;
     int iters = prm.power_iters;
     if (!L.ev_ready) {
-      k_power_init<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, v);
+      pdl_launch(k_power_init<R>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, v);
       L.ev_ready = true;
     } else {
       iters = prm.power_iters_warm > 0 ? prm.power_iters_warm : prm.power_iters;
     }
     for (int it = 0; it < iters; ++it) {
       dot<R>(S, L.ndof, v, v, L.lam2 + 1, s);
-      k_normalize<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.lam2 + 1, v);
+      pdl_launch(k_normalize<R>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.lam2 + 1, v);
       k_only_apply<R>(L, v, L.d, s);
-      k_dinv<R><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.d, L.diag, v);
+      pdl_launch(k_dinv<R>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.d, L.diag, v);
     }
     dot<R>(S, L.ndof, v, v, L.lam2, s);          // ||D^-1 K v_prev||^2 with ||v_prev|| = 1
     int deg = coarsest ? MAXDEG : prm.cheb_degree;
-    k_cheb_coeffs<<<1, 32, 0, s>>>(L.lam2, deg, prm.cheb_ratio, prm.cheb_safety, L.cheb);
+    pdl_launch(k_cheb_coeffs, 1, 32, 0, s, L.lam2, deg, prm.cheb_ratio, prm.cheb_safety, L.cheb);
   }
   return cudaGetLastError() == cudaSuccess ? MW_OK : MW_ERR_CUDA;
 }
@@ -1389,12 +1476,12 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
   R *xr = pc[0], *r = pc[1], *p = pc[3], *Ap = pc[4];
   R*& z = pc[2];
   double* sc = S->sc;   // [0] rz, [1] pAp, [2] rr, [3] bb, [4] rz_new
-  k_copy<R, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
-  k_set<R><<<grid_for(n, 256), 256, 0, s>>>(n, R(0), xr);
+  pdl_launch(k_copy<R, double>, grid_for(n, 256), 256, 0, s, n, b, r);
+  pdl_launch(k_set<R>, grid_for(n, 256), 256, 0, s, n, R(0), xr);
   dot<R>(S, n, r, r, sc + 3, s);
   double bb = read_scalar(sc + 3, s);
   if (!(bb > 0)) {
-    k_set<double><<<grid_for(n, 256), 256, 0, s>>>(n, 0.0, x);
+    pdl_launch(k_set<double>, grid_for(n, 256), 256, 0, s, n, 0.0, x);
     *relres = 0;
     return 0;
   }
@@ -1408,24 +1495,24 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
     std::swap(zout, L.x);
   };
   precond(r, z);
-  k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
+  pdl_launch(k_copy<R, R>, grid_for(n, 256), 256, 0, s, n, z, p);
   dot<R>(S, n, r, z, sc + 0, s);
   int it = 0;
   double rr = bb;
   for (it = 1; it <= maxit; ++it) {
     k_only_apply<R>(L, p, Ap, s);
     dot<R>(S, n, p, Ap, sc + 1, s);
-    k_pcg_update<R><<<grid_for(n, 256), 256, 0, s>>>(n, sc + 0, sc + 1, p, Ap, xr, r);
+    pdl_launch(k_pcg_update<R>, grid_for(n, 256), 256, 0, s, n, sc + 0, sc + 1, p, Ap, xr, r);
     dot<R>(S, n, r, r, sc + 2, s);
     rr = read_scalar(sc + 2, s);
     if (!std::isfinite(rr)) break;
     if (rr <= rtol * rtol * bb) break;
     precond(r, z);
     dot<R>(S, n, r, z, sc + 4, s);
-    k_xpby_ratio<R><<<grid_for(n, 256), 256, 0, s>>>(n, z, sc + 4, sc + 0, p);
+    pdl_launch(k_xpby_ratio<R>, grid_for(n, 256), 256, 0, s, n, z, sc + 4, sc + 0, p);
     cudaMemcpyAsync(sc + 0, sc + 4, sizeof(double), cudaMemcpyDeviceToDevice, s);
   }
-  k_copy<double, R><<<grid_for(n, 256), 256, 0, s>>>(n, xr, x);
+  pdl_launch(k_copy<double, R>, grid_for(n, 256), 256, 0, s, n, xr, x);
   *relres = std::sqrt(rr / bb);
   return it > maxit ? maxit : it;
 }
@@ -1465,13 +1552,13 @@ static void mass_solve_kernels(mw_stokes* S, const double* w, const double* b, d
     }
     double* xin = bufs[(K - k) % 2];
     double* xout = bufs[(K - 1 - k) % 2];
-    k_mass_cheb<<<grid_for(n, 256), 256, 0, s>>>(g, w, b, xin, xout, S->tP2, dg, c1, c2, k == 0);
+    pdl_launch(k_mass_cheb, grid_for(n, 256), 256, 0, s, g, w, b, xin, xout, S->tP2, dg, c1, c2, k == 0);
   }
 }
 
 static void remove_mean(mw_stokes* S, int64_t n, double* x, cudaStream_t s) {
   dsum(S, n, x, S->sc + 40, s);
-  k_sub_mean<<<grid_for(n, 256), 256, 0, s>>>(n, S->sc + 40, x);
+  pdl_launch(k_sub_mean, grid_for(n, 256), 256, 0, s, n, S->sc + 40, x);
 }
 
 // Full saddle residual in FP64: (RV, RP) = (f, h) - [K G; G^T 0] (V, P).  Returns ||R||/||b||
@@ -1515,6 +1602,7 @@ static int solve_K(mw_stokes* S, int prec, const double* b, double* x, double rt
 // Convergence history row k in the reference's terms (uzawa3_solver_L2.py:85-88, cd_u_eta.py):
 // xiV = ||alpha d_k||, xiP = ||alpha p_k||, alpha, beta.  hist is [4][len] (xiV, xiP, alpha, beta).
 __global__ void k_history(const double* __restrict__ sc, double* __restrict__ hist, int len, int k) {
+  pdl_entry();
   const double alpha = sc[0] / sc[1];
   hist[k] = fabs(alpha) * sqrt(sc[6]);
   hist[len + k] = fabs(alpha) * sqrt(sc[5]);
@@ -1546,12 +1634,12 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
     a.u = V; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64;
     a.yP = S->rP;
     launch_apply<double, AM_APPLY>(g, a, s);                 // rP = G^T V (yV not written)
-    if (h) k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
+    if (h) pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
   }
   remove_mean(S, np, S->rP, s);
   mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
   remove_mean(S, np, S->wP, s);
-  k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, S->dP);
+  pdl_launch(k_copy<double, double>, grid_for(np, 256), 256, 0, s, np, S->wP, S->dP);
   double* sc = S->sc + 24;    // [0] rw, [1] dSd, [2] rw_new, [3] rr0, [4] rr
   dot<double>(S, np, S->rP, S->wP, sc + 0, s);
   dot<double>(S, np, S->rP, S->rP, sc + 3, s);
@@ -1575,15 +1663,15 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
       dot<double>(S, np, S->dP, S->dP, sc + 5, s);
       dot<double>(S, nv, S->z, S->z, sc + 6, s);
     }
-    k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, 1.0, S->dP, P);
-    k_axpy_ratio<double, double><<<grid_for(nv, 256), 256, 0, s>>>(nv, sc + 0, sc + 1, -1.0, S->z, V);
-    k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, sc + 0, sc + 1, -1.0, S->GTz, S->rP);
+    pdl_launch(k_axpy_ratio<double, double>, grid_for(np, 256), 256, 0, s, np, sc + 0, sc + 1, 1.0, S->dP, P);
+    pdl_launch(k_axpy_ratio<double, double>, grid_for(nv, 256), 256, 0, s, nv, sc + 0, sc + 1, -1.0, S->z, V);
+    pdl_launch(k_axpy_ratio<double, double>, grid_for(np, 256), 256, 0, s, np, sc + 0, sc + 1, -1.0, S->GTz, S->rP);
     remove_mean(S, np, S->rP, s);
     mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
     remove_mean(S, np, S->wP, s);
     dot<double>(S, np, S->rP, S->wP, sc + 2, s);
-    if (hist) k_history<<<1, 1, 0, s>>>(sc, sp.history, sp.history_len, info->outer_iters);
-    k_xpby_ratio<double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, sc + 2, sc + 0, S->dP);
+    if (hist) pdl_launch(k_history, 1, 1, 0, s, sc, sp.history, sp.history_len, info->outer_iters);
+    pdl_launch(k_xpby_ratio<double>, grid_for(np, 256), 256, 0, s, np, S->wP, sc + 2, sc + 0, S->dP);
     cudaMemcpyAsync(sc + 0, sc + 2, sizeof(double), cudaMemcpyDeviceToDevice, s);
     info->outer_iters += 1;
     dot<double>(S, np, S->rP, S->rP, sc + 4, s);
@@ -1618,6 +1706,7 @@ enum DevSlot {
 constexpr double DEV_INNER_BUDGET = 40000, DEV_OUTER_BUDGET = 4000;
 
 __global__ void k_dev_pcg_init(double* sc, cudaGraphConditionalHandle hw) {
+  pdl_entry();
   sc[P_IT] = 0;
   const double bb = sc[P_BB];
   cudaGraphSetConditional(hw, (bb > 0 && isfinite(bb)) ? 1u : 0u);
@@ -1625,6 +1714,7 @@ __global__ void k_dev_pcg_init(double* sc, cudaGraphConditionalHandle hw) {
 
 __global__ void k_dev_pcg_check(double* sc, double rtol, int maxit, cudaGraphConditionalHandle hw,
                                 cudaGraphConditionalHandle hi) {
+  pdl_entry();
   const double it = sc[P_IT] + 1;
   sc[P_IT] = it;
   const double rr = sc[P_RR];
@@ -1634,9 +1724,11 @@ __global__ void k_dev_pcg_check(double* sc, double rtol, int maxit, cudaGraphCon
   cudaGraphSetConditional(hi, go ? 1u : 0u);
 }
 
-__global__ void k_dev_pcg_done(double* sc) { sc[I_INNER] += sc[P_IT]; }
+__global__ void k_dev_pcg_done(double* sc) {
+  pdl_entry(); sc[I_INNER] += sc[P_IT]; }
 
 __global__ void k_dev_uz_init(double* sc, int max_outer, cudaGraphConditionalHandle hw) {
+  pdl_entry();
   sc[U_IT] = 0;
   cudaGraphSetConditional(hw, (max_outer > 0 && isfinite(sc[U_RR0]) && sc[I_STATUS] == 0) ? 1u : 0u);
 }
@@ -1645,6 +1737,7 @@ __global__ void k_dev_uz_init(double* sc, int max_outer, cudaGraphConditionalHan
 // (check_true), on the Schur residual reduction, at max_outer or at the work cap (status 3)
 __global__ void k_dev_uz_check(double* sc, double reduction, int check_true, double tol, int max_outer,
                                cudaGraphConditionalHandle hw) {
+  pdl_entry();
   const double it = sc[U_IT] + 1;
   sc[U_IT] = it;
   sc[I_OUTER] += 1;
@@ -1659,6 +1752,7 @@ __global__ void k_dev_uz_check(double* sc, double reduction, int check_true, dou
 }
 
 __global__ void k_dev_hist(const double* sc, double* hist, int len) {
+  pdl_entry();
   const int k = (int)sc[I_OUTER];
   if (k < 0 || k >= len) return;
   const double alpha = sc[U_RW] / sc[U_DSD];
@@ -1668,9 +1762,11 @@ __global__ void k_dev_hist(const double* sc, double* hist, int len) {
   hist[3 * len + k] = sc[U_RWN] / sc[U_RW];
 }
 
-__global__ void k_dev_rel(double* sc) { sc[T_REL] = sqrt(sc[T_RV] + sc[T_RP]) / sc[S_BNORM]; }
+__global__ void k_dev_rel(double* sc) {
+  pdl_entry(); sc[T_REL] = sqrt(sc[T_RV] + sc[T_RP]) / sc[S_BNORM]; }
 
 __global__ void k_dev_solve_init(double* sc) {
+  pdl_entry();
   sc[S_BNORM] = sqrt(sc[S_BB] + sc[S_BH]);
   sc[S_NREF] = 0;
   sc[I_OUTER] = 0;
@@ -1679,19 +1775,22 @@ __global__ void k_dev_solve_init(double* sc) {
 }
 
 __global__ void k_dev_ref_init(double* sc, double tol, int max_refine, cudaGraphConditionalHandle hw) {
+  pdl_entry();
   sc[S_REL0] = sc[T_REL];
   const double r = sc[T_REL];
   cudaGraphSetConditional(hw, (isfinite(r) && r > tol && max_refine > 0) ? 1u : 0u);
 }
 
 __global__ void k_dev_ref_check(double* sc, double tol, int max_refine, cudaGraphConditionalHandle hw) {
+  pdl_entry();
   sc[S_NREF] += 1;
   const double r = sc[T_REL];
   const bool go = isfinite(r) && r > tol && sc[S_NREF] < (double)max_refine && sc[I_STATUS] == 0;
   cudaGraphSetConditional(hw, go ? 1u : 0u);
 }
 
-__global__ void k_copy1(const double* src, double* dst) { *dst = *src; }
+__global__ void k_copy1(const double* src, double* dst) {
+  pdl_entry(); *dst = *src; }
 
 // A conditional handle in the graph being captured on s (its value is set by kernels of that graph).
 static bool cond_handle(cudaStream_t s, cudaGraphConditionalHandle* h) {
@@ -1749,31 +1848,31 @@ static bool pcg_K_dev(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, do
     L.b = saved_b;
     std::swap(zout, L.x);
   };
-  k_copy<R, double><<<grid_for(n, 256), 256, 0, s>>>(n, b, r);
-  k_set<R><<<grid_for(n, 256), 256, 0, s>>>(n, R(0), xr);
+  pdl_launch(k_copy<R, double>, grid_for(n, 256), 256, 0, s, n, b, r);
+  pdl_launch(k_set<R>, grid_for(n, 256), 256, 0, s, n, R(0), xr);
   dot<R>(S, n, r, r, sc + P_BB, s);
   precond(r, z, s);
-  k_copy<R, R><<<grid_for(n, 256), 256, 0, s>>>(n, z, p);
+  pdl_launch(k_copy<R, R>, grid_for(n, 256), 256, 0, s, n, z, p);
   dot<R>(S, n, r, z, sc + P_RZ, s);
   cudaGraphConditionalHandle hw, hi;
   if (!cond_handle(s, &hw)) return false;
-  k_dev_pcg_init<<<1, 1, 0, s>>>(sc, hw);
+  pdl_launch(k_dev_pcg_init, 1, 1, 0, s, sc, hw);
   if (!cond_node(s, b1, cudaGraphCondTypeWhile, hw)) return false;
   // body: one CG step and the convergence test, then (if continuing) the next search direction
   k_only_apply<R>(L, p, Ap, b1);
   dot<R>(S, n, p, Ap, sc + P_PAP, b1);
-  k_pcg_update<R><<<grid_for(n, 256), 256, 0, b1>>>(n, sc + P_RZ, sc + P_PAP, p, Ap, xr, r);
+  pdl_launch(k_pcg_update<R>, grid_for(n, 256), 256, 0, b1, n, sc + P_RZ, sc + P_PAP, p, Ap, xr, r);
   dot<R>(S, n, r, r, sc + P_RR, b1);
   if (!cond_handle(b1, &hi)) return false;
-  k_dev_pcg_check<<<1, 1, 0, b1>>>(sc, rtol, maxit, hw, hi);
+  pdl_launch(k_dev_pcg_check, 1, 1, 0, b1, sc, rtol, maxit, hw, hi);
   if (!cond_node(b1, b2, cudaGraphCondTypeIf, hi)) return false;
   precond(r, z, b2);
   dot<R>(S, n, r, z, sc + P_RZN, b2);
-  k_xpby_ratio<R><<<grid_for(n, 256), 256, 0, b2>>>(n, z, sc + P_RZN, sc + P_RZ, p);
-  k_copy1<<<1, 1, 0, b2>>>(sc + P_RZN, sc + P_RZ);
+  pdl_launch(k_xpby_ratio<R>, grid_for(n, 256), 256, 0, b2, n, z, sc + P_RZN, sc + P_RZ, p);
+  pdl_launch(k_copy1, 1, 1, 0, b2, sc + P_RZN, sc + P_RZ);
   if (!cond_end(b2) || !cond_end(b1)) return false;
-  k_copy<double, R><<<grid_for(n, 256), 256, 0, s>>>(n, xr, x);
-  k_dev_pcg_done<<<1, 1, 0, s>>>(sc);
+  pdl_launch(k_copy<double, R>, grid_for(n, 256), 256, 0, s, n, xr, x);
+  pdl_launch(k_dev_pcg_done, 1, 1, 0, s, sc);
   return true;
 }
 
@@ -1795,7 +1894,7 @@ static void true_residual_dev(mw_stokes* S, const double* V, const double* P, co
   const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
   dot<double>(S, nv, S->RV, S->RV, S->sc + T_RV, s);
   dot<double>(S, np, S->RP, S->RP, S->sc + T_RP, s);
-  k_dev_rel<<<1, 1, 0, s>>>(S->sc);
+  pdl_launch(k_dev_rel, 1, 1, 0, s, S->sc);
 }
 
 // Schur-complement CG (the recurrences of the host version `uzawa`) recorded with a device WHILE
@@ -1819,17 +1918,17 @@ static bool uzawa_dev(mw_stokes* S, const mw_solve_params& sp, int prec, const d
     a.u = V; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64;
     a.yP = S->rP;
     launch_apply<double, AM_APPLY>(g, a, s);
-    if (h) k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
+    if (h) pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
   }
   remove_mean(S, np, S->rP, s);
   mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
   remove_mean(S, np, S->wP, s);
-  k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->wP, S->dP);
+  pdl_launch(k_copy<double, double>, grid_for(np, 256), 256, 0, s, np, S->wP, S->dP);
   dot<double>(S, np, S->rP, S->wP, sc + U_RW, s);
   dot<double>(S, np, S->rP, S->rP, sc + U_RR0, s);
   cudaGraphConditionalHandle hw;
   if (!cond_handle(s, &hw)) return false;
-  k_dev_uz_init<<<1, 1, 0, s>>>(sc, sp.max_outer, hw);
+  pdl_launch(k_dev_uz_init, 1, 1, 0, s, sc, sp.max_outer, hw);
   if (!cond_node(s, b1, cudaGraphCondTypeWhile, hw)) return false;
   {
     ApplyArgs<double> a = args0<double>();
@@ -1849,19 +1948,20 @@ static bool uzawa_dev(mw_stokes* S, const mw_solve_params& sp, int prec, const d
     dot<double>(S, np, S->dP, S->dP, sc + U_D2, b1);
     dot<double>(S, nv, S->z, S->z, sc + U_Z2, b1);
   }
-  k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, b1>>>(np, sc + U_RW, sc + U_DSD, 1.0, S->dP, P);
-  k_axpy_ratio<double, double><<<grid_for(nv, 256), 256, 0, b1>>>(nv, sc + U_RW, sc + U_DSD, -1.0, S->z, V);
-  k_axpy_ratio<double, double><<<grid_for(np, 256), 256, 0, b1>>>(np, sc + U_RW, sc + U_DSD, -1.0, S->GTz, S->rP);
+  pdl_launch(k_axpy_ratio<double, double>, grid_for(np, 256), 256, 0, b1, np, sc + U_RW, sc + U_DSD, 1.0, S->dP, P);
+  pdl_launch(k_axpy_ratio<double, double>, grid_for(nv, 256), 256, 0, b1, nv, sc + U_RW, sc + U_DSD, -1.0, S->z, V);
+  pdl_launch(k_axpy_ratio<double, double>, grid_for(np, 256), 256, 0, b1, np, sc + U_RW, sc + U_DSD, -1.0, S->GTz,
+             S->rP);
   remove_mean(S, np, S->rP, b1);
   mass_solve(S, w, S->rP, S->wP, sp.mass_iters, b1);
   remove_mean(S, np, S->wP, b1);
   dot<double>(S, np, S->rP, S->wP, sc + U_RWN, b1);
-  if (hist) k_dev_hist<<<1, 1, 0, b1>>>(sc, sp.history, sp.history_len);
-  k_xpby_ratio<double><<<grid_for(np, 256), 256, 0, b1>>>(np, S->wP, sc + U_RWN, sc + U_RW, S->dP);
-  k_copy1<<<1, 1, 0, b1>>>(sc + U_RWN, sc + U_RW);
+  if (hist) pdl_launch(k_dev_hist, 1, 1, 0, b1, sc, sp.history, sp.history_len);
+  pdl_launch(k_xpby_ratio<double>, grid_for(np, 256), 256, 0, b1, np, S->wP, sc + U_RWN, sc + U_RW, S->dP);
+  pdl_launch(k_copy1, 1, 1, 0, b1, sc + U_RWN, sc + U_RW);
   dot<double>(S, np, S->rP, S->rP, sc + U_RR, b1);
   if (check_true) true_residual_dev(S, V, P, f, h, b1);
-  k_dev_uz_check<<<1, 1, 0, b1>>>(sc, reduction, check_true ? 1 : 0, sp.tol, sp.max_outer, hw);
+  pdl_launch(k_dev_uz_check, 1, 1, 0, b1, sc, reduction, check_true ? 1 : 0, sp.tol, sp.max_outer, hw);
   return cond_end(b1);
 }
 
@@ -1872,34 +1972,34 @@ static bool stokes_solve_record(mw_stokes* S, const double* f, const double* h, 
   const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
   double* sc = S->sc;
   if (!sp.use_guess) {
-    k_set<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 0.0, V);
-    k_set<double><<<grid_for(np, 256), 256, 0, s>>>(np, 0.0, P);
+    pdl_launch(k_set<double>, grid_for(nv, 256), 256, 0, s, nv, 0.0, V);
+    pdl_launch(k_set<double>, grid_for(np, 256), 256, 0, s, np, 0.0, P);
   }
   dot<double>(S, nv, f, f, sc + S_BB, s);
   dot<double>(S, np, h, h, sc + S_BH, s);
-  k_dev_solve_init<<<1, 1, 0, s>>>(sc);
+  pdl_launch(k_dev_solve_init, 1, 1, 0, s, sc);
   true_residual_dev(S, V, P, f, h, s);
   cudaGraphConditionalHandle hc;
   if (!cond_handle(s, &hc)) return false;
   if (sp.precision == MW_F64) {
-    k_dev_ref_init<<<1, 1, 0, s>>>(sc, sp.tol, 1, hc);        // records the initial residual; gate on tol
+    pdl_launch(k_dev_ref_init, 1, 1, 0, s, sc, sp.tol, 1, hc);        // records the initial residual; gate on tol
     if (!cond_node(s, S->bs[0], cudaGraphCondTypeIf, hc)) return false;
     if (!uzawa_dev(S, sp, MW_F64, f, h, V, P, 0.0, true, s, 1)) return false;
     if (!cond_end(S->bs[0])) return false;
     true_residual_dev(S, V, P, f, h, s);
   } else {
-    k_dev_ref_init<<<1, 1, 0, s>>>(sc, sp.tol, sp.max_refine, hc);
+    pdl_launch(k_dev_ref_init, 1, 1, 0, s, sc, sp.tol, sp.max_refine, hc);
     if (!cond_node(s, S->bs[0], cudaGraphCondTypeWhile, hc)) return false;
     cudaStream_t b = S->bs[0];
-    k_copy<double, double><<<grid_for(nv, 256), 256, 0, b>>>(nv, S->RV, S->f);
-    k_copy<double, double><<<grid_for(np, 256), 256, 0, b>>>(np, S->RP, S->h);
-    k_set<double><<<grid_for(nv, 256), 256, 0, b>>>(nv, 0.0, S->cV);
-    k_set<double><<<grid_for(np, 256), 256, 0, b>>>(np, 0.0, S->cP);
+    pdl_launch(k_copy<double, double>, grid_for(nv, 256), 256, 0, b, nv, S->RV, S->f);
+    pdl_launch(k_copy<double, double>, grid_for(np, 256), 256, 0, b, np, S->RP, S->h);
+    pdl_launch(k_set<double>, grid_for(nv, 256), 256, 0, b, nv, 0.0, S->cV);
+    pdl_launch(k_set<double>, grid_for(np, 256), 256, 0, b, np, 0.0, S->cP);
     if (!uzawa_dev(S, sp, MW_F32, S->f, S->h, S->cV, S->cP, sp.sweep_reduction, false, s, 1)) return false;
-    k_axpy<double><<<grid_for(nv, 256), 256, 0, b>>>(nv, 1.0, S->cV, V);
-    k_axpy<double><<<grid_for(np, 256), 256, 0, b>>>(np, 1.0, S->cP, P);
+    pdl_launch(k_axpy<double>, grid_for(nv, 256), 256, 0, b, nv, 1.0, S->cV, V);
+    pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, b, np, 1.0, S->cP, P);
     true_residual_dev(S, V, P, f, h, b);
-    k_dev_ref_check<<<1, 1, 0, b>>>(sc, sp.tol, sp.max_refine, hc);
+    pdl_launch(k_dev_ref_check, 1, 1, 0, b, sc, sp.tol, sp.max_refine, hc);
     if (!cond_end(b)) return false;
   }
   return true;
@@ -1907,6 +2007,7 @@ static bool stokes_solve_record(mw_stokes* S, const double* f, const double* h, 
 
 template <typename R>
 __global__ void k_cast(int64_t n, const double* __restrict__ a, R* __restrict__ b) {
+  pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     b[i] = (R)a[i];
 }
@@ -2009,19 +2110,26 @@ int mw_stokes_levels(const mw_stokes* S, int32_t precision) {
 int mw_stokes_set_viscosity(mw_stokes* S, const double* etaq, const double* eta_e, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t nel = (int64_t)S->fine.nx * S->fine.nz;
-  k_cast<double><<<grid_for(nel * 9, 256), 256, 0, s>>>(nel * 9, etaq, S->etaq64);
-  if (S->has32) k_cast<float><<<grid_for(nel * 9, 256), 256, 0, s>>>(nel * 9, etaq, S->etaq32);
-  k_inv_eta_e<<<grid_for(nel, 256), 256, 0, s>>>(nel, etaq, eta_e, S->etae_w);
-  k_diag<double><<<grid_for((int64_t)S->fine.nnx * S->fine.nnz, 128), 128, 0, s>>>(S->fine, S->etaq64, S->diag64);
+  pdl_launch(k_cast<double>, grid_for(nel * 9, 256), 256, 0, s, nel * 9, etaq, S->etaq64);
+  if (S->has32) pdl_launch(k_cast<float>, grid_for(nel * 9, 256), 256, 0, s, nel * 9, etaq, S->etaq32);
+  pdl_launch(k_inv_eta_e, grid_for(nel, 256), 256, 0, s, nel, etaq, eta_e, S->etae_w);
+  pdl_launch(k_diag<double>, grid_for((int64_t)S->fine.nnx * S->fine.nnz, 128), 128, 0, s, S->fine, S->etaq64,
+             S->diag64);
   const int64_t np = (int64_t)(S->fine.nx + 1) * (S->fine.nz + 1);
-  k_mass_diag<<<grid_for(np, 256), 256, 0, s>>>(S->fine, nullptr, S->mdiag);      // M
-  k_mass_diag<<<grid_for(np, 256), 256, 0, s>>>(S->fine, S->etae_w, S->medi);     // M_eta
+  pdl_launch(k_mass_diag, grid_for(np, 256), 256, 0, s, S->fine, nullptr, S->mdiag);      // M
+  pdl_launch(k_mass_diag, grid_for(np, 256), 256, 0, s, S->fine, S->etae_w, S->medi);     // M_eta
   S->dirty64 = S->dirty32 = true;
   if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
   return MW_OK;
 }
 
+// The kernels read and write velocity vectors one (u, w) node pair per access, so velocity arrays
+// passed in must be aligned to a pair: 16 bytes in FP64, 8 in FP32 (a misaligned array is refused
+// here instead of faulting on the device).
+static bool pair_aligned(const void* p, size_t pair_bytes) { return ((uintptr_t)p % pair_bytes) == 0; }
+
 int mw_stokes_apply(mw_stokes* S, const double* u, const double* p, double* yV, double* yP, void* stream) {
+  if (!pair_aligned(u, 16) || !pair_aligned(yV, 16)) return MW_ERR_BAD_ARG;
   ApplyArgs<double> a = args0<double>();
   a.u = u; a.p = p; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64; a.yV = yV; a.yP = yP;
   launch_apply<double, AM_APPLY>(S->fine, a, (cudaStream_t)stream);
@@ -2030,7 +2138,7 @@ int mw_stokes_apply(mw_stokes* S, const double* u, const double* p, double* yV, 
 }
 
 int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV, float* yP, void* stream) {
-  if (!S->has32) return MW_ERR_BAD_ARG;
+  if (!S->has32 || !pair_aligned(u, 8) || !pair_aligned(yV, 8)) return MW_ERR_BAD_ARG;
   if (ensure_hierarchy(S, MW_F32, (cudaStream_t)stream)) return MW_ERR_CUDA;
   ApplyArgs<float> a = args0<float>();
   a.u = u; a.p = p; a.eta = S->etaq32; a.fix = S->fixV; a.diag = S->H32.L[0].diag; a.yV = yV; a.yP = yP;
@@ -2044,14 +2152,14 @@ int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, vo
   if (int rc = ensure_hierarchy(S, precision, s)) return rc;
   if (precision == MW_F32) {
     Level<float>& L = S->H32.L[0];
-    k_copy<float, float><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, (const float*)b, L.b);
+    pdl_launch(k_copy<float, float>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, (const float*)b, L.b);
     vcycle(S->H32, 0, S->prm.cheb_degree, s);
-    k_copy<float, float><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.x, (float*)x);
+    pdl_launch(k_copy<float, float>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.x, (float*)x);
   } else {
     Level<double>& L = S->H64.L[0];
-    k_copy<double, double><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, (const double*)b, L.b);
+    pdl_launch(k_copy<double, double>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, (const double*)b, L.b);
     vcycle(S->H64, 0, S->prm.cheb_degree, s);
-    k_copy<double, double><<<grid_for(L.ndof, 256), 256, 0, s>>>(L.ndof, L.x, (double*)x);
+    pdl_launch(k_copy<double, double>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.x, (double*)x);
   }
   MW_CHECK_LAUNCH();
   return MW_OK;
@@ -2062,6 +2170,7 @@ static void leave(mw_stokes* S, cudaStream_t caller, cudaStream_t s);
 
 int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,
                       int32_t* iters, double* relres, void* stream) {
+  if (!b || !x || !pair_aligned(b, 16) || !pair_aligned(x, 16)) return MW_ERR_BAD_ARG;
   double rr = 0;
   cudaStream_t caller = (cudaStream_t)stream;
   cudaStream_t s = enter(S, caller);
@@ -2080,7 +2189,7 @@ int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* 
 // of G^T V - h with its mean removed.
 int mw_stokes_uzawa_residual(mw_stokes* S, int32_t precision, const double* f, const double* h, const double* P,
                              double rtol, int32_t maxit, double* V, double* norm_out, void* stream) {
-  if (!f || !h || !P || !norm_out) return MW_ERR_BAD_ARG;
+  if (!f || !h || !P || !norm_out || !pair_aligned(f, 16) || !pair_aligned(V, 16)) return MW_ERR_BAD_ARG;
   cudaStream_t caller = (cudaStream_t)stream;
   cudaStream_t s = enter(S, caller);
   int rc = ensure_hierarchy(S, precision, s);
@@ -2096,7 +2205,7 @@ int mw_stokes_uzawa_residual(mw_stokes* S, int32_t precision, const double* f, c
     ApplyArgs<double> b = args0<double>();
     b.u = Vo; b.eta = S->etaq64; b.fix = S->fixV; b.diag = S->diag64; b.yP = S->rP;
     launch_apply<double, AM_APPLY>(g, b, s);                 // rP = G^T V
-    k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, -1.0, h, S->rP);
+    pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
     remove_mean(S, np, S->rP, s);
     dot<double>(S, np, S->rP, S->rP, S->sc + 54, s);
     double v = 0;
@@ -2111,6 +2220,7 @@ int mw_stokes_uzawa_residual(mw_stokes* S, int32_t precision, const double* f, c
 
 int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const double* f, const double* h, double* RV,
                        double* RP, double* norm_out, void* stream) {
+  if (!f || !h || !pair_aligned(V, 16) || !pair_aligned(f, 16)) return MW_ERR_BAD_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   double r = true_residual(S, V, P, f, h, 0.0, s);
   if (RV) cudaMemcpyAsync(RV, S->RV, sizeof(double) * 2 * S->fine.nnx * S->fine.nnz, cudaMemcpyDeviceToDevice, s);
@@ -2165,6 +2275,7 @@ static int stokes_solve_in_capture(mw_stokes* S, const double* f, const double* 
 
 int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
                     mw_solve_info* info, void* stream) {
+  if (!pair_aligned(f, 16) || !pair_aligned(solV, 16)) return MW_ERR_BAD_ARG;
   cudaStream_t caller = (cudaStream_t)stream;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (caller != nullptr && cudaStreamIsCapturing(caller, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
@@ -2299,8 +2410,8 @@ static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, dou
   if (!f || !h || !solV || !solP) return MW_ERR_BAD_ARG;
   if (int rc = ensure_hierarchy(S, sp.precision == MW_F32 ? MW_F32 : MW_F64, s)) return rc;
   if (!sp.use_guess) {
-    k_set<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 0.0, solV);
-    k_set<double><<<grid_for(np, 256), 256, 0, s>>>(np, 0.0, solP);
+    pdl_launch(k_set<double>, grid_for(nv, 256), 256, 0, s, nv, 0.0, solV);
+    pdl_launch(k_set<double>, grid_for(np, 256), 256, 0, s, np, 0.0, solP);
   }
   // ||b||
   dot<double>(S, nv, f, f, S->sc + 52, s);
@@ -2332,15 +2443,15 @@ static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, dou
       // solve A (cV, cP) = (RV, RP): copy the residual into f/h slots, zero guess
       double* fr = S->f;
       double* hr = S->h;
-      k_copy<double, double><<<grid_for(nv, 256), 256, 0, s>>>(nv, S->RV, fr);
-      k_copy<double, double><<<grid_for(np, 256), 256, 0, s>>>(np, S->RP, hr);
-      k_set<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 0.0, cV);
+      pdl_launch(k_copy<double, double>, grid_for(nv, 256), 256, 0, s, nv, S->RV, fr);
+      pdl_launch(k_copy<double, double>, grid_for(np, 256), 256, 0, s, np, S->RP, hr);
+      pdl_launch(k_set<double>, grid_for(nv, 256), 256, 0, s, nv, 0.0, cV);
       double* cPr = S->cP;
-      k_set<double><<<grid_for(np, 256), 256, 0, s>>>(np, 0.0, cPr);
+      pdl_launch(k_set<double>, grid_for(np, 256), 256, 0, s, np, 0.0, cPr);
       rc = uzawa(S, sp, MW_F32, fr, hr, cV, cPr, sp.sweep_reduction, false, 0.0, &inf, s);
       if (rc) break;
-      k_axpy<double><<<grid_for(nv, 256), 256, 0, s>>>(nv, 1.0, cV, solV);
-      k_axpy<double><<<grid_for(np, 256), 256, 0, s>>>(np, 1.0, cPr, solP);
+      pdl_launch(k_axpy<double>, grid_for(nv, 256), 256, 0, s, nv, 1.0, cV, solV);
+      pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, 1.0, cPr, solP);
       inf.refinements += 1;
       rel = true_residual(S, solV, solP, f, h, bnorm, s);
       inf.rel_residual = rel;

@@ -80,13 +80,17 @@ class GPUModel:
         self.gq_out = Z(3)
         self.material = ops.material_struct(cfg)
         precs = ("f64",) if stokes == "f64" else ("f32",)
-        self.solver = StokesSolver(box, self.bc_fix_V, eta_ref=cfg.eta_ref, L_ref=self.L_ref, precisions=precs)
+        # Smoothing degree per arithmetic: an FP64 V-cycle is apply-bound, so one Chebyshev step per
+        # sweep with more PCG iterations is faster; in FP32 two steps per sweep pay for themselves.
+        self.solver = StokesSolver(box, self.bc_fix_V, eta_ref=cfg.eta_ref, L_ref=self.L_ref, precisions=precs,
+                                   cheb_degree=1 if stokes == "f64" else 2)
         self.last_solve = {}
         self.istep = 0
         self.guess = None      # optional callable(model) -> (solV, solP) used as the Stokes initial guess
         self.solve_kw = {}     # extra mw_solve_params fields (e.g. mass_iters, sweep_reduction)
         self.graph = None      # recorded time step (capture_step)
         self._replayed = False
+        self._capturing = False
         ops.locate(box, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
 
     # ------------------------------------------------------------------------------------------
@@ -120,27 +124,40 @@ class GPUModel:
         """Record one whole time step as a CUDA graph; later step() calls replay it (one launch per
         step, no host synchronisation).  The Stokes and energy solves record their loops as
         conditional nodes; their outcomes are read from the device by diagnostics().  Runs one
-        eager step first when none has run (it sizes every workspace).  A guess hook runs host
-        code between the solves' inputs and the solve, so a model with one cannot be captured."""
-        if self.guess is not None:
-            raise ValueError("a Stokes guess hook runs host code and cannot be recorded into a graph")
+        eager step first when none has run (it sizes every workspace).  A guess hook runs device
+        work between the solves' inputs and the solve, so it can only be left out of the record
+        while it is idle (``hook.idle()`` true: the solve starts from the previous solution); a step
+        whose hook is not idle runs eagerly, with the hook, and later idle steps replay again."""
+        if self.guess is not None and not self._guess_idle():
+            raise ValueError("a Stokes guess hook that is not idle runs device work and cannot be recorded")
         if self.istep == 0:
             self.step()
         torch.cuda.synchronize()
         self._phases = None
         g = torch.cuda.CUDAGraph()
-        with ops.workspace_scope(self):
-            with torch.cuda.graph(g, capture_error_mode="thread_local"):
-                self._step_body()
+        self._capturing = True
+        try:
+            with ops.workspace_scope(self):
+                with torch.cuda.graph(g, capture_error_mode="thread_local"):
+                    self._step_body()
+        finally:
+            self._capturing = False
         self.istep -= 1                 # the capture recorded the step; nothing ran
         self.graph = g
 
+    def _guess_idle(self):
+        idle = getattr(self.guess, "idle", None)
+        return bool(idle()) if idle is not None else False
+
     def step(self):
-        if self.graph is not None:
+        if self.graph is not None and (self.guess is None or self._guess_idle()):
+            if self.guess is not None:
+                self.guess(self)        # an idle hook only keeps its tally; it launches nothing
             self.graph.replay()
             self.istep += 1
             self._replayed = True
             return
+        self._replayed = False
         with ops.workspace_scope(self):
             self._step_body()
 
@@ -182,7 +199,8 @@ class GPUModel:
                                 self.L_ref, out=dict(rhs_f=self.rhs_f, rhs_h=self.rhs_h))
         self.solver.set_viscosity(qf["etaq"], self.eta_e)
         if self.guess is not None:
-            self.guess(self)
+            if not self._capturing:
+                self.guess(self)
         elif self.warm_start != "previous":
             self.solV.zero_()
             self.solP.zero_()

@@ -425,6 +425,11 @@ class LearnedGuess:
         self.picks = {k: 0 for k in ("previous", "increment", "learned", "zero")}
         self.last = {}
 
+    def idle(self):
+        """True when the next call launches nothing (the solve starts from the previous solution),
+        so a recorded time step may stand in for the step with this hook."""
+        return not (self.cold or self.judge == "every")
+
     def reset(self):
         """Forget the previous solution (the next step is a cold start)."""
         self.cold = True

@@ -54,3 +54,42 @@ def test_recorded_ensemble_matches_models_alone():
         assert d["stokes"]["converged"] == 1
         for xa, xb in zip(st, _state(m)):
             assert np.array_equal(xa, xb), cfg.name
+
+
+def test_recorded_step_with_idle_learned_guess():
+    """The learned guess is consulted at cold starts only; while it is idle the recorded step
+    stands in for the step with the hook, and a reset (cold start) runs eagerly with the hook."""
+    import os
+    from meeuuw_b200 import configs
+    from meeuuw_b200.timestep import GPUModel
+    from meeuuw_b200.unet import LearnedGuess, UNet
+    weights = os.path.join(os.path.dirname(os.path.dirname(__file__)), "meeuuw_b200", "weights", "unet_fk128.npz")
+    net = UNet.load(weights)
+    cfg = configs.fk_convection(32, seed=7, Ra=1e5)
+    host = configs.build_host_model(cfg)
+    a = GPUModel(cfg, host, stokes="mixed")
+    b = GPUModel(cfg, host, stokes="mixed")
+    a.guess, b.guess = LearnedGuess(a, net), LearnedGuess(b, net)
+    for _ in range(4):
+        a.step()
+    b.step()                                # the cold start consults the network
+    assert b.guess.idle()
+    b.capture_step()
+    for _ in range(3):
+        b.step()
+    assert b._replayed
+    for xa, xb in zip(_state(a), _state(b)):
+        assert np.array_equal(xa, xb)
+    assert a.guess.picks == b.guess.picks
+    a.guess.reset()
+    b.guess.reset()
+    a.step()
+    b.step()                                # cold again: eager, with the hook
+    assert not b._replayed and b.guess.idle()
+    a.step()
+    b.step()                                # idle: the recorded step again
+    assert b._replayed
+    da, db = a.diagnostics(), b.diagnostics()
+    for xa, xb in zip(_state(a), _state(b)):
+        assert np.array_equal(xa, xb)
+    assert a.guess.picks == b.guess.picks and da["vrms"] == db["vrms"]

@@ -136,7 +136,7 @@ def run_ours(args):
     # ---- product path: mixed precision, learned warm start (gated; previous-step fallback) ----
     model = GPUModel(cfg, host, stokes="mixed", tol=1e-8)
     if args.host_loops:
-        model.solve_kw = dict(host_loops=1)
+        model.solve_kw = dict(model.solve_kw, host_loops=1)
     learned = None
     wpath = os.path.join(ROOT, "meeuuw_b200", "weights", "unet_fk128.npz")
     if os.path.exists(wpath):

@@ -5,7 +5,8 @@
 // (build_matrix_energy.py:133-137, nel*81 values) are used directly: y = A x is a node-centric
 // gather over the (up to 4) incident elements in ascending element order -- the summed COO
 // matrix applied without forming it -- and the system is solved by Jacobi-preconditioned
-// BiCGSTAB in FP64 to a relative residual tolerance.
+// BiCGSTAB in FP64 to a relative residual tolerance.  The solve first regroups the rows by node
+// class (k_energy_rows) so that every matvec of the iteration reads them coalesced.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -44,6 +45,122 @@ __global__ void k_energy_matvec(mw_box b, const double* __restrict__ vv, const d
         for (int j = 0; j < 9; ++j) acc += row[j] * x[q2_node(ex, ez, j, nnx)];
         dg += row[kl];
       }
+    y[n] = mode == 1 ? rhs[n] - acc : acc;
+    if (diag) diag[n] = dg;
+  }
+}
+
+// ---------------------------------------------------------------- row planes of the solver
+// The solve keeps the element-matrix rows grouped by node class (the lattice parity of the node),
+// each class's rows stored as coefficient planes coef[(slot * 9 + j) * M + m] (m the node's index
+// in its class, M the class size), so one warp reads 32 consecutive nodes' coefficient j in one
+// coalesced access.  Classes and their incident elements, in ascending element order (the order
+// the node-centric sum above visits them):
+//   0 centre (odd ix, odd iz):          (ez, ex) local 8
+//   1 horizontal midpoint (odd, even):  (ez-1, ex) local 6, (ez, ex) local 4
+//   2 vertical midpoint (even, odd):    (ez, ex-1) local 5, (ez, ex) local 7
+//   3 corner (even, even):              (ez-1, ex-1) 2, (ez-1, ex) 3, (ez, ex-1) 1, (ez, ex) 0
+// Slots of boundary nodes without the element hold zeros and are skipped.
+struct RowPlanes {
+  int mx[4], mz[4], slots[4];
+  int64_t m0[5];          // first node of each class in the flat index (m0[4] = all nodes)
+  int64_t off[4];         // first coefficient of each class
+  int64_t total;          // coefficients
+};
+
+inline RowPlanes row_planes(mw_box b) {
+  RowPlanes P;
+  const int mx[4] = {b.nelx, b.nelx, b.nelx + 1, b.nelx + 1}, mz[4] = {b.nelz, b.nelz + 1, b.nelz, b.nelz + 1};
+  const int sl[4] = {1, 2, 2, 4};
+  int64_t m = 0, o = 0;
+  for (int c = 0; c < 4; ++c) {
+    P.mx[c] = mx[c]; P.mz[c] = mz[c]; P.slots[c] = sl[c];
+    P.m0[c] = m;
+    P.off[c] = o;
+    m += (int64_t)mx[c] * mz[c];
+    o += (int64_t)sl[c] * 9 * mx[c] * mz[c];
+  }
+  P.m0[4] = m;
+  P.total = o;
+  return P;
+}
+
+// entry c of a per-class table in the kernel parameters, without indexing them at run time
+// (which would copy the parameter block to local memory)
+template <typename T>
+MW_D T pick(const T (&a)[4], int c) { return c == 0 ? a[0] : (c == 1 ? a[1] : (c == 2 ? a[2] : a[3])); }
+
+// element (ex, ez) and the node's local index kl in it for slot s of class c's node (i, k);
+// false when the mesh has no such element
+MW_D bool slot_element(int c, int s, int i, int k, const mw_box& b, int* ex, int* ez, int* kl) {
+  int dx = 0, dz = 0;          // element offset from (i, k)
+  if (c == 0) { *kl = 8; }
+  else if (c == 1) { dz = s == 0 ? -1 : 0; *kl = s == 0 ? 6 : 4; }
+  else if (c == 2) { dx = s == 0 ? -1 : 0; *kl = s == 0 ? 5 : 7; }
+  else { dz = s < 2 ? -1 : 0; dx = (s & 1) ? 0 : -1; *kl = s == 0 ? 2 : (s == 1 ? 3 : (s == 2 ? 1 : 0)); }
+  *ex = i + dx;
+  *ez = k + dz;
+  return *ex >= 0 && *ex < b.nelx && *ez >= 0 && *ez < b.nelz;
+}
+
+// class of flat node index t and its index m in the class
+MW_D int class_of(const RowPlanes& P, int64_t t, int64_t* m) {
+  const int c = t >= P.m0[1] ? (t >= P.m0[2] ? (t >= P.m0[3] ? 3 : 2) : 1) : 0;
+  *m = t - (c == 0 ? P.m0[0] : (c == 1 ? P.m0[1] : (c == 2 ? P.m0[2] : P.m0[3])));
+  return c;
+}
+
+// coefficient planes from VV_T (nel*81, build_matrix_energy.py:133-137): one thread per (node, slot)
+__global__ void k_energy_rows(mw_box b, RowPlanes P, const double* __restrict__ vv, double* __restrict__ coef) {
+  pdl_entry();
+  const int64_t nrow = P.total / 9;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrow; r += (int64_t)gridDim.x * blockDim.x) {
+    const int c = r >= P.off[3] / 9 ? 3 : (r >= P.off[2] / 9 ? 2 : (r >= P.off[1] / 9 ? 1 : 0));
+    const int mxc = pick(P.mx, c);
+    const int64_t off = pick(P.off, c);
+    const int64_t M = (int64_t)mxc * pick(P.mz, c);
+    const int64_t q = r - off / 9;
+    const int s = (int)(q / M);
+    const int64_t m = q - s * M;
+    const int i = (int)(m % mxc), k = (int)(m / mxc);
+    int ex, ez, kl;
+    double* dst = coef + off + (int64_t)s * 9 * M + m;
+    if (slot_element(c, s, i, k, b, &ex, &ez, &kl)) {
+      const double* row = vv + (((int64_t)ez * b.nelx + ex) * 81 + kl * 9);
+#pragma unroll
+      for (int j = 0; j < 9; ++j) dst[j * M] = row[j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < 9; ++j) dst[j * M] = 0.0;
+    }
+  }
+}
+
+// k_energy_matvec on the coefficient planes: the same products summed in the same order
+__global__ void k_energy_matvec_rows(mw_box b, RowPlanes P, const double* __restrict__ coef,
+                                     const double* __restrict__ x, const double* __restrict__ rhs,
+                                     double* __restrict__ y, double* __restrict__ diag, int mode) {
+  pdl_entry();
+  const int nnx = 2 * b.nelx + 1;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < P.m0[4]; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t m;
+    const int c = class_of(P, t, &m);
+    const int mxc = pick(P.mx, c);
+    const int64_t M = (int64_t)mxc * pick(P.mz, c);
+    const int i = (int)(m % mxc), k = (int)(m / mxc);
+    const int ix = 2 * i + ((c == 0 || c == 1) ? 1 : 0), iz = 2 * k + ((c == 0 || c == 2) ? 1 : 0);
+    const double* cf = coef + pick(P.off, c) + m;
+    const int nslot = pick(P.slots, c);
+    double acc = 0.0, dg = 0.0;
+    for (int s = 0; s < nslot; ++s) {
+      int ex, ez, kl;
+      if (!slot_element(c, s, i, k, b, &ex, &ez, &kl)) continue;
+      const double* row = cf + (int64_t)s * 9 * M;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) acc += row[j * M] * x[q2_node(ex, ez, j, nnx)];
+      dg += row[kl * M];
+    }
+    const int64_t n = (int64_t)iz * nnx + ix;
     y[n] = mode == 1 ? rhs[n] - acc : acc;
     if (diag) diag[n] = dg;
   }
@@ -182,7 +299,7 @@ extern "C" {
 
 size_t mw_energy_solve_workspace_bytes(mw_box box) {
   int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  return (size_t)(9 * nn + 512) * sizeof(double);
+  return (size_t)(9 * nn + 512 + row_planes(box).total) * sizeof(double);   // vectors, scalars, row planes
 }
 
 int mw_energy_device_info(mw_box box, const void* work, int32_t* iters, double* relres, void* stream) {
@@ -318,8 +435,11 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
     cudaStreamSynchronize(s);
     return h;
   };
+  const RowPlanes RP = row_planes(box);
+  double* coef = w + 9 * n + 512;
+  pdl_launch(k_energy_rows, grid_for(RP.total / 9, 256), 256, 0, s, box, RP, VV_T, coef);
   // r = b - A T (T is the initial guess), diag
-  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, T, rhs, r, dg, 1);
+  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, T, rhs, r, dg, 1);
   cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   dot(rhs, rhs, sc + 10);
   dot(r, r, sc + 11);
@@ -331,11 +451,11 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
     dot(r0, r, sc + 0);                                       // rho
     pdl_launch(k_bicg_p, grid_for(n, 256), 256, 0, s, n, sc, r, v, p, it == 1);
     pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, s, n, p, dg, ph);
-    pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, ph, nullptr, v, nullptr, 0);
+    pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, ph, nullptr, v, nullptr, 0);
     dot(r0, v, sc + 4);
     pdl_launch(k_bicg_s, grid_for(n, 256), 256, 0, s, n, sc, r, v, sv);
     pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, s, n, sv, dg, sh);
-    pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, sh, nullptr, t, nullptr, 0);
+    pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, sh, nullptr, t, nullptr, 0);
     dot(t, sv, sc + 5);
     dot(t, t, sc + 6);
     pdl_launch(k_bicg_x, grid_for(n, 256), 256, 0, s, n, sc, ph, sh, sv, t, T, r);
@@ -360,12 +480,15 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
          *sh = w + 7 * n, *dg = w + 8 * n;
   double* part = w + 9 * n;
   double* sc = part + 300;
+  const RowPlanes RP = row_planes(box);
+  double* coef = w + 9 * n + 512;
   const int NBk = 296;
   auto dot = [&](const double* a, const double* b2, double* out, cudaStream_t st) {
     pdl_launch(k_edot_partial, NBk, 256, 0, st, n, a, b2, part);
     pdl_launch(k_edot_final, 1, 256, 0, st, part, NBk, out);
   };
-  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, s, box, VV_T, T, rhs, r, dg, 1);
+  pdl_launch(k_energy_rows, grid_for(RP.total / 9, 256), 256, 0, s, box, RP, VV_T, coef);
+  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, T, rhs, r, dg, 1);
   cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   dot(rhs, rhs, sc + 10, s);
   dot(r, r, sc + 11, s);
@@ -392,11 +515,11 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
   dot(r0, r, sc + 0, b);
   pdl_launch(k_bicg_p_dev, grid_for(n, 256), 256, 0, b, n, sc, r, v, p);
   pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, b, n, p, dg, ph);
-  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, b, box, VV_T, ph, nullptr, v, nullptr, 0);
+  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, b, box, RP, coef, ph, nullptr, v, nullptr, 0);
   dot(r0, v, sc + 4, b);
   pdl_launch(k_bicg_s, grid_for(n, 256), 256, 0, b, n, sc, r, v, sv);
   pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, b, n, sv, dg, sh);
-  pdl_launch(k_energy_matvec, grid_for(n, 256), 256, 0, b, box, VV_T, sh, nullptr, t, nullptr, 0);
+  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, b, box, RP, coef, sh, nullptr, t, nullptr, 0);
   dot(t, sv, sc + 5, b);
   dot(t, t, sc + 6, b);
   pdl_launch(k_bicg_x, grid_for(n, 256), 256, 0, b, n, sc, ph, sh, sv, t, T, r);

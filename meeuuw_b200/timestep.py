@@ -33,9 +33,11 @@ class GPUModel:
         self.L_ref = (cfg.Lx + cfg.Lz) / 2
         self.volume = cfg.Lx * cfg.Lz
         self.stokes_precision, self.scheme, self.tol, self.warm_start = stokes, scheme, tol, warm_start
-        # inner multigrid-PCG tolerance: loose under FP64 refinement (mixed), tight without it (the
-        # FP64 Schur iteration needs accurate inner solves to converge from a cold start)
-        self.inner_rtol = inner_rtol if inner_rtol is not None else (1e-2 if stokes == "mixed" else 1e-10)
+        # inner multigrid-PCG tolerance: loose under FP64 refinement (mixed; 2e-2 is the fastest
+        # setting whose vrms stays within 1e-7 of the FP64 solve at 512x512), tight without it (the
+        # reference's inner solves are direct, cd_u_eta.py:29,50; the FP64 Schur iteration also
+        # needs accurate inner solves to converge from a cold start)
+        self.inner_rtol = inner_rtol if inner_rtol is not None else (2e-2 if stokes == "mixed" else 1e-10)
         D = lambda a, dt=None: torch.as_tensor(a, dtype=dt).to(device).contiguous()
         self.tables = fe_tables.device_tables(device)
         self.geo = fe_tables.uniform_geometry(nel, box.hx, box.hz, device)
@@ -87,7 +89,9 @@ class GPUModel:
         self.last_solve = {}
         self.istep = 0
         self.guess = None      # optional callable(model) -> (solV, solP) used as the Stokes initial guess
-        self.solve_kw = {}     # extra mw_solve_params fields (e.g. mass_iters, sweep_reduction)
+        # extra mw_solve_params fields: six Chebyshev steps on the M_eta preconditioner of the
+        # Schur complement leave the outer iteration counts of the FK step unchanged (vs 12)
+        self.solve_kw = dict(mass_iters=6)
         self.graph = None      # recorded time step (capture_step)
         self._replayed = False
         self._capturing = False

@@ -272,6 +272,8 @@ typedef struct {
   double cheb_safety;     /* lambda_max estimate multiplier                                          */
   int32_t power_iters;    /* power iterations for lambda_max(D^-1 K) per level (first viscosity)    */
   int32_t power_iters_warm; /* power iterations on later viscosities, warm-started                   */
+  int32_t tail_nel;       /* levels with at most this many elements run each V-cycle as one launch of
+                             one CTA (0: a launch per smoothing step, residual and transfer)        */
 } mw_stokes_params;
 
 typedef struct {

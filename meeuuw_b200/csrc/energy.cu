@@ -279,6 +279,12 @@ __global__ void k_bicg_check(double* sc, double rtol, int maxit, cudaGraphCondit
   cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && it < (double)maxit) ? 1u : 0u);
 }
 
+// Workspace of the solve (doubles): nine node vectors, then the dot-product partials, the device
+// scalars and the row planes.
+constexpr int E_NB = 1184;                 // dot-product CTAs (8 per SM) and partial slots
+constexpr int64_t E_SC = E_NB + 16;        // scalars, after the partials
+constexpr int64_t E_COEF = E_SC + 256;     // row planes, after the scalars
+
 struct EnergyGraph {
   int dev;
   const void *VV, *rhs, *T, *work;
@@ -299,12 +305,12 @@ extern "C" {
 
 size_t mw_energy_solve_workspace_bytes(mw_box box) {
   int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  return (size_t)(9 * nn + 512 + row_planes(box).total) * sizeof(double);   // vectors, scalars, row planes
+  return (size_t)(9 * nn + E_COEF + row_planes(box).total) * sizeof(double);
 }
 
 int mw_energy_device_info(mw_box box, const void* work, int32_t* iters, double* relres, void* stream) {
   const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  const double* sc = (const double*)work + 9 * n + 300;
+  const double* sc = (const double*)work + 9 * n + E_SC;
   double q[3];
   cudaStream_t s = (cudaStream_t)stream;
   cudaMemcpyAsync(q, sc + 10, sizeof(q), cudaMemcpyDeviceToHost, s);
@@ -378,7 +384,7 @@ static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs
   }
   if (!legacy && cudaGraphLaunch(exec, s) != cudaSuccess) { cudaGetLastError(); return false; }
   const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  const double* sc = (const double*)work + 9 * n + 300;
+  const double* sc = (const double*)work + 9 * n + E_SC;
   double q[3];
   cudaMemcpyAsync(q, sc + 10, sizeof(q), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return false;
@@ -422,9 +428,9 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
   double* w = (double*)work;
   double *r = w, *r0 = w + n, *p = w + 2 * n, *v = w + 3 * n, *sv = w + 4 * n, *t = w + 5 * n, *ph = w + 6 * n,
          *sh = w + 7 * n, *dg = w + 8 * n;
-  double* part = w + 9 * n;         // 296 partials
-  double* sc = part + 300;          // scalar slots
-  const int NBk = 296;
+  double* part = w + 9 * n;         // dot-product partials
+  double* sc = w + 9 * n + E_SC;    // scalar slots
+  const int NBk = E_NB;
   auto dot = [&](const double* a, const double* b2, double* out) {
     pdl_launch(k_edot_partial, NBk, 256, 0, s, n, a, b2, part);
     pdl_launch(k_edot_final, 1, 256, 0, s, part, NBk, out);
@@ -436,7 +442,7 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
     return h;
   };
   const RowPlanes RP = row_planes(box);
-  double* coef = w + 9 * n + 512;
+  double* coef = w + 9 * n + E_COEF;
   pdl_launch(k_energy_rows, grid_for(RP.total / 9, 256), 256, 0, s, box, RP, VV_T, coef);
   // r = b - A T (T is the initial guess), diag
   pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, T, rhs, r, dg, 1);
@@ -479,10 +485,10 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
   double *r = w, *r0 = w + n, *p = w + 2 * n, *v = w + 3 * n, *sv = w + 4 * n, *t = w + 5 * n, *ph = w + 6 * n,
          *sh = w + 7 * n, *dg = w + 8 * n;
   double* part = w + 9 * n;
-  double* sc = part + 300;
+  double* sc = w + 9 * n + E_SC;
   const RowPlanes RP = row_planes(box);
-  double* coef = w + 9 * n + 512;
-  const int NBk = 296;
+  double* coef = w + 9 * n + E_COEF;
+  const int NBk = E_NB;
   auto dot = [&](const double* a, const double* b2, double* out, cudaStream_t st) {
     pdl_launch(k_edot_partial, NBk, 256, 0, st, n, a, b2, part);
     pdl_launch(k_edot_final, 1, 256, 0, st, part, NBk, out);

@@ -15,6 +15,7 @@
 // Dirichlet semantics (identical to SpMV with the reference's eliminated COO): fixed velocity
 // dofs are zeroed before the element products; fixed rows return diag(K)_i * u_i; G rows of
 // fixed dofs are zero.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -282,6 +283,9 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
   const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
+  // Chebyshev coefficients, read now so that no epilogue load waits on them
+  const double c1 = MODE == AM_CHEB ? a.cheb[0] : 0.0;
+  const R c2 = MODE == AM_CHEB ? R(a.cheb[1]) : R(0);
   // ---- prefetch: the epilogue's node vectors (owned elements), the element viscosities ----
   // slot j of an owned element: 0 centre (2ex+1, 2ez+1), 1 bottom midpoint (2ex+1, 2ez),
   // 2 left midpoint (2ex, 2ez+1), 3 corner (2ex, 2ez)
@@ -381,35 +385,32 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     const int64_t n = (int64_t)iz * g.nnx + ix;
     const int li = (iz - lz0) * LX + (ix - lx0);
     const uchar2 ff = sfix[li];
+    const bool fixed = (ff.x | ff.y) && use_u;       // calls without a velocity (G p only) pass no diagonal
+    const bool pre = NPRE && slot >= 0;
+    // every load first, none depending on another
     R2 uu = su2[li];                                 // the staged velocity: exact on free dofs
+    R2 dg{R(0), R(0)}, bb{R(0), R(0)}, dd{R(0), R(0)};
+    if (MODE == AM_CHEB) dg = pre ? spre[(4 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.diag)[n];
+    else if (fixed) dg = reinterpret_cast<const R2*>(a.diag)[n];
+    if (fixed) uu = reinterpret_cast<const R2*>(a.u)[n];
+    if (MODE != AM_APPLY) bb = pre ? spre[slot * TX * TZ + tid] : reinterpret_cast<const R2*>(a.bV)[n];
+    if (MODE == AM_CHEB && c1 != 0.0)                // restart steps never read the old direction
+      dd = pre ? spre[(8 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.d)[n];
     R2 y;
     y.x = y0;
     y.y = y1;
-    if (ff.x | ff.y) {
-      // eliminated rows act as K_ii u_i; calls without a velocity (G p only) pass no diagonal
-      R2 fy{R(0), R(0)};
-      if (use_u) {
-        const R2 dg = reinterpret_cast<const R2*>(a.diag)[n];
-        uu = reinterpret_cast<const R2*>(a.u)[n];
-        fy = R2{dg.x * uu.x, dg.y * uu.y};
-      }
+    if (ff.x | ff.y) {                               // eliminated rows act as K_ii u_i
+      const R2 fy = fixed ? R2{dg.x * uu.x, dg.y * uu.y} : R2{R(0), R(0)};
       if (ff.x) y.x = fy.x;
       if (ff.y) y.y = fy.y;
     }
     if (MODE == AM_APPLY) {
       reinterpret_cast<R2*>(a.yV)[n] = y;
     } else if (MODE == AM_RESID) {
-      const R2 bb = NPRE && slot >= 0 ? spre[slot * TX * TZ + tid] : reinterpret_cast<const R2*>(a.bV)[n];
       reinterpret_cast<R2*>(a.yV)[n] = R2{bb.x - y.x, bb.y - y.y};
     } else {   // Chebyshev step: d = c1 d + c2 D^-1 (b - y); x_out = u + d
-      const bool pre = NPRE && slot >= 0;
-      const R2 bb = pre ? spre[slot * TX * TZ + tid] : reinterpret_cast<const R2*>(a.bV)[n];
-      const R2 dg = pre ? spre[(4 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.diag)[n];
-      const double c1 = a.cheb[0];
-      const R c2 = R(a.cheb[1]);
       R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
-      if (c1 != 0.0) {                               // restart steps never read the old direction
-        const R2 dd = pre ? spre[(8 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.d)[n];
+      if (c1 != 0.0) {
         dn.x += R(c1) * dd.x;
         dn.y += R(c1) * dd.y;
       }
@@ -580,40 +581,64 @@ MW_D double rw(int J, int o) {
   return 0.0;
 }
 
+// Full-weighting restriction of the fine residual to coarse node n (the transpose of the Q2
+// prolongation below); with cheb_c also the coarse level's first Chebyshev step from a zero
+// guess: x_c = d_c = (1/theta_c) D_c^-1 b_c.
+template <typename R>
+MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
+                        R* __restrict__ bc, double c0, bool cheb, const R* __restrict__ diag_c, R* __restrict__ xc,
+                        R* __restrict__ dc, int64_t n) {
+  int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
+  // The nonzero taps lie at offsets -3, -1, 0, 1, 3 (the weight at +-2 is zero).  All stencil
+  // values are loaded first (predicated), then summed in ascending offset order.
+  constexpr int OFF[5] = {-3, -1, 0, 1, 3};
+  R v0[5][5], v1[5][5];
+#pragma unroll
+  for (int tz = 0; tz < 5; ++tz)
+#pragma unroll
+    for (int tx = 0; tx < 5; ++tx) {
+      const int fz = 2 * J + OFF[tz], fx = 2 * I + OFF[tx];
+      const bool ok = rw(J, OFF[tz]) != 0.0 && rw(I, OFF[tx]) != 0.0 && fz >= 0 && fz < gf.nnz && fx >= 0 &&
+                      fx < gf.nnx;
+      const int64_t m = ok ? (int64_t)fz * gf.nnx + fx : 0;
+      v0[tz][tx] = ok ? rf[2 * m] : R(0);
+      v1[tz][tx] = ok ? rf[2 * m + 1] : R(0);
+    }
+  double s0 = 0, s1 = 0;
+#pragma unroll
+  for (int tz = 0; tz < 5; ++tz) {
+    const double wz = rw(J, OFF[tz]);
+    const int fz = 2 * J + OFF[tz];
+    const bool okz = wz != 0.0 && fz >= 0 && fz < gf.nnz;
+#pragma unroll
+    for (int tx = 0; tx < 5; ++tx) {
+      const double wx = rw(I, OFF[tx]);
+      const int fx = 2 * I + OFF[tx];
+      if (okz && wx != 0.0 && fx >= 0 && fx < gf.nnx) {
+        s0 += wz * wx * (double)v0[tz][tx];
+        s1 += wz * wx * (double)v1[tz][tx];
+      }
+    }
+  }
+  const R b0 = fixc[2 * n] ? R(0) : (R)s0, b1 = fixc[2 * n + 1] ? R(0) : (R)s1;
+  bc[2 * n] = b0;
+  bc[2 * n + 1] = b1;
+  if (cheb) {
+    const R x0 = R(c0) * b0 / diag_c[2 * n], x1 = R(c0) * b1 / diag_c[2 * n + 1];
+    xc[2 * n] = x0; dc[2 * n] = x0;
+    xc[2 * n + 1] = x1; dc[2 * n + 1] = x1;
+  }
+}
+
 template <typename R>
 __global__ void k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
                            R* __restrict__ bc, const double* __restrict__ cheb_c, const R* __restrict__ diag_c,
                            R* __restrict__ xc, R* __restrict__ dc) {
   pdl_entry();
-  // also performs the coarse level's first Chebyshev step from a zero guess when cheb_c != null:
-  // x_c = d_c = (1/theta_c) D_c^-1 b_c
   const double c0 = cheb_c ? cheb_c[1] : 0.0;
   const int64_t nn = (int64_t)gc.nnx * gc.nnz;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
-    int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
-    double s0 = 0, s1 = 0;
-    for (int oz = -3; oz <= 3; ++oz) {
-      double wz = rw(J, oz);
-      int fz = 2 * J + oz;
-      if (wz == 0.0 || fz < 0 || fz >= gf.nnz) continue;
-      for (int ox = -3; ox <= 3; ++ox) {
-        double wx = rw(I, ox);
-        int fx = 2 * I + ox;
-        if (wx == 0.0 || fx < 0 || fx >= gf.nnx) continue;
-        int64_t m = (int64_t)fz * gf.nnx + fx;
-        s0 += wz * wx * (double)rf[2 * m];
-        s1 += wz * wx * (double)rf[2 * m + 1];
-      }
-    }
-    const R b0 = fixc[2 * n] ? R(0) : (R)s0, b1 = fixc[2 * n + 1] ? R(0) : (R)s1;
-    bc[2 * n] = b0;
-    bc[2 * n + 1] = b1;
-    if (cheb_c) {
-      const R x0 = R(c0) * b0 / diag_c[2 * n], x1 = R(c0) * b1 / diag_c[2 * n + 1];
-      xc[2 * n] = x0; dc[2 * n] = x0;
-      xc[2 * n + 1] = x1; dc[2 * n + 1] = x1;
-    }
-  }
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x)
+    restrict_node(gf, gc, rf, fixc, bc, c0, cheb_c != nullptr, diag_c, xc, dc, n);
 }
 
 // 1D Q2 prolongation: fine node i from coarse nodes
@@ -626,27 +651,45 @@ MW_D int pw(int i, int* J, double* w) {
   return 3;
 }
 
+// x_f += P x_c at fine node n (free dofs only)
+template <typename R>
+MW_D void prolong_node(const LevelGeo& gf, const LevelGeo& gc, const R* __restrict__ xc,
+                       const uint8_t* __restrict__ fixf, R* __restrict__ xf, int64_t n) {
+  int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
+  int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
+  double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
+  int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
+  R v0[3][3], v1[3][3];                             // all taps loaded first, then summed in order
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const bool ok = a < nzw && b < nxw;
+      const int64_t m = ok ? (int64_t)Jz[a] * gc.nnx + Jx[b] : 0;
+      v0[a][b] = ok ? xc[2 * m] : R(0);
+      v1[a][b] = ok ? xc[2 * m + 1] : R(0);
+    }
+  double s0 = 0, s1 = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      if (a < nzw && b < nxw) {
+        double w = wz[a] * wx[b];
+        s0 += w * (double)v0[a][b];
+        s1 += w * (double)v1[a][b];
+      }
+  if (!fixf[2 * n]) xf[2 * n] += (R)s0;
+  if (!fixf[2 * n + 1]) xf[2 * n + 1] += (R)s1;
+}
+
 template <typename R>
 __global__ void k_prolong_add(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc, const uint8_t* __restrict__ fixf,
                               R* __restrict__ xf) {
   pdl_entry();
   const int64_t nn = (int64_t)gf.nnx * gf.nnz;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
-    int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
-    int Jx[3], Jz[3];
-    double wx[3], wz[3];
-    int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
-    double s0 = 0, s1 = 0;
-    for (int a = 0; a < nzw; ++a)
-      for (int b = 0; b < nxw; ++b) {
-        int64_t m = (int64_t)Jz[a] * gc.nnx + Jx[b];
-        double w = wz[a] * wx[b];
-        s0 += w * (double)xc[2 * m];
-        s1 += w * (double)xc[2 * m + 1];
-      }
-    if (!fixf[2 * n]) xf[2 * n] += (R)s0;
-    if (!fixf[2 * n + 1]) xf[2 * n + 1] += (R)s1;
-  }
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x)
+    prolong_node(gf, gc, xc, fixf, xf, n);
 }
 
 template <typename R>
@@ -1068,9 +1111,14 @@ __global__ void k_sum_partial(int64_t n, const double* __restrict__ x, double* _
 }
 
 // ================================================================= solver object
-constexpr int NB = 296;           // reduction blocks
+constexpr int NB = 1184;          // reduction partials: up to 8 CTAs per SM
+
+// CTAs of a reduction over n values: enough to keep HBM busy on long vectors (at least 4 values
+// per thread), one on short ones
+static int nb_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(NB, (n + 1023) / 1024)); }
 constexpr int MAXLEV = 12;
 constexpr int MAXDEG = 8;
+constexpr int MAX_TAIL = 6;       // levels of the one-CTA V-cycle tail
 
 template <typename R>
 struct Level {
@@ -1103,6 +1151,8 @@ struct Hierarchy {
   double* Ainv = nullptr;    // coarsest dense inverse (double)
   int nd = 0;
   bool dense = true;
+  int tail0 = 0;             // first level of the one-CTA V-cycle tail (0: none)
+  size_t tail_smem = 0;      // its dynamic shared memory (element products of the largest tail level)
 };
 
 }  // namespace mw
@@ -1145,10 +1195,16 @@ struct mw_stokes {
   cudaStream_t ws = nullptr;
   cudaStream_t bs[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};   // capture streams of loop bodies
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // side branch of the hierarchy setup (the coarsest level's dense inverse)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   ~mw_stokes() {
     for (auto& e : graphs) cudaGraphExecDestroy(e.exec);
     if (ev_in) cudaEventDestroy(ev_in);
     if (ev_out) cudaEventDestroy(ev_out);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (ws) cudaStreamDestroy(ws);
     for (auto b : bs)
       if (b) cudaStreamDestroy(b);
@@ -1175,7 +1231,17 @@ static void plan_levels(Hierarchy<R>& H, const LevelGeo& fine, const mw_stokes_p
   const Level<R>& lc = H.L[H.nlev - 1];
   H.nd = (int)lc.ndof;
   H.dense = H.nd <= prm.dense_max;
+  // the one-CTA tail: from the first level (below the fine one) with at most tail_nel elements
+  H.tail0 = 0;
+  H.tail_smem = 0;
+  if (prm.tail_nel > 0)
+    for (int l = 1; l < H.nlev; ++l)
+      if (H.L[l].nel <= prm.tail_nel && H.nlev - l <= MAX_TAIL) { H.tail0 = l; break; }
+  for (int l = H.tail0; H.tail0 && l < H.nlev; ++l)
+    H.tail_smem = std::max(H.tail_smem, (size_t)H.L[l].nel * 18 * sizeof(R));
 }
+
+
 
 template <typename R>
 static void carve(Hierarchy<R>& H, Arena& A, const uint8_t* fine_fix) {
@@ -1240,12 +1306,13 @@ static ApplyArgs<R> args0() {
 
 template <typename R>
 static void dot(mw_stokes* S, int64_t n, const R* x, const R* y, double* out, cudaStream_t s) {
-  pdl_launch(k_dot1<R>, NB, 256, 0, s, n, x, y, S->red, S->counter, out);
+  pdl_launch(k_dot1<R>, nb_for(n), 256, 0, s, n, x, y, S->red, S->counter, out);
 }
 
 static void dsum(mw_stokes* S, int64_t n, const double* x, double* out, cudaStream_t s) {
-  pdl_launch(k_sum_partial, NB, 256, 0, s, n, x, S->red);
-  pdl_launch(k_dot_final, 1, 256, 0, s, S->red, NB, out);
+  const int nb = nb_for(n);
+  pdl_launch(k_sum_partial, nb, 256, 0, s, n, x, S->red);
+  pdl_launch(k_dot_final, 1, 256, 0, s, S->red, nb, out);
 }
 
 template <typename R>
@@ -1253,6 +1320,202 @@ static void k_only_apply(const Level<R>& L, const R* x, R* y, cudaStream_t s) {
   ApplyArgs<R> a = args0<R>();
   a.u = x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = y;
   launch_apply<R, AM_APPLY>(L.g, a, s);
+}
+
+// ---------------------------------------------------------------- coarse levels in one CTA
+// The levels with at most tail_nel elements take part in every V-cycle as one launch of one CTA
+// (k_vtail): smoothing, residual, restriction, the coarsest solve and prolongation run as phases
+// separated by barriers, in place of about six latency-bound launches per level.  Each phase
+// repeats the arithmetic of the multi-launch path in the same order -- the same element products,
+// node sums over the incident elements in ascending element order, the same epilogues, the shared
+// restriction and prolongation bodies -- so both paths give identical results.
+template <typename R>
+struct TailLevel {
+  LevelGeo g;
+  const R* eta;
+  const uint8_t* fix;
+  const R* diag;
+  R *x, *t, *b, *r, *d;
+  const double* cheb;
+};
+
+template <typename R>
+struct TailArgs {
+  TailLevel<R> L[MAX_TAIL];
+  int n;               // tail levels (the last one is the coarsest)
+  int degree;          // smoothing steps per sweep
+  int first_done;      // the first tail level's x = d were written by the restriction into it
+  int dense, nd;       // coarsest level: dense inverse Ainv (nd unknowns), else MAXDEG smoothing
+  const double* Ainv;
+};
+
+template <typename R>
+constexpr int tail_threads() { return sizeof(R) == 4 ? 512 : 256; }
+
+// One operator apply of tail level L on u: AM_RESID writes r = b - K u, AM_CHEB the Chebyshev
+// step (d, xo) with coefficient pair cheb.  Element products go through shared memory (sye).
+template <typename R, int MODE>
+MW_D void tail_apply(const TailLevel<R>& L, const R* __restrict__ u, R* __restrict__ xo, const double* cheb,
+                     R* __restrict__ sye) {
+  typedef typename Vec2<R>::T R2;
+  const LevelGeo& g = L.g;
+  const int nel = g.nx * g.nz;
+  const R sxe = R(2.0 / g.hx), sze = R(2.0 / g.hz), jace = R(g.hx * g.hz / 4.0), se = R(g.s);
+  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+    const int ex = e % g.nx, ez = e / g.nx;
+    __align__(16) R ue[18];
+    R pe[4] = {R(0), R(0), R(0), R(0)}, ye[18], ype[4], eq[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int64_t n = q2_node(ex, ez, k, g.nnx);
+      ue[2 * k] = L.fix[2 * n] ? R(0) : u[2 * n];
+      ue[2 * k + 1] = L.fix[2 * n + 1] ? R(0) : u[2 * n + 1];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) eq[q] = L.eta[(int64_t)e * 9 + q];
+    element_apply<R>(sxe, sze, jace, se, ue, pe, eq, ye, ype, false);
+#pragma unroll
+    for (int k = 0; k < 18; ++k) sye[e * 18 + k] = ye[k];
+  }
+  __syncthreads();
+  const int64_t nn = (int64_t)g.nnx * g.nnz;
+  for (int64_t n = threadIdx.x; n < nn; n += blockDim.x) {
+    const int ix = (int)(n % g.nnx), iz = (int)(n / g.nnx);
+    const bool xo_ = ix & 1, zo = iz & 1;
+    const int xa = xo_ ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
+    const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = (iz >> 1);
+    const bool vxa = xa >= 0, vxb = !xo_ && xb < g.nx;
+    const bool vza = za >= 0, vzb = !zo && zb < g.nz;
+    const int dxa = xo_ ? 1 : 2, dza = zo ? 1 : 2;
+    R2 y;
+    y.x = 0;
+    y.y = 0;
+    if (vza) {
+      if (vxa) { const R* ye = sye + (za * g.nx + xa) * 18; int k = q2_local_idx(dxa, dza);
+                 y.x += ye[2 * k]; y.y += ye[2 * k + 1]; }
+      if (vxb) { const R* ye = sye + (za * g.nx + xb) * 18; int k = q2_local_idx(0, dza);
+                 y.x += ye[2 * k]; y.y += ye[2 * k + 1]; }
+    }
+    if (vzb) {
+      if (vxa) { const R* ye = sye + (zb * g.nx + xa) * 18; int k = q2_local_idx(dxa, 0);
+                 y.x += ye[2 * k]; y.y += ye[2 * k + 1]; }
+      if (vxb) { const R* ye = sye + (zb * g.nx + xb) * 18; int k = q2_local_idx(0, 0);
+                 y.x += ye[2 * k]; y.y += ye[2 * k + 1]; }
+    }
+    const uint8_t f0 = L.fix[2 * n], f1 = L.fix[2 * n + 1];
+    const R2 uu = reinterpret_cast<const R2*>(u)[n];
+    if (f0 | f1) {                                   // eliminated rows act as K_ii u_i
+      const R2 dg = reinterpret_cast<const R2*>(L.diag)[n];
+      const R2 fy{dg.x * uu.x, dg.y * uu.y};
+      if (f0) y.x = fy.x;
+      if (f1) y.y = fy.y;
+    }
+    const R2 bb = reinterpret_cast<const R2*>(L.b)[n];
+    if (MODE == AM_RESID) {
+      reinterpret_cast<R2*>(L.r)[n] = R2{bb.x - y.x, bb.y - y.y};
+    } else {                                         // d = c1 d + c2 D^-1 (b - y); xo = u + d
+      const R2 dg = reinterpret_cast<const R2*>(L.diag)[n];
+      const double c1 = cheb[0];
+      const R c2 = R(cheb[1]);
+      R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
+      if (c1 != 0.0) {
+        const R2 dd = reinterpret_cast<const R2*>(L.d)[n];
+        dn.x += R(c1) * dd.x;
+        dn.y += R(c1) * dd.y;
+      }
+      reinterpret_cast<R2*>(L.d)[n] = dn;
+      reinterpret_cast<R2*>(xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
+    }
+  }
+  __syncthreads();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
+  pdl_entry();
+  extern __shared__ __align__(16) unsigned char tail_smem[];
+  R* sye = reinterpret_cast<R*>(tail_smem);
+  __shared__ TailLevel<R> sL[MAX_TAIL];
+#pragma unroll
+  for (int l = 0; l < MAX_TAIL; ++l)
+    if (threadIdx.x == l && l < A.n) sL[l] = A.L[l];
+  __syncthreads();
+  R* xs[MAX_TAIL];
+  R* ts[MAX_TAIL];
+  for (int l = 0; l < A.n; ++l) { xs[l] = sL[l].x; ts[l] = sL[l].t; }
+  auto cheb_step = [&](int l, int k) {             // Chebyshev step k: x_out in t, then swap
+    tail_apply<R, AM_CHEB>(sL[l], xs[l], ts[l], sL[l].cheb + 2 * k, sye);
+    R* tmp = xs[l]; xs[l] = ts[l]; ts[l] = tmp;
+  };
+  auto smooth_tail = [&](int l, int degree, bool zero_start, bool first_done) {
+    const TailLevel<R>& L = sL[l];
+    if (first_done) {
+      // x = d = (1/theta) D^-1 b was written by the restriction
+    } else if (zero_start) {
+      const R c = (R)L.cheb[1];
+      const int64_t n = 2LL * L.g.nnx * L.g.nnz;
+      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        R v = c * L.b[i] / L.diag[i];
+        xs[l][i] = v; L.d[i] = v;
+      }
+      __syncthreads();
+    } else {
+      cheb_step(l, 0);
+    }
+    for (int k = 1; k < degree; ++k) cheb_step(l, k);
+  };
+  // down: pre-smoothing, residual, restriction (with the coarse level's first Chebyshev step)
+  for (int l = 0; l + 1 < A.n; ++l) {
+    const bool fd = l == 0 ? A.first_done != 0 : true;
+    smooth_tail(l, A.degree, !fd, fd);
+    tail_apply<R, AM_RESID>(sL[l], xs[l], nullptr, nullptr, sye);
+    const TailLevel<R>& F = sL[l];
+    const TailLevel<R>& C = sL[l + 1];
+    const bool fuse = !(l + 2 == A.n && A.dense);
+    const double c0 = fuse ? C.cheb[1] : 0.0;
+    const int64_t ncn = (int64_t)C.g.nnx * C.g.nnz;
+    for (int64_t n = threadIdx.x; n < ncn; n += blockDim.x)
+      restrict_node(F.g, C.g, F.r, C.fix, C.b, c0, fuse, C.diag, xs[l + 1], C.d, n);
+    __syncthreads();
+  }
+  {  // coarsest level
+    const int l = A.n - 1;
+    if (A.dense) {
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+      const R* b = sL[l].b;
+      for (int row = warp; row < A.nd; row += nwarp) {
+        double sacc = 0;
+        for (int j = lane; j < A.nd; j += 32) sacc += A.Ainv[(int64_t)row * A.nd + j] * (double)b[j];
+        for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
+        if (lane == 0) xs[l][row] = (R)sacc;
+      }
+      __syncthreads();
+    } else {
+      const bool fd = A.n == 1 ? A.first_done != 0 : true;
+      smooth_tail(l, MAXDEG, !fd, fd);
+    }
+  }
+  // up: prolongation and post-smoothing
+  for (int l = A.n - 2; l >= 0; --l) {
+    const TailLevel<R>& F = sL[l];
+    const TailLevel<R>& C = sL[l + 1];
+    const int64_t nfn = (int64_t)F.g.nnx * F.g.nnz;
+    for (int64_t n = threadIdx.x; n < nfn; n += blockDim.x) prolong_node(F.g, C.g, xs[l + 1], F.fix, xs[l], n);
+    __syncthreads();
+    smooth_tail(l, A.degree, false, false);
+  }
+}
+
+// Dynamic shared memory of the tail kernel beyond the default 48 KB; false (tail off) on failure.
+template <typename R>
+static bool tail_smem_ok(const Hierarchy<R>& H) {
+  if (!H.tail0) return true;
+  if (H.tail_smem <= 48 * 1024) return true;
+  if (cudaFuncSetAttribute(k_vtail<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)H.tail_smem) ==
+      cudaSuccess)
+    return true;
+  cudaGetLastError();
+  return false;
 }
 
 // Chebyshev smoothing of level L: x (in/out) with rhs b, `steps` steps; zero_start -> x = 0 on entry.
@@ -1280,9 +1543,51 @@ static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s, boo
   }
 }
 
+// The host's record of the x/t pointer swaps the smoothing of levels l.. performs in one V-cycle
+// (what the multi-launch path does as it launches, and k_vtail does on the device).
+template <typename R>
+static void smooth_swaps(Level<R>& L, int degree, bool zero_start, bool first_done) {
+  const int n = (!first_done && !zero_start ? 1 : 0) + (degree - 1);
+  for (int i = 0; i < n; ++i) std::swap(L.x, L.t);
+}
+
+template <typename R>
+static void tail_swaps(Hierarchy<R>& H, int l, int degree, bool first_done) {
+  Level<R>& L = H.L[l];
+  if (l == H.nlev - 1) {
+    if (!H.dense) smooth_swaps(L, MAXDEG, !first_done, first_done);
+    return;
+  }
+  smooth_swaps(L, degree, !first_done, first_done);
+  tail_swaps(H, l + 1, degree, !(l + 1 == H.nlev - 1 && H.dense));
+  smooth_swaps(L, degree, false, false);
+}
+
+template <typename R>
+static void launch_tail(Hierarchy<R>& H, int l0, int degree, bool first_done, cudaStream_t s) {
+  TailArgs<R> A;
+  memset(&A, 0, sizeof(A));
+  A.n = H.nlev - l0;
+  for (int i = 0; i < A.n; ++i) {
+    const Level<R>& L = H.L[l0 + i];
+    A.L[i] = TailLevel<R>{L.g, L.eta, L.fix, L.diag, L.x, L.t, L.b, L.r, L.d, L.cheb};
+  }
+  A.degree = degree;
+  A.first_done = first_done ? 1 : 0;
+  A.dense = H.dense ? 1 : 0;
+  A.nd = H.nd;
+  A.Ainv = H.Ainv;
+  pdl_launch(k_vtail<R>, 1, tail_threads<R>(), H.tail_smem, s, A);
+}
+
 template <typename R>
 static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool first_done = false) {
   Level<R>& L = H.L[l];
+  if (H.tail0 > 0 && l == H.tail0) {               // the coarse levels in one launch
+    launch_tail(H, l, degree, first_done, s);
+    tail_swaps(H, l, degree, first_done);
+    return;
+  }
   if (l == H.nlev - 1) {
     if (H.dense) {
       int nd = H.nd;
@@ -1406,6 +1711,7 @@ __global__ void k_normalize(int64_t n, const double* __restrict__ nrm2, R* __res
 template <typename R>
 static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
   const mw_stokes_params& prm = S->prm;
+  // coarse viscosities, fixed masks and diagonals of every level (a short chain)
   for (int l = 0; l < H.nlev; ++l) {
     Level<R>& L = H.L[l];
     if (l > 0) {
@@ -1414,30 +1720,51 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
       pdl_launch(k_fix_coarse<R>, grid_for(L.nn, 256), 256, 0, s, L.g, F.fix, F.g.nnx, L.fix);
     }
     pdl_launch(k_diag<R>, grid_for(L.nn, 128), 128, 0, s, L.g, L.eta, L.diag);
-    const bool coarsest = l == H.nlev - 1;
-    if (coarsest && H.dense) {
-      pdl_launch(k_dense_assemble<R>, 1, 1024, 0, s, L.g, L.eta, L.fix, H.Ainv);
-      const size_t smem = sizeof(double) * ((size_t)H.nd * H.nd + H.nd);
-      int dev = 0, optin = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-      // the attribute is set once per device and size (so that a setup recorded into a CUDA graph
-      // issues no attribute call)
-      static size_t smem_set[64] = {0};
-      bool smem_ok = dev >= 0 && dev < 64 && smem <= smem_set[dev];
-      if (!smem_ok && smem <= (size_t)optin &&
-          cudaFuncSetAttribute(k_gauss_jordan_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-              cudaSuccess) {
-        smem_ok = true;
-        if (dev >= 0 && dev < 64) smem_set[dev] = smem;
-      }
-      if (smem_ok)
-        pdl_launch(k_gauss_jordan_smem, 1, 1024, smem, s, H.nd, H.Ainv);
-      else
-        pdl_launch(k_gauss_jordan, 1, 1024, sizeof(double) * H.nd, s, H.nd, H.Ainv);
-      continue;
+  }
+  // the coarsest level's dense inverse occupies one SM for most of a millisecond: it runs on a
+  // side branch (forked from and joined back into s by events, which a stream capture records as
+  // two graph branches) while the power iterations of the other levels run on s
+  const bool dense = H.dense;
+  cudaStream_t ds = s;
+  if (dense) {
+    if (!S->side && (cudaStreamCreateWithFlags(&S->side, cudaStreamNonBlocking) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&S->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
+      cudaGetLastError();
+      if (S->side) cudaStreamDestroy(S->side);
+      S->side = nullptr;
     }
-    // power iteration v <- D^-1 K v / |v|, warm-started from the previous viscosity's vector
+    if (S->side && cudaEventRecord(S->ev_fork, s) == cudaSuccess &&
+        cudaStreamWaitEvent(S->side, S->ev_fork, 0) == cudaSuccess)
+      ds = S->side;
+    else
+      cudaGetLastError();
+    Level<R>& L = H.L[H.nlev - 1];
+    pdl_launch(k_dense_assemble<R>, 1, 1024, 0, ds, L.g, L.eta, L.fix, H.Ainv);
+    const size_t smem = sizeof(double) * ((size_t)H.nd * H.nd + H.nd);
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    // the attribute is set once per device and size (so that a setup recorded into a CUDA graph
+    // issues no attribute call)
+    static size_t smem_set[64] = {0};
+    bool smem_ok = dev >= 0 && dev < 64 && smem <= smem_set[dev];
+    if (!smem_ok && smem <= (size_t)optin &&
+        cudaFuncSetAttribute(k_gauss_jordan_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+            cudaSuccess) {
+      smem_ok = true;
+      if (dev >= 0 && dev < 64) smem_set[dev] = smem;
+    }
+    if (smem_ok)
+      pdl_launch(k_gauss_jordan_smem, 1, 1024, smem, ds, H.nd, H.Ainv);
+    else
+      pdl_launch(k_gauss_jordan, 1, 1024, sizeof(double) * H.nd, ds, H.nd, H.Ainv);
+  }
+  // Chebyshev intervals: power iteration v <- D^-1 K v / |v| per smoothed level, warm-started
+  // from the previous viscosity's vector
+  for (int l = 0; l < H.nlev - (dense ? 1 : 0); ++l) {
+    Level<R>& L = H.L[l];
+    const bool coarsest = l == H.nlev - 1;
     R* v = L.ev;
     int iters = prm.power_iters;
     if (!L.ev_ready) {
@@ -1455,6 +1782,10 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
     dot<R>(S, L.ndof, v, v, L.lam2, s);          // ||D^-1 K v_prev||^2 with ||v_prev|| = 1
     int deg = coarsest ? MAXDEG : prm.cheb_degree;
     pdl_launch(k_cheb_coeffs, 1, 32, 0, s, L.lam2, deg, prm.cheb_ratio, prm.cheb_safety, L.cheb);
+  }
+  if (ds != s) {
+    cudaEventRecord(S->ev_join, ds);
+    cudaStreamWaitEvent(s, S->ev_join, 0);
   }
   return cudaGetLastError() == cudaSuccess ? MW_OK : MW_ERR_CUDA;
 }
@@ -2042,6 +2373,7 @@ void mw_stokes_default_params(mw_stokes_params* p) {
   p->coarse_min = 4; p->dense_max = 700; p->cheb_degree = 2; p->cheb_ratio = 8.0; p->cheb_safety = 1.1;
   p->power_iters = 12;
   p->power_iters_warm = 3;
+  p->tail_nel = 0;
 }
 
 void mw_solve_default_params(mw_solve_params* p) {
@@ -2068,6 +2400,8 @@ int mw_stokes_create(mw_box box, mw_stokes_params prm, const uint8_t* bc_fix_V, 
   size_t need = do_layout(S, nullptr, true);
   if (work_bytes < need) { delete S; return MW_ERR_WORKSPACE; }
   do_layout(S, (char*)work, false);
+  if (S->has32 && !tail_smem_ok(S->H32)) S->H32.tail0 = 0;
+  if (S->has64 && !tail_smem_ok(S->H64)) S->H64.tail0 = 0;
   if (cudaMemset(S->counter, 0, sizeof(unsigned) * 4) != cudaSuccess) { delete S; return MW_ERR_CUDA; }
   *out = S;
   return MW_OK;

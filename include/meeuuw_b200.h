@@ -273,7 +273,8 @@ typedef struct {
   int32_t power_iters;    /* power iterations for lambda_max(D^-1 K) per level (first viscosity)    */
   int32_t power_iters_warm; /* power iterations on later viscosities, warm-started                   */
   int32_t tail_nel;       /* levels with at most this many elements run each V-cycle as one launch of
-                             one CTA (0: a launch per smoothing step, residual and transfer)        */
+                             one cluster (0: a launch per smoothing step, residual and transfer)    */
+  int32_t cheb_degree_coarse; /* Chebyshev steps per sweep below the finest level (0: cheb_degree)   */
 } mw_stokes_params;
 
 typedef struct {

@@ -584,10 +584,10 @@ MW_D double rw(int J, int o) {
 // Full-weighting restriction of the fine residual to coarse node n (the transpose of the Q2
 // prolongation below); with cheb_c also the coarse level's first Chebyshev step from a zero
 // guess: x_c = d_c = (1/theta_c) D_c^-1 b_c.
+// (no __restrict__: the cluster tail reads values written earlier in the same kernel)
 template <typename R>
-MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
-                        R* __restrict__ bc, double c0, bool cheb, const R* __restrict__ diag_c, R* __restrict__ xc,
-                        R* __restrict__ dc, int64_t n) {
+MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, const uint8_t* fixc, R* bc, double c0,
+                        bool cheb, const R* diag_c, R* xc, R* dc, int64_t n) {
   int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
   // The nonzero taps lie at offsets -3, -1, 0, 1, 3 (the weight at +-2 is zero).  All stencil
   // values are loaded first (predicated), then summed in ascending offset order.
@@ -653,8 +653,7 @@ MW_D int pw(int i, int* J, double* w) {
 
 // x_f += P x_c at fine node n (free dofs only)
 template <typename R>
-MW_D void prolong_node(const LevelGeo& gf, const LevelGeo& gc, const R* __restrict__ xc,
-                       const uint8_t* __restrict__ fixf, R* __restrict__ xf, int64_t n) {
+MW_D void prolong_node(const LevelGeo& gf, const LevelGeo& gc, const R* xc, const uint8_t* fixf, R* xf, int64_t n) {
   int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
   int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
   double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
@@ -1127,6 +1126,7 @@ struct Level {
   R *eta, *diag, *x, *b, *r, *d, *t;
   uint8_t* fix;
   double* cheb;       // 2*MAXDEG coefficients
+  int deg;            // Chebyshev steps per smoothing sweep on this level
   double* lam2;
   R* ev;              // power-iteration vector, kept between viscosity updates (warm start)
   bool ev_ready;
@@ -1151,8 +1151,9 @@ struct Hierarchy {
   double* Ainv = nullptr;    // coarsest dense inverse (double)
   int nd = 0;
   bool dense = true;
-  int tail0 = 0;             // first level of the one-CTA V-cycle tail (0: none)
-  size_t tail_smem = 0;      // its dynamic shared memory (element products of the largest tail level)
+  int tail0 = 0;             // first level of the cluster V-cycle tail (0: none)
+  int64_t tail_len = 0;      // element products of its largest level (18 per element)
+  R* tail_ye = nullptr;      // their global scratch
 };
 
 }  // namespace mw
@@ -1220,6 +1221,7 @@ static void plan_levels(Hierarchy<R>& H, const LevelGeo& fine, const mw_stokes_p
   while (true) {
     Level<R>& l = H.L[H.nlev++];
     l.g = g;
+    l.deg = (H.nlev == 1 || prm.cheb_degree_coarse <= 0) ? prm.cheb_degree : prm.cheb_degree_coarse;
     l.nn = (int64_t)g.nnx * g.nnz; l.ndof = 2 * l.nn; l.nel = (int64_t)g.nx * g.nz;
     bool can = (g.nx % 2 == 0) && (g.nz % 2 == 0) && (g.nx / 2 >= prm.coarse_min) && (g.nz / 2 >= prm.coarse_min) &&
                H.nlev < MAXLEV && (l.nel > (int64_t)prm.coarse_min * prm.coarse_min);
@@ -1233,12 +1235,11 @@ static void plan_levels(Hierarchy<R>& H, const LevelGeo& fine, const mw_stokes_p
   H.dense = H.nd <= prm.dense_max;
   // the one-CTA tail: from the first level (below the fine one) with at most tail_nel elements
   H.tail0 = 0;
-  H.tail_smem = 0;
+  H.tail_len = 0;
   if (prm.tail_nel > 0)
     for (int l = 1; l < H.nlev; ++l)
       if (H.L[l].nel <= prm.tail_nel && H.nlev - l <= MAX_TAIL) { H.tail0 = l; break; }
-  for (int l = H.tail0; H.tail0 && l < H.nlev; ++l)
-    H.tail_smem = std::max(H.tail_smem, (size_t)H.L[l].nel * 18 * sizeof(R));
+  for (int l = H.tail0; H.tail0 && l < H.nlev; ++l) H.tail_len = std::max(H.tail_len, H.L[l].nel * 18);
 }
 
 
@@ -1261,6 +1262,7 @@ static void carve(Hierarchy<R>& H, Arena& A, const uint8_t* fine_fix) {
     L.ev_ready = false;
   }
   H.Ainv = H.dense ? (double*)A.take(sizeof(double) * (size_t)H.nd * H.nd) : nullptr;
+  H.tail_ye = H.tail0 ? (R*)A.take(sizeof(R) * H.tail_len) : nullptr;
 }
 
 static size_t layout(mw_stokes* S, Arena& A) {
@@ -1322,13 +1324,27 @@ static void k_only_apply(const Level<R>& L, const R* x, R* y, cudaStream_t s) {
   launch_apply<R, AM_APPLY>(L.g, a, s);
 }
 
-// ---------------------------------------------------------------- coarse levels in one CTA
-// The levels with at most tail_nel elements take part in every V-cycle as one launch of one CTA
-// (k_vtail): smoothing, residual, restriction, the coarsest solve and prolongation run as phases
-// separated by barriers, in place of about six latency-bound launches per level.  Each phase
-// repeats the arithmetic of the multi-launch path in the same order -- the same element products,
-// node sums over the incident elements in ascending element order, the same epilogues, the shared
-// restriction and prolongation bodies -- so both paths give identical results.
+// ---------------------------------------------------------------- coarse levels in one cluster
+// The levels with at most tail_nel elements take part in every V-cycle as one launch of one thread
+// block cluster (k_vtail): smoothing, residual, restriction, the coarsest solve and prolongation
+// run as phases separated by cluster barriers (release / acquire at cluster scope, which orders
+// the global-memory writes of one phase before the reads of the next on every SM of the cluster),
+// in place of about six latency-bound launches per level.  Each phase repeats the arithmetic of the
+// multi-launch path in the same order -- the same element products, node sums over the incident
+// elements in ascending element order, the same epilogues, the shared restriction and
+// prolongation bodies -- so both paths give identical results.  Pointers written in one phase and
+// read in a later one carry no __restrict__, so their loads stay on the coherent path.
+constexpr int TAIL_CLUSTER = 8;
+
+MW_D void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+MW_D unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
 template <typename R>
 struct TailLevel {
   LevelGeo g;
@@ -1337,31 +1353,32 @@ struct TailLevel {
   const R* diag;
   R *x, *t, *b, *r, *d;
   const double* cheb;
+  int deg;
 };
 
 template <typename R>
 struct TailArgs {
   TailLevel<R> L[MAX_TAIL];
   int n;               // tail levels (the last one is the coarsest)
-  int degree;          // smoothing steps per sweep
   int first_done;      // the first tail level's x = d were written by the restriction into it
   int dense, nd;       // coarsest level: dense inverse Ainv (nd unknowns), else MAXDEG smoothing
   const double* Ainv;
+  R* ye;               // element products (global scratch, 18 per element of the largest level)
 };
 
 template <typename R>
 constexpr int tail_threads() { return sizeof(R) == 4 ? 512 : 256; }
 
 // One operator apply of tail level L on u: AM_RESID writes r = b - K u, AM_CHEB the Chebyshev
-// step (d, xo) with coefficient pair cheb.  Element products go through shared memory (sye).
+// step (d, xo) with coefficient pair cheb.  Element products go through the global scratch sye;
+// this is thread t0 of the nt threads of the cluster.
 template <typename R, int MODE>
-MW_D void tail_apply(const TailLevel<R>& L, const R* __restrict__ u, R* __restrict__ xo, const double* cheb,
-                     R* __restrict__ sye) {
+MW_D void tail_apply(const TailLevel<R>& L, const R* u, R* xo, const double* cheb, R* sye, int t0, int nt) {
   typedef typename Vec2<R>::T R2;
   const LevelGeo& g = L.g;
   const int nel = g.nx * g.nz;
   const R sxe = R(2.0 / g.hx), sze = R(2.0 / g.hz), jace = R(g.hx * g.hz / 4.0), se = R(g.s);
-  for (int e = threadIdx.x; e < nel; e += blockDim.x) {
+  for (int e = t0; e < nel; e += nt) {
     const int ex = e % g.nx, ez = e / g.nx;
     __align__(16) R ue[18];
     R pe[4] = {R(0), R(0), R(0), R(0)}, ye[18], ype[4], eq[9];
@@ -1377,9 +1394,9 @@ MW_D void tail_apply(const TailLevel<R>& L, const R* __restrict__ u, R* __restri
 #pragma unroll
     for (int k = 0; k < 18; ++k) sye[e * 18 + k] = ye[k];
   }
-  __syncthreads();
+  cluster_barrier();
   const int64_t nn = (int64_t)g.nnx * g.nnz;
-  for (int64_t n = threadIdx.x; n < nn; n += blockDim.x) {
+  for (int64_t n = t0; n < nn; n += nt) {
     const int ix = (int)(n % g.nnx), iz = (int)(n / g.nnx);
     const bool xo_ = ix & 1, zo = iz & 1;
     const int xa = xo_ ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
@@ -1427,14 +1444,15 @@ MW_D void tail_apply(const TailLevel<R>& L, const R* __restrict__ u, R* __restri
       reinterpret_cast<R2*>(xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
     }
   }
-  __syncthreads();
+  cluster_barrier();
 }
 
 template <typename R>
-__global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
+__global__ void __cluster_dims__(TAIL_CLUSTER, 1, 1) __launch_bounds__(tail_threads<R>(), 1)
+k_vtail(TailArgs<R> A) {
   pdl_entry();
-  extern __shared__ __align__(16) unsigned char tail_smem[];
-  R* sye = reinterpret_cast<R*>(tail_smem);
+  R* sye = A.ye;
+  const int t0 = (int)(cluster_rank() * blockDim.x + threadIdx.x), nt = (int)(TAIL_CLUSTER * blockDim.x);
   __shared__ TailLevel<R> sL[MAX_TAIL];
 #pragma unroll
   for (int l = 0; l < MAX_TAIL; ++l)
@@ -1444,7 +1462,7 @@ __global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
   R* ts[MAX_TAIL];
   for (int l = 0; l < A.n; ++l) { xs[l] = sL[l].x; ts[l] = sL[l].t; }
   auto cheb_step = [&](int l, int k) {             // Chebyshev step k: x_out in t, then swap
-    tail_apply<R, AM_CHEB>(sL[l], xs[l], ts[l], sL[l].cheb + 2 * k, sye);
+    tail_apply<R, AM_CHEB>(sL[l], xs[l], ts[l], sL[l].cheb + 2 * k, sye, t0, nt);
     R* tmp = xs[l]; xs[l] = ts[l]; ts[l] = tmp;
   };
   auto smooth_tail = [&](int l, int degree, bool zero_start, bool first_done) {
@@ -1454,11 +1472,11 @@ __global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
     } else if (zero_start) {
       const R c = (R)L.cheb[1];
       const int64_t n = 2LL * L.g.nnx * L.g.nnz;
-      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      for (int64_t i = t0; i < n; i += nt) {
         R v = c * L.b[i] / L.diag[i];
         xs[l][i] = v; L.d[i] = v;
       }
-      __syncthreads();
+      cluster_barrier();
     } else {
       cheb_step(l, 0);
     }
@@ -1467,21 +1485,21 @@ __global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
   // down: pre-smoothing, residual, restriction (with the coarse level's first Chebyshev step)
   for (int l = 0; l + 1 < A.n; ++l) {
     const bool fd = l == 0 ? A.first_done != 0 : true;
-    smooth_tail(l, A.degree, !fd, fd);
-    tail_apply<R, AM_RESID>(sL[l], xs[l], nullptr, nullptr, sye);
+    smooth_tail(l, sL[l].deg, !fd, fd);
+    tail_apply<R, AM_RESID>(sL[l], xs[l], nullptr, nullptr, sye, t0, nt);
     const TailLevel<R>& F = sL[l];
     const TailLevel<R>& C = sL[l + 1];
     const bool fuse = !(l + 2 == A.n && A.dense);
     const double c0 = fuse ? C.cheb[1] : 0.0;
     const int64_t ncn = (int64_t)C.g.nnx * C.g.nnz;
-    for (int64_t n = threadIdx.x; n < ncn; n += blockDim.x)
+    for (int64_t n = t0; n < ncn; n += nt)
       restrict_node(F.g, C.g, F.r, C.fix, C.b, c0, fuse, C.diag, xs[l + 1], C.d, n);
-    __syncthreads();
+    cluster_barrier();
   }
   {  // coarsest level
     const int l = A.n - 1;
     if (A.dense) {
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+      const int lane = t0 & 31, warp = t0 >> 5, nwarp = nt >> 5;
       const R* b = sL[l].b;
       for (int row = warp; row < A.nd; row += nwarp) {
         double sacc = 0;
@@ -1489,7 +1507,7 @@ __global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
         for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
         if (lane == 0) xs[l][row] = (R)sacc;
       }
-      __syncthreads();
+      cluster_barrier();
     } else {
       const bool fd = A.n == 1 ? A.first_done != 0 : true;
       smooth_tail(l, MAXDEG, !fd, fd);
@@ -1500,23 +1518,13 @@ __global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail(TailArgs<R> A) {
     const TailLevel<R>& F = sL[l];
     const TailLevel<R>& C = sL[l + 1];
     const int64_t nfn = (int64_t)F.g.nnx * F.g.nnz;
-    for (int64_t n = threadIdx.x; n < nfn; n += blockDim.x) prolong_node(F.g, C.g, xs[l + 1], F.fix, xs[l], n);
-    __syncthreads();
-    smooth_tail(l, A.degree, false, false);
+    for (int64_t n = t0; n < nfn; n += nt) prolong_node(F.g, C.g, xs[l + 1], F.fix, xs[l], n);
+    cluster_barrier();
+    smooth_tail(l, sL[l].deg, false, false);
   }
 }
 
-// Dynamic shared memory of the tail kernel beyond the default 48 KB; false (tail off) on failure.
-template <typename R>
-static bool tail_smem_ok(const Hierarchy<R>& H) {
-  if (!H.tail0) return true;
-  if (H.tail_smem <= 48 * 1024) return true;
-  if (cudaFuncSetAttribute(k_vtail<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)H.tail_smem) ==
-      cudaSuccess)
-    return true;
-  cudaGetLastError();
-  return false;
-}
+
 
 // Chebyshev smoothing of level L: x (in/out) with rhs b, `steps` steps; zero_start -> x = 0 on entry.
 template <typename R>
@@ -1552,40 +1560,40 @@ static void smooth_swaps(Level<R>& L, int degree, bool zero_start, bool first_do
 }
 
 template <typename R>
-static void tail_swaps(Hierarchy<R>& H, int l, int degree, bool first_done) {
+static void tail_swaps(Hierarchy<R>& H, int l, bool first_done) {
   Level<R>& L = H.L[l];
   if (l == H.nlev - 1) {
     if (!H.dense) smooth_swaps(L, MAXDEG, !first_done, first_done);
     return;
   }
-  smooth_swaps(L, degree, !first_done, first_done);
-  tail_swaps(H, l + 1, degree, !(l + 1 == H.nlev - 1 && H.dense));
-  smooth_swaps(L, degree, false, false);
+  smooth_swaps(L, L.deg, !first_done, first_done);
+  tail_swaps(H, l + 1, !(l + 1 == H.nlev - 1 && H.dense));
+  smooth_swaps(L, L.deg, false, false);
 }
 
 template <typename R>
-static void launch_tail(Hierarchy<R>& H, int l0, int degree, bool first_done, cudaStream_t s) {
+static void launch_tail(Hierarchy<R>& H, int l0, bool first_done, cudaStream_t s) {
   TailArgs<R> A;
   memset(&A, 0, sizeof(A));
   A.n = H.nlev - l0;
   for (int i = 0; i < A.n; ++i) {
     const Level<R>& L = H.L[l0 + i];
-    A.L[i] = TailLevel<R>{L.g, L.eta, L.fix, L.diag, L.x, L.t, L.b, L.r, L.d, L.cheb};
+    A.L[i] = TailLevel<R>{L.g, L.eta, L.fix, L.diag, L.x, L.t, L.b, L.r, L.d, L.cheb, L.deg};
   }
-  A.degree = degree;
   A.first_done = first_done ? 1 : 0;
   A.dense = H.dense ? 1 : 0;
   A.nd = H.nd;
   A.Ainv = H.Ainv;
-  pdl_launch(k_vtail<R>, 1, tail_threads<R>(), H.tail_smem, s, A);
+  A.ye = H.tail_ye;
+  pdl_launch(k_vtail<R>, TAIL_CLUSTER, tail_threads<R>(), 0, s, A);
 }
 
 template <typename R>
-static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool first_done = false) {
+static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = false) {
   Level<R>& L = H.L[l];
   if (H.tail0 > 0 && l == H.tail0) {               // the coarse levels in one launch
-    launch_tail(H, l, degree, first_done, s);
-    tail_swaps(H, l, degree, first_done);
+    launch_tail(H, l, first_done, s);
+    tail_swaps(H, l, first_done);
     return;
   }
   if (l == H.nlev - 1) {
@@ -1598,16 +1606,16 @@ static void vcycle(Hierarchy<R>& H, int l, int degree, cudaStream_t s, bool firs
     return;
   }
   Level<R>& C = H.L[l + 1];
-  smooth(L, degree, !first_done, s, first_done);
+  smooth(L, L.deg, !first_done, s, first_done);
   ApplyArgs<R> a = args0<R>();
   a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.r; a.bV = L.b;
   launch_apply<R, AM_RESID>(L.g, a, s);
   const bool fuse = !(l + 1 == H.nlev - 1 && H.dense);
   pdl_launch(k_restrict<R>, grid_for(C.nn, 256), 256, 0, s, L.g, C.g, L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
              C.x, C.d);
-  vcycle(H, l + 1, degree, s, fuse);
+  vcycle(H, l + 1, s, fuse);
   pdl_launch(k_prolong_add<R>, grid_for(L.nn, 256), 256, 0, s, L.g, C.g, C.x, L.fix, L.x);
-  smooth(L, degree, false, s);
+  smooth(L, L.deg, false, s);
 }
 
 // Replays the kernels `record` issues on s from a CUDA graph cached under (kind, host state).
@@ -1684,9 +1692,9 @@ static void vload(Hierarchy<R>& H, const std::vector<void*>& v) {
 
 // One V-cycle of hierarchy H (degree-`degree` Chebyshev smoothing) from a cached graph.
 template <typename R>
-static void vcycle_run(mw_stokes* S, Hierarchy<R>& H, int degree, cudaStream_t s) {
-  const int kind = (sizeof(R) == 4 ? 1 : 2) * 64 + degree;
-  graph_run(S, kind, [&]() { vcycle(H, 0, degree, s); }, [&]() { return vstate(H); },
+static void vcycle_run(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
+  const int kind = (sizeof(R) == 4 ? 1 : 2) * 64;
+  graph_run(S, kind, [&]() { vcycle(H, 0, s); }, [&]() { return vstate(H); },
             [&](const std::vector<void*>& v) { vload(H, v); }, s);
 }
 
@@ -1780,7 +1788,7 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
       pdl_launch(k_dinv<R>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.d, L.diag, v);
     }
     dot<R>(S, L.ndof, v, v, L.lam2, s);          // ||D^-1 K v_prev||^2 with ||v_prev|| = 1
-    int deg = coarsest ? MAXDEG : prm.cheb_degree;
+    int deg = coarsest ? MAXDEG : L.deg;
     pdl_launch(k_cheb_coeffs, 1, 32, 0, s, L.lam2, deg, prm.cheb_ratio, prm.cheb_safety, L.cheb);
   }
   if (ds != s) {
@@ -1821,7 +1829,7 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
   auto precond = [&](R* rin, R*& zout) {
     R* saved_b = L.b;
     L.b = rin;
-    vcycle_run(S, H, S->prm.cheb_degree, s);
+    vcycle_run(S, H, s);
     L.b = saved_b;
     std::swap(zout, L.x);
   };
@@ -2175,7 +2183,7 @@ static bool pcg_K_dev(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, do
   auto precond = [&](R* rin, R*& zout, cudaStream_t st) {
     R* saved_b = L.b;
     L.b = rin;
-    vcycle(H, 0, S->prm.cheb_degree, st);
+    vcycle(H, 0, st);
     L.b = saved_b;
     std::swap(zout, L.x);
   };
@@ -2400,8 +2408,6 @@ int mw_stokes_create(mw_box box, mw_stokes_params prm, const uint8_t* bc_fix_V, 
   size_t need = do_layout(S, nullptr, true);
   if (work_bytes < need) { delete S; return MW_ERR_WORKSPACE; }
   do_layout(S, (char*)work, false);
-  if (S->has32 && !tail_smem_ok(S->H32)) S->H32.tail0 = 0;
-  if (S->has64 && !tail_smem_ok(S->H64)) S->H64.tail0 = 0;
   if (cudaMemset(S->counter, 0, sizeof(unsigned) * 4) != cudaSuccess) { delete S; return MW_ERR_CUDA; }
   *out = S;
   return MW_OK;
@@ -2487,12 +2493,12 @@ int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, vo
   if (precision == MW_F32) {
     Level<float>& L = S->H32.L[0];
     pdl_launch(k_copy<float, float>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, (const float*)b, L.b);
-    vcycle(S->H32, 0, S->prm.cheb_degree, s);
+    vcycle(S->H32, 0, s);
     pdl_launch(k_copy<float, float>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.x, (float*)x);
   } else {
     Level<double>& L = S->H64.L[0];
     pdl_launch(k_copy<double, double>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, (const double*)b, L.b);
-    vcycle(S->H64, 0, S->prm.cheb_degree, s);
+    vcycle(S->H64, 0, s);
     pdl_launch(k_copy<double, double>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.x, (double*)x);
   }
   MW_CHECK_LAUNCH();

@@ -7,6 +7,7 @@
 // matrix applied without forming it -- and the system is solved by Jacobi-preconditioned
 // BiCGSTAB in FP64 to a relative residual tolerance.  The solve first regroups the rows by node
 // class (k_energy_rows) so that every matvec of the iteration reads them coalesced.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -136,36 +137,6 @@ __global__ void k_energy_rows(mw_box b, RowPlanes P, const double* __restrict__ 
   }
 }
 
-// k_energy_matvec on the coefficient planes: the same products summed in the same order
-__global__ void k_energy_matvec_rows(mw_box b, RowPlanes P, const double* __restrict__ coef,
-                                     const double* __restrict__ x, const double* __restrict__ rhs,
-                                     double* __restrict__ y, double* __restrict__ diag, int mode) {
-  pdl_entry();
-  const int nnx = 2 * b.nelx + 1;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < P.m0[4]; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t m;
-    const int c = class_of(P, t, &m);
-    const int mxc = pick(P.mx, c);
-    const int64_t M = (int64_t)mxc * pick(P.mz, c);
-    const int i = (int)(m % mxc), k = (int)(m / mxc);
-    const int ix = 2 * i + ((c == 0 || c == 1) ? 1 : 0), iz = 2 * k + ((c == 0 || c == 2) ? 1 : 0);
-    const double* cf = coef + pick(P.off, c) + m;
-    const int nslot = pick(P.slots, c);
-    double acc = 0.0, dg = 0.0;
-    for (int s = 0; s < nslot; ++s) {
-      int ex, ez, kl;
-      if (!slot_element(c, s, i, k, b, &ex, &ez, &kl)) continue;
-      const double* row = cf + (int64_t)s * 9 * M;
-#pragma unroll
-      for (int j = 0; j < 9; ++j) acc += row[j * M] * x[q2_node(ex, ez, j, nnx)];
-      dg += row[kl * M];
-    }
-    const int64_t n = (int64_t)iz * nnx + ix;
-    y[n] = mode == 1 ? rhs[n] - acc : acc;
-    if (diag) diag[n] = dg;
-  }
-}
-
 __global__ void k_edot_partial(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
                                double* __restrict__ part) {
   pdl_entry();
@@ -201,88 +172,187 @@ __global__ void k_edot_final(const double* __restrict__ part, int nb, double* __
 }
 
 // BiCGSTAB vector updates with device scalars s[]: see the host loop for the slot meaning.
-// p = r + beta (p - omega v), beta = (rho_new/rho_old) (alpha/omega)
-__global__ void k_bicg_p(int64_t n, const double* __restrict__ s, const double* __restrict__ r,
-                         const double* __restrict__ v, double* __restrict__ p, int first) {
-  pdl_entry();
-  const double beta = first ? 0.0 : (s[0] / s[1]) * (s[2] / s[3]);
-  const double om = first ? 0.0 : s[3];
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);   // first pass never reads p, v
+// Deterministic grid-wide sums of K values per thread: block sums go to part[k * gridDim.x + block],
+// the last block to arrive adds them in block order, writes *out[k] and resets the counter.  Called
+// once, by every thread, at the end of a kernel.
+template <int K>
+MW_D void grid_sums(double (&v)[K], double* part, unsigned* counter, double* const (&out)[K]) {
+  __shared__ double sh[K][32];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double t = v[k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0) sh[k][wid] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double t = 0;
+      for (int w = 0; w < nw; ++w) t += sh[k][w];
+      part[k * gridDim.x + blockIdx.x] = t;
+    }
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double t = 0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) t += ((volatile double*)part)[k * gridDim.x + i];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    __syncthreads();
+    if (lane == 0) sh[k][wid] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double u = 0;
+      for (int w = 0; w < nw; ++w) u += sh[k][w];
+      *out[k] = u;
+    }
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
-// the same update with the first-iteration switch read from the device iteration count sc[12]
-__global__ void k_bicg_p_dev(int64_t n, const double* __restrict__ s, const double* __restrict__ r,
-                             const double* __restrict__ v, double* __restrict__ p) {
+// k_energy_matvec on the coefficient planes: the same products summed in the same order.  ND = 1
+// also sums (a0, y) (the iteration's (r0, v)), ND = 2 sums (y, a0) and (y, y) ((t, s), (t, t)).
+template <int ND>
+__global__ void k_energy_matvec_rows(mw_box b, RowPlanes P, const double* __restrict__ coef,
+                                     const double* __restrict__ x, const double* __restrict__ rhs,
+                                     double* __restrict__ y, double* __restrict__ diag, int mode,
+                                     const double* __restrict__ a0, double* __restrict__ part,
+                                     unsigned* __restrict__ counter, double* o0, double* o1) {
   pdl_entry();
-  const bool first = s[12] == 0.0;
-  const double beta = first ? 0.0 : (s[0] / s[1]) * (s[2] / s[3]);
-  const double om = first ? 0.0 : s[3];
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    p[i] = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);
-}
-
-__global__ void k_scale_diag(int64_t n, const double* __restrict__ x, const double* __restrict__ d,
-                             double* __restrict__ y) {
-  pdl_entry();
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] = x[i] / d[i];
-}
-
-// s = r - alpha v, alpha = rho / (r0, v) = s[0] / s[4]
-__global__ void k_bicg_s(int64_t n, const double* __restrict__ sc, const double* __restrict__ r,
-                         const double* __restrict__ v, double* __restrict__ sv) {
-  pdl_entry();
-  const double alpha = sc[0] / sc[4];
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    sv[i] = r[i] - alpha * v[i];
-}
-
-// x += alpha phat + omega shat ; r = s - omega t ; omega = (t,s)/(t,t) = sc[5]/sc[6]
-__global__ void k_bicg_x(int64_t n, double* __restrict__ sc, const double* __restrict__ ph,
-                         const double* __restrict__ sh, const double* __restrict__ sv, const double* __restrict__ t,
-                         double* __restrict__ x, double* __restrict__ r) {
-  pdl_entry();
-  const double alpha = sc[0] / sc[4];
-  const double omega = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] += alpha * ph[i] + omega * sh[i];
-    r[i] = sv[i] - omega * t[i];
+  const int nnx = 2 * b.nelx + 1;
+  double v[ND > 0 ? ND : 1] = {};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < P.m0[4]; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t m;
+    const int c = class_of(P, t, &m);
+    const int mxc = pick(P.mx, c);
+    const int64_t M = (int64_t)mxc * pick(P.mz, c);
+    const int i = (int)(m % mxc), k = (int)(m / mxc);
+    const int ix = 2 * i + ((c == 0 || c == 1) ? 1 : 0), iz = 2 * k + ((c == 0 || c == 2) ? 1 : 0);
+    const double* cf = coef + pick(P.off, c) + m;
+    const int nslot = pick(P.slots, c);
+    double acc = 0.0, dg = 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {                   // unrolled and predicated: the slots' loads overlap
+      int ex, ez, kl;
+      if (s < nslot && slot_element(c, s, i, k, b, &ex, &ez, &kl)) {
+        const double* row = cf + (int64_t)s * 9 * M;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) acc += row[j * M] * x[q2_node(ex, ez, j, nnx)];
+        dg += row[kl * M];
+      }
+    }
+    const int64_t n = (int64_t)iz * nnx + ix;
+    y[n] = mode == 1 ? rhs[n] - acc : acc;
+    if (diag) diag[n] = dg;
+    if (ND == 1) v[0] += a0[n] * acc;
+    if (ND == 2) {
+      v[0] += acc * a0[n];
+      v[ND - 1] += acc * acc;
+    }
+  }
+  if (ND == 1) {
+    double* const out[1] = {o0};
+    grid_sums<1>(*reinterpret_cast<double(*)[1]>(v), part, counter, out);
+  } else if (ND == 2) {
+    double* const out[2] = {o0, o1};
+    grid_sums<2>(*reinterpret_cast<double(*)[2]>(v), part, counter, out);
   }
 }
 
-// keep alpha (slot 2) and omega (slot 3) of this iteration, rho_old (slot 1) <- rho (slot 0)
-__global__ void k_bicg_roll(double* sc) {
+// Scalar slots of the iteration (sc): 0 rho = (r0, r), 1 rho of the previous iteration, 2 alpha,
+// 3 omega, 4 (r0, v), 5 (t, s), 6 (t, t), 7 (r0, r) of the new residual, 10 (b, b), 11 (r, r),
+// 12 iteration count.  Each iteration is six launches: the direction update, A p^ with (r0, v),
+// the s update, A s^ with (t, s) and (t, t), the x / r update with (r, r) and (r0, r), the scalar
+// roll with the loop test.
+
+// p = r + beta (p - omega v), beta = (rho/rho_old) (alpha/omega) (p = r on the first iteration);
+// p^ = D^-1 p
+__global__ void k_bicg_p(int64_t n, const double* __restrict__ sc, const double* __restrict__ r,
+                         const double* __restrict__ v, double* __restrict__ p, const double* __restrict__ dg,
+                         double* __restrict__ ph) {
+  pdl_entry();
+  const bool first = sc[12] == 0.0;
+  const double beta = first ? 0.0 : (sc[0] / sc[1]) * (sc[2] / sc[3]);
+  const double om = first ? 0.0 : sc[3];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double pi = first ? r[i] : r[i] + beta * (p[i] - om * v[i]);   // the first pass never reads p, v
+    p[i] = pi;
+    ph[i] = pi / dg[i];
+  }
+}
+
+// s = r - alpha v, alpha = rho / (r0, v); s^ = D^-1 s
+__global__ void k_bicg_s(int64_t n, const double* __restrict__ sc, const double* __restrict__ r,
+                         const double* __restrict__ v, double* __restrict__ sv, const double* __restrict__ dg,
+                         double* __restrict__ sh) {
+  pdl_entry();
+  const double alpha = sc[0] / sc[4];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double si = r[i] - alpha * v[i];
+    sv[i] = si;
+    sh[i] = si / dg[i];
+  }
+}
+
+// x += alpha p^ + omega s^ ; r = s - omega t ; omega = (t, s) / (t, t); then (r, r) -> sc[11] and
+// (r0, r) -> sc[7]
+__global__ void k_bicg_x(int64_t n, double* __restrict__ sc, const double* __restrict__ ph,
+                         const double* __restrict__ sh, const double* __restrict__ sv, const double* __restrict__ t,
+                         const double* __restrict__ r0, double* __restrict__ x, double* __restrict__ r,
+                         double* __restrict__ part, unsigned* __restrict__ counter) {
+  pdl_entry();
+  const double alpha = sc[0] / sc[4];
+  const double omega = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
+  double v[2] = {0.0, 0.0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] += alpha * ph[i] + omega * sh[i];
+    const double ri = sv[i] - omega * t[i];
+    r[i] = ri;
+    v[0] += ri * ri;
+    v[1] += r0[i] * ri;
+  }
+  double* const out[2] = {sc + 11, sc + 7};
+  grid_sums<2>(v, part, counter, out);
+}
+
+// keep alpha (slot 2) and omega (slot 3) of this iteration, rho_old <- rho, rho <- (r0, r);
+// count the iteration and, inside a recorded graph (use_h), set the loop condition: continue while
+// the residual is finite, above rtol * ||b|| and the count is below maxit
+__global__ void k_bicg_roll(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h, int use_h) {
   pdl_entry();
   if (threadIdx.x || blockIdx.x) return;
   sc[2] = sc[0] / sc[4];
   sc[3] = sc[6] != 0.0 ? sc[5] / sc[6] : 0.0;
   sc[1] = sc[0];
-}
-
-// ---- the iteration as a recorded CUDA graph with a device WHILE loop ----
-// sc[12] = iteration count; the loop runs while the residual is finite, above rtol * ||b|| and
-// the count is below maxit.
-__global__ void k_bicg_init(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h) {
-  pdl_entry();
-  if (!(sc[10] > 0)) sc[10] = 1.0;
-  sc[12] = 0;
-  const double rr = sc[11];
-  cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && maxit > 0) ? 1u : 0u);
-}
-
-__global__ void k_bicg_check(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h) {
-  pdl_entry();
+  sc[0] = sc[7];
   const double it = sc[12] + 1;
   sc[12] = it;
   const double rr = sc[11];
-  cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && it < (double)maxit) ? 1u : 0u);
+  if (use_h) cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && it < (double)maxit) ? 1u : 0u);
+}
+
+// ---- the iteration as a recorded CUDA graph with a device WHILE loop ----
+// sc[12] = iteration count; rho = (r0, r) = (r, r) to start with (r0 = r)
+__global__ void k_bicg_init(double* sc, double rtol, int maxit, cudaGraphConditionalHandle h, int use_h) {
+  pdl_entry();
+  if (!(sc[10] > 0)) sc[10] = 1.0;
+  sc[12] = 0;
+  sc[0] = sc[11];
+  const double rr = sc[11];
+  if (use_h) cudaGraphSetConditional(h, (isfinite(rr) && rr > rtol * rtol * sc[10] && maxit > 0) ? 1u : 0u);
 }
 
 // Workspace of the solve (doubles): nine node vectors, then the dot-product partials, the device
 // scalars and the row planes.
-constexpr int E_NB = 1184;                 // dot-product CTAs (8 per SM) and partial slots
-constexpr int64_t E_SC = E_NB + 16;        // scalars, after the partials
+constexpr int E_NB = 1184;                 // dot-product CTAs (8 per SM); two partials per CTA
+constexpr int64_t E_SC = 2 * E_NB + 16;    // scalars, after the partials (slot 200: the arrival counter)
 constexpr int64_t E_COEF = E_SC + 256;     // row planes, after the scalars
 
 struct EnergyGraph {
@@ -325,6 +395,63 @@ int mw_energy_matvec(mw_box box, const double* VV_T, const double* x, double* y,
   pdl_launch(k_energy_matvec, grid_for(nn, 256), 256, 0, (cudaStream_t)stream, box, VV_T, x, nullptr, y, nullptr, 0);
   MW_CHECK_LAUNCH();
   return MW_OK;
+}
+
+// The buffers of the solve in its workspace (doubles): r, r0, p, v, s, t, p^, s^, diag, the
+// dot-product partials, the scalar slots (the arrival counter of the fused dot products in slot
+// 200) and the row planes.
+struct EnergyBufs {
+  int64_t n;
+  double *r, *r0, *p, *v, *sv, *t, *ph, *sh, *dg, *part, *sc, *coef;
+  unsigned* counter;
+  RowPlanes RP;
+  int grid;               // CTAs of the node kernels (at most E_NB: one partial slot each)
+};
+
+static EnergyBufs energy_bufs(mw_box box, void* work) {
+  EnergyBufs E;
+  E.n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  double* w = (double*)work;
+  const int64_t n = E.n;
+  E.r = w; E.r0 = w + n; E.p = w + 2 * n; E.v = w + 3 * n; E.sv = w + 4 * n; E.t = w + 5 * n;
+  E.ph = w + 6 * n; E.sh = w + 7 * n; E.dg = w + 8 * n;
+  E.part = w + 9 * n;
+  E.sc = w + 9 * n + E_SC;
+  E.counter = reinterpret_cast<unsigned*>(E.sc + 200);
+  E.coef = w + 9 * n + E_COEF;
+  E.RP = row_planes(box);
+  E.grid = std::min(grid_for(n, 256), E_NB);
+  return E;
+}
+
+// Row planes from VV_T, r = b - A T (T holds the initial guess) with diag(A), r0 = r, (b, b) and
+// (r, r) into sc[10], sc[11].
+static void energy_start(const EnergyBufs& E, mw_box box, const double* VV_T, const double* rhs, double* T,
+                         cudaStream_t s) {
+  cudaMemsetAsync(E.counter, 0, sizeof(unsigned), s);
+  pdl_launch(k_energy_rows, grid_for(E.RP.total / 9, 256), 256, 0, s, box, E.RP, VV_T, E.coef);
+  pdl_launch(k_energy_matvec_rows<0>, E.grid, 256, 0, s, box, E.RP, E.coef, T, rhs, E.r, E.dg, 1, nullptr,
+             nullptr, nullptr, nullptr, nullptr);
+  cudaMemcpyAsync(E.r0, E.r, sizeof(double) * E.n, cudaMemcpyDeviceToDevice, s);
+  const double* a[2] = {rhs, E.r};
+  for (int k = 0; k < 2; ++k) {
+    pdl_launch(k_edot_partial, E_NB, 256, 0, s, E.n, a[k], a[k], E.part);
+    pdl_launch(k_edot_final, 1, 256, 0, s, E.part, E_NB, E.sc + 10 + k);
+  }
+}
+
+// One BiCGSTAB iteration (Jacobi-preconditioned), six launches; with use_h the last one sets the
+// WHILE condition of the recorded loop.
+static void energy_iteration(const EnergyBufs& E, mw_box box, double* T, double rtol, int maxit,
+                             cudaGraphConditionalHandle h, int use_h, cudaStream_t s) {
+  pdl_launch(k_bicg_p, E.grid, 256, 0, s, E.n, E.sc, E.r, E.v, E.p, E.dg, E.ph);
+  pdl_launch(k_energy_matvec_rows<1>, E.grid, 256, 0, s, box, E.RP, E.coef, E.ph, nullptr, E.v, nullptr, 0, E.r0,
+             E.part, E.counter, E.sc + 4, nullptr);
+  pdl_launch(k_bicg_s, E.grid, 256, 0, s, E.n, E.sc, E.r, E.v, E.sv, E.dg, E.sh);
+  pdl_launch(k_energy_matvec_rows<2>, E.grid, 256, 0, s, box, E.RP, E.coef, E.sh, nullptr, E.t, nullptr, 0, E.sv,
+             E.part, E.counter, E.sc + 5, E.sc + 6);
+  pdl_launch(k_bicg_x, E.grid, 256, 0, s, E.n, E.sc, E.ph, E.sh, E.sv, E.t, E.r0, T, E.r, E.part, E.counter);
+  pdl_launch(k_bicg_roll, 1, 32, 0, s, E.sc, rtol, maxit, h, use_h);
 }
 
 // Records the BiCGSTAB solve on the capturing stream s (body captured on b); false on failure.
@@ -424,50 +551,21 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
     }
   }
   cudaStream_t s = (cudaStream_t)stream;
-  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  double* w = (double*)work;
-  double *r = w, *r0 = w + n, *p = w + 2 * n, *v = w + 3 * n, *sv = w + 4 * n, *t = w + 5 * n, *ph = w + 6 * n,
-         *sh = w + 7 * n, *dg = w + 8 * n;
-  double* part = w + 9 * n;         // dot-product partials
-  double* sc = w + 9 * n + E_SC;    // scalar slots
-  const int NBk = E_NB;
-  auto dot = [&](const double* a, const double* b2, double* out) {
-    pdl_launch(k_edot_partial, NBk, 256, 0, s, n, a, b2, part);
-    pdl_launch(k_edot_final, 1, 256, 0, s, part, NBk, out);
-  };
+  const EnergyBufs E = energy_bufs(box, work);
   auto rd = [&](const double* d) {
     double h = 0;
     cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     return h;
   };
-  const RowPlanes RP = row_planes(box);
-  double* coef = w + 9 * n + E_COEF;
-  pdl_launch(k_energy_rows, grid_for(RP.total / 9, 256), 256, 0, s, box, RP, VV_T, coef);
-  // r = b - A T (T is the initial guess), diag
-  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, T, rhs, r, dg, 1);
-  cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
-  dot(rhs, rhs, sc + 10);
-  dot(r, r, sc + 11);
-  double bb = rd(sc + 10);
-  double rr = rd(sc + 11);
+  energy_start(E, box, VV_T, rhs, T, s);
+  pdl_launch(k_bicg_init, 1, 1, 0, s, E.sc, rtol, maxit, cudaGraphConditionalHandle(0), 0);
+  double bb = rd(E.sc + 10);
+  double rr = rd(E.sc + 11);
   int it = 0;
-  if (!(bb > 0)) bb = 1.0;
   for (it = 1; it <= maxit && rr > rtol * rtol * bb; ++it) {
-    dot(r0, r, sc + 0);                                       // rho
-    pdl_launch(k_bicg_p, grid_for(n, 256), 256, 0, s, n, sc, r, v, p, it == 1);
-    pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, s, n, p, dg, ph);
-    pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, ph, nullptr, v, nullptr, 0);
-    dot(r0, v, sc + 4);
-    pdl_launch(k_bicg_s, grid_for(n, 256), 256, 0, s, n, sc, r, v, sv);
-    pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, s, n, sv, dg, sh);
-    pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, sh, nullptr, t, nullptr, 0);
-    dot(t, sv, sc + 5);
-    dot(t, t, sc + 6);
-    pdl_launch(k_bicg_x, grid_for(n, 256), 256, 0, s, n, sc, ph, sh, sv, t, T, r);
-    pdl_launch(k_bicg_roll, 1, 32, 0, s, sc);
-    dot(r, r, sc + 11);
-    rr = rd(sc + 11);
+    energy_iteration(E, box, T, rtol, maxit, cudaGraphConditionalHandle(0), 0, s);
+    rr = rd(E.sc + 11);
     if (!std::isfinite(rr)) break;
   }
   if (iters) *iters = it - 1;
@@ -480,24 +578,8 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
 
 static bool energy_record(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int maxit,
                           void* work, cudaStream_t s, cudaStream_t b) {
-  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
-  double* w = (double*)work;
-  double *r = w, *r0 = w + n, *p = w + 2 * n, *v = w + 3 * n, *sv = w + 4 * n, *t = w + 5 * n, *ph = w + 6 * n,
-         *sh = w + 7 * n, *dg = w + 8 * n;
-  double* part = w + 9 * n;
-  double* sc = w + 9 * n + E_SC;
-  const RowPlanes RP = row_planes(box);
-  double* coef = w + 9 * n + E_COEF;
-  const int NBk = E_NB;
-  auto dot = [&](const double* a, const double* b2, double* out, cudaStream_t st) {
-    pdl_launch(k_edot_partial, NBk, 256, 0, st, n, a, b2, part);
-    pdl_launch(k_edot_final, 1, 256, 0, st, part, NBk, out);
-  };
-  pdl_launch(k_energy_rows, grid_for(RP.total / 9, 256), 256, 0, s, box, RP, VV_T, coef);
-  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, s, box, RP, coef, T, rhs, r, dg, 1);
-  cudaMemcpyAsync(r0, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
-  dot(rhs, rhs, sc + 10, s);
-  dot(r, r, sc + 11, s);
+  const EnergyBufs E = energy_bufs(box, work);
+  energy_start(E, box, VV_T, rhs, T, s);
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   cudaGraph_t g = nullptr;
   const cudaGraphNode_t* deps = nullptr;
@@ -505,7 +587,7 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
   if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, nullptr, nullptr) != cudaSuccess) return false;
   cudaGraphConditionalHandle h;
   if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return false;
-  pdl_launch(k_bicg_init, 1, 1, 0, s, sc, rtol, maxit, h);
+  pdl_launch(k_bicg_init, 1, 1, 0, s, E.sc, rtol, maxit, h, 1);
   if (cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd) != cudaSuccess) return false;
   cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
   prm.conditional.handle = h;
@@ -517,21 +599,7 @@ static bool energy_record(mw_box box, const double* VV_T, const double* rhs, dou
   if (cudaStreamBeginCaptureToGraph(b, prm.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                     cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     return false;
-  // body: one BiCGSTAB iteration (the host loop's kernels, first-iteration branch on sc[12])
-  dot(r0, r, sc + 0, b);
-  pdl_launch(k_bicg_p_dev, grid_for(n, 256), 256, 0, b, n, sc, r, v, p);
-  pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, b, n, p, dg, ph);
-  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, b, box, RP, coef, ph, nullptr, v, nullptr, 0);
-  dot(r0, v, sc + 4, b);
-  pdl_launch(k_bicg_s, grid_for(n, 256), 256, 0, b, n, sc, r, v, sv);
-  pdl_launch(k_scale_diag, grid_for(n, 256), 256, 0, b, n, sv, dg, sh);
-  pdl_launch(k_energy_matvec_rows, grid_for(n, 256), 256, 0, b, box, RP, coef, sh, nullptr, t, nullptr, 0);
-  dot(t, sv, sc + 5, b);
-  dot(t, t, sc + 6, b);
-  pdl_launch(k_bicg_x, grid_for(n, 256), 256, 0, b, n, sc, ph, sh, sv, t, T, r);
-  pdl_launch(k_bicg_roll, 1, 32, 0, b, sc);
-  dot(r, r, sc + 11, b);
-  pdl_launch(k_bicg_check, 1, 1, 0, b, sc, rtol, maxit, h);
+  energy_iteration(E, box, T, rtol, maxit, h, 1, b);         // the body: one iteration and the loop test
   cudaGraph_t gb = nullptr;
   return cudaStreamEndCapture(b, &gb) == cudaSuccess;
 }

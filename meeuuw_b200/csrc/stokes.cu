@@ -315,33 +315,80 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     }
   }
   // ---- stage velocity (masked; one vector load per node), pressure ----
+  // A fixed number of nodes per thread, all loads issued before any shared-memory store, so the
+  // staging costs one memory round trip rather than one per node.
   const R2* u2 = reinterpret_cast<const R2*>(a.u);
   const uchar2* f2 = reinterpret_cast<const uchar2*>(a.fix);
   R2* su2 = reinterpret_cast<R2*>(su);
-  for (int i = tid; i < LZ * LX; i += APPLY_THREADS) {
+  constexpr int NST = (LZ * LX + APPLY_THREADS - 1) / APPLY_THREADS;
+  constexpr int NSP = (PZ * PX + APPLY_THREADS - 1) / APPLY_THREADS;
+  R2 sv[NST];
+  uchar2 sf[NST];
+  R spv[NSP];
+  if constexpr (sizeof(R) == 8) {                    // FP64: one node at a time (fewer live registers)
+    for (int i = tid; i < LZ * LX; i += APPLY_THREADS) {
+      const int lz = i / LX, lx = i - lz * LX;
+      const int ix = lx0 + lx, iz = lz0 + lz;
+      R2 v;
+      v.x = 0; v.y = 0;
+      uchar2 ff = make_uchar2(0, 0);
+      if (ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
+        const int64_t n = (int64_t)iz * g.nnx + ix;
+        ff = f2[n];
+        if (use_u) {
+          const R2 uu = u2[n];
+          v.x = ff.x ? R(0) : uu.x;
+          v.y = ff.y ? R(0) : uu.y;
+        }
+      }
+      su2[i] = v;
+      sfix[i] = ff;
+    }
+    if (use_p)
+      for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
+        int jz = i / PX, jx = i % PX;
+        int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
+        sp[i] = (px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz) ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+      }
+  } else {
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int i = tid + k * APPLY_THREADS;
     const int lz = i / LX, lx = i - lz * LX;
     const int ix = lx0 + lx, iz = lz0 + lz;
-    R2 v;
-    v.x = 0; v.y = 0;
-    uchar2 ff = make_uchar2(0, 0);
-    if (ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
+    sv[k].x = 0; sv[k].y = 0;
+    sf[k] = make_uchar2(0, 0);
+    if (i < LZ * LX && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
       const int64_t n = (int64_t)iz * g.nnx + ix;
-      ff = f2[n];
-      if (use_u) {
-        const R2 uu = u2[n];
-        v.x = ff.x ? R(0) : uu.x;
-        v.y = ff.y ? R(0) : uu.y;
-      }
+      sf[k] = f2[n];
+      if (use_u) sv[k] = u2[n];
     }
-    su2[i] = v;
-    sfix[i] = ff;
   }
-  if (use_p)
-    for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
-      int jz = i / PX, jx = i % PX;
-      int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
-      sp[i] = (px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz) ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+#pragma unroll
+  for (int k = 0; k < NSP; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    const int jz = i / PX, jx = i % PX;
+    const int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
+    spv[k] = (use_p && i < PZ * PX && px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz)
+                 ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+  }
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    if (i < LZ * LX) {
+      R2 v;
+      v.x = sf[k].x ? R(0) : sv[k].x;
+      v.y = sf[k].y ? R(0) : sv[k].y;
+      su2[i] = v;
+      sfix[i] = sf[k];
     }
+  }
+#pragma unroll
+  for (int k = 0; k < NSP; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    if (use_p && i < PZ * PX) sp[i] = spv[k];
+  }
+  }
   __syncthreads();
   // ---- element products ----
   if (tid < NEL_T) {

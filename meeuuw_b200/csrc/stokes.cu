@@ -276,6 +276,9 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   constexpr int NPRE = sizeof(R) == 8 ? 0 : (MODE == AM_CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
   __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ __align__(16) R2 spre[(NPRE ? NPRE : 1) * 4 * TX * TZ];
+  constexpr int NJ = APPLY_THREADS - TX * TZ;         // spare threads: right column and top row nodes
+  static_assert(2 * TZ + 1 + 2 * TX <= 2 * NJ, "the spare threads take at most two boundary nodes each");
+  __shared__ __align__(16) R2 sspare[(NPRE ? NPRE : 1) * 2 * NJ];
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
   __shared__ uchar2 sfix[LZ * LX];          // Dirichlet flags of the staged nodes
@@ -300,6 +303,28 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         if (NPRE == 3) {
           cp_async_pair<R>(&spre[(4 + j) * TX * TZ + tid], a.diag + 2 * n);
           cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
+        }
+      }
+    }
+  }
+  // the spare threads' boundary nodes (at most 2 TZ + 1 + 2 TX = 49, two per spare thread)
+  const bool lastx = ex0 + TX >= g.nx, lastz = ez0 + TZ >= g.nz;
+  const int oz1 = lastz ? 2 * g.nz + 1 : 2 * (ez0 + TZ);
+  const int ncol_v = lastx ? oz1 - 2 * ez0 : 0;
+  const int nrow_v = lastz ? (lastx ? 2 * (g.nx - ex0) : 2 * TX) : 0;
+  if (NPRE && a.yV && tid >= TX * TZ && (lastx || lastz)) {
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int j = tid - TX * TZ + it * NJ;
+      if (j < ncol_v + nrow_v) {
+        const int ix = j < ncol_v ? 2 * g.nx : 2 * ex0 + (j - ncol_v);
+        const int iz = j < ncol_v ? 2 * ez0 + j : 2 * g.nz;
+        const int64_t n = (int64_t)iz * g.nnx + ix;
+        const int q = tid - TX * TZ;
+        cp_async_pair<R>(&sspare[it * NJ + q], a.bV + 2 * n);
+        if (NPRE == 3) {
+          cp_async_pair<R>(&sspare[(2 + it) * NJ + q], a.diag + 2 * n);
+          cp_async_pair<R>(&sspare[(4 + it) * NJ + q], a.d + 2 * n);
         }
       }
     }
@@ -425,9 +450,13 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   // and left edge midpoints, lower-left corner) and its lower-left pressure node, with the element
   // local indices known at compile time; the spare threads take the nodes on the right and top
   // mesh boundary, which belong to no element's lower-left quadrant.
-  const bool lastx = ex0 + TX >= g.nx, lastz = ez0 + TZ >= g.nz;
-  // velocity node epilogue: Dirichlet rows, then the mode's output.  slot >= 0: an owned
-  // element's node whose b, diag, d were prefetched; slot < 0: read them here.
+  // prefetched value of array k (0 b, 1 diag, 2 d): slots 0-3 are an owned element's nodes,
+  // slots 4-5 a spare thread's two boundary nodes
+  auto pre_at = [&](int k, int slot) -> R2 {
+    return slot < 4 ? spre[(4 * k + slot) * TX * TZ + tid] : sspare[(2 * k + slot - 4) * NJ + (tid - TX * TZ)];
+  };
+  // velocity node epilogue: Dirichlet rows, then the mode's output.  slot >= 0: b, diag, d were
+  // prefetched; slot < 0: read them here.
   auto emit = [&](int ix, int iz, R y0, R y1, int slot) {
     const int64_t n = (int64_t)iz * g.nnx + ix;
     const int li = (iz - lz0) * LX + (ix - lx0);
@@ -437,12 +466,12 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     // every load first, none depending on another
     R2 uu = su2[li];                                 // the staged velocity: exact on free dofs
     R2 dg{R(0), R(0)}, bb{R(0), R(0)}, dd{R(0), R(0)};
-    if (MODE == AM_CHEB) dg = pre ? spre[(4 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.diag)[n];
+    if (MODE == AM_CHEB) dg = pre ? pre_at(1, slot) : reinterpret_cast<const R2*>(a.diag)[n];
     else if (fixed) dg = reinterpret_cast<const R2*>(a.diag)[n];
     if (fixed) uu = reinterpret_cast<const R2*>(a.u)[n];
-    if (MODE != AM_APPLY) bb = pre ? spre[slot * TX * TZ + tid] : reinterpret_cast<const R2*>(a.bV)[n];
+    if (MODE != AM_APPLY) bb = pre ? pre_at(0, slot) : reinterpret_cast<const R2*>(a.bV)[n];
     if (MODE == AM_CHEB && c1 != 0.0)                // restart steps never read the old direction
-      dd = pre ? spre[(8 + slot) * TX * TZ + tid] : reinterpret_cast<const R2*>(a.d)[n];
+      dd = pre ? pre_at(2, slot) : reinterpret_cast<const R2*>(a.d)[n];
     R2 y;
     y.x = y0;
     y.y = y1;
@@ -466,7 +495,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     }
   };
   // any velocity node of the tile (incident elements found from the node's parity)
-  auto node_generic = [&](int ix, int iz) {
+  auto node_generic = [&](int ix, int iz, int slot) {
     const bool xo = ix & 1, zo = iz & 1;
     const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
     const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = (iz >> 1);
@@ -488,7 +517,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
                  y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
     }
-    emit(ix, iz, y0, y1, -1);
+    emit(ix, iz, y0, y1, slot);
   };
   // any pressure node of the tile
   auto pnode_generic = [&](int px, int pz) {
@@ -548,14 +577,15 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   } else if (lastx || lastz) {
     // right column ix = 2 nx (rows of this tile) and top row iz = 2 nz (columns of this tile,
     // the corner taken by the column)
-    const int j0 = tid - TX * TZ, nj = APPLY_THREADS - TX * TZ;
+    const int j0 = tid - TX * TZ, nj = NJ;
     if (a.yV) {
-      const int oz1 = lastz ? 2 * g.nz + 1 : 2 * (ez0 + TZ);
-      const int ncol = lastx ? oz1 - 2 * ez0 : 0;
-      const int nrow = lastz ? (lastx ? 2 * (g.nx - ex0) : 2 * TX) : 0;
-      for (int j = j0; j < ncol + nrow; j += nj) {
-        if (j < ncol) node_generic(2 * g.nx, 2 * ez0 + j);
-        else node_generic(2 * ex0 + (j - ncol), 2 * g.nz);
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {                // the nodes whose vectors were prefetched
+        const int j = j0 + it * nj;
+        if (j < ncol_v + nrow_v) {
+          if (j < ncol_v) node_generic(2 * g.nx, 2 * ez0 + j, 4 + it);
+          else node_generic(2 * ex0 + (j - ncol_v), 2 * g.nz, 4 + it);
+        }
       }
     }
     if (a.yP) {

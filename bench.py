@@ -295,7 +295,7 @@ def roofline_apply(model, torch):
     achieved = algo / (us * 1e-6) / 1e9
     # DRAM bytes (read + write) of one launch at 512x512 from an ncu capture of this kernel
     # (profiles/k_apply_fp32_fk512.txt); other sizes scale with the element count
-    traffic = int(20168704 * nel / 262144)
+    traffic = int(20162560 * nel / 262144)
     return {"kernel": "mw::k_apply<float, AM_APPLY> (fine level, 512x512)", "bound": "hbm", "achieved": achieved,
             "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "us_per_launch": us,
             "algorithmic_bytes": algo,

@@ -662,8 +662,9 @@ MW_D double rw(int J, int o) {
 // prolongation below); with cheb_c also the coarse level's first Chebyshev step from a zero
 // guess: x_c = d_c = (1/theta_c) D_c^-1 b_c.
 // (no __restrict__: the cluster tail reads values written earlier in the same kernel)
-template <typename R>
-MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, const uint8_t* fixc, R* bc, double c0,
+// fetch(fz, fx, &v0, &v1) reads the residual pair of fine node (fx, fz) (global or shared memory).
+template <typename R, typename Fetch>
+MW_D void restrict_core(const LevelGeo& gf, const LevelGeo& gc, Fetch fetch, const uint8_t* fixc, R* bc, double c0,
                         bool cheb, const R* diag_c, R* xc, R* dc, int64_t n) {
   int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
   // The nonzero taps lie at offsets -3, -1, 0, 1, 3 (the weight at +-2 is zero).  All stencil
@@ -677,9 +678,9 @@ MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, con
       const int fz = 2 * J + OFF[tz], fx = 2 * I + OFF[tx];
       const bool ok = rw(J, OFF[tz]) != 0.0 && rw(I, OFF[tx]) != 0.0 && fz >= 0 && fz < gf.nnz && fx >= 0 &&
                       fx < gf.nnx;
-      const int64_t m = ok ? (int64_t)fz * gf.nnx + fx : 0;
-      v0[tz][tx] = ok ? rf[2 * m] : R(0);
-      v1[tz][tx] = ok ? rf[2 * m + 1] : R(0);
+      v0[tz][tx] = R(0);
+      v1[tz][tx] = R(0);
+      if (ok) fetch(fz, fx, &v0[tz][tx], &v1[tz][tx]);
     }
   double s0 = 0, s1 = 0;
 #pragma unroll
@@ -708,14 +709,61 @@ MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, con
 }
 
 template <typename R>
-__global__ void k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
-                           R* __restrict__ bc, const double* __restrict__ cheb_c, const R* __restrict__ diag_c,
-                           R* __restrict__ xc, R* __restrict__ dc) {
+MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, const uint8_t* fixc, R* bc, double c0,
+                        bool cheb, const R* diag_c, R* xc, R* dc, int64_t n) {
+  auto fetch = [&](int fz, int fx, R* a0, R* a1) {
+    const int64_t m = (int64_t)fz * gf.nnx + fx;
+    *a0 = rf[2 * m];
+    *a1 = rf[2 * m + 1];
+  };
+  restrict_core(gf, gc, fetch, fixc, bc, c0, cheb, diag_c, xc, dc, n);
+}
+
+// The restriction over a tile of RTX x RTZ coarse nodes (one per thread): the fine residual the
+// tile's stencils reach is staged in shared memory with coalesced loads (all issued before the
+// stores), then each node sums its taps from there -- the same terms in the same order as
+// restrict_node.
+constexpr int RTX = 32, RTZ = 8;
+constexpr int RFX = 2 * RTX + 5, RFZ = 2 * RTZ + 5;      // fine offsets -3 .. 2 (RT - 1) + 3
+
+template <typename R>
+__global__ void __launch_bounds__(RTX * RTZ) k_restrict(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf,
+                                                        const uint8_t* __restrict__ fixc, R* __restrict__ bc,
+                                                        const double* __restrict__ cheb_c,
+                                                        const R* __restrict__ diag_c, R* __restrict__ xc,
+                                                        R* __restrict__ dc) {
   pdl_entry();
+  typedef typename Vec2<R>::T R2;
+  __shared__ R2 sr[RFZ * RFX];
   const double c0 = cheb_c ? cheb_c[1] : 0.0;
-  const int64_t nn = (int64_t)gc.nnx * gc.nnz;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x)
-    restrict_node(gf, gc, rf, fixc, bc, c0, cheb_c != nullptr, diag_c, xc, dc, n);
+  const int I0 = blockIdx.x * RTX, J0 = blockIdx.y * RTZ;
+  const int fx0 = 2 * I0 - 3, fz0 = 2 * J0 - 3;
+  const int tid = threadIdx.x;
+  constexpr int NL = (RFZ * RFX + RTX * RTZ - 1) / (RTX * RTZ);
+  const R2* rf2 = reinterpret_cast<const R2*>(rf);
+  R2 v[NL];
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {
+    const int i = tid + k * RTX * RTZ;
+    const int lz = i / RFX, lx = i - lz * RFX;
+    const int fx = fx0 + lx, fz = fz0 + lz;
+    v[k].x = 0; v[k].y = 0;
+    if (i < RFZ * RFX && fx >= 0 && fx < gf.nnx && fz >= 0 && fz < gf.nnz) v[k] = rf2[(int64_t)fz * gf.nnx + fx];
+  }
+#pragma unroll
+  for (int k = 0; k < NL; ++k) {
+    const int i = tid + k * RTX * RTZ;
+    if (i < RFZ * RFX) sr[i] = v[k];
+  }
+  __syncthreads();
+  const int I = I0 + tid % RTX, J = J0 + tid / RTX;
+  if (I >= gc.nnx || J >= gc.nnz) return;
+  auto fetch = [&](int fz, int fx, R* a0, R* a1) {
+    const R2 t = sr[(fz - fz0) * RFX + (fx - fx0)];
+    *a0 = t.x;
+    *a1 = t.y;
+  };
+  restrict_core(gf, gc, fetch, fixc, bc, c0, cheb_c != nullptr, diag_c, xc, dc, (int64_t)J * gc.nnx + I);
 }
 
 // 1D Q2 prolongation: fine node i from coarse nodes
@@ -1688,7 +1736,8 @@ static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = fal
   a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.r; a.bV = L.b;
   launch_apply<R, AM_RESID>(L.g, a, s);
   const bool fuse = !(l + 1 == H.nlev - 1 && H.dense);
-  pdl_launch(k_restrict<R>, grid_for(C.nn, 256), 256, 0, s, L.g, C.g, L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
+  pdl_launch(k_restrict<R>, dim3((C.g.nnx + RTX - 1) / RTX, (C.g.nnz + RTZ - 1) / RTZ), RTX * RTZ, 0, s, L.g, C.g,
+             L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
              C.x, C.d);
   vcycle(H, l + 1, s, fuse);
   pdl_launch(k_prolong_add<R>, grid_for(L.nn, 256), 256, 0, s, L.g, C.g, C.x, L.fix, L.x);

@@ -807,13 +807,53 @@ MW_D void prolong_node(const LevelGeo& gf, const LevelGeo& gc, const R* xc, cons
   if (!fixf[2 * n + 1]) xf[2 * n + 1] += (R)s1;
 }
 
+// The prolongation over a tile of PTX x PTZ fine nodes (one per thread): the coarse values the tile
+// reaches (coarse x from X0/2 to X0/2 + PTX/2, z likewise) are staged in shared memory, then each
+// node sums its taps from there in the order of prolong_node and updates its (u, w) pair with one
+// vector load and store.
+constexpr int PTX = 32, PTZ = 8;
+constexpr int PCX = PTX / 2 + 1, PCZ = PTZ / 2 + 1;
+
 template <typename R>
-__global__ void k_prolong_add(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc, const uint8_t* __restrict__ fixf,
-                              R* __restrict__ xf) {
+__global__ void __launch_bounds__(PTX * PTZ) k_prolong_add(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc,
+                                                           const uint8_t* __restrict__ fixf, R* __restrict__ xf) {
   pdl_entry();
-  const int64_t nn = (int64_t)gf.nnx * gf.nnz;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x)
-    prolong_node(gf, gc, xc, fixf, xf, n);
+  typedef typename Vec2<R>::T R2;
+  __shared__ R2 sc2[PCZ * PCX];
+  const int X0 = blockIdx.x * PTX, Z0 = blockIdx.y * PTZ;
+  const int cx0 = X0 / 2, cz0 = Z0 / 2;
+  const int tid = threadIdx.x;
+  if (tid < PCZ * PCX) {
+    const int jz = tid / PCX, jx = tid - jz * PCX;
+    const int cx = cx0 + jx, cz = cz0 + jz;
+    R2 v;
+    v.x = 0; v.y = 0;
+    if (cx < gc.nnx && cz < gc.nnz) v = reinterpret_cast<const R2*>(xc)[(int64_t)cz * gc.nnx + cx];
+    sc2[tid] = v;
+  }
+  __syncthreads();
+  const int ix = X0 + tid % PTX, iz = Z0 + tid / PTX;
+  if (ix >= gf.nnx || iz >= gf.nnz) return;
+  const int64_t n = (int64_t)iz * gf.nnx + ix;
+  const uchar2 ff = reinterpret_cast<const uchar2*>(fixf)[n];
+  R2 x = reinterpret_cast<const R2*>(xf)[n];
+  int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
+  double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
+  const int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
+  double s0 = 0, s1 = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      if (a < nzw && b < nxw) {
+        const R2 v = sc2[(Jz[a] - cz0) * PCX + (Jx[b] - cx0)];
+        double w = wz[a] * wx[b];
+        s0 += w * (double)v.x;
+        s1 += w * (double)v.y;
+      }
+  if (!ff.x) x.x += (R)s0;
+  if (!ff.y) x.y += (R)s1;
+  reinterpret_cast<R2*>(xf)[n] = x;
 }
 
 template <typename R>
@@ -1740,7 +1780,8 @@ static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = fal
              L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
              C.x, C.d);
   vcycle(H, l + 1, s, fuse);
-  pdl_launch(k_prolong_add<R>, grid_for(L.nn, 256), 256, 0, s, L.g, C.g, C.x, L.fix, L.x);
+  pdl_launch(k_prolong_add<R>, dim3((L.g.nnx + PTX - 1) / PTX, (L.g.nnz + PTZ - 1) / PTZ), PTX * PTZ, 0, s, L.g, C.g,
+             C.x, L.fix, L.x);
   smooth(L, L.deg, false, s);
 }
 

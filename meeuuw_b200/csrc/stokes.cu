@@ -1187,17 +1187,12 @@ __global__ void k_mass_cheb(LevelGeo g, const double* __restrict__ w, const doub
   }
 }
 
-// Deterministic single-launch dot product: block partials, then the last block to finish sums
-// them in block order (threadfence + arrival counter, reset for the next call).
-template <typename R>
-__global__ void k_dot1(int64_t n, const R* __restrict__ x, const R* __restrict__ y, double* __restrict__ part,
-                       unsigned* __restrict__ counter, double* __restrict__ out) {
-  pdl_entry();
+// The grid-wide sum of one value per thread, finished in the same launch: block partials in
+// part[block], the last block to arrive adds them in block order into *out and resets the counter
+// (threadfence + arrival counter).  Called once, by every thread, at the end of a kernel.
+MW_D void grid_sum_last(double v, double* part, unsigned* counter, double* out) {
   __shared__ double sh[32];
   __shared__ bool last;
-  double v = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v += (double)x[i] * (double)y[i];
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (lane == 0) sh[wid] = v;
@@ -1227,17 +1222,37 @@ __global__ void k_dot1(int64_t n, const R* __restrict__ x, const R* __restrict__
   }
 }
 
-// x += (num/den) p ; r -= (num/den) Ap   (one launch for both PCG updates)
+// Deterministic single-launch dot product: block partials, then the last block to finish sums
+// them in block order (threadfence + arrival counter, reset for the next call).
 template <typename R>
-__global__ void k_pcg_update(int64_t n, const double* __restrict__ num, const double* __restrict__ den,
-                             const R* __restrict__ p, const R* __restrict__ Ap, R* __restrict__ x, R* __restrict__ r) {
+__global__ void k_dot1(int64_t n, const R* __restrict__ x, const R* __restrict__ y, double* __restrict__ part,
+                       unsigned* __restrict__ counter, double* __restrict__ out) {
+  pdl_entry();
+  double v = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v += (double)x[i] * (double)y[i];
+  grid_sum_last(v, part, counter, out);
+}
+
+// x += (num/den) p ; r -= (num/den) Ap, and (r, r) of the new residual into *rr, summed exactly as
+// k_dot1 sums it on the same grid (one launch for the CG step and its convergence norm)
+template <typename R>
+__global__ void k_pcg_update_rr(int64_t n, const double* __restrict__ num, const double* __restrict__ den,
+                                const R* __restrict__ p, const R* __restrict__ Ap, R* __restrict__ x,
+                                R* __restrict__ r, double* __restrict__ part, unsigned* __restrict__ counter,
+                                double* __restrict__ rr) {
   pdl_entry();
   const double a = *num / *den;
+  double v = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] = (R)((double)x[i] + a * (double)p[i]);
-    r[i] = (R)((double)r[i] - a * (double)Ap[i]);
+    const R ri = (R)((double)r[i] - a * (double)Ap[i]);
+    r[i] = ri;
+    v += (double)ri * (double)ri;
   }
+  grid_sum_last(v, part, counter, rr);
 }
+
 
 // element weights 1/eta_e for M_eta (eta_e = mean of the qpoint viscosities of the element)
 __global__ void k_inv_eta_e(int64_t nel, const double* __restrict__ etaq, const double* __restrict__ eta_e,
@@ -2008,8 +2023,7 @@ static int pcg_K(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, double*
   for (it = 1; it <= maxit; ++it) {
     k_only_apply<R>(L, p, Ap, s);
     dot<R>(S, n, p, Ap, sc + 1, s);
-    pdl_launch(k_pcg_update<R>, grid_for(n, 256), 256, 0, s, n, sc + 0, sc + 1, p, Ap, xr, r);
-    dot<R>(S, n, r, r, sc + 2, s);
+    pdl_launch(k_pcg_update_rr<R>, nb_for(n), 256, 0, s, n, sc + 0, sc + 1, p, Ap, xr, r, S->red, S->counter, sc + 2);
     rr = read_scalar(sc + 2, s);
     if (!std::isfinite(rr)) break;
     if (rr <= rtol * rtol * bb) break;
@@ -2367,8 +2381,8 @@ static bool pcg_K_dev(mw_stokes* S, Hierarchy<R>& H, R** pc, const double* b, do
   // body: one CG step and the convergence test, then (if continuing) the next search direction
   k_only_apply<R>(L, p, Ap, b1);
   dot<R>(S, n, p, Ap, sc + P_PAP, b1);
-  pdl_launch(k_pcg_update<R>, grid_for(n, 256), 256, 0, b1, n, sc + P_RZ, sc + P_PAP, p, Ap, xr, r);
-  dot<R>(S, n, r, r, sc + P_RR, b1);
+  pdl_launch(k_pcg_update_rr<R>, nb_for(n), 256, 0, b1, n, sc + P_RZ, sc + P_PAP, p, Ap, xr, r, S->red, S->counter,
+             sc + P_RR);
   if (!cond_handle(b1, &hi)) return false;
   pdl_launch(k_dev_pcg_check, 1, 1, 0, b1, sc, rtol, maxit, hw, hi);
   if (!cond_node(b1, b2, cudaGraphCondTypeIf, hi)) return false;

@@ -12,7 +12,7 @@ and contrast log-uniform, random smooth initial temperatures), in the units of
 ``mw_unet_features`` / ``mw_unet_targets``: velocity / (Ra / geometric-mean viscosity) and the
 dynamic pressure / Ra, each normalised by its RMS over the grid, plus the two log10 RMS scales as
 extra output channels.  At run time ``LearnedGuess`` proposes guesses and the solver starts from
-whichever has the smallest FP64 Stokes residual, the previous step's solution included.
+whichever has the smallest Uzawa residual, the previous step's solution included.
 """
 import ctypes
 import math

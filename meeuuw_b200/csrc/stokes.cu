@@ -122,7 +122,9 @@ constexpr int LX = 2 * TX + 3, LZ = 2 * TZ + 3;// staged lattice nodes (35 x 19)
 constexpr int PX = TX + 2, PZ = TZ + 2;        // staged pressure nodes (18 x 10)
 constexpr int APPLY_THREADS = 160;
 
-enum ApplyMode { AM_APPLY = 0, AM_RESID = 1, AM_CHEB = 2 };
+// AM_CHEB_Z: the second Chebyshev step of a sweep from a zero guess with the first one folded in:
+// the velocity staged is x0 = (1/theta) D^-1 b (the first step's x and d), computed on the fly
+enum ApplyMode { AM_APPLY = 0, AM_RESID = 1, AM_CHEB = 2, AM_CHEB_Z = 3 };
 
 template <typename R> struct Vec2;
 template <> struct Vec2<float> { typedef float2 T; };
@@ -143,6 +145,7 @@ struct ApplyArgs {
   R* d;
   R* xo;
   const double* cheb; // device coefficients {c1, c2}
+  const double* cheb0;// AM_CHEB_Z: the first step's pair {0, 1/theta}
 };
 
 // Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points: strain rate B u
@@ -273,7 +276,8 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   // node vectors the epilogue reads for the four nodes each owned element emits (b; b, diag, d),
   // fetched asynchronously while the element products run (FP32; the FP64 kernel's shared memory
   // is already at the 48 KB static limit)
-  constexpr int NPRE = sizeof(R) == 8 ? 0 : (MODE == AM_CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
+  constexpr bool CHEB = MODE == AM_CHEB || MODE == AM_CHEB_Z;
+  constexpr int NPRE = sizeof(R) == 8 ? 0 : (CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
   __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ __align__(16) R2 spre[(NPRE ? NPRE : 1) * 4 * TX * TZ];
   constexpr int NJ = APPLY_THREADS - TX * TZ;         // spare threads: right column and top row nodes
@@ -287,8 +291,9 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   const int tid = threadIdx.x;
   const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
   // Chebyshev coefficients, read now so that no epilogue load waits on them
-  const double c1 = MODE == AM_CHEB ? a.cheb[0] : 0.0;
-  const R c2 = MODE == AM_CHEB ? R(a.cheb[1]) : R(0);
+  const double c1 = CHEB ? a.cheb[0] : 0.0;
+  const R c2 = CHEB ? R(a.cheb[1]) : R(0);
+  const R cz = MODE == AM_CHEB_Z ? R(a.cheb0[1]) : R(0);
   // ---- prefetch: the epilogue's node vectors (owned elements), the element viscosities ----
   // slot j of an owned element: 0 centre (2ex+1, 2ez+1), 1 bottom midpoint (2ex+1, 2ez),
   // 2 left midpoint (2ex, 2ez+1), 3 corner (2ex, 2ez)
@@ -302,7 +307,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         cp_async_pair<R>(&spre[j * TX * TZ + tid], a.bV + 2 * n);
         if (NPRE == 3) {
           cp_async_pair<R>(&spre[(4 + j) * TX * TZ + tid], a.diag + 2 * n);
-          cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
+          if (MODE != AM_CHEB_Z) cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
         }
       }
     }
@@ -324,7 +329,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         cp_async_pair<R>(&sspare[it * NJ + q], a.bV + 2 * n);
         if (NPRE == 3) {
           cp_async_pair<R>(&sspare[(2 + it) * NJ + q], a.diag + 2 * n);
-          cp_async_pair<R>(&sspare[(4 + it) * NJ + q], a.d + 2 * n);
+          if (MODE != AM_CHEB_Z) cp_async_pair<R>(&sspare[(4 + it) * NJ + q], a.d + 2 * n);
         }
       }
     }
@@ -386,7 +391,13 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     if (i < LZ * LX && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
       const int64_t n = (int64_t)iz * g.nnx + ix;
       sf[k] = f2[n];
-      if (use_u) sv[k] = u2[n];
+      if (MODE == AM_CHEB_Z) {                       // x0 = (1/theta) D^-1 b
+        const R2 bb = reinterpret_cast<const R2*>(a.bV)[n], dg = reinterpret_cast<const R2*>(a.diag)[n];
+        sv[k].x = cz * bb.x / dg.x;
+        sv[k].y = cz * bb.y / dg.y;
+      } else if (use_u) {
+        sv[k] = u2[n];
+      }
     }
   }
 #pragma unroll
@@ -466,12 +477,17 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     // every load first, none depending on another
     R2 uu = su2[li];                                 // the staged velocity: exact on free dofs
     R2 dg{R(0), R(0)}, bb{R(0), R(0)}, dd{R(0), R(0)};
-    if (MODE == AM_CHEB) dg = pre ? pre_at(1, slot) : reinterpret_cast<const R2*>(a.diag)[n];
+    if (CHEB) dg = pre ? pre_at(1, slot) : reinterpret_cast<const R2*>(a.diag)[n];
     else if (fixed) dg = reinterpret_cast<const R2*>(a.diag)[n];
-    if (fixed) uu = reinterpret_cast<const R2*>(a.u)[n];
+    if (fixed && MODE != AM_CHEB_Z) uu = reinterpret_cast<const R2*>(a.u)[n];
     if (MODE != AM_APPLY) bb = pre ? pre_at(0, slot) : reinterpret_cast<const R2*>(a.bV)[n];
     if (MODE == AM_CHEB && c1 != 0.0)                // restart steps never read the old direction
       dd = pre ? pre_at(2, slot) : reinterpret_cast<const R2*>(a.d)[n];
+    if (MODE == AM_CHEB_Z) {                         // the first step's x and d, both x0
+      const R2 x0{cz * bb.x / dg.x, cz * bb.y / dg.y};
+      if (fixed) uu = x0;
+      dd = x0;
+    }
     R2 y;
     y.x = y0;
     y.y = y1;
@@ -1713,6 +1729,22 @@ static void smooth(Level<R>& L, int degree, bool zero_start, cudaStream_t s, boo
   if (first_done) {
     // x = d = (1/theta) D^-1 b was written by the restriction kernel
   } else if (zero_start) {
+    if constexpr (sizeof(R) == 4) if (degree >= 2) {  // steps 0 and 1 in one launch (FP32)
+      ApplyArgs<R> a = args0<R>();
+      a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
+      a.cheb = L.cheb + 2;
+      a.cheb0 = L.cheb;
+      launch_apply<R, AM_CHEB_Z>(L.g, a, s);
+      std::swap(L.x, L.t);
+      for (int k = 2; k < degree; ++k) {
+        ApplyArgs<R> b = args0<R>();
+        b.u = L.x; b.eta = L.eta; b.fix = L.fix; b.diag = L.diag; b.yV = L.d; b.bV = L.b; b.d = L.d; b.xo = L.t;
+        b.cheb = L.cheb + 2 * k;
+        launch_apply<R, AM_CHEB>(L.g, b, s);
+        std::swap(L.x, L.t);
+      }
+      return;
+    }
     pdl_launch(k_cheb_first<R>, grid_for(n, 256), 256, 0, s, n, L.cheb, L.b, L.diag, L.x, L.d);
   } else {
     // restart the recurrence from the current x: d = (1/theta) D^-1 r; x += d

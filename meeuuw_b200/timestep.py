@@ -82,10 +82,13 @@ class GPUModel:
         self.gq_out = Z(3)
         self.material = ops.material_struct(cfg)
         precs = ("f64",) if stokes == "f64" else ("f32",)
-        # Smoothing degree per arithmetic: an FP64 V-cycle is apply-bound, so one Chebyshev step per
-        # sweep with more PCG iterations is faster; in FP32 two steps per sweep pay for themselves.
+        # Smoothing per arithmetic: an FP64 V-cycle is apply-bound, so one Chebyshev step per sweep
+        # with more PCG iterations is faster; in FP32 two steps per sweep pay for themselves, and six
+        # warm-started power iterations per viscosity update (three in FP64) give the Chebyshev
+        # intervals that make the mixed solve fastest (measured on the 512x512 FK step).
         self.solver = StokesSolver(box, self.bc_fix_V, eta_ref=cfg.eta_ref, L_ref=self.L_ref, precisions=precs,
-                                   cheb_degree=1 if stokes == "f64" else 2)
+                                   cheb_degree=1 if stokes == "f64" else 2,
+                                   power_iters_warm=3 if stokes == "f64" else 6)
         self.last_solve = {}
         self.istep = 0
         self.guess = None      # optional callable(model) -> (solV, solP) used as the Stokes initial guess

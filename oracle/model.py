@@ -10,6 +10,8 @@ nodal pressure (``:2051``), time step (``:2112-2139``), energy assembly and solv
 (``:2186-2235``), heat flux and Nu (``:2259-2308``), nodal strain rate
 (``:2385``), vrms (``:2512``), advection (``:2726``) and locate (``:2862``).
 """
+import time
+
 import numpy as np
 
 from . import assembly, pic, post, solvers
@@ -41,6 +43,10 @@ class OracleModel:
         self.dt1_mem = 1e50
         self.dt2_mem = 1e50
         self.istep = 0
+        # solver options (defaults: the reference's): keyword arguments of solvers.cd_u_eta /
+        # solvers.uzawa3_solver_L2 and of solvers.energy_solve
+        self.stokes_kw = {}
+        self.energy_kw = {}
         gx, gz = cfg.gxz
         self.gxq = np.full((m.nel, 9), float(gx))
         self.gzq = np.full((m.nel, 9), float(gz))
@@ -66,12 +72,21 @@ class OracleModel:
         c, m = self.cfg, self.mesh
         n = len(self.x)
         out = {}
+        # wall time of each phase of the step (s), in the order they run
+        self.phase_seconds = times = {}
+        clock = [time.perf_counter()]
+
+        def mark(phase):
+            t = time.perf_counter()
+            times[phase] = times.get(phase, 0.0) + t - clock[0]
+            clock[0] = t
         ip = lambda phi: pic.interpolate_field_on_particles(n, self.active, self.r, self.t, self.iel, phi, m.icon_V)
         s_exx, s_ezz, s_exz, s_p = ip(self.exx_n), ip(self.ezz_n), ip(self.exz_n), ip(self.q)
         s_T = ip(self.T) if c.solve_T else np.zeros(n)
         out.update(swarm_exx=s_exx, swarm_ezz=s_ezz, swarm_exz=s_exz, swarm_p=s_p, swarm_T=s_T)
         rho, eta, hcond, hcapa, hprod, alpha = self.material(s_T)
         out.update(swarm_rho=rho, swarm_eta=eta)
+        mark("interpolation+material")
         rho_e, eta_e, cnt = pic.project_particles_on_elements(m.nel, n, self.active, rho, eta, self.iel, c.averaging)
         if cnt.min() == 0:
             raise SystemExit("ABORT: an element contains no particle!")   # meeuuw.py:1198-1199
@@ -102,6 +117,7 @@ class OracleModel:
         ezzq = post.project_nodal_field_onto_qpoints(self.ezz_n, m.N_V, m.icon_V)
         exzq = post.project_nodal_field_onto_qpoints(self.exz_n, m.N_V, m.icon_V)
         out.update(rhoq=rhoq, etaq=etaq, Tq=Tq)
+        mark("projections")
         # Stokes
         blocks = solver in ("cd_u_eta", "uzawa3")
         res = assembly.build_matrix_stokes(
@@ -112,6 +128,7 @@ class OracleModel:
             False, m.xq, blocks)
         VV_Stokes, rhs_f, rhs_h = res[0], res[1], res[2]
         out.update(rhs_f=rhs_f, rhs_h=rhs_h)
+        mark("stokes assembly")
         A = solvers.stokes_full(m, VV_Stokes if not blocks else self._full_from_blocks(res))
         if solver == "direct":
             sol = solvers.direct_solve(A, rhs_f, rhs_h)
@@ -119,9 +136,11 @@ class OracleModel:
         else:
             K, G, GT, M, Me, H = solvers.stokes_blocks(m, *res[3:])
             if solver == "cd_u_eta":
-                solV, solP, nit = solvers.cd_u_eta(K, G, GT, M, Me, H, rhs_f, rhs_h, m.Nfem_P)[:3]
+                solV, solP, nit = solvers.cd_u_eta(K, G, GT, M, Me, H, rhs_f, rhs_h, m.Nfem_P,
+                                                   **self.stokes_kw)[:3]
             else:
                 solV, solP, nit = solvers.uzawa3_solver_L2(K, G, GT, M, H, rhs_f, rhs_h, m.Nfem_P)[:3]
+        mark("stokes solve")
         out["stokes_residual"] = solvers.stokes_relative_residual(A, np.concatenate([solV, solP]), rhs_f, rhs_h)
         out["stokes_iterations"] = nit
         out["solV"], out["solP"] = solV.copy(), solP.copy()
@@ -138,6 +157,7 @@ class OracleModel:
         uq = post.project_nodal_field_onto_qpoints(u, m.N_V, m.icon_V)
         wq = post.project_nodal_field_onto_qpoints(w, m.N_V, m.icon_V)
         out.update(u=u, w=w, p=p, q=self.q.copy(), dt=dt, pressure_offset=offset)
+        mark("pressure, dt")
         Nu = np.nan
         if c.solve_T:
             z9 = np.zeros((m.nel, 9))
@@ -145,7 +165,9 @@ class OracleModel:
                 0, m.nel, 9, 9, m.nn_V, T_mem, m.icon_V, rhoq, etaq, Tq, uq, wq, hcondq, hcapaq, alphaq,
                 hprodq, exxq, ezzq, exzq, z9, z9, m.JxWq, m.N_V, m.dNdr_V, m.dNdt_V, m.jcbi00q,
                 m.jcbi01q, m.jcbi10q, m.jcbi11q, self.bc_fix_T, self.bc_val_T, dt, c.formulation, c.rho0)
-            self.T = solvers.energy_solve(m, VV_T, rhs_T)
+            mark("energy assembly")
+            self.T = solvers.energy_solve(m, VV_T, rhs_T, **self.energy_kw)
+            mark("energy solve")
             dTdx, dTdz, qx, qz = post.compute_nodal_heat_flux(
                 m.icon_V, self.T, hcond_n, m.nn_V, m.dNdr_V_n, m.dNdt_V_n, m.jcbi00n, m.jcbi01n,
                 m.jcbi10n, m.jcbi11n)
@@ -158,12 +180,14 @@ class OracleModel:
         Tq_new = Tq
         vrms, Tavrg, _ = post.compute_global_quantities(uq, wq, Tq_new, rhoq, m.JxWq, m.volume)
         out.update(vrms=vrms, Nu=Nu, exx_n=self.exx_n.copy())
+        mark("heat flux, Nu, strain rate, vrms")
         pic.advect_particles___box(c.RKorder, dt, n, self.x, self.z, self.active, u, w, m.Lx, m.Lz,
                                    m.hx, m.hz, m.nelx, m.icon_V, m.x_V, m.z_V)
         self.r, self.t, self.iel = pic.locate_particles___box(
             n, self.active, self.x, self.z, m.hx, m.hz, m.x_V, m.z_V, m.icon_V, m.nelx)
         if not pic.locate_bounds_ok(self.r, self.t):
             raise SystemExit("r value out of bounds")
+        mark("advection+locate")
         out.update(swarm_x=self.x.copy(), swarm_z=self.z.copy(), swarm_iel=self.iel.copy())
         self.istep += 1
         return out

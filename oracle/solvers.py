@@ -74,14 +74,23 @@ def uzawa3_solver_L2(K_mat, G_mat, GT_mat, MP_mat, H_mat, f_rhs, h_rhs, Nfem_P, 
     return solV, solP, k + 1, xiV, xiP, alphas
 
 
-def cd_u_eta(K, G, GT, M, M_eta, H, f, h, Nfem_P, tol=1e-6, niter=100):
-    """cd_u_eta.py:13-99 with innerK = innerM = 'splu'."""
+def _splu_spd(K, permc_spec):
+    """SuperLU of the symmetric positive definite K with a symmetric fill-reducing ordering:
+    the same factorisation up to round-off as ``splu(K)``, with far less fill on large meshes."""
+    if permc_spec is None:
+        return sla.splu(K)
+    return sla.splu(K, permc_spec=permc_spec, diag_pivot_thresh=0.0, options=dict(SymmetricMode=True))
+
+
+def cd_u_eta(K, G, GT, M, M_eta, H, f, h, Nfem_P, tol=1e-6, niter=100, permc_spec=None):
+    """cd_u_eta.py:13-99 with innerK = innerM = 'splu'.  ``permc_spec`` (e.g. "MMD_AT_PLUS_A")
+    only reorders K's factorisation (SuperLU's default COLAMD runs out of memory at 512x512)."""
     xiV = np.zeros(niter)
     xiP = np.zeros(niter)
     alphas = np.zeros(niter)
     betas = np.zeros(niter)
     solP = np.zeros(Nfem_P)
-    LU_K = sla.splu(K)
+    LU_K = _splu_spd(K, permc_spec)
     solV = LU_K.solve(f)                                               # (B)
     LU_M = sla.splu(M)
     LU_Me = sla.splu(M_eta)
@@ -108,11 +117,13 @@ def cd_u_eta(K, G, GT, M, M_eta, H, f, h, Nfem_P, tol=1e-6, niter=100):
     return solV, solP, k + 1, xiV, xiP, alphas, betas
 
 
-def energy_solve(mesh, VV_T, rhs):
-    """meeuuw.py:2232-2235."""
+def energy_solve(mesh, VV_T, rhs, permc_spec=None):
+    """meeuuw.py:2232-2235 (``permc_spec`` only reorders the factorisation)."""
     II, JJ = mesh.coo_T()
     A = sps.coo_matrix((VV_T, (II, JJ)), shape=(mesh.nn_V, mesh.nn_V)).tocsr()
-    return sla.spsolve(A, rhs)
+    if permc_spec is None:
+        return sla.spsolve(A, rhs)
+    return sla.spsolve(A, rhs, permc_spec=permc_spec)
 
 
 def stokes_relative_residual(A, sol, rhs_f, rhs_h):

@@ -228,10 +228,16 @@ int mw_compute_nu(mw_box box, const double* T, const double* dTdx_n, const doubl
  * fixed file-scope device array sized for at most MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS boundary
  * elements, 2*(nelx+nelz) (2.25 MiB, held by every GPU that loads the library until exit);
  * larger meshes return MW_ERR_TOO_LARGE.  The call makes no cudaMalloc/cudaFree and calls no
- * allocating routine.  The first call on a device looks up the array's device address (set-up)
- * and should therefore come before any stream capture.  All calls share the one array: calls
- * that overlap on the GPU (different streams, same device) race and must be serialised by the
- * caller.  Output: the same 13 values as mw_compute_nu. */
+ * allocating routine.  The first call in a CUDA context does the set-up: it looks up the array's
+ * device address (cudaGetSymbolAddress) and, under CUDA's lazy module loading, that lookup loads
+ * the library's post-processing module together with the 2.25 MiB array -- so device free memory
+ * drops once, at that first call, unless another post-processing entry point ran first.  Make the
+ * first call before the simulation's memory state must stay fixed and before any stream capture.
+ * The address is cached per context (by its unique id), so a cudaDeviceReset or a different
+ * context repeats the set-up.  All calls share the one array and each call writes every slot it
+ * reads, so nothing needs clearing between calls; calls that overlap on the GPU (different
+ * streams, same device) race and must be serialised by the caller.  Output: the same 13 values as
+ * mw_compute_nu. */
 #define MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS 32768
 int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, const double* dTdz_n,
                           const double* hcond_n, mw_gauss3 g, double* out13, void* stream);

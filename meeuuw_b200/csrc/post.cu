@@ -7,8 +7,12 @@
 // Node fields that the reference accumulates element by element are computed node-centrically:
 // each node sums its (up to 4) incident elements in ascending element order, then divides by the
 // count -- the reference's order, without atomics.  Global sums use a fixed two-level tree
-// (deterministic, not the reference's sequential order); the short boundary sums of the surface
-// pressure offset and of Nu are summed sequentially in the reference's element order.
+// (deterministic, not the reference's sequential order).  The surface pressure offset's boundary
+// sum runs sequentially in the reference's element order; the four boundary sums of Nu use one
+// warp per side, lane-strided partial sums then a fixed warp-shuffle tree (deterministic, but not
+// the reference's sequential order: values agree to round-off).
+#include <cuda.h>
+
 #include <mutex>
 
 #include "common.cuh"
@@ -193,7 +197,7 @@ __global__ void k_nodal_grad(mw_box b, int mode, const double* __restrict__ u, c
 }
 
 // compute_Nu (postprocessors.py:114-248): per boundary element and Gauss point terms in parallel,
-// then the four sides summed sequentially in element order by four threads.
+// then each side summed by one warp (lane-strided partials, fixed warp-shuffle tree).
 __global__ void k_nu_terms(mw_box b, const double* __restrict__ T, const double* __restrict__ dTdx,
                            const double* __restrict__ dTdz, const double* __restrict__ hc, mw_gauss3 g,
                            double* __restrict__ terms) {
@@ -514,21 +518,57 @@ int mw_compute_nu(mw_box box, const double* T, const double* dTdx_n, const doubl
   return MW_OK;
 }
 
-// Device address of g_nu_scratch, looked up once per device (host code cannot use the symbol
-// itself as a device pointer).
-static double* nu_scratch_for_current_device(int* status) {
+// Device address of g_nu_scratch for the calling thread's current context (host code cannot use the
+// symbol itself as a device pointer).  The address belongs to the context the module was loaded
+// into, so it is cached per context, keyed by the context's process-unique id (cuCtxGetId): after a
+// cudaDeviceReset, or under another context on the same device, the address is looked up again.
+// The two driver calls are resolved through the runtime (no link-time dependency on libcuda).
+typedef CUresult (*PFN_ctx_get_current)(CUcontext*);
+typedef CUresult (*PFN_ctx_get_id)(CUcontext, unsigned long long*);
+
+static void* driver_fn(const char* name) {
+  cudaDriverEntryPointQueryResult q;
+  void* p = nullptr;
+  if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+    return nullptr;
+  return p;
+}
+
+static double* nu_scratch_for_current_context(int* status) {
   static std::mutex mtx;
-  static double* addr[64] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { *status = MW_ERR_CUDA; return nullptr; }
+  struct Entry { unsigned long long id; double* addr; };
+  static Entry cache[64] = {};
+  static int used = 0, next = 0;
+  static PFN_ctx_get_current ctx_get_current = nullptr;
+  static PFN_ctx_get_id ctx_get_id = nullptr;
+  *status = MW_ERR_CUDA;
   std::lock_guard<std::mutex> lock(mtx);
-  if (!addr[dev]) {
-    double* p = nullptr;
-    if (cudaGetSymbolAddress((void**)&p, g_nu_scratch) != cudaSuccess || !p) { *status = MW_ERR_CUDA; return nullptr; }
-    addr[dev] = p;
+  if (!ctx_get_current || !ctx_get_id) {
+    ctx_get_current = (PFN_ctx_get_current)driver_fn("cuCtxGetCurrent");
+    ctx_get_id = (PFN_ctx_get_id)driver_fn("cuCtxGetId");
+    if (!ctx_get_current || !ctx_get_id) return nullptr;
   }
+  CUcontext ctx = nullptr;
+  CUresult cr = ctx_get_current(&ctx);
+  if (cr != CUDA_SUCCESS && cr != CUDA_ERROR_NOT_INITIALIZED) return nullptr;
+  unsigned long long id = 0;
+  if (ctx) {
+    if (ctx_get_id(ctx, &id) != CUDA_SUCCESS) return nullptr;
+    for (int i = 0; i < used; ++i)
+      if (cache[i].id == id) { *status = MW_OK; return cache[i].addr; }
+  }
+  // set-up: the runtime makes the current device's primary context current if none is, and loads
+  // this file's module (with g_nu_scratch) if it is not loaded yet
+  double* p = nullptr;
+  if (cudaGetSymbolAddress((void**)&p, g_nu_scratch) != cudaSuccess || !p) return nullptr;
+  if (!ctx) {
+    if (ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx || ctx_get_id(ctx, &id) != CUDA_SUCCESS) return nullptr;
+  }
+  cache[next] = Entry{id, p};
+  next = (next + 1) % 64;
+  if (used < 64) ++used;
   *status = MW_OK;
-  return addr[dev];
+  return p;
 }
 
 int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, const double* dTdz_n,
@@ -537,7 +577,7 @@ int mw_compute_nu_noalloc(mw_box box, const double* T, const double* dTdx_n, con
   const int64_t nbound = 2LL * box.nelx + 2LL * box.nelz;
   if (nbound > MW_NU_NOALLOC_MAX_BOUNDARY_ELEMENTS) return MW_ERR_TOO_LARGE;
   int st = MW_OK;
-  double* scratch = nu_scratch_for_current_device(&st);
+  double* scratch = nu_scratch_for_current_context(&st);
   if (st != MW_OK) return st;
   // every scratch slot the final sum reads is written by k_nu_terms first: nothing to clear
   cudaStream_t s = (cudaStream_t)stream;

@@ -10,8 +10,9 @@ inner solves, FP64 refinement) warm-started from the previous step; the plain FP
 measured beside it.  With N > 1 each rank advances its own independent model (replicas: a
 single model does not shard), so `value` is the sum over ranks of timesteps/s ("weak").
 
-`--impl reference` times the CPU oracle (a restatement of the reference's Numba/SciPy path) on a
-bounded sample and extrapolates to the same workload.
+`--impl reference` times the CPU oracle (a restatement of the reference's Numba/SciPy path, pinned
+to the reference's own functions and driver) on a bounded sample: one full timestep of the same
+model at 256x256 (and 128x128), measured, reported at 512x512 scaled by the element count.
 """
 import argparse
 import json
@@ -193,6 +194,7 @@ def run_ours(args):
 
     # ---- roofline of the dominant kernel: fine-level operator apply (FP32), CUDA events ----
     roof = roofline_apply(model, torch)
+    kroof = kernel_rooflines(model, torch, roof["peak"])
 
     # ---- plain FP64 path (same problem, same warm start) ----
     plain = None
@@ -219,6 +221,11 @@ def run_ours(args):
                     "Nu_rel_diff": abs(da["Nu"] - db["Nu"]) / abs(db["Nu"]),
                     "T_max_abs_diff": float((ma.T - mb.T).abs().max().item())}
         del ma, mb
+
+    # ---- both arms' first step against the FP64 oracle's first step (512x512, stored) ----
+    vs_oracle = None
+    if rank == 0 and not args.no_plain:
+        vs_oracle = step1_vs_oracle(torch, wpath if learned else None)
 
     # ---- end to end through host buffers ----
     e2e = None
@@ -249,17 +256,132 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (swarm state ~0.5 GB, fields ~0.2 GB)"},
             "clocks": clk.summary(), "gpu_launches": launches, "kernel_mix_per_step": kernel_mix,
-            "roofline": roof, "e2e": e2e, "plain_fp64": plain,
+            "roofline": roof, "kernel_rooflines": kroof, "e2e": e2e, "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
             "last_step": {"vrms": diag["vrms"], "Nu": diag["Nu"], "dt": diag["dt"], "stokes": diag["stokes"],
                           "energy_iters_relres": list(getattr(model, "energy_info", (None, None)))},
             "phases_ms_per_step": phase_ms,
             "mixed_vs_fp64": accuracy,
+            "step1_vs_fp64_oracle": vs_oracle,
             "warm_start_picks": dict(learned.picks) if learned else None,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     replicas.finalize()
+
+
+def kernel_rooflines(model, torch, peak_gbs):
+    """The particle kernels and the FP32 Stokes assembly on the bench's model, each timed alone with
+    CUDA events on its stream (mean of `reps` launches after a warm-up), against HBM: algorithmic
+    bytes per launch / duration.  Algorithmic bytes count each per-particle or per-element array once
+    and each nodal array the kernel gathers from once.  The particle kernels run in FP64 (the
+    reference's arithmetic), so their FP64 issue rate, not HBM, is what bounds them; the FP32
+    assembly also reports FLOP/s against the FP32 non-tensor peak (148 SMs x 128 lanes x 2 x the
+    maximum SM clock)."""
+    from meeuuw_b200 import ops
+    m, b = model, model.box
+    n, nel, nn, npp = m.npart, m.nel, m.nn, m.np_
+    nact = int(m.active.sum().item())
+    P = m.props
+    reps = 10
+
+    def timed(fn, prep=None):
+        for _ in range(2):
+            if prep:
+                prep()
+            fn()
+        tot = 0.0
+        for _ in range(reps):
+            if prep:
+                prep()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            fn()
+            e.record()
+            torch.cuda.synchronize()
+            tot += s.elapsed_time(e)
+        return tot * 1000.0 / reps
+
+    out = {}
+
+    def add(name, us, algo, **kw):
+        gbs = algo / (us * 1e-6) / 1e9
+        out[name] = dict(us_per_launch=us, algorithmic_bytes=int(algo), achieved_gbs=gbs, frac_hbm=gbs / peak_gbs, **kw)
+
+    r, t, iel = torch.empty_like(m.r), torch.empty_like(m.t), torch.empty_like(m.iel)
+    add("k_locate", timed(lambda: ops.locate(b, m.active, m.x, m.z, r, t, iel, m.err)), 37 * nact + (n - nact) * 13)
+    nodal = dict(exx=m.exx_n, ezz=m.ezz_n, exz=m.exz_n, q=m.q, T=m.T)
+    props = {k: torch.empty_like(v) for k, v in P.items()}
+    add("k_interp_material", timed(lambda: ops.interp_material(b, m.active, m.r, m.t, m.iel, m.mat, nodal,
+                                                               m.material, props)),
+        109 * n + 5 * 8 * nn)
+    x, z, act = m.x.clone(), m.z.clone(), m.active.clone()
+    up, wp = torch.empty_like(m.x), torch.empty_like(m.x)
+
+    def prep_adv():
+        x.copy_(m.x)
+        z.copy_(m.z)
+        act.copy_(m.active)
+    dtv = float(m.dt_out[0].item()) or 1e-6
+    add("k_advect (RK%d)" % m.cfg.RKorder, timed(lambda: ops.advect(b, m.cfg.RKorder, dtv, x, z, act, m.u, m.w, up, wp,
+                                                                   m.err), prep_adv),
+        50 * n + 2 * 8 * nn, bound_note="FP64 issue (4 stages: element index, reduced coordinates, Q2 basis, 18 gathers)")
+    # FP32 Stokes assembly, the full layout (the drop-in's build_matrix_stokes; the time step's solve
+    # is matrix-free and does not assemble)
+    q = m.stokes_inputs()
+    res = ops.assemble_stokes(b, False, 1, q, m.tables, m.bc_fix_V, m.bc_val_V, m.cfg.eta_ref, m.L_ref)
+    us = timed(lambda: ops.assemble_stokes(b, False, 1, q, m.tables, m.bc_fix_V, m.bc_val_V, m.cfg.eta_ref, m.L_ref,
+                                           out=res))
+    algo = nel * (9 * 9 * 8 + 8 + 468 * 4) + 2 * nn * 9 + 2 * nn * 8 + npp * 8
+    flops = 1.7e4 * nel
+    sm_mhz = None
+    try:
+        sm_mhz = float(subprocess.run(["nvidia-smi", "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits",
+                                       f"--id={torch.cuda.current_device()}"], capture_output=True, text=True,
+                                      timeout=5).stdout.strip())
+    except Exception:
+        pass
+    fp32_peak = 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
+    add("k_assemble_stokes<float> (full VV)", us, algo, gflop=flops / 1e9, tflops=flops / (us * 1e-6) / 1e12,
+        frac_fp32_peak=flops / (us * 1e-6) / 1e12 / fp32_peak, fp32_peak_tflops=fp32_peak)
+    del res
+    torch.cuda.empty_cache()
+    return out
+
+
+def step1_vs_oracle(torch, weights):
+    """Both arms' first step of the 512x512 model (seed 1000) against the FP64 oracle's first step
+    (tests/golden/oracle_fk512_step1.npz: the oracle restating the reference, cd_u_eta with SuperLU):
+    relative vrms, Nu and dt errors and the largest T error on the stored nodes."""
+    import numpy as np
+
+    from meeuuw_b200 import configs
+    from meeuuw_b200.timestep import GPUModel
+    path = os.path.join(ROOT, "tests", "golden", "oracle_fk512_step1.npz")
+    if not os.path.exists(path):
+        return None
+    d = np.load(path)
+    meta = json.loads(str(d["meta"]))
+    cfg = configs.fk_convection(meta["n"], seed=meta["seed"])
+    host = configs.build_host_model(cfg)
+    out = {"oracle": {"vrms": float(d["vrms"]), "Nu": float(d["Nu"]), "solver": meta["solver"],
+                      "stokes_relative_residual": float(d["stokes_residual"])}}
+    for arm in ("product", "plain_fp64"):
+        m = GPUModel(cfg, host, stokes="mixed" if arm == "product" else "f64", tol=1e-8)
+        if arm == "product" and weights:
+            from meeuuw_b200.unet import LearnedGuess, UNet
+            m.guess = LearnedGuess(m, UNet.load(weights), judge="cold")
+        m.step()
+        dd = m.diagnostics()
+        T = m.T.cpu().numpy()[d["nodes"]]
+        out[arm] = {"vrms_rel_err": abs(dd["vrms"] / float(d["vrms"]) - 1),
+                    "Nu_rel_err": abs(dd["Nu"] / float(d["Nu"]) - 1),
+                    "dt_rel_err": abs(dd["dt"] / float(d["dt"]) - 1), "T_max_abs_err": float(np.abs(T - d["T"]).max()),
+                    "stokes_outer_iters": dd["stokes"].get("outer_iters"),
+                    "stokes_inner_iters": dd["stokes"].get("inner_iters")}
+        del m
+        torch.cuda.empty_cache()
+    return out
 
 
 def roofline_apply(model, torch):
@@ -342,36 +464,47 @@ def run_e2e(model, torch, K, world, barrier, max_over_ranks):
 
 
 # ---------------------------------------------------------------------------------------- CPU
-def cpu_phase_times(n, seed=0):
-    """One oracle timestep at n x n of the FK workload, per-phase wall times (s)."""
-    import numpy as np
-
+def cpu_step(n, seed=1000):
+    """One full oracle timestep (the first) of the FK workload at n x n, measured: wall time (s),
+    per-phase times (s), the Stokes iteration count and the element count.  The oracle restates
+    the reference's numpy/Numba/SciPy path (SuperLU inner solves of cd_u_eta; K factorised under a
+    symmetric minimum-degree ordering, which only reorders the factorisation -- SuperLU's default
+    COLAMD ordering runs out of memory at 512x512)."""
     from meeuuw_b200 import configs
     from oracle.model import OracleModel
     cfg = configs.fk_convection(n, seed=seed)
     host = configs.build_host_model(cfg)
     om = OracleModel(cfg, host)
+    om.stokes_kw = dict(permc_spec="MMD_AT_PLUS_A")
+    om.energy_kw = dict(permc_spec="MMD_AT_PLUS_A")
     t0 = time.perf_counter()
     out = om.step(solver="cd_u_eta")
-    t1 = time.perf_counter()
-    return t1 - t0, out
+    t = time.perf_counter() - t0
+    return t, dict(om.phase_seconds), int(out["stokes_iterations"]), cfg.nel
 
 
-def cpu_baseline_sample(n_target, sizes=(32, 64)):
-    """Oracle timesteps at two small sizes; elementwise phases scale with n^2, the total is fitted
-    as a power law in n and extrapolated to n_target."""
-    import math
-    ts = []
-    for n in sizes:
-        t, _ = cpu_phase_times(n)
-        ts.append(t)
-    a = math.log(ts[1] / ts[0]) / math.log(sizes[1] / sizes[0])
-    a = max(a, 2.0)
-    t_target = ts[1] * (n_target / sizes[1]) ** a
-    return {"value": 1.0 / t_target, "unit": "timesteps/s", "cores": 1, "kind": "port",
-            "sample": f"oracle timestep (numpy/SciPy, cd_u_eta with SuperLU) at {sizes[0]}^2 and {sizes[1]}^2: "
-                      f"{ts[0]:.2f} s and {ts[1]:.2f} s; extrapolated to {n_target}^2 with the fitted exponent "
-                      f"{a:.2f}", "sample_seconds": ts}
+def cpu_sample(n_target, n_sample, repeats=1):
+    """Measured oracle timesteps at n_sample x n_sample (median of `repeats`), reported in
+    timesteps/s of the n_target x n_target workload by scaling with the element count (linear).
+    Linear scaling is a lower bound on the CPU's time at n_target: the sparse factorisation and the
+    Schur iteration grow faster than the element count (one full 512x512 oracle step took 423 s on
+    one core where a 128x128 step took 11.7 s), so the reported value favours the CPU."""
+    runs = [cpu_step(n_sample) for _ in range(max(1, repeats))]
+    runs.sort(key=lambda r: r[0])
+    t, phases, its, nel = runs[len(runs) // 2]
+    scale = (n_target / n_sample) ** 2
+    return {"value": 1.0 / (t * scale), "unit": "timesteps/s", "cores": 1, "kind": "port",
+            "sample": (f"one full oracle timestep of the FK model at {n_sample}x{n_sample} (numpy/SciPy; cd_u_eta "
+                       f"with SuperLU, {its} Schur iterations), measured {t:.2f} s (median of {len(runs)}); "
+                       f"scaled to {n_target}x{n_target} by the element count (x{scale:g}, linear: a lower "
+                       f"bound on the CPU's time there)"),
+            "measured": {"n": n_sample, "seconds_per_step": t, "timesteps_per_s": 1.0 / t,
+                         "phases_s": {k: round(v, 4) for k, v in phases.items()}},
+            "cores_note": "single-threaded: the reference's Numba kernels are serial and SuperLU is serial"}
+
+
+def cpu_baseline_sample(n_target):
+    return cpu_sample(n_target, 128)
 
 
 def run_reference(args):
@@ -379,19 +512,20 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    nsz = (32, 64)
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_phase_times(nsz[0])
-    samples = []
-    for _ in range(max(1, min(args.steps, 3))):
-        samples.append(cpu_baseline_sample(args.n, nsz))
-    v = sorted(s["value"] for s in samples)[len(samples) // 2]
+    # a bounded sample of the workload: the full oracle step at 256x256, measured; 128x128 beside it
+    # shows how the step grows with the element count
+    small = cpu_sample(args.n, 128)
+    nrep = max(1, min(args.steps, 2))
+    big = cpu_sample(args.n, 256, repeats=nrep)
+    v = big["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
-            "steps": len(samples), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": nrep, "warmup": 0, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded FK convection)",
-            "config": {"workload": f"fk_convection {args.n}x{args.n} Q2xQ1 (CPU oracle sample, extrapolated)"},
-            "cpu_baseline": {"value": v, "unit": "timesteps/s", "cores": 1, "kind": "port",
-                             "sample": samples[0]["sample"]},
+            "config": {"workload": f"fk_convection {args.n}x{args.n} Q2xQ1, Ra=1e6, eta=exp(-ln(1e5) T), geometric "
+                                   f"averaging, RK4, 16 particles/element, Crank-Nicolson energy (CPU oracle: "
+                                   f"measured at 256x256, scaled by element count)"},
+            "cpu_baseline": {k: big[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "measured": {"256": big["measured"], "128": small["measured"]},
             "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -3,7 +3,8 @@
 Run in a container that holds the reference checkout (it is read from
 ``/root/reference``; nothing at test time reads it):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py lsq      # least-squares fits and population control only
 
 Each case stores its inputs and the reference outputs in ``tests/golden/*.npz``.
 Sizes are small so the fixtures stay a few hundred KB.  Inputs are seeded.
@@ -32,6 +33,7 @@ def _import_reference():
     import build_pressure_mesh as bpm
     import build_velocity_connectivity as bvc
     import build_velocity_mesh as bvm
+    import compute_center_coordinates as ccc
     import cd_u_eta as cde
     import compute_nodal_heat_flux as cnh
     import compute_nodal_pressure as cnp
@@ -264,6 +266,126 @@ def case_solvers(R, rng, n=8):
                 out_cd_alpha=cd[5], out_cd_beta=cd[6])
 
 
+def case_lsq(R, rng, M):
+    """Least-squares P1/Q1 fits (pic_functions.py:1098-1285), the driver's limiter loop
+    (meeuuw.py:1241-1248, h = hx) and qpoint evaluation (meeuuw.py:1517-1532).  Some particles are
+    inactive with x = z = 0 and iel = 0, as advection and locate leave them: the reference's mask
+    (swarm_iel == iel) counts them in element 0."""
+    nelx, nelz, hx, hz = M["nelx"], M["nelz"], M["hx"], M["hz"]
+    nel = nelx * nelz
+    ppe = 12
+    npart = nel * ppe
+    iel = np.repeat(np.arange(nel), ppe).astype(np.int32)
+    perm = rng.permutation(npart)
+    iel = iel[perm]
+    r0, t0 = rng.uniform(-1, 1, npart), rng.uniform(-1, 1, npart)
+    x = (iel % nelx + (r0 + 1) / 2) * hx
+    z = (iel // nelx + (t0 + 1) / 2) * hz
+    active = rng.uniform(size=npart) > 0.06
+    x[~active] = 0.0
+    z[~active] = 0.0
+    iel[~active] = 0
+    rho = rng.uniform(0.9, 1.1, npart)
+    eta = np.exp(rng.uniform(-2, 2, npart))
+    x_e, z_e, _, _ = R.ccc.compute_center_coordinates("box", nel, M["x_V"], M["z_V"], M["icon_V"])
+    d = dict(swarm_x=x, swarm_z=z, swarm_iel=iel, swarm_active=active, swarm_rho=rho, swarm_eta=eta, x_e=x_e, z_e=z_e)
+    P1 = R.pf.compute_ls_coefficients_P1(nel, x_e, z_e, x, z, iel, rho, eta)
+    Q1 = R.pf.compute_ls_coefficients_Q1(nel, x_e, z_e, x, z, iel, rho, eta)
+    for k, v in zip(("rho_a", "rho_b", "rho_c", "eta_a", "eta_b", "eta_c", "rho_min", "rho_max", "eta_min",
+                     "eta_max"), P1):
+        d["out_P1_" + k] = np.array(v)
+    for k, v in zip(("rho_a", "rho_b", "rho_c", "rho_d", "eta_a", "eta_b", "eta_c", "eta_d", "rho_min", "rho_max",
+                     "eta_min", "eta_max"), Q1):
+        d["out_Q1_" + k] = np.array(v)
+    lim = {f: (d[f"out_P1_{f}_b"].copy(), d[f"out_P1_{f}_c"].copy()) for f in ("rho", "eta")}
+    for e in range(nel):                                              # meeuuw.py:1241-1248
+        for f in ("rho", "eta"):
+            lim[f][0][e], lim[f][1][e] = R.pf.limiter(d[f"out_P1_{f}_a"][e], lim[f][0][e], lim[f][1][e],
+                                                      d[f"out_P1_{f}_min"][e], d[f"out_P1_{f}_max"][e], hx)
+    xq, zq = M["xq"], M["zq"]
+    for f in ("rho", "eta"):
+        d[f"out_P1lim_{f}_b"], d[f"out_P1lim_{f}_c"] = lim[f]
+        a_, b_, c_ = d[f"out_P1_{f}_a"], lim[f][0], lim[f][1]
+        q = np.zeros((nel, 9))
+        for e in range(nel):                                          # meeuuw.py:1517-1523
+            for iq in range(9):
+                q[e, iq] = a_[e] + b_[e] * (xq[e, iq] - x_e[e]) + c_[e] * (zq[e, iq] - z_e[e])
+        d[f"out_P1_{f}q"] = q
+        a_, b_, c_, dd = (d[f"out_Q1_{f}_{k}"] for k in "abcd")
+        q = np.zeros((nel, 9))
+        for e in range(nel):                                          # meeuuw.py:1524-1532
+            for iq in range(9):
+                q[e, iq] = (a_[e] + b_[e] * (xq[e, iq] - x_e[e]) + c_[e] * (zq[e, iq] - z_e[e])
+                            + dd[e] * (xq[e, iq] - x_e[e]) * (zq[e, iq] - z_e[e]))
+        d[f"out_Q1_{f}q"] = q
+    # the limiter on its own, over slopes that trip both of its branches
+    c0 = rng.uniform(0, 1, 64)
+    c1, c2 = rng.uniform(-4, 4, 64), rng.uniform(-4, 4, 64)
+    c1[:4] = [0.0, -0.0, 1e-3, -1e-3]
+    lo, hi = c0 - rng.uniform(0, 0.5, 64), c0 + rng.uniform(0, 0.5, 64)
+    L = np.array([R.pf.limiter(c0[i], c1[i], c2[i], lo[i], hi[i], 0.25) for i in range(64)])
+    d.update(lim_c0=c0, lim_c1=c1, lim_c2=c2, lim_S=lo, lim_L=hi, lim_h=0.25, out_lim=L)
+    return d
+
+
+def case_population(R, rng, M):
+    """population_control (pic_functions.py:1621-1812) after an advection step: counts and element
+    indices from the start of the step, positions and active flags after advection.  The reference
+    draws r, t with random.uniform(-0.95, 0.95); the uniform numbers it consumes are stored."""
+    import io
+    nelx, nelz, hx, hz = M["nelx"], M["nelz"], M["hx"], M["hz"]
+    nel = nelx * nelz
+    per = np.full(nel, 9)
+    per[[3, 7, 13, 20]] = [5, 7, 3, 6]                                 # depleted elements
+    iel = np.concatenate([np.repeat(np.arange(nel), per), np.zeros(40, dtype=np.int64)]).astype(np.int32)
+    npart = len(iel)                                                   # + a pool of 40 inactive particles
+    active = np.concatenate([np.ones(per.sum(), dtype=bool), np.zeros(40, dtype=bool)])
+    perm = rng.permutation(npart)                                      # not stored element by element
+    iel, active = iel[perm], active[perm]
+    nparticle_e = np.bincount(iel[active], minlength=nel).astype(np.int32)   # counts at the step start
+    step_active = active.copy()
+    # advection moved the particles (positions from the step's end, element indices from its start)
+    # and pushed two of element 7's and one of element 10's particles out of the box
+    r0, t0 = rng.uniform(-0.9, 0.9, npart), rng.uniform(-0.9, 0.9, npart)
+    x = (iel % nelx + (r0 + 1) / 2) * hx
+    z = (iel // nelx + (t0 + 1) / 2) * hz
+    for e, k in ((7, 2), (10, 1)):
+        active[np.flatnonzero((iel == e) & active)[:k]] = False
+    x[~active] = 0.0
+    z[~active] = 0.0
+    d = dict(nparticle_min=7, nparticle_e=nparticle_e, step_active=step_active, swarm_active=active.copy(),
+             swarm_iel=iel.copy(), swarm_x=x.copy(), swarm_z=z.copy(), swarm_r=rng.uniform(-1, 1, npart),
+             swarm_t=rng.uniform(-1, 1, npart), swarm_u=rng.uniform(-1, 1, npart), swarm_w=rng.uniform(-1, 1, npart),
+             swarm_eta=np.exp(rng.uniform(-2, 2, npart)), swarm_mat=rng.integers(0, 2, npart).astype(np.int8))
+    needed = int(np.maximum(0, 7 - nparticle_e).sum())
+    random.seed(77)
+    d["draws"] = np.array([random.random() for _ in range(2 * needed)])
+    wf = np.zeros((2, npart))
+    wf[d["swarm_mat"], np.arange(npart)] = 1.0
+    arrs = {k: d[k].copy() for k in ("swarm_active", "swarm_iel", "swarm_r", "swarm_t", "swarm_x", "swarm_z",
+                                     "swarm_u", "swarm_w", "swarm_eta")}
+    random.seed(77)
+    R.pf.population_control(1, M["x_V"], M["z_V"], M["icon_V"], nel, 7, npart, nparticle_e, arrs["swarm_active"],
+                            np.arange(npart), arrs["swarm_iel"], arrs["swarm_r"], arrs["swarm_t"], arrs["swarm_x"],
+                            arrs["swarm_z"], arrs["swarm_u"], arrs["swarm_w"], np.zeros(npart), arrs["swarm_eta"], wf,
+                            np.zeros(npart), np.zeros(npart), False, 2, io.StringIO(), "")
+    for k, v in arrs.items():
+        d["out_" + k] = v
+    d["out_swarm_mat"] = np.argmax(wf, axis=0).astype(np.int8)
+    d["needed"] = needed
+    return d
+
+
+def main_lsq():
+    """Only the least-squares and population-control fixtures (their own seeded generator)."""
+    R = _import_reference()
+    rng = np.random.default_rng(20261204)
+    M = mesh_case(R, 6, 4, 1.5, 1.0)
+    np.savez_compressed(os.path.join(HERE, "lsq.npz"), **case_lsq(R, rng, M))
+    np.savez_compressed(os.path.join(HERE, "population.npz"), **case_population(R, rng, M))
+    print("wrote lsq.npz, population.npz")
+
+
 def main():
     R = _import_reference()
     rng = np.random.default_rng(20261203)
@@ -301,4 +423,7 @@ def write_signatures():
 
 if __name__ == "__main__":
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
-    main()
+    if sys.argv[1:] == ["lsq"]:
+        main_lsq()
+    else:
+        main()

@@ -39,6 +39,9 @@ extern "C" {
 #define MW_FLAG_EMPTY_ELEMENT 8     /* meeuuw.py:1198-1199 "an element contains no particle" */
 #define MW_FLAG_NONFINITE 16        /* NaN/Inf met in a solver reduction */
 #define MW_FLAG_ITER_LIMIT 32       /* a bounded device loop gave up */
+#define MW_FLAG_POP_UNAVAILABLE 64  /* pic_functions.py:1722-1733 "population_control: not available yet" */
+#define MW_FLAG_POP_MASK_EMPTY 128  /* pic_functions.py:1747-1748 "population_control: mask empty" */
+#define MW_FLAG_POP_DRAWS 256       /* population control needs more uniform numbers than were passed */
 
 #define MW_MAX_FIELDS 8
 
@@ -125,6 +128,61 @@ int mw_project_nodes(mw_box box, int32_t flavour, int32_t nfield, const int32_t*
 /* project_nodal_{V,P,T}field_onto_qpoints, project_nodal_field_onto_qpoints.py:12-62.
  * N is the device (9 x m) basis table (N_V for MW_SPACE_Q2, N_P otherwise); phiq is (nel, 9). */
 int mw_nodal_to_qpoints(mw_box box, int32_t space, const double* N, const double* phi, double* phiq, void* stream);
+
+/* ======================= least-squares projections, population control ======================= */
+
+/* compute_ls_coefficients_P1 (ncoef 3: a + b dx + c dz) and compute_ls_coefficients_Q1 (ncoef 4:
+ * + d dx dz), pic_functions.py:1098-1285, for up to MW_MAX_FIELDS particle fields at once, with
+ * dx, dz measured from the element centre (node 8).  offsets/order must bin EVERY particle
+ * (mw_bin_particles with an all-ones active array): the reference's mask swarm_iel == iel takes
+ * inactive particles, which locate leaves at iel 0, into element 0's fit.  Per element the normal
+ * equations are summed particle by particle in index order, each sum as the reference forms it,
+ * and solved by Gaussian elimination with partial pivoting (the reference calls LAPACK's solve).
+ * coef[f]: (nel, ncoef) row-major; fmin[f], fmax[f] (may be NULL): the particle extrema per element
+ * (pic_functions.py:1164-1167).  limit_h > 0 (P1 only) limits the slopes as the driver does:
+ * limiter(), pic_functions.py:1068-1089, called with h = hx at meeuuw.py:1241-1248.  Elements
+ * without particles set MW_FLAG_EMPTY_ELEMENT (the driver aborts before, meeuuw.py:1198). */
+typedef struct {
+  const double* phi[MW_MAX_FIELDS];
+  double* coef[MW_MAX_FIELDS];
+  double* fmin[MW_MAX_FIELDS];
+  double* fmax[MW_MAX_FIELDS];
+  int32_t n;
+} mw_ls_fields;
+int mw_ls_fit(mw_box box, int32_t ncoef, const int32_t* offsets, const int32_t* order, const double* x,
+              const double* z, mw_ls_fields fields, double limit_h, int32_t* err, void* stream);
+
+/* The fits at the quadrature points, meeuuw.py:1517-1532 (particle_rho/eta_projection
+ * "least_squares_P1/Q1"): phiq[e, q] = a + b (xq - x_e) + c (zq - z_e) [+ d (xq - x_e)(zq - z_e)].
+ * coef (nel, ncoef); xq, zq, phiq (nel, 9). */
+int mw_ls_to_qpoints(mw_box box, int32_t ncoef, const double* coef, const double* xq, const double* zq,
+                     double* phiq, void* stream);
+
+/* population_control, pic_functions.py:1621-1812, on the box path's particle arrays (an int8
+ * material id in place of the weight fractions).  Called where the driver calls it
+ * (meeuuw.py:2846-2850): after advection, before locate.  counts, offsets and order are the step's
+ * binning (mw_bin_particles over the step-start active flags and element indices); active, x, z are
+ * the values after advection.  Each element with fewer than nparticle_min particles receives
+ * inactive particles, taken in index order, at reduced coordinates r, t = -0.95 + 1.9 u (the
+ * reference's random.uniform(-0.95, 0.95), r first); each takes the material id of the nearest
+ * particle of its element (the first in index order on a tie, as np.argmin; that particle's index
+ * goes to source[pid], if source is not NULL, so a caller can copy other per-particle data such as
+ * weight fractions) and, for every field in `avg`, the mean of the element's particles
+ * (np.average: numpy's pairwise summation order; eta, u, w on the box path, strain or melt
+ * fraction where a caller carries them).  draws: 2 * max_new uniform [0, 1) numbers, two per added
+ * particle in the order the reference consumes them; or NULL: the numbers come from a
+ * counter-based generator keyed by `seed`.  The number of particles added is written to *added
+ * (device int32).  Errors set device flags (no particle is added): MW_FLAG_POP_UNAVAILABLE when more
+ * particles are needed than are inactive, MW_FLAG_POP_DRAWS when more than max_new are needed;
+ * MW_FLAG_POP_MASK_EMPTY marks a flagged element without active particles.  mat and source may be
+ * NULL. */
+typedef struct { double* f[MW_MAX_FIELDS]; int32_t n; } mw_pc_fields;
+size_t mw_population_workspace_bytes(int32_t nel, int64_t nparticle);
+int mw_population_control(mw_box box, int32_t nparticle_min, int64_t nparticle, const int32_t* counts,
+                          const int32_t* offsets, const int32_t* order, uint8_t* active, int32_t* iel, double* r,
+                          double* t, double* x, double* z, int8_t* mat, int32_t* source, mw_pc_fields avg,
+                          const double* draws, int64_t max_new, uint64_t seed, int32_t* added, void* work,
+                          size_t work_bytes, int32_t* err, void* stream);
 
 /* ======================= element assembly ======================= */
 

@@ -15,12 +15,14 @@ MW_OK = 0
 STATUS = {0: "MW_OK", 1: "MW_ERR_BAD_ARG", 2: "MW_ERR_CUDA", 3: "MW_ERR_NOT_CONVERGED", 4: "MW_ERR_WORKSPACE",
           5: "MW_ERR_DEVICE_FLAG"}
 FLAG_R_OUT, FLAG_T_OUT, FLAG_ELEMENT_RANGE, FLAG_EMPTY_ELEMENT, FLAG_NONFINITE, FLAG_ITER_LIMIT = 1, 2, 4, 8, 16, 32
+FLAG_POP_UNAVAILABLE, FLAG_POP_MASK_EMPTY, FLAG_POP_DRAWS = 64, 128, 256
 MAX_FIELDS = 8
 AVG = {"arithmetic": 0, "geometric": 1, "harmonic": 2}
 SPACE_Q2, SPACE_Q1_ON_V, SPACE_Q1 = 0, 1, 2
 MATERIAL_BOUSSINESQ, MATERIAL_TWO = 0, 1
 
 c_void_p, c_int32, c_int64, c_double, c_size_t = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_size_t
+c_uint64 = ctypes.c_uint64
 
 
 class MwBox(ctypes.Structure):
@@ -71,6 +73,15 @@ class MwSwarmProps(ctypes.Structure):
 
 _lib = None
 
+class MwLsFields(ctypes.Structure):
+    _fields_ = [("phi", c_void_p * 8), ("coef", c_void_p * 8), ("fmin", c_void_p * 8), ("fmax", c_void_p * 8),
+                ("n", c_int32)]
+
+
+class MwPcFields(ctypes.Structure):
+    _fields_ = [("f", c_void_p * 8), ("n", c_int32)]
+
+
 # name -> (restype, argtypes)
 _PROTOS = {
     "mw_locate_box": (c_int32, [MwBox, c_int64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
@@ -90,6 +101,12 @@ _PROTOS = {
     "mw_project_nodes": (c_int32, [MwBox, c_int32, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
     "mw_nodal_to_qpoints": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mw_ls_fit": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, MwLsFields, c_double, c_void_p,
+                            c_void_p]),
+    "mw_ls_to_qpoints": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mw_population_workspace_bytes": (c_size_t, [c_int32, c_int64]),
+    "mw_population_control": (c_int32, [MwBox, c_int32, c_int64] + [c_void_p] * 11 + [MwPcFields, c_void_p, c_int64,
+                                        c_uint64, c_void_p, c_void_p, c_size_t, c_void_p, c_void_p]),
     "mw_assemble_stokes_workspace_bytes": (c_size_t, [MwBox]),
     "mw_assemble_stokes": (c_int32, [MwBox, c_int32, c_int32, MwStokesIn, MwStokesOut, c_void_p, c_size_t, c_void_p]),
     "mw_stokes_rhs_body": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,

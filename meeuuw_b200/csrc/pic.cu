@@ -562,6 +562,347 @@ __global__ void k_nodal_to_q(mw_box b, int space, const double* __restrict__ Nta
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// Least-squares particle fits (pic_functions.py:1098-1285) and their slope limiter
+// (pic_functions.py:1068-1089).  One thread per element sums the normal equations over the
+// element's bin in particle-index order -- each accumulator in the reference's order, products
+// formed as the reference writes them ((sx*sx)*sz, sx*(sz*sz), (v*sx)*sz) -- then solves them by
+// Gaussian elimination with partial pivoting (the reference calls LAPACK's solve).
+struct LsFields {
+  const double* phi[MW_MAX_FIELDS];
+  double* coef[MW_MAX_FIELDS];
+  double* fmin[MW_MAX_FIELDS];
+  double* fmax[MW_MAX_FIELDS];
+  int n;
+};
+
+// Python's min(a, b): a unless b < a
+MW_D double py_min(double a, double b) { return b < a ? b : a; }
+MW_D double py_sign(double v) { return v < 0 ? -1.0 : 1.0; }
+
+// limiter(c_0, c_1, c_2, S, L, h), pic_functions.py:1068-1089
+MW_D void ls_limiter(double c0, double& c1, double& c2, double S, double L, double h) {
+  const double k_u = py_min(c0 - S, L - c0);
+  double k_l = (fabs(c1) + fabs(c2)) * h / 2;
+  if (k_l > k_u) {
+    const double c_max = k_u * 2 / h;
+    c1 = py_sign(c1) * py_min(fabs(c1), c_max);
+    c2 = py_sign(c2) * py_min(fabs(c2), c_max);
+  }
+  k_l = (fabs(c1) + fabs(c2)) * h / 2;
+  if (k_l > k_u) {
+    const double c_change = (k_l - k_u) / h;
+    c1 = py_sign(c1) * (fabs(c1) - c_change);
+    c2 = py_sign(c2) * (fabs(c2) - c_change);
+  }
+}
+
+// Solve A x = b in place (b -> x) for the NC x NC system: Gaussian elimination, partial pivoting
+// (first largest magnitude in the column).  Returns false on a zero pivot.
+template <int NC>
+MW_D bool small_solve(double (&A)[NC][NC], double (&b)[NC]) {
+#pragma unroll
+  for (int k = 0; k < NC; ++k) {
+    int piv = k;
+    double best = fabs(A[k][k]);
+#pragma unroll
+    for (int i = k + 1; i < NC; ++i)
+      if (fabs(A[i][k]) > best) { best = fabs(A[i][k]); piv = i; }
+    if (best == 0.0) return false;
+    if (piv != k) {
+#pragma unroll
+      for (int j = 0; j < NC; ++j) { double tmp = A[k][j]; A[k][j] = A[piv][j]; A[piv][j] = tmp; }
+      double tmp = b[k]; b[k] = b[piv]; b[piv] = tmp;
+    }
+#pragma unroll
+    for (int i = k + 1; i < NC; ++i) {
+      const double l = A[i][k] / A[k][k];
+#pragma unroll
+      for (int j = k + 1; j < NC; ++j) A[i][j] = A[i][j] - l * A[k][j];
+      b[i] = b[i] - l * b[k];
+    }
+  }
+#pragma unroll
+  for (int k = NC - 1; k >= 0; --k) {
+    double s = b[k];
+#pragma unroll
+    for (int j = k + 1; j < NC; ++j) s = s - A[k][j] * b[j];
+    b[k] = s / A[k][k];
+  }
+  return true;
+}
+
+// element centre x_V[icon_V[8, iel]] = i hx / 2 with i = 2 ex + 1 (build_velocity_mesh.py:116-117)
+MW_D double x_centre(const mw_box& b, int ex) { return ((double)(2 * ex + 1) * b.hx) / 2; }
+MW_D double z_centre(const mw_box& b, int ez) { return ((double)(2 * ez + 1) * b.hz) / 2; }
+
+template <int NC>
+__global__ void k_ls_fit(mw_box b, const int32_t* __restrict__ offsets, const int32_t* __restrict__ order,
+                         const double* __restrict__ x, const double* __restrict__ z, LsFields f, double limit_h,
+                         int32_t* err) {
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    const int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
+    const double xe = x_centre(b, ex), ze = z_centre(b, ez);
+    const int b0 = offsets[e], b1 = offsets[e + 1];
+    if (b1 == b0) { set_flag(err, MW_FLAG_EMPTY_ELEMENT); continue; }
+    double A[NC][NC];
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < NC; ++j) A[i][j] = 0.0;
+    A[0][0] = (double)(b1 - b0);
+    for (int j = b0; j < b1; ++j) {                       // pic_functions.py:1134-1146 / :1226-1246
+      const int p = order[j];
+      const double sx = x[p] - xe, sz = z[p] - ze;
+      A[0][1] += sx;
+      A[0][2] += sz;
+      if (NC == 4) A[0][3] += sx * sz;
+      A[1][1] += sx * sx;
+      A[1][2] += sx * sz;
+      if (NC == 4) A[1][3] += (sx * sx) * sz;
+      A[2][2] += sz * sz;
+      if (NC == 4) {
+        A[2][3] += sx * (sz * sz);
+        A[3][3] += (sx * sx) * (sz * sz);
+      }
+    }
+#pragma unroll
+    for (int i = 1; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < i; ++j) A[i][j] = A[j][i];
+    for (int fi = 0; fi < f.n; ++fi) {
+      const double* phi = f.phi[fi];
+      double rhs[NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i) rhs[i] = 0.0;
+      double vmin = 0.0, vmax = 0.0;
+      for (int j = b0; j < b1; ++j) {
+        const int p = order[j];
+        const double sx = x[p] - xe, sz = z[p] - ze, v = phi[p];
+        rhs[0] += v;
+        rhs[1] += v * sx;
+        rhs[2] += v * sz;
+        if (NC == 4) rhs[3] += (v * sx) * sz;
+        if (j == b0 || v < vmin) vmin = v;                 // np.min / np.max (:1164-1167)
+        if (j == b0 || v > vmax) vmax = v;
+      }
+      double M[NC][NC];
+#pragma unroll
+      for (int i = 0; i < NC; ++i)
+#pragma unroll
+        for (int j = 0; j < NC; ++j) M[i][j] = A[i][j];
+      if (!small_solve<NC>(M, rhs)) set_flag(err, MW_FLAG_NONFINITE);
+      if (NC == 3 && limit_h > 0.0) ls_limiter(rhs[0], rhs[1], rhs[2], vmin, vmax, limit_h);   // meeuuw.py:1241-1248
+#pragma unroll
+      for (int i = 0; i < NC; ++i) f.coef[fi][e * NC + i] = rhs[i];
+      if (f.fmin[fi]) f.fmin[fi][e] = vmin;
+      if (f.fmax[fi]) f.fmax[fi][e] = vmax;
+    }
+  }
+}
+
+// a + b (xq - x_e) + c (zq - z_e) [+ d (xq - x_e)(zq - z_e)] at every qpoint (meeuuw.py:1517-1532)
+template <int NC>
+__global__ void k_ls_q(mw_box b, const double* __restrict__ coef, const double* __restrict__ xq,
+                       const double* __restrict__ zq, double* __restrict__ phiq) {
+  const int64_t nq = (int64_t)b.nelx * b.nelz * 9;
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < nq; g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = g / 9;
+    const int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
+    const double* c = coef + e * NC;
+    const double dx = xq[g] - x_centre(b, ex), dz = zq[g] - z_centre(b, ez);
+    double v = c[0] + c[1] * dx + c[2] * dz;
+    if (NC == 4) v = v + c[3] * dx * dz;
+    phiq[g] = v;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Population control (pic_functions.py:1621-1812).
+//
+// numpy's pairwise summation of a float64 array (np.add.reduce, so np.mean / np.average): < 8
+// values sequentially from 0; up to 128 in eight interleaved partial sums combined as a tree,
+// then the remainder; longer arrays split at an 8-aligned half.  v(k) is the k-th value.
+template <typename V>
+MW_D double np_pairwise(const V& v, int k0, int n) {
+  if (n < 8) {
+    double res = 0.0;
+    for (int i = 0; i < n; ++i) res += v(k0 + i);
+    return res;
+  }
+  if (n <= 128) {
+    double r[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r[j] = v(k0 + j);
+    int i = 8;
+    for (; i < n - (n % 8); i += 8)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) r[j] += v(k0 + i + j);
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; i < n; ++i) res += v(k0 + i);
+    return res;
+  }
+  int n2 = n / 2;
+  n2 -= n2 % 8;
+  return np_pairwise(v, k0, n2) + np_pairwise(v, k0 + n2, n - n2);
+}
+
+// counter-based uniform [0, 1) numbers (SplitMix64 finaliser, 53-bit mantissa)
+MW_D double splitmix_u01(uint64_t seed, uint64_t k) {
+  uint64_t zz = seed + (k + 1) * 0x9E3779B97F4A7C15ull;
+  zz = (zz ^ (zz >> 30)) * 0xBF58476D1CE4E5B9ull;
+  zz = (zz ^ (zz >> 27)) * 0x94D049BB133111EBull;
+  zz ^= zz >> 31;
+  return (double)(zz >> 11) * (1.0 / 9007199254740992.0);
+}
+
+__global__ void k_pc_need(int32_t nel, int32_t nmin, const int32_t* __restrict__ counts, int32_t* __restrict__ need) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t d = nmin - counts[e];
+    need[e] = d > 0 ? d : 0;                                      // :1655-1657
+  }
+}
+
+__global__ void k_pc_flag(int64_t n, const uint8_t* __restrict__ active, int32_t* __restrict__ flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    flag[i] = active[i] ? 0 : 1;
+}
+
+__global__ void k_pc_list(int64_t n, const int32_t* __restrict__ flag, const int32_t* __restrict__ off,
+                          int32_t* __restrict__ avail) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (flag[i]) avail[off[i]] = (int32_t)i;                     // :1680-1688, index order
+}
+
+// totals: need_off[nel] (particles needed), avail_off[n] (inactive particles)
+__global__ void k_pc_check(const int32_t* __restrict__ need_total, const int32_t* __restrict__ avail_total,
+                           int64_t max_new, int32_t* __restrict__ added, int32_t* err) {
+  if (threadIdx.x || blockIdx.x) return;
+  const int32_t need = *need_total, avail = *avail_total;
+  int32_t a = need;
+  if (need > avail) { set_flag(err, MW_FLAG_POP_UNAVAILABLE); a = 0; }      // :1722-1733
+  else if ((int64_t)need > max_new) { set_flag(err, MW_FLAG_POP_DRAWS); a = 0; }
+  *added = a;
+}
+
+struct PcFields {
+  double* f[MW_MAX_FIELDS];
+  int n;
+};
+
+// One thread per added particle j: its element (need_off[e] <= j < need_off[e + 1]), its particle
+// (avail[j]), its position from two uniform numbers, the nearest particle's material and the
+// element particles' means of the `avg` fields (eta, u, w on the box path; :1739-1799).  The
+// element's particles are its step-start bin filtered by the current active flags, read before any
+// flag changes (k_pc_commit sets them); added particles are inactive, so no thread reads a value
+// another one writes.
+__global__ void k_pc_fill(mw_box b, const int32_t* __restrict__ need_off, const int32_t* __restrict__ offsets,
+                          const int32_t* __restrict__ order, const int32_t* __restrict__ avail,
+                          const int32_t* __restrict__ added, const uint8_t* __restrict__ active, int32_t* iel,
+                          double* r, double* t, double* x, double* z, int8_t* mat, int32_t* source, PcFields avg,
+                          const double* __restrict__ draws, uint64_t seed, int64_t max_new, int32_t* err) {
+  const int32_t total = *added;
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  const int nnx = 2 * b.nelx + 1;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < max_new && j < total;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = nel - 1;                                // last e with need_off[e] <= j
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) / 2;
+      if (need_off[mid] <= j) lo = mid; else hi = mid - 1;
+    }
+    const int64_t e = lo;
+    const int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
+    const int b0 = offsets[e], b1 = offsets[e + 1];
+    int m = 0;
+    for (int k = b0; k < b1; ++k) m += active[order[k]] ? 1 : 0;
+    if (m == 0) { set_flag(err, MW_FLAG_POP_MASK_EMPTY); continue; }      // :1747-1748
+    const int pid = avail[j];
+    const double lo_ = -0.95, hi_ = 0.95;                       // random.uniform(-0.95, 0.95)
+    const double u0 = draws ? draws[2 * j] : splitmix_u01(seed, 2 * (uint64_t)j);
+    const double u1 = draws ? draws[2 * j + 1] : splitmix_u01(seed, 2 * (uint64_t)j + 1);
+    const double rr = lo_ + (hi_ - lo_) * u0, tt = lo_ + (hi_ - lo_) * u1;
+    double N[9];
+    q2_basis<double>(rr, tt, N);
+    double xn = 0.0, zn = 0.0;
+    for (int k = 0; k < 9; ++k) {                                 // np.dot(N, x_V[icon_V[:, iel]])
+      const int64_t nd = q2_node(ex, ez, k, nnx);
+      const int ix = (int)(nd % nnx), iz = (int)(nd / nnx);
+      xn = xn + N[k] * (((double)ix * b.hx) / 2);
+      zn = zn + N[k] * (((double)iz * b.hz) / 2);
+    }
+    // nearest particle (the first in index order on ties, as np.argmin)
+    double best = 0.0;
+    int bi = -1;
+    for (int k = b0; k < b1; ++k) {
+      const int q = order[k];
+      if (!active[q]) continue;
+      const double dx = x[q] - xn, dz = z[q] - zn;
+      const double d = dx * dx + dz * dz;
+      if (bi < 0 || d < best) { best = d; bi = q; }
+    }
+    auto nth = [&](int kk) -> int {                              // the kk-th particle of the mask
+      int c = 0;
+      for (int k = b0; k < b1; ++k) {
+        const int q = order[k];
+        if (!active[q]) continue;
+        if (c == kk) return q;
+        ++c;
+      }
+      return order[b0];
+    };
+    for (int fi = 0; fi < avg.n; ++fi) {                          // np.average(field[mask])
+      double* fld = avg.f[fi];
+      const double sm = np_pairwise([&](int kk) { return fld[nth(kk)]; }, 0, m);
+      fld[pid] = sm / m;
+    }
+    iel[pid] = (int32_t)e;
+    r[pid] = rr;
+    t[pid] = tt;
+    x[pid] = xn;
+    z[pid] = zn;
+    if (mat) mat[pid] = mat[bi];
+    if (source) source[pid] = bi;
+  }
+}
+
+__global__ void k_pc_commit(const int32_t* __restrict__ avail, const int32_t* __restrict__ added, int64_t max_new,
+                            uint8_t* __restrict__ active) {
+  const int32_t total = *added;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < max_new && j < total;
+       j += (int64_t)gridDim.x * blockDim.x)
+    active[avail[j]] = 1;
+}
+
+// Exclusive scan of any length (block scans, recursively over the block totals).
+static int scan_any(const int32_t* in, int32_t* out, int64_t n, int32_t* scratch, size_t scratch_ints,
+                    cudaStream_t s) {
+  const int T = 1024;
+  const int64_t nb = (n + T - 1) / T;
+  if (nb <= 1) {
+    k_scan_block<<<1, T, 0, s>>>(in, out, nullptr, n);
+    MW_CHECK_LAUNCH();
+    return MW_OK;
+  }
+  if ((size_t)(2 * nb) > scratch_ints) return MW_ERR_WORKSPACE;
+  int32_t* bsum = scratch;
+  int32_t* bpre = scratch + nb;
+  k_scan_block<<<(unsigned)nb, T, 0, s>>>(in, out, bsum, n);
+  MW_CHECK_LAUNCH();
+  int rc = scan_any(bsum, bpre, nb, scratch + 2 * nb, scratch_ints - 2 * nb, s);
+  if (rc) return rc;
+  k_scan_add<<<(unsigned)nb, T, 0, s>>>(out, bpre, n);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+static size_t scan_any_ints(int64_t n) {
+  size_t s = 0;
+  for (int64_t m = (n + 1023) / 1024; m > 1; m = (m + 1023) / 1024) s += 2 * m;
+  return s + 64;
+}
+
 }  // namespace mw
 
 using namespace mw;
@@ -690,6 +1031,95 @@ int mw_nodal_to_qpoints(mw_box box, int32_t space, const double* N, const double
   int64_t nq = (int64_t)box.nelx * box.nelz * 9;
   k_nodal_to_q<<<grid_for(nq, 256), 256, 0, (cudaStream_t)stream>>>(box, space, N, phi, phiq);
   MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_ls_fit(mw_box box, int32_t ncoef, const int32_t* offsets, const int32_t* order, const double* x,
+              const double* z, mw_ls_fields fields, double limit_h, int32_t* err, void* stream) {
+  if (!box_ok(box) || !(ncoef == 3 || ncoef == 4) || fields.n < 1 || fields.n > MW_MAX_FIELDS || !offsets ||
+      !order || !x || !z)
+    return MW_ERR_BAD_ARG;
+  if (ncoef == 4 && limit_h > 0.0) return MW_ERR_BAD_ARG;       // the reference limits P1 fits only
+  LsFields f;
+  f.n = fields.n;
+  for (int i = 0; i < fields.n; ++i) {
+    if (!fields.phi[i] || !fields.coef[i]) return MW_ERR_BAD_ARG;
+    f.phi[i] = fields.phi[i]; f.coef[i] = fields.coef[i]; f.fmin[i] = fields.fmin[i]; f.fmax[i] = fields.fmax[i];
+  }
+  const int64_t nel = (int64_t)box.nelx * box.nelz;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (ncoef == 3) k_ls_fit<3><<<grid_for(nel, 128), 128, 0, s>>>(box, offsets, order, x, z, f, limit_h, err);
+  else k_ls_fit<4><<<grid_for(nel, 128), 128, 0, s>>>(box, offsets, order, x, z, f, 0.0, err);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_ls_to_qpoints(mw_box box, int32_t ncoef, const double* coef, const double* xq, const double* zq,
+                     double* phiq, void* stream) {
+  if (!box_ok(box) || !(ncoef == 3 || ncoef == 4) || !coef || !xq || !zq || !phiq) return MW_ERR_BAD_ARG;
+  const int64_t nq = (int64_t)box.nelx * box.nelz * 9;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (ncoef == 3) k_ls_q<3><<<grid_for(nq, 256), 256, 0, s>>>(box, coef, xq, zq, phiq);
+  else k_ls_q<4><<<grid_for(nq, 256), 256, 0, s>>>(box, coef, xq, zq, phiq);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+size_t mw_population_workspace_bytes(int32_t nel, int64_t nparticle) {
+  const size_t ints = (size_t)2 * (nel + 1) + (size_t)3 * (nparticle + 1) + scan_any_ints(nel + 1) +
+                      scan_any_ints(nparticle + 1) + 64;
+  return ints * sizeof(int32_t);
+}
+
+int mw_population_control(mw_box box, int32_t nparticle_min, int64_t nparticle, const int32_t* counts,
+                          const int32_t* offsets, const int32_t* order, uint8_t* active, int32_t* iel, double* r,
+                          double* t, double* x, double* z, int8_t* mat, int32_t* source, mw_pc_fields avg,
+                          const double* draws, int64_t max_new, uint64_t seed, int32_t* added, void* work,
+                          size_t work_bytes, int32_t* err, void* stream) {
+  if (!box_ok(box) || nparticle < 1 || nparticle > INT32_MAX - 1 || !counts || !offsets || !order || !active ||
+      !iel || !r || !t || !x || !z || !added || !work || avg.n < 0 || avg.n > MW_MAX_FIELDS)
+    return MW_ERR_BAD_ARG;
+  PcFields pf;
+  pf.n = avg.n;
+  for (int i = 0; i < avg.n; ++i) {
+    if (!avg.f[i]) return MW_ERR_BAD_ARG;
+    pf.f[i] = avg.f[i];
+  }
+  const int32_t nel = box.nelx * box.nelz;
+  if (work_bytes < mw_population_workspace_bytes(nel, nparticle)) return MW_ERR_WORKSPACE;
+  if (!draws) max_new = nparticle;                 // the device draws as many numbers as it needs
+  if (max_new < 0) return MW_ERR_BAD_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t* need = (int32_t*)work;
+  int32_t* need_off = need + (nel + 1);
+  int32_t* flag = need_off + (nel + 1);
+  int32_t* avail_off = flag + (nparticle + 1);
+  int32_t* avail = avail_off + (nparticle + 1);
+  int32_t* scratch = avail + (nparticle + 1);
+  const size_t scratch_ints = work_bytes / sizeof(int32_t) - (size_t)(scratch - need);
+  k_pc_need<<<grid_for(nel, 256), 256, 0, s>>>(nel, nparticle_min, counts, need);
+  MW_CHECK_LAUNCH();
+  int rc = scan_any(need, need_off, nel, scratch, scratch_ints, s);
+  if (rc) return rc;
+  k_total<<<1, 32, 0, s>>>(need, need_off, nel);
+  MW_CHECK_LAUNCH();
+  k_pc_flag<<<grid_for(nparticle, 256), 256, 0, s>>>(nparticle, active, flag);
+  MW_CHECK_LAUNCH();
+  rc = scan_any(flag, avail_off, nparticle, scratch, scratch_ints, s);
+  if (rc) return rc;
+  k_total<<<1, 32, 0, s>>>(flag, avail_off, nparticle);
+  MW_CHECK_LAUNCH();
+  k_pc_list<<<grid_for(nparticle, 256), 256, 0, s>>>(nparticle, flag, avail_off, avail);
+  MW_CHECK_LAUNCH();
+  k_pc_check<<<1, 32, 0, s>>>(need_off + nel, avail_off + nparticle, max_new, added, err);
+  MW_CHECK_LAUNCH();
+  if (max_new > 0) {
+    k_pc_fill<<<grid_for(max_new, 128), 128, 0, s>>>(box, need_off, offsets, order, avail, added, active, iel, r, t,
+                                                     x, z, mat, source, pf, draws, seed, max_new, err);
+    MW_CHECK_LAUNCH();
+    k_pc_commit<<<grid_for(max_new, 256), 256, 0, s>>>(avail, added, max_new, active);
+    MW_CHECK_LAUNCH();
+  }
   return MW_OK;
 }
 

@@ -365,3 +365,51 @@ def gemm_bf16_tn(A, B, out=None, bias=None, relu=False, splits=1, out_bf16=False
         wp, wb = None, ctypes.c_size_t(0)
     call("mw_gemm_bf16_tn", M, N, K, ptr(A), A.stride(0), ptr(B), B.stride(0), ep, wp, wb, ptr(err), stream_ptr())
     return out
+
+
+# ---------------------------------------------------------------- least squares, population control
+def ls_fit(box, ncoef, offsets, order, x, z, fields, limit_h=0.0, err=None):
+    """compute_ls_coefficients_P1 (ncoef 3) / _Q1 (ncoef 4) for the particle fields `fields`, with
+    the driver's slope limiter when limit_h > 0 (P1).  offsets/order: bins of every particle.
+    Returns [(coef (nel, ncoef), fmin (nel), fmax (nel)) per field]."""
+    nel = box.nelx * box.nelz
+    outs = [(_empty(nel * ncoef, like=x).view(nel, ncoef), _empty(nel, like=x), _empty(nel, like=x))
+            for _ in fields]
+    for i in range(0, len(fields), L.MAX_FIELDS):
+        fs = L.MwLsFields()
+        chunk = list(range(i, min(len(fields), i + L.MAX_FIELDS)))
+        for k, j in enumerate(chunk):
+            fs.phi[k] = fields[j].data_ptr()
+            fs.coef[k] = outs[j][0].data_ptr()
+            fs.fmin[k] = outs[j][1].data_ptr()
+            fs.fmax[k] = outs[j][2].data_ptr()
+        fs.n = len(chunk)
+        call("mw_ls_fit", box, int(ncoef), ptr(offsets), ptr(order), ptr(x), ptr(z), fs, float(limit_h), ptr(err),
+             stream_ptr())
+    return outs
+
+
+def ls_to_qpoints(box, coef, xq, zq, out=None):
+    """meeuuw.py:1517-1532: the fit evaluated at the quadrature points, (nel, 9)."""
+    out = torch.empty_like(xq) if out is None else out
+    call("mw_ls_to_qpoints", box, int(coef.shape[1]), ptr(coef), ptr(xq), ptr(zq), ptr(out), stream_ptr())
+    return out
+
+
+def population_control(box, nparticle_min, counts, offsets, order, active, iel, r, t, x, z, mat=None, avg=(),
+                       source=None, draws=None, seed=0, added=None, err=None):
+    """population_control (pic_functions.py:1621-1812).  avg: per-particle fields the new particles
+    take as their element's mean.  Returns the device scalar holding the number of particles added."""
+    n = x.numel()
+    nel = box.nelx * box.nelz
+    added = torch.zeros(1, dtype=i32, device=x.device) if added is None else added
+    pf = L.MwPcFields()
+    for k, f in enumerate(avg):
+        pf.f[k] = f.data_ptr()
+    pf.n = len(avg)
+    wp, wb = workspace("population").get(L.lib().mw_population_workspace_bytes(nel, n))
+    max_new = draws.numel() // 2 if draws is not None else n
+    call("mw_population_control", box, int(nparticle_min), n, ptr(counts), ptr(offsets), ptr(order),
+         ptr(as_u8(active)), ptr(iel), ptr(r), ptr(t), ptr(x), ptr(z), ptr(mat), ptr(source), pf, ptr(draws),
+         int(max_new), ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), ptr(added), wp, wb, ptr(err), stream_ptr())
+    return added

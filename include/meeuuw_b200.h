@@ -356,6 +356,10 @@ typedef struct {
   int32_t history_len;    /* xiP = ||alpha p||, alpha, beta (the reference's array_xiV/xiP/alpha/beta) */
   int32_t host_loops;     /* 0: loops as CUDA-graph conditional nodes (one graph launch per solve, the  */
                           /* default); 1: loops driven by the host (one synchronisation per iteration) */
+  double sweep_target;    /* MW_F32: > 0 stops each refinement sweep's Schur iteration at the reduction */
+                          /* max(sweep_reduction, sweep_target * tol / current relative residual), so a */
+                          /* sweep that starts near tol does only what reaching sweep_target * tol    */
+                          /* needs; 0: every sweep reduces by sweep_reduction                          */
 } mw_solve_params;
 
 typedef struct {

@@ -2245,11 +2245,20 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
 // waits for the host.  Every loop is bounded by its iteration cap (max_inner, max_outer,
 // max_refine) and by a total work cap, both decided on the device.  Scalars live in S->sc from
 // slot 64 on.
+// Schur-residual reduction of a refinement sweep that starts at relative residual `rel`: the fixed
+// sweep_reduction, or with target > 0 the smaller reduction target * tol / rel (at most 0.5).
+MW_HD double sweep_target_reduction(double sweep_reduction, double target, double tol, double rel) {
+  if (!(target > 0) || !(rel > 0)) return sweep_reduction;
+  double r = target * tol / rel;
+  if (r > 0.5) r = 0.5;
+  return r > sweep_reduction ? r : sweep_reduction;
+}
+
 enum DevSlot {
   P_RZ = 64, P_PAP, P_RR, P_BB, P_RZN, P_IT,                 // inner PCG
   U_RW = 72, U_DSD, U_RWN, U_RR0, U_RR, U_IT, U_D2, U_Z2,    // Schur CG
   T_RV = 84, T_RP, T_REL,                                     // true residual
-  S_BB = 88, S_BH, S_BNORM, S_REL0, S_NREF,                   // solve
+  S_BB = 88, S_BH, S_BNORM, S_REL0, S_NREF, S_RED,           // solve
   I_OUTER = 96, I_INNER, I_STATUS                             // info
 };
 
@@ -2294,6 +2303,7 @@ __global__ void k_dev_uz_check(double* sc, double reduction, int check_true, dou
   sc[U_IT] = it;
   sc[I_OUTER] += 1;
   const double rr = sc[U_RR];
+  if (reduction < 0) reduction = sc[S_RED];                   // this sweep's target (k_dev_sweep_red)
   bool go = it < (double)max_outer;
   if (!isfinite(rr)) { sc[I_STATUS] = 2; go = false; }
   if (sc[I_OUTER] >= DEV_OUTER_BUDGET && sc[I_STATUS] == 0) sc[I_STATUS] = 3;
@@ -2339,6 +2349,13 @@ __global__ void k_dev_ref_check(double* sc, double tol, int max_refine, cudaGrap
   const double r = sc[T_REL];
   const bool go = isfinite(r) && r > tol && sc[S_NREF] < (double)max_refine && sc[I_STATUS] == 0;
   cudaGraphSetConditional(hw, go ? 1u : 0u);
+}
+
+// the reduction a refinement sweep's Schur iteration aims for: sweep_reduction, or -- with
+// target > 0 -- the smaller reduction that takes the current residual to target * tol
+__global__ void k_dev_sweep_red(double* sc, double sweep_reduction, double target, double tol) {
+  pdl_entry();
+  sc[S_RED] = sweep_target_reduction(sweep_reduction, target, tol, sc[T_REL]);
 }
 
 __global__ void k_copy1(const double* src, double* dst) {
@@ -2547,7 +2564,8 @@ static bool stokes_solve_record(mw_stokes* S, const double* f, const double* h, 
     pdl_launch(k_copy<double, double>, grid_for(np, 256), 256, 0, b, np, S->RP, S->h);
     pdl_launch(k_set<double>, grid_for(nv, 256), 256, 0, b, nv, 0.0, S->cV);
     pdl_launch(k_set<double>, grid_for(np, 256), 256, 0, b, np, 0.0, S->cP);
-    if (!uzawa_dev(S, sp, MW_F32, S->f, S->h, S->cV, S->cP, sp.sweep_reduction, false, s, 1)) return false;
+    pdl_launch(k_dev_sweep_red, 1, 1, 0, b, sc, sp.sweep_reduction, sp.sweep_target, sp.tol);
+    if (!uzawa_dev(S, sp, MW_F32, S->f, S->h, S->cV, S->cP, -1.0, false, s, 1)) return false;
     pdl_launch(k_axpy<double>, grid_for(nv, 256), 256, 0, b, nv, 1.0, S->cV, V);
     pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, b, np, 1.0, S->cP, P);
     true_residual_dev(S, V, P, f, h, b);
@@ -2600,7 +2618,7 @@ void mw_stokes_default_params(mw_stokes_params* p) {
 void mw_solve_default_params(mw_solve_params* p) {
   memset(p, 0, sizeof(*p));
   p->scheme = MW_SCHEME_CD_U_ETA; p->precision = MW_F64; p->tol = 1e-8; p->max_outer = 200;
-  p->max_inner = 500; p->inner_rtol = 1e-10; p->max_refine = 20; p->sweep_reduction = 1e-3;
+  p->max_inner = 500; p->inner_rtol = 1e-10; p->max_refine = 20; p->sweep_reduction = 1e-3; p->sweep_target = 0.0;
   p->mass_iters = 12; p->use_guess = 0;
 }
 
@@ -2865,6 +2883,7 @@ static bool stokes_solve_graph(mw_stokes* S, const double* f, const double* h, d
   key_add(key, sp.tol);
   key_add(key, sp.inner_rtol);
   key_add(key, sp.sweep_reduction);
+  key_add(key, sp.sweep_target);
   std::vector<void*> h32 = vstate(S->H32), h64 = vstate(S->H64);
   key.insert(key.end(), h32.begin(), h32.end());
   key.insert(key.end(), h64.begin(), h64.end());
@@ -3001,7 +3020,8 @@ static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, dou
       pdl_launch(k_set<double>, grid_for(nv, 256), 256, 0, s, nv, 0.0, cV);
       double* cPr = S->cP;
       pdl_launch(k_set<double>, grid_for(np, 256), 256, 0, s, np, 0.0, cPr);
-      rc = uzawa(S, sp, MW_F32, fr, hr, cV, cPr, sp.sweep_reduction, false, 0.0, &inf, s);
+      rc = uzawa(S, sp, MW_F32, fr, hr, cV, cPr, sweep_target_reduction(sp.sweep_reduction, sp.sweep_target, sp.tol, rel),
+                 false, 0.0, &inf, s);
       if (rc) break;
       pdl_launch(k_axpy<double>, grid_for(nv, 256), 256, 0, s, nv, 1.0, cV, solV);
       pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, 1.0, cPr, solP);

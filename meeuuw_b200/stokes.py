@@ -24,7 +24,7 @@ class MwSolveParams(ctypes.Structure):
                 ("max_inner", c_int32), ("inner_rtol", c_double), ("max_refine", c_int32),
                 ("sweep_reduction", c_double), ("mass_iters", c_int32),
                 ("use_guess", c_int32), ("history", c_void_p), ("history_len", c_int32),
-                ("host_loops", c_int32)]
+                ("host_loops", c_int32), ("sweep_target", c_double)]
 
 
 class MwSolveInfo(ctypes.Structure):

@@ -10,7 +10,11 @@
   product path (mixed precision, learned warm start) and of the plain FP64 path, against the
   FP64 oracle's step (``oracle_fk512_step1.npz``, ``make_oracle_golden.py``).
 
-The device solves Stokes to an FP64 relative residual of 1e-8 (the benchmark's tolerance).
+The product path (mixed precision) solves Stokes to an FP64 relative residual of 1e-8, the
+benchmark's tolerance; its refinement sweeps land well below it.  The plain FP64 path stops at the
+first Schur iteration under its tolerance, and on these buoyancy-driven problems a relative
+residual of 1e-8 -- dominated by the hydrostatic part of the load -- still leaves vrms off by up
+to 4e-4 at 32x32 (measured), so the FP64 arm runs at 1e-10 here.
 Bars: vrms, Nu and dt within 1e-6 relative per step; T within 1e-7; u, w, p, q within 1e-6 of
 their maximum (strain rates 1e-4: derivatives); particle element indices, active flags,
 material ids and per-element counts bit-exact; positions within 1e-8.
@@ -34,7 +38,7 @@ def run_gpu(cfg, nsteps, stokes, guess=False):
     from meeuuw_b200 import configs
     from meeuuw_b200.timestep import GPUModel
     host = configs.build_host_model(cfg)
-    gm = GPUModel(cfg, host, stokes=stokes, tol=1e-8)
+    gm = GPUModel(cfg, host, stokes=stokes, tol=1e-8 if stokes == "mixed" else 1e-10)
     if guess:
         from meeuuw_b200.unet import LearnedGuess, UNet
         gm.guess = LearnedGuess(gm, UNet.load(WEIGHTS), judge="cold")

@@ -7,7 +7,8 @@ same function names with the same positional signatures and return tuples:
     build_matrix_energy.build_matrix_energy
     locate_particles.locate_particles
     pic_functions.locate_particles___box, interpolate_field_on_particles, advect_particles___box,
-                  project_particles_on_elements, project_particle_field_on_nodes_{1,2,3,4}
+                  project_particles_on_elements, project_particle_field_on_nodes_{1,2,3,4},
+                  compute_ls_coefficients_P1, compute_ls_coefficients_Q1, population_control
     project_nodal_field_onto_qpoints.project_nodal_{P,V,T}field_onto_qpoints
     uzawa3_solver_L2.uzawa3_solver_L2, cd_u_eta.cd_u_eta
     compute_pressure_offset.compute_pressure_offset
@@ -30,7 +31,8 @@ TABLE = {
     "pic_functions": ["locate_particles___box", "interpolate_field_on_particles", "advect_particles___box",
                       "project_particles_on_elements", "project_particle_field_on_nodes_1",
                       "project_particle_field_on_nodes_2", "project_particle_field_on_nodes_3",
-                      "project_particle_field_on_nodes_4"],
+                      "project_particle_field_on_nodes_4", "compute_ls_coefficients_P1",
+                      "compute_ls_coefficients_Q1", "population_control"],
     "project_nodal_field_onto_qpoints": ["project_nodal_Pfield_onto_qpoints", "project_nodal_Vfield_onto_qpoints",
                                          "project_nodal_Tfield_onto_qpoints"],
     "uzawa3_solver_L2": ["uzawa3_solver_L2"],

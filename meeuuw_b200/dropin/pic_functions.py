@@ -122,3 +122,100 @@ def project_particle_field_on_nodes_4(nel, nn_V, nparticle, swarm_active, swarm_
 __all__ = ["locate_particles___box", "interpolate_field_on_particles", "advect_particles___box",
            "project_particles_on_elements", "project_particle_field_on_nodes_1", "project_particle_field_on_nodes_2",
            "project_particle_field_on_nodes_3", "project_particle_field_on_nodes_4"]
+
+
+# ---------------------------------------------------------------- least squares, population control
+def _ls(order, nel, x_e, z_e, swarm_x, swarm_z, swarm_iel, swarm_rho, swarm_eta):
+    nelx, nelz = _box_of_centres(x_e, z_e, nel)
+    host = host_mode(swarm_x, swarm_rho)
+    n = len(swarm_x)
+    iel = dev(swarm_iel, i32)[:n]
+    every = torch.ones(n, dtype=torch.uint8, device="cuda")        # the reference's mask: swarm_iel == iel
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    counts, offsets, order_ = ops.bin_particles(nel, every, iel, err=err)
+    b = box(nelx, nelz, 2 * float(x_e[0]), 2 * float(z_e[0]))
+    out = ops.ls_fit(b, order, offsets, order_, dev(swarm_x, f64)[:n], dev(swarm_z, f64)[:n],
+                     [dev(swarm_rho, f64)[:n], dev(swarm_eta, f64)[:n]], err=err)
+    if int(err.item()) & L.FLAG_EMPTY_ELEMENT:
+        raise ValueError("least squares fit: an element contains no particle")
+    (cr, rmin, rmax), (ce, emin, emax) = out
+    coefs = [back(cr[:, j].contiguous(), host) for j in range(order)] + \
+            [back(ce[:, j].contiguous(), host) for j in range(order)]
+    return tuple(coefs) + (back(rmin, host), back(rmax, host), back(emin, host), back(emax, host))
+
+
+def _box_of_centres(x_e, z_e, nel):
+    """(nelx, nelz) of a uniform box from its element centres (x_V of node 8)."""
+    xe = x_e.detach().cpu().numpy() if isinstance(x_e, torch.Tensor) else x_e
+    ze = z_e.detach().cpu().numpy() if isinstance(z_e, torch.Tensor) else z_e
+    nelx = int(round(float(xe.max() - xe.min()) / float(2 * xe[0]))) + 1 if nel > 1 else 1
+    if nelx < 1 or nel % nelx:
+        raise NotImplementedError("least squares fits: element centres of a uniform box expected")
+    return nelx, nel // nelx
+
+
+def compute_ls_coefficients_P1(nel, x_e, z_e, swarm_x, swarm_z, swarm_iel, swarm_rho, swarm_eta):
+    """pic_functions.py:1098-1172: (rho a, b, c, eta a, b, c, rho min, max, eta min, max)."""
+    return _ls(3, nel, x_e, z_e, swarm_x, swarm_z, swarm_iel, swarm_rho, swarm_eta)
+
+
+def compute_ls_coefficients_Q1(nel, x_e, z_e, swarm_x, swarm_z, swarm_iel, swarm_rho, swarm_eta):
+    """pic_functions.py:1182-1285: (rho a, b, c, d, eta a, b, c, d, rho min, max, eta min, max)."""
+    return _ls(4, nel, x_e, z_e, swarm_x, swarm_z, swarm_iel, swarm_rho, swarm_eta)
+
+
+def population_control(istep, x_V, z_V, icon_V, nel, nparticle_min, nparticle, nparticle_e, swarm_active, swarm_id,
+                       swarm_iel, swarm_r, swarm_t, swarm_x, swarm_z, swarm_u, swarm_w, swarm_strain, swarm_eta,
+                       swarm_wf, swarm_F, swarm_paint, use_melting, nmat, ptcl_active_file, output_folder):
+    """pic_functions.py:1621-1812 on the device, in place.  The reduced coordinates come from
+    Python's `random` exactly as the reference draws them (random.uniform(-0.95, 0.95), r then t,
+    per added particle); the weight fractions of each new particle are copied from the nearest
+    particle, strain (and melt fraction) averaged over its element, paint set to -1."""
+    import random
+
+    import numpy as np
+    nx, nz = box_dims(icon_V, nel)
+    ne = np.asarray(nparticle_e.detach().cpu().numpy() if isinstance(nparticle_e, torch.Tensor) else nparticle_e)
+    needed = int(np.maximum(0, nparticle_min - ne).sum())
+    print("     -> nparticle_min=", nparticle_min)
+    print("     -> number of needed particles", needed)
+    if needed == 0:
+        print("     -> no population control needed")
+        return
+    act = dev_u8(swarm_active)
+    available = int(nparticle - int(act.sum().item()))
+    ptcl_active_file.write("%d %d %d %d\n" % (istep, nparticle - available, needed, available))
+    ptcl_active_file.flush()
+    if needed > available:
+        raise ValueError("population_control: not available yet")
+    draws = torch.tensor([random.random() for _ in range(2 * needed)], dtype=f64, device="cuda")
+    b = box(nx, nz)
+    iel = dev(swarm_iel, i32)
+    counts, offsets, order = ops.bin_particles(nel, act, iel)      # the mask: active, swarm_iel == iel
+    x, z, r, t = dev(swarm_x, f64), dev(swarm_z, f64), dev(swarm_r, f64), dev(swarm_t, f64)
+    avg = [dev(a, f64) for a in (swarm_eta, swarm_u, swarm_w, swarm_strain)]
+    if use_melting:
+        avg.append(dev(swarm_F, f64))
+    src = torch.full((nparticle,), -1, dtype=torch.int32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ops.population_control(b, int(nparticle_min), dev(ne, i32), offsets, order, act, iel, r, t, x, z, avg=avg,
+                           source=src, draws=draws, err=err)
+    flags = int(err.item())
+    if flags & L.FLAG_POP_MASK_EMPTY:
+        raise ValueError("population_control: mask empty")
+    if flags & L.FLAG_POP_UNAVAILABLE:
+        raise ValueError("population_control: not available yet")
+    new = torch.nonzero(src >= 0).flatten()
+    wf = dev(swarm_wf, f64)
+    wf[:, new] = wf[:, src[new].long()]
+    paint = dev(swarm_paint)
+    paint[new] = -1
+    for dst, s in ((swarm_active, act), (swarm_iel, iel), (swarm_r, r), (swarm_t, t), (swarm_x, x), (swarm_z, z),
+                   (swarm_eta, avg[0]), (swarm_u, avg[1]), (swarm_w, avg[2]), (swarm_strain, avg[3]),
+                   (swarm_wf, wf), (swarm_paint, paint)):
+        copy_into(dst, s)
+    if use_melting:
+        copy_into(swarm_F, avg[4])
+
+
+__all__ += ["compute_ls_coefficients_P1", "compute_ls_coefficients_Q1", "population_control"]

@@ -134,3 +134,47 @@ def test_population_control_errors(M):
                            a["swarm_iel"], a["swarm_r"], a["swarm_t"], a["swarm_x"], a["swarm_z"], err=err,
                            draws=D(np.tile(g["draws"], 8)))
     assert int(err.item()) & _lib.FLAG_POP_MASK_EMPTY
+
+
+def test_dropin_ls_coefficients_match_reference(M):
+    """The drop-ins under the reference's names, with host (numpy) arrays in and out."""
+    from meeuuw_b200.dropin import pic_functions as pf
+    g = golden("lsq")
+    P1 = pf.compute_ls_coefficients_P1(24, g["x_e"], g["z_e"], g["swarm_x"], g["swarm_z"], g["swarm_iel"],
+                                       g["swarm_rho"], g["swarm_eta"])
+    names = ("rho_a", "rho_b", "rho_c", "eta_a", "eta_b", "eta_c", "rho_min", "rho_max", "eta_min", "eta_max")
+    for v, k in zip(P1, names):
+        assert isinstance(v, np.ndarray) and rel_err(v, g["out_P1_" + k]) < 1e-12, k
+    Q1 = pf.compute_ls_coefficients_Q1(24, g["x_e"], g["z_e"], g["swarm_x"], g["swarm_z"], g["swarm_iel"],
+                                       g["swarm_rho"], g["swarm_eta"])
+    names = ("rho_a", "rho_b", "rho_c", "rho_d", "eta_a", "eta_b", "eta_c", "eta_d", "rho_min", "rho_max",
+             "eta_min", "eta_max")
+    for v, k in zip(Q1, names):
+        assert rel_err(v, g["out_Q1_" + k]) < 1e-12, k
+
+
+def test_dropin_population_control_matches_reference(M):
+    """Same arguments, same random draws (random.seed), same in-place results as the reference."""
+    import io
+    import random
+    from meeuuw_b200.dropin import pic_functions as pf
+    g = golden("population")
+    n = len(g["swarm_x"])
+    a = {k: g[k].copy() for k in ("swarm_active", "swarm_iel", "swarm_r", "swarm_t", "swarm_x", "swarm_z",
+                                  "swarm_u", "swarm_w", "swarm_eta")}
+    wf = np.zeros((2, n))
+    wf[g["swarm_mat"], np.arange(n)] = 1.0
+    paint = np.zeros(n, dtype=np.int32)
+    log = io.StringIO()
+    random.seed(77)
+    pf.population_control(1, M["x_V"], M["z_V"], M["icon_V"], 24, 7, n, g["nparticle_e"], a["swarm_active"],
+                          np.arange(n), a["swarm_iel"], a["swarm_r"], a["swarm_t"], a["swarm_x"], a["swarm_z"],
+                          a["swarm_u"], a["swarm_w"], np.zeros(n), a["swarm_eta"], wf, np.zeros(n), paint, False, 2,
+                          log, "")
+    for k in ("swarm_active", "swarm_iel", "swarm_r", "swarm_t"):
+        assert np.array_equal(a[k], g["out_" + k]), k
+    for k in ("swarm_x", "swarm_z", "swarm_u", "swarm_w", "swarm_eta"):
+        assert rel_err(a[k], g["out_" + k]) < 1e-14, k
+    assert np.array_equal(np.argmax(wf, axis=0), g["out_swarm_mat"])
+    assert (paint == -1).sum() == int(g["needed"])
+    assert log.getvalue().split()[2] == str(int(g["needed"]))

@@ -51,6 +51,32 @@ class StepConfig:
     formulation: str = "BA"
     nstep: int = 20
     seed: int = 0
+    # qpoint density / viscosity from the particles (meeuuw.py:1503-1562): "elemental" (element
+    # means) or the least-squares fits "least_squares_P1" (with the slope limiter) / "least_squares_Q1"
+    particle_rho_projection: str = "elemental"
+    particle_eta_projection: str = "elemental"
+    # population control after advection (pic_functions.py:1621-1812); 0 -> the reference's default
+    # int(0.85 nparticle_per_dim^2) (set_default_parameters.py:112)
+    allow_population_control: bool = False
+    nparticle_min: int = 0
+
+    @property
+    def nmin(self):
+        return self.nparticle_min if self.nparticle_min > 0 else int(self.nparticle_per_dim ** 2 * 0.85)
+
+    @property
+    def ls_order(self):
+        """3 (P1) or 4 (Q1) when a least-squares projection is used, else 0 (meeuuw.py:1225-1297)."""
+        p = (self.particle_rho_projection, self.particle_eta_projection)
+        if "least_squares_P1" in p:
+            return 3
+        if "least_squares_Q1" in p:
+            return 4
+        return 0
+
+    def population_seed(self, istep):
+        """Key of the device generator that draws population control's reduced coordinates."""
+        return (self.seed * 1000003 + istep) & 0xFFFFFFFFFFFFFFFF
 
     @property
     def nel(self):

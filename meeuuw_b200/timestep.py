@@ -96,6 +96,16 @@ class GPUModel:
         # Schur complement leave the outer iteration counts of the FK step unchanged (vs 12)
         self.solve_kw = dict(mass_iters=6)
         self.graph = None      # recorded time step (capture_step)
+        if cfg.ls_order:       # least-squares projections: qpoint coordinates, bins of every particle
+            xV = torch.as_tensor(host.x_V, dtype=f64, device=device)
+            zV = torch.as_tensor(host.z_V, dtype=f64, device=device)
+            self.xq, self.zq = E(nel, 9), E(nel, 9)
+            ops.nodal_to_qpoints(box, L.SPACE_Q2, self.tables["N_V"], xV, self.xq)
+            ops.nodal_to_qpoints(box, L.SPACE_Q2, self.tables["N_V"], zV, self.zq)
+            self.every = torch.ones(npart, dtype=torch.uint8, device=device)
+            self.ls_bins = (E(nel, dt=torch.int32), E(nel + 1, dt=torch.int32), E(npart, dt=torch.int32))
+        if cfg.allow_population_control:
+            self.pc_added = Z(1, dt=torch.int32)
         self._replayed = False
         self._capturing = False
         ops.locate(box, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
@@ -137,6 +147,9 @@ class GPUModel:
         whose hook is not idle runs eagerly, with the hook, and later idle steps replay again."""
         if self.guess is not None and not self._guess_idle():
             raise ValueError("a Stokes guess hook that is not idle runs device work and cannot be recorded")
+        if self.cfg.allow_population_control:
+            # the generator key of population control changes every step; a record would freeze it
+            raise ValueError("steps with population control run eagerly (their random draws are keyed by the step)")
         if self.istep == 0:
             self.step()
         torch.cuda.synchronize()
@@ -186,9 +199,18 @@ class GPUModel:
             ops.project_nodes(b, 2, [(P[k], "arithmetic") for k in ("hcond", "hcapa", "hprod", "alpha")],
                               self.offsets, self.order, self.r, self.t, [nd[k] for k in ("hcond", "hcapa", "hprod",
                                                                                         "alpha")])
-        # qpoint fields (meeuuw.py:1503-1590, "elemental" rho/eta)
+        # qpoint fields (meeuuw.py:1503-1590, "elemental" rho/eta, or the least-squares fits)
         qf = self.qf
         ops.elemental_to_qpoints(self.rho_e, self.eta_e, qf["rhoq"], qf["etaq"])
+        if c.ls_order:                                                   # meeuuw.py:1225-1297
+            cnt, off, order = self.ls_bins
+            ops.bin_particles(self.nel, self.every, self.iel, cnt, off, order, self.err)
+            (cr, _, _), (ce, _, _) = ops.ls_fit(b, c.ls_order, off, order, self.x, self.z, [P["rho"], P["eta"]],
+                                                limit_h=b.hx if c.ls_order == 3 else 0.0, err=self.err)
+            if c.particle_rho_projection.startswith("least_squares"):
+                ops.ls_to_qpoints(b, cr, self.xq, self.zq, qf["rhoq"])
+            if c.particle_eta_projection.startswith("least_squares"):
+                ops.ls_to_qpoints(b, ce, self.xq, self.zq, qf["etaq"])
         if c.solve_T:
             ops.nodal_to_qpoints(b, L.SPACE_Q2, tb["N_V"], self.T, qf["Tq"])
             for k in ("hcapa", "hcond", "hprod", "alpha"):
@@ -248,6 +270,10 @@ class GPUModel:
         # advect and locate (meeuuw.py:2726, 2862)
         ops.advect(b, c.RKorder, 0.0, self.x, self.z, self.active, self.u, self.w, self.up, self.wp, self.err,
                    dt_dev=self.dt_out)
+        if c.allow_population_control and c.RKorder > 0:                 # meeuuw.py:2846-2850
+            ops.population_control(b, c.nmin, self.counts, self.offsets, self.order, self.active, self.iel, self.r,
+                                   self.t, self.x, self.z, mat=self.mat, avg=(P["eta"], self.up, self.wp),
+                                   seed=c.population_seed(self.istep), added=self.pc_added, err=self.err)
         ops.locate(b, self.active, self.x, self.z, self.r, self.t, self.iel, self.err)
         self._mark("end")
         self.istep += 1
@@ -277,3 +303,7 @@ class GPUModel:
             raise SystemExit("t value out of bounds")                             # locate_particles.py:63-64
         if err & L.FLAG_ELEMENT_RANGE:
             raise SystemExit("particle outside the mesh")
+        if err & L.FLAG_POP_UNAVAILABLE:
+            raise ValueError("population_control: not available yet")          # pic_functions.py:1722-1733
+        if err & L.FLAG_POP_MASK_EMPTY:
+            raise ValueError("population_control: mask empty")                  # pic_functions.py:1747-1748

@@ -145,3 +145,15 @@ def population_control(x_V, z_V, icon_V, nel, nparticle_min, nparticle_e, swarm_
             swarm_w[pid] = avg_w
             counter += 1
     return counter
+
+
+def splitmix_u01(seed, n):
+    """The device generator of population control (k_pc_fill's splitmix_u01): n uniform [0, 1)
+    numbers for key `seed`, the k-th from the SplitMix64 finaliser of seed + (k + 1) * golden."""
+    with np.errstate(over="ignore"):
+        k = np.arange(n, dtype=np.uint64)
+        z = np.uint64(seed) + (k + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)

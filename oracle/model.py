@@ -14,7 +14,7 @@ import time
 
 import numpy as np
 
-from . import assembly, pic, post, solvers
+from . import assembly, lsq, pic, post, solvers
 from .fe import BoxMesh
 
 
@@ -98,6 +98,17 @@ class OracleModel:
         out["eta_n"] = proj(eta, c.averaging)
         rhoq = np.repeat(rho_e[:, None], 9, axis=1)                      # "elemental", meeuuw.py:1512
         etaq = np.repeat(eta_e[:, None], 9, axis=1)
+        if c.ls_order:                                                   # meeuuw.py:1225-1297, 1517-1562
+            x_e, z_e = m.x_V[m.icon_V[8]], m.z_V[m.icon_V[8]]
+            coefs, fmin, fmax = lsq.ls_coefficients(c.ls_order, m.nel, x_e, z_e, self.x, self.z, self.iel,
+                                                    [rho, eta])
+            if c.ls_order == 3:
+                coefs = [lsq.limit_p1(cf, lo, hi, m.hx) for cf, lo, hi in zip(coefs, fmin, fmax)]
+            out.update(ls_rho=coefs[0], ls_eta=coefs[1])
+            if c.particle_rho_projection.startswith("least_squares"):
+                rhoq = lsq.ls_to_qpoints(coefs[0], m.xq, m.zq, x_e, z_e)
+            if c.particle_eta_projection.startswith("least_squares"):
+                etaq = lsq.ls_to_qpoints(coefs[1], m.xq, m.zq, x_e, z_e)
         if c.solve_T:
             hcond_n = proj(hcond, None)
             hcapa_n = proj(hcapa, None)
@@ -181,8 +192,14 @@ class OracleModel:
         vrms, Tavrg, _ = post.compute_global_quantities(uq, wq, Tq_new, rhoq, m.JxWq, m.volume)
         out.update(vrms=vrms, Nu=Nu, exx_n=self.exx_n.copy())
         mark("heat flux, Nu, strain rate, vrms")
-        pic.advect_particles___box(c.RKorder, dt, n, self.x, self.z, self.active, u, w, m.Lx, m.Lz,
-                                   m.hx, m.hz, m.nelx, m.icon_V, m.x_V, m.z_V)
+        _, _, up, wp, _ = pic.advect_particles___box(c.RKorder, dt, n, self.x, self.z, self.active, u, w, m.Lx,
+                                                     m.Lz, m.hx, m.hz, m.nelx, m.icon_V, m.x_V, m.z_V)
+        if c.allow_population_control and c.RKorder > 0:                # meeuuw.py:2846-2850
+            need = int(np.maximum(0, c.nmin - cnt).sum())
+            draws = lsq.splitmix_u01(c.population_seed(self.istep), 2 * need)
+            out["population_added"] = lsq.population_control(
+                m.x_V, m.z_V, m.icon_V, m.nel, c.nmin, cnt, self.active, self.iel, self.r, self.t, self.x, self.z,
+                up, wp, eta, self.mat, draws)
         self.r, self.t, self.iel = pic.locate_particles___box(
             n, self.active, self.x, self.z, m.hx, m.hz, m.x_V, m.z_V, m.icon_V, m.nelx)
         if not pic.locate_bounds_ok(self.r, self.t):

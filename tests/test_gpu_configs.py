@@ -10,11 +10,12 @@
   product path (mixed precision, learned warm start) and of the plain FP64 path, against the
   FP64 oracle's step (``oracle_fk512_step1.npz``, ``make_oracle_golden.py``).
 
-The product path (mixed precision) solves Stokes to an FP64 relative residual of 1e-8, the
-benchmark's tolerance; its refinement sweeps land well below it.  The plain FP64 path stops at the
-first Schur iteration under its tolerance, and on these buoyancy-driven problems a relative
-residual of 1e-8 -- dominated by the hydrostatic part of the load -- still leaves vrms off by up
-to 4e-4 at 32x32 (measured), so the FP64 arm runs at 1e-10 here.
+Against the reference's driver (direct solves) both arms solve Stokes to an FP64 relative residual
+of 1e-10: these tests check the composition of the step, and on these buoyancy-driven problems a
+relative residual of 1e-8 -- a norm dominated by the hydrostatic part of the load -- still leaves
+vrms off by 3e-6 (mixed, 16x16 FK cold start) to 4e-4 (FP64, which stops at the first iterate under
+the tolerance) on the small meshes (measured).  The 512x512 test runs the product path at the
+benchmark's own 1e-8 and holds it to the 1e-6 bar.
 Bars: vrms, Nu and dt within 1e-6 relative per step; T within 1e-7; u, w, p, q within 1e-6 of
 their maximum (strain rates 1e-4: derivatives); particle element indices, active flags,
 material ids and per-element counts bit-exact; positions within 1e-8.
@@ -34,11 +35,11 @@ WEIGHTS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
                        "unet_fk128.npz")
 
 
-def run_gpu(cfg, nsteps, stokes, guess=False):
+def run_gpu(cfg, nsteps, stokes, guess=False, tol=1e-10):
     from meeuuw_b200 import configs
     from meeuuw_b200.timestep import GPUModel
     host = configs.build_host_model(cfg)
-    gm = GPUModel(cfg, host, stokes=stokes, tol=1e-8 if stokes == "mixed" else 1e-10)
+    gm = GPUModel(cfg, host, stokes=stokes, tol=tol)
     if guess:
         from meeuuw_b200.unet import LearnedGuess, UNet
         gm.guess = LearnedGuess(gm, UNet.load(WEIGHTS), judge="cold")
@@ -47,7 +48,7 @@ def run_gpu(cfg, nsteps, stokes, guess=False):
         gm.step()
         d = gm.diagnostics()
         gm.check()
-        assert d["stokes"]["converged"] == 1
+        assert d["stokes"]["converged"] == 1, d["stokes"]
         steps.append((d["vrms"], d["Nu"], d["dt"]))
     return gm, steps
 
@@ -120,7 +121,8 @@ def test_config1_fk512_first_step_vs_fp64_oracle(arm):
     d = golden("oracle_fk512_step1")
     meta = json.loads(str(d["meta"]))
     cfg = configs.fk_convection(meta["n"], seed=meta["seed"])
-    gm, steps = run_gpu(cfg, 1, "mixed" if arm == "product" else "f64", guess=(arm == "product"))
+    gm, steps = run_gpu(cfg, 1, "mixed" if arm == "product" else "f64", guess=(arm == "product"),
+                        tol=1e-8 if arm == "product" else 1e-10)
     vrms, nu, dt = steps[0]
     assert abs(vrms / d["vrms"] - 1) < 1e-6, (vrms, float(d["vrms"]))
     assert abs(nu / d["Nu"] - 1) < 1e-6, (nu, float(d["Nu"]))

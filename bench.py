@@ -40,6 +40,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="skip the torch-profiler launch count")
     ap.add_argument("--roofline-only", action="store_true", help="set up the model, time the operator apply, exit")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="set up the model, run the warm-up steps, time the particle kernels and the FP32 assembly, exit")
     ap.add_argument("--host-loops", action="store_true",
                     help="solver loops driven from the host (same kernels; lets a kernel profiler list every launch)")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -148,6 +150,14 @@ def run_ours(args):
         from meeuuw_b200 import fe_tables
         model.solver.set_viscosity(torch.ones(model.nel, 9, dtype=torch.float64, device="cuda"), None)
         print(json.dumps({"roofline": roofline_apply(model, torch)}), flush=True)
+        return
+    if args.kernels_only:
+        for _ in range(args.warmup):
+            model.step()
+        model.check()
+        roof = roofline_apply(model, torch)
+        print(json.dumps({"roofline": roof, "kernel_rooflines": kernel_rooflines(model, torch, roof["peak"])}),
+              flush=True)
         return
     dev_index = torch.cuda.current_device()
     with ClockSampler(dev_index) as clk:

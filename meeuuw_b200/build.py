@@ -22,6 +22,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-I", os.path.join(ROOT, "include")]
 NO_FMA = {"pic.cu"}
+# extra nvcc flags for measurements (e.g. MW_NVCC_FLAGS="-DMW_APPLY_MINB=6"); empty by default
+EXTRA = os.environ.get("MW_NVCC_FLAGS", "").split()
 
 
 def nvcc():
@@ -39,9 +41,9 @@ def _compile(src, verbose):
     obj = os.path.join(BUILD, src[:-3] + ".o")
     dep = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
     dep.append(os.path.join(ROOT, "include", "meeuuw_b200.h"))
-    if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in dep):
+    if not EXTRA and os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in dep):
         return obj
-    cmd = [nvcc()] + ARCH + COMMON + (["-fmad=false"] if src in NO_FMA else []) + \
+    cmd = [nvcc()] + ARCH + COMMON + EXTRA + (["-fmad=false"] if src in NO_FMA else []) + \
         ["-c", os.path.join(CSRC, src), "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
@@ -58,7 +60,7 @@ def build(verbose=False):
     os.makedirs(BUILD, exist_ok=True)
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), sources()))
-    if os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
+    if not EXTRA and os.path.exists(LIB) and all(os.path.getmtime(LIB) >= os.path.getmtime(o) for o in objs):
         return LIB
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lcuda"]
     r = subprocess.run(cmd, capture_output=True, text=True)

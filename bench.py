@@ -362,7 +362,9 @@ def kernel_rooflines(model, torch, peak_gbs):
 def step1_vs_oracle(torch, weights):
     """Both arms' first step of the 512x512 model (seed 1000) against the FP64 oracle's first step
     (tests/golden/oracle_fk512_step1.npz: the oracle restating the reference, cd_u_eta with SuperLU):
-    relative vrms, Nu and dt errors and the largest T error on the stored nodes."""
+    relative vrms, Nu and dt errors and the largest T error on the stored nodes.  The first step is
+    a cold start, so the product path's learned guess (the U-Net on the pooled 128x128 fields) is
+    measured here against the same path started from zero (Schur / multigrid-PCG iterations, time)."""
     import numpy as np
 
     from meeuuw_b200 import configs
@@ -376,19 +378,28 @@ def step1_vs_oracle(torch, weights):
     host = configs.build_host_model(cfg)
     out = {"oracle": {"vrms": float(d["vrms"]), "Nu": float(d["Nu"]), "solver": meta["solver"],
                       "stokes_relative_residual": float(d["stokes_residual"])}}
-    for arm in ("product", "plain_fp64"):
-        m = GPUModel(cfg, host, stokes="mixed" if arm == "product" else "f64", tol=1e-8)
+    for arm in ("product", "product_zero_guess", "plain_fp64"):
+        m = GPUModel(cfg, host, stokes="f64" if arm == "plain_fp64" else "mixed", tol=1e-8)
         if arm == "product" and weights:
             from meeuuw_b200.unet import LearnedGuess, UNet
             m.guess = LearnedGuess(m, UNet.load(weights), judge="cold")
+        if arm == "product_zero_guess":
+            m.warm_start = "zero"
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         m.step()
+        e1.record()
         dd = m.diagnostics()
         T = m.T.cpu().numpy()[d["nodes"]]
         out[arm] = {"vrms_rel_err": abs(dd["vrms"] / float(d["vrms"]) - 1),
                     "Nu_rel_err": abs(dd["Nu"] / float(d["Nu"]) - 1),
                     "dt_rel_err": abs(dd["dt"] / float(d["dt"]) - 1), "T_max_abs_err": float(np.abs(T - d["T"]).max()),
                     "stokes_outer_iters": dd["stokes"].get("outer_iters"),
-                    "stokes_inner_iters": dd["stokes"].get("inner_iters")}
+                    "stokes_inner_iters": dd["stokes"].get("inner_iters"),
+                    "first_step_ms": e0.elapsed_time(e1)}
+        if arm == "product" and weights:
+            out[arm]["warm_start_pick"] = dict(m.guess.picks)
         del m
         torch.cuda.empty_cache()
     return out

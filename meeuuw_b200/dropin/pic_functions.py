@@ -189,7 +189,11 @@ def population_control(istep, x_V, z_V, icon_V, nel, nparticle_min, nparticle, n
     if needed > available:
         raise ValueError("population_control: not available yet")
     draws = torch.tensor([random.random() for _ in range(2 * needed)], dtype=f64, device="cuda")
-    b = box(nx, nz)
+    xv = x_V.detach().cpu().numpy() if isinstance(x_V, torch.Tensor) else np.asarray(x_V)
+    zv = z_V.detach().cpu().numpy() if isinstance(z_V, torch.Tensor) else np.asarray(z_V)
+    hx, hz = 2 * float(xv[1] - xv[0]), 2 * float(zv[2 * nx + 1] - zv[0])   # x-fastest Q2 lattice
+    check_coords(x_V, z_V, nx, nz, hx, hz)
+    b = box(nx, nz, hx, hz)
     iel = dev(swarm_iel, i32)
     counts, offsets, order = ops.bin_particles(nel, act, iel)      # the mask: active, swarm_iel == iel
     x, z, r, t = dev(swarm_x, f64), dev(swarm_z, f64), dev(swarm_r, f64), dev(swarm_t, f64)

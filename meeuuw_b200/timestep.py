@@ -34,10 +34,12 @@ class GPUModel:
         self.volume = cfg.Lx * cfg.Lz
         self.stokes_precision, self.scheme, self.tol, self.warm_start = stokes, scheme, tol, warm_start
         # inner multigrid-PCG tolerance: loose under FP64 refinement (mixed; 2e-2 is the fastest
-        # setting whose vrms stays within 1e-7 of the FP64 solve at 512x512), tight without it (the
-        # reference's inner solves are direct, cd_u_eta.py:29,50; the FP64 Schur iteration also
-        # needs accurate inner solves to converge from a cold start)
-        self.inner_rtol = inner_rtol if inner_rtol is not None else (2e-2 if stokes == "mixed" else 1e-10)
+        # setting whose vrms stays within 1e-7 of the FP64 solve at 512x512); without refinement
+        # (plain FP64) the loosest setting with which the Schur iteration converges on every step,
+        # the cold start included: on the 512x512 FK model 1e-9 does (93 ms per warm step, 97 at
+        # 1e-10), 1e-8 ... 1e-7 stall at the first step (200 Schur iterations, residual ~1e-8 to
+        # 1e-7) although they would be faster on warm steps (86 ... 77 ms) (measured)
+        self.inner_rtol = inner_rtol if inner_rtol is not None else (2e-2 if stokes == "mixed" else 1e-9)
         D = lambda a, dt=None: torch.as_tensor(a, dtype=dt).to(device).contiguous()
         self.tables = fe_tables.device_tables(device)
         self.geo = fe_tables.uniform_geometry(nel, box.hx, box.hz, device)

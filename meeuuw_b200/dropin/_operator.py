@@ -39,7 +39,10 @@ class Operator:
         S = _solvers.get(key)
         if S is None:
             precs = ("f32",) if precision == "mixed" else ("f64",)
-            S = StokesSolver(self.box, self.fix, eta_ref=self.eta_ref, L_ref=self.L_ref, precisions=precs)
+            # the time stepper's smoothing settings per arithmetic (meeuuw_b200/timestep.py)
+            S = StokesSolver(self.box, self.fix, eta_ref=self.eta_ref, L_ref=self.L_ref, precisions=precs,
+                             cheb_degree=2 if precision == "mixed" else 1,
+                             power_iters_warm=6 if precision == "mixed" else 3)
             _solvers.clear()          # one operator size at a time keeps the device memory bounded
             _solvers[key] = S
         if getattr(S, "_op", None) is not self:

@@ -595,11 +595,28 @@ def run_ensemble(args):
         ens.close()
         del ens
         torch.cuda.empty_cache()
-        ens = Ensemble(cfgs, stokes="mixed", graphs=True)      # one eager step per model, then capture
+        # recorded steps; every model's cold first step runs eagerly with its learned guess (models whose
+        # grid the network cannot take start from zero), then the step is recorded
+        guess, nguess = None, [0]
+        wpath = os.path.join(ROOT, "meeuuw_b200", "weights", "unet_fk128.npz")
+        if os.path.exists(wpath):
+            from meeuuw_b200.unet import LearnedGuess, UNet
+            net = UNet.load(wpath)
+
+            def guess(m):
+                try:
+                    g = LearnedGuess(m, net, judge="cold")
+                except ValueError:
+                    return None
+                nguess[0] += 1
+                return g
+        ens = Ensemble(cfgs, stokes="mixed", graphs=True, guess=guess)
+        cold_learned = ens.first_step_info
         ms, n = timed(ens)
         modes["graphs"] = {"model_steps_per_s": n / (ms / 1000.0), "ms_per_step": ms / args.steps}
     diag = ens.diagnostics()
     mixed = [d["vrms"] for d in diag]
+    have_guess = [m.guess is not None for m in ens.models]
     converged = sum(1 for i, d in enumerate(diag) if ens.active[i] and d["stokes"]["converged"] == 1)
     active = list(ens.active)
     retired = dict(ens.retired)
@@ -619,6 +636,18 @@ def run_ensemble(args):
         ref.close()
         torch.cuda.empty_cache()
         return out
+    # the same models' cold starts from zero (mixed), for the learned guess's gain
+    ens0 = Ensemble(cfgs, stokes="mixed", graphs=True)
+    cold_zero = ens0.first_step_info
+    ens0.close()
+    del ens0
+    torch.cuda.empty_cache()
+    sel = [i for i in range(len(cfgs)) if have_guess[i]]
+    cold = {"models_with_learned_guess": len(sel), "models": len(cfgs),
+            "schur_iters_learned": sum(cold_learned[i]["outer_iters"] for i in sel),
+            "schur_iters_zero": sum(cold_zero[i]["outer_iters"] for i in sel),
+            "pcg_iters_learned": sum(cold_learned[i]["inner_iters"] for i in sel),
+            "pcg_iters_zero": sum(cold_zero[i]["inner_iters"] for i in sel)}
     fp64, act64 = fp64_run(1e-8)
     tight, act_t = fp64_run(1e-10)
     both = [i for i in range(len(cfgs)) if active[i] and act64[i] and act_t[i]]
@@ -646,6 +675,7 @@ def run_ensemble(args):
             "modes": modes,
             "models_retired": retired,
             "stokes_converged_models": converged,
+            "cold_start_first_step": cold,
             "vrms_rel_err_vs_fp64_1e-10": {"models": len(err), "max": err[-1] if err else None,
                                            "median": err[len(err) // 2] if err else None,
                                            "p90": err[int(0.9 * (len(err) - 1))] if err else None},

@@ -50,10 +50,15 @@ class Ensemble:
 
     def __init__(self, cfgs, stokes="mixed", threads=8, tol=1e-8, guess=None, graphs=False):
         """graphs=True records each model's whole time step as one CUDA graph (after one eager
-        step); a step of the ensemble is then one graph launch per model, issued from one thread."""
+        step); a step of the ensemble is then one graph launch per model, issued from one thread.
+        guess: a factory model -> Stokes guess hook (e.g. unet.LearnedGuess, consulted at the cold
+        start); with graphs the cold first step runs eagerly with the hook, then the step is
+        recorded (the hook is idle from then on).  first_step_info holds each model's first-step
+        solver statistics when that step ran here."""
         self.cfgs = list(cfgs)
         self.streams, self.models = [], []
-        self.graphs = bool(graphs) and guess is None
+        self.graphs = bool(graphs)
+        self.first_step_info = []
         for cfg in self.cfgs:
             st = torch.cuda.Stream()
             with torch.cuda.stream(st):
@@ -61,13 +66,18 @@ class Ensemble:
                 if guess is not None:
                     m.guess = guess(m)
                 if self.graphs:
+                    m.step()                      # the cold start (with the hook, if any)
+                    self.first_step_info.append(dict(m.last_solve))
                     m.capture_step()
             self.streams.append(st)
             self.models.append(m)
         torch.cuda.synchronize()
+        if self.graphs:
+            self.steps_done = len(self.models)
         self.active = [True] * len(self.models)
         self.retired = {}            # model index -> the reference's abort message
-        self.steps_done = 0          # model-steps taken by active models
+        if not self.graphs:
+            self.steps_done = 0      # model-steps taken by active models
         self.threads = 0
         self.pool = None
         self.set_threads(threads)

@@ -381,6 +381,11 @@ class WarmStart:
         self.pscale, self.ghyd = pressure_scales(Ra, alphaT, rho0, s)
         self.f = max(1, box.nelx // n_net)
         self.gx, self.gz = box.nelx // self.f, box.nelz // self.f
+        # the network halves the grid three times and concatenates the skips after upsampling, so
+        # the grid it sees must divide by 8; the pooling factor must divide the mesh
+        if box.nelx % self.f or box.nelz % self.f or self.gx % 8 or self.gz % 8:
+            raise ValueError(f"a {box.nelx}x{box.nelz} mesh maps to a {self.gx}x{self.gz} network grid; the "
+                             f"network needs multiples of 8 (and the pooling factor {self.f} to divide the mesh)")
         self.fix = bc_fix_V.view(torch.uint8) if bc_fix_V.dtype == torch.bool else bc_fix_V
         self.stats = torch.empty(2, dtype=torch.float64, device="cuda")
         self.scales = torch.empty(2, dtype=torch.float64, device="cuda")

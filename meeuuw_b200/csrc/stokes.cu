@@ -2610,7 +2610,12 @@ void mw_stokes_default_params(mw_stokes_params* p) {
   memset(p, 0, sizeof(*p));
   p->eta_ref = 1.0; p->L_ref = 1.0; p->precisions = 3;
   p->coarse_min = 4; p->dense_max = 700; p->cheb_degree = 2; p->cheb_ratio = 8.0; p->cheb_safety = 1.1;
-  p->power_iters = 12;
+  // 40 cold power iterations: with 12 the lambda_max estimate of the RT set-up's K (no slip top and
+  // bottom, 0.9142 x 1 box) came out low enough on the 128x128 and 256x256 levels that the Chebyshev
+  // smoother amplified the top of the spectrum and multigrid-PCG stalled (500 iterations); with 40
+  // it converges in 6 (FP64) / 16 (mixed) Schur iterations from a cold start (measured).  The
+  // warm-started updates of later viscosities keep their own count.
+  p->power_iters = 40;
   p->power_iters_warm = 3;
   p->tail_nel = 0;
 }

@@ -18,7 +18,7 @@ def pair(cfg, nsteps, pool_every=0):
     if pool_every:                               # a pool of inactive particles population control can reuse
         host.arrays["swarm_active"][::pool_every] = False
     om = OracleModel(cfg, host)
-    gm = GPUModel(cfg, host, stokes="mixed", tol=1e-8)
+    gm = GPUModel(cfg, host, stokes="mixed", tol=1e-10)     # parity of the step, not of the tolerance
     outs = []
     for _ in range(nsteps):
         o = om.step()

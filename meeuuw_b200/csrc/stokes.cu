@@ -124,7 +124,10 @@ constexpr int APPLY_THREADS = 160;
 
 // AM_CHEB_Z: the second Chebyshev step of a sweep from a zero guess with the first one folded in:
 // the velocity staged is x0 = (1/theta) D^-1 b (the first step's x and d), computed on the fly
-enum ApplyMode { AM_APPLY = 0, AM_RESID = 1, AM_CHEB = 2, AM_CHEB_Z = 3 };
+// AM_CHEB_P: the first Chebyshev step after the coarse-grid correction with the prolongation folded
+// in: the velocity staged is x + P x_c (free dofs), computed from a staged tile of the coarse
+// correction with the taps and rounding of k_prolong_add, so the V-cycle needs no prolongation launch.
+enum ApplyMode { AM_APPLY = 0, AM_RESID = 1, AM_CHEB = 2, AM_CHEB_Z = 3, AM_CHEB_P = 4 };
 
 template <typename R> struct Vec2;
 template <> struct Vec2<float> { typedef float2 T; };
@@ -146,6 +149,8 @@ struct ApplyArgs {
   R* xo;
   const double* cheb; // device coefficients {c1, c2}
   const double* cheb0;// AM_CHEB_Z: the first step's pair {0, 1/theta}
+  const R* xc;        // AM_CHEB_P: the coarse correction (interleaved u, w) ...
+  LevelGeo gc;        // ... on this coarse level
 };
 
 // Element contribution of K u_el + G p_el and G^T u_el at the 9 Gauss points: strain rate B u
@@ -255,6 +260,45 @@ MW_D int q2_local_idx(int dx, int dz) {
   return dx == 0 ? 3 : (dx == 1 ? 6 : 2);
 }
 
+// 1D Q2 prolongation: fine node i from coarse nodes
+MW_D int pw(int i, int* J, double* w) {
+  if (!(i & 1)) { J[0] = i / 2; w[0] = 1.0; return 1; }
+  int E = i / 4;
+  J[0] = 2 * E; J[1] = 2 * E + 1; J[2] = 2 * E + 2;
+  if ((i & 3) == 1) { w[0] = 0.375; w[1] = 0.75; w[2] = -0.125; }
+  else { w[0] = -0.125; w[1] = 0.75; w[2] = 0.375; }
+  return 3;
+}
+
+// (P x_c) at fine lattice node (ix, iz): the taps summed in double in a fixed order (z outer, x
+// inner) with explicit fused multiply-adds, so every path that prolongs (the prolongation kernel,
+// the cluster tail, the Chebyshev step with the prolongation folded in) rounds alike.
+// coarse(Jz, Jx) returns the coarse node's (u, w) pair.
+template <typename V>
+MW_D void prolong_taps(int ix, int iz, const V& coarse, double* s0, double* s1) {
+  int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
+  double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
+  const int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
+  double a0 = 0, a1 = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      if (a < nzw && b < nxw) {
+        const auto v = coarse(Jz[a], Jx[b]);
+        const double w = wz[a] * wx[b];
+        a0 = fma(w, (double)v.x, a0);
+        a1 = fma(w, (double)v.y, a1);
+      }
+  *s0 = a0;
+  *s1 = a1;
+}
+
+// the coarse-correction tile the AM_CHEB_P staging reads: coarse lattice nodes [ex0 - 2, ex0 + 17]
+// x [ez0 - 2, ez0 + 9] cover every tap of the staged fine nodes [2 ex0 - 2, 2 ex0 + 32] x
+// [2 ez0 - 2, 2 ez0 + 16]
+constexpr int CLX = 20, CLZ = 12;
+
 #ifndef MW_APPLY_MINB
 #define MW_APPLY_MINB 5      // resident FP32 apply CTAs per SM the register budget is sized for
 #endif
@@ -276,7 +320,8 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   // node vectors the epilogue reads for the four nodes each owned element emits (b; b, diag, d),
   // fetched asynchronously while the element products run (FP32; the FP64 kernel's shared memory
   // is already at the 48 KB static limit)
-  constexpr bool CHEB = MODE == AM_CHEB || MODE == AM_CHEB_Z;
+  constexpr bool CHEB = MODE == AM_CHEB || MODE == AM_CHEB_Z || MODE == AM_CHEB_P;
+  constexpr bool PRO = MODE == AM_CHEB_P;
   constexpr int NPRE = sizeof(R) == 8 ? 0 : (CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
   __shared__ __align__(16) R su[LZ * LX * 2];
   __shared__ __align__(16) R2 spre[(NPRE ? NPRE : 1) * 4 * TX * TZ];
@@ -286,6 +331,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   __shared__ R sp[PZ * PX];
   __shared__ R sye[NEL_T * 22];
   __shared__ uchar2 sfix[LZ * LX];          // Dirichlet flags of the staged nodes
+  __shared__ __align__(16) R2 scx[PRO ? CLZ * CLX : 1];   // AM_CHEB_P: the coarse correction tile
   const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
@@ -307,7 +353,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         cp_async_pair<R>(&spre[j * TX * TZ + tid], a.bV + 2 * n);
         if (NPRE == 3) {
           cp_async_pair<R>(&spre[(4 + j) * TX * TZ + tid], a.diag + 2 * n);
-          if (MODE != AM_CHEB_Z) cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
+          if (MODE == AM_CHEB) cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
         }
       }
     }
@@ -329,7 +375,7 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         cp_async_pair<R>(&sspare[it * NJ + q], a.bV + 2 * n);
         if (NPRE == 3) {
           cp_async_pair<R>(&sspare[(2 + it) * NJ + q], a.diag + 2 * n);
-          if (MODE != AM_CHEB_Z) cp_async_pair<R>(&sspare[(4 + it) * NJ + q], a.d + 2 * n);
+          if (MODE == AM_CHEB) cp_async_pair<R>(&sspare[(4 + it) * NJ + q], a.d + 2 * n);
         }
       }
     }
@@ -344,6 +390,29 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       for (int q = 0; q < 9; ++q) eq[q] = eg[q];
     }
   }
+  // ---- AM_CHEB_P: the coarse correction tile (loaded now, stored after the fine loads) ----
+  constexpr int NCT = PRO ? (CLZ * CLX + APPLY_THREADS - 1) / APPLY_THREADS : 1;
+  R2 cv[NCT];
+  const int cx0 = ex0 - 2, cz0 = ez0 - 2;
+  if constexpr (PRO) {
+#pragma unroll
+    for (int k = 0; k < NCT; ++k) {
+      const int i = tid + k * APPLY_THREADS;
+      const int jz = i / CLX, jx = i - jz * CLX;
+      const int cx = cx0 + jx, cz = cz0 + jz;
+      cv[k].x = 0; cv[k].y = 0;
+      if (i < CLZ * CLX && cx >= 0 && cx < a.gc.nnx && cz >= 0 && cz < a.gc.nnz)
+        cv[k] = reinterpret_cast<const R2*>(a.xc)[(int64_t)cz * a.gc.nnx + cx];
+    }
+  }
+  // x + P x_c on the free dofs of fine node (ix, iz) (the arithmetic of k_prolong_add)
+  auto corrected = [&](int ix, int iz, R2 x, uchar2 ff) -> R2 {
+    double s0, s1;
+    prolong_taps(ix, iz, [&](int jz, int jx) { return scx[(jz - cz0) * CLX + (jx - cx0)]; }, &s0, &s1);
+    if (!ff.x) x.x += (R)s0;
+    if (!ff.y) x.y += (R)s1;
+    return x;
+  };
   // ---- stage velocity (masked; one vector load per node), pressure ----
   // A fixed number of nodes per thread, all loads issued before any shared-memory store, so the
   // staging costs one memory round trip rather than one per node.
@@ -356,6 +425,12 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
   uchar2 sf[NST];
   R spv[NSP];
   if constexpr (sizeof(R) == 8) {                    // FP64: one node at a time (fewer live registers)
+    if constexpr (PRO) {
+#pragma unroll
+      for (int k = 0; k < NCT; ++k)
+        if (tid + k * APPLY_THREADS < CLZ * CLX) scx[tid + k * APPLY_THREADS] = cv[k];
+      __syncthreads();
+    }
     for (int i = tid; i < LZ * LX; i += APPLY_THREADS) {
       const int lz = i / LX, lx = i - lz * LX;
       const int ix = lx0 + lx, iz = lz0 + lz;
@@ -366,7 +441,8 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
         const int64_t n = (int64_t)iz * g.nnx + ix;
         ff = f2[n];
         if (use_u) {
-          const R2 uu = u2[n];
+          R2 uu = u2[n];
+          if constexpr (PRO) uu = corrected(ix, iz, uu, ff);
           v.x = ff.x ? R(0) : uu.x;
           v.y = ff.y ? R(0) : uu.y;
         }
@@ -407,6 +483,19 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     const int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
     spv[k] = (use_p && i < PZ * PX && px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz)
                  ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+  }
+  if constexpr (PRO) {
+#pragma unroll
+    for (int k = 0; k < NCT; ++k)
+      if (tid + k * APPLY_THREADS < CLZ * CLX) scx[tid + k * APPLY_THREADS] = cv[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NST; ++k) {
+      const int i = tid + k * APPLY_THREADS;
+      const int lz = i / LX, lx = i - lz * LX;
+      const int ix = lx0 + lx, iz = lz0 + lz;
+      if (i < LZ * LX && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) sv[k] = corrected(ix, iz, sv[k], sf[k]);
+    }
   }
 #pragma unroll
   for (int k = 0; k < NST; ++k) {
@@ -782,43 +871,14 @@ __global__ void __launch_bounds__(RTX * RTZ) k_restrict(LevelGeo gf, LevelGeo gc
   restrict_core(gf, gc, fetch, fixc, bc, c0, cheb_c != nullptr, diag_c, xc, dc, (int64_t)J * gc.nnx + I);
 }
 
-// 1D Q2 prolongation: fine node i from coarse nodes
-MW_D int pw(int i, int* J, double* w) {
-  if (!(i & 1)) { J[0] = i / 2; w[0] = 1.0; return 1; }
-  int E = i / 4;
-  J[0] = 2 * E; J[1] = 2 * E + 1; J[2] = 2 * E + 2;
-  if ((i & 3) == 1) { w[0] = 0.375; w[1] = 0.75; w[2] = -0.125; }
-  else { w[0] = -0.125; w[1] = 0.75; w[2] = 0.375; }
-  return 3;
-}
-
 // x_f += P x_c at fine node n (free dofs only)
 template <typename R>
 MW_D void prolong_node(const LevelGeo& gf, const LevelGeo& gc, const R* xc, const uint8_t* fixf, R* xf, int64_t n) {
-  int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
-  int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
-  double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
-  int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
-  R v0[3][3], v1[3][3];                             // all taps loaded first, then summed in order
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      const bool ok = a < nzw && b < nxw;
-      const int64_t m = ok ? (int64_t)Jz[a] * gc.nnx + Jx[b] : 0;
-      v0[a][b] = ok ? xc[2 * m] : R(0);
-      v1[a][b] = ok ? xc[2 * m + 1] : R(0);
-    }
-  double s0 = 0, s1 = 0;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-      if (a < nzw && b < nxw) {
-        double w = wz[a] * wx[b];
-        s0 += w * (double)v0[a][b];
-        s1 += w * (double)v1[a][b];
-      }
+  typedef typename Vec2<R>::T R2;
+  const int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
+  double s0, s1;
+  prolong_taps(ix, iz, [&](int jz, int jx) { return reinterpret_cast<const R2*>(xc)[(int64_t)jz * gc.nnx + jx]; },
+               &s0, &s1);
   if (!fixf[2 * n]) xf[2 * n] += (R)s0;
   if (!fixf[2 * n + 1]) xf[2 * n + 1] += (R)s1;
 }
@@ -853,20 +913,8 @@ __global__ void __launch_bounds__(PTX * PTZ) k_prolong_add(LevelGeo gf, LevelGeo
   const int64_t n = (int64_t)iz * gf.nnx + ix;
   const uchar2 ff = reinterpret_cast<const uchar2*>(fixf)[n];
   R2 x = reinterpret_cast<const R2*>(xf)[n];
-  int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
-  double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
-  const int nxw = pw(ix, Jx, wx), nzw = pw(iz, Jz, wz);
-  double s0 = 0, s1 = 0;
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int b = 0; b < 3; ++b)
-      if (a < nzw && b < nxw) {
-        const R2 v = sc2[(Jz[a] - cz0) * PCX + (Jx[b] - cx0)];
-        double w = wz[a] * wx[b];
-        s0 += w * (double)v.x;
-        s1 += w * (double)v.y;
-      }
+  double s0, s1;
+  prolong_taps(ix, iz, [&](int jz, int jx) { return sc2[(jz - cz0) * PCX + (jx - cx0)]; }, &s0, &s1);
   if (!ff.x) x.x += (R)s0;
   if (!ff.y) x.y += (R)s1;
   reinterpret_cast<R2*>(xf)[n] = x;
@@ -1827,9 +1875,23 @@ static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = fal
              L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
              C.x, C.d);
   vcycle(H, l + 1, s, fuse);
-  pdl_launch(k_prolong_add<R>, dim3((L.g.nnx + PTX - 1) / PTX, (L.g.nnz + PTZ - 1) / PTZ), PTX * PTZ, 0, s, L.g, C.g,
-             C.x, L.fix, L.x);
-  smooth(L, L.deg, false, s);
+  // x += P x_c folded into the first post-smoothing step (AM_CHEB_P: the restart step, which reads
+  // the corrected x only through its staging), then the remaining steps
+  {
+    ApplyArgs<R> a = args0<R>();
+    a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
+    a.cheb = L.cheb;                    // step-0 pair {0, 1/theta}
+    a.xc = C.x; a.gc = C.g;
+    launch_apply<R, AM_CHEB_P>(L.g, a, s);
+    std::swap(L.x, L.t);
+  }
+  for (int k = 1; k < L.deg; ++k) {
+    ApplyArgs<R> a = args0<R>();
+    a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.d; a.bV = L.b; a.d = L.d; a.xo = L.t;
+    a.cheb = L.cheb + 2 * k;
+    launch_apply<R, AM_CHEB>(L.g, a, s);
+    std::swap(L.x, L.t);
+  }
 }
 
 // Replays the kernels `record` issues on s from a CUDA graph cached under (kind, host state).

@@ -18,46 +18,22 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "common.cuh"
+#include "q2_ref.cuh"
 
 namespace mw {
 
 // ---------------------------------------------------------------- reference-element tables
-struct RefTables {
-  double dr[81], dt[81];   // d N_V / d r, d t at the 9 Gauss points  [q*9+k]
-  double NV[81];           // N_V at the Gauss points
-  double NP[36];           // N_P at the Gauss points   [q*4+k]
-  double wq[9];            // Gauss weights
-};
 __constant__ RefTables c_ref;
 static bool g_ref_ready = false;
 
-// The same reference-element values as compile-time expressions for the operator kernels: inside
-// fully unrolled loops they fold into immediates, and the terms whose basis value vanishes at a
-// Gauss point (a third of them: the 1D Q2 functions are 0 or 1 at the middle point) disappear.
-// Gauss point q = 3 i + j sits at (r, s) = (g_i, g_j), g = (-sqrt(3/5), 0, sqrt(3/5)).
-constexpr double GQ = 0.77459666924148337704;      // sqrt(3/5)
-MW_HD constexpr double gpt(int i) { return i == 0 ? -GQ : (i == 1 ? 0.0 : GQ); }
-MW_HD constexpr double gwt(int i) { return i == 1 ? 8.0 / 9.0 : 5.0 / 9.0; }
-// 1D Q2 Lagrange functions on nodes -1, 0, 1 (a = 0, 1, 2) and their derivatives
-MW_HD constexpr double lq(int a, double x) { return a == 0 ? 0.5 * x * (x - 1.0) : (a == 1 ? 1.0 - x * x : 0.5 * x * (x + 1.0)); }
-MW_HD constexpr double dlq(int a, double x) { return a == 0 ? x - 0.5 : (a == 1 ? -2.0 * x : x + 0.5); }
-MW_HD constexpr int kdx(int k) { return (k == 0 || k == 3 || k == 7) ? 0 : ((k == 1 || k == 2 || k == 5) ? 2 : 1); }
-MW_HD constexpr int kdz(int k) { return (k == 0 || k == 1 || k == 4) ? 0 : ((k == 2 || k == 3 || k == 6) ? 2 : 1); }
-MW_HD constexpr double ref_dr(int q, int k) { return dlq(kdx(k), gpt(q / 3)) * lq(kdz(k), gpt(q % 3)); }
-MW_HD constexpr double ref_dt(int q, int k) { return lq(kdx(k), gpt(q / 3)) * dlq(kdz(k), gpt(q % 3)); }
-MW_HD constexpr double ref_np(int q, int k) {
-  return 0.25 * (k == 0 || k == 3 ? 1.0 - gpt(q / 3) : 1.0 + gpt(q / 3)) *
-         (k == 0 || k == 1 ? 1.0 - gpt(q % 3) : 1.0 + gpt(q % 3));
-}
-MW_HD constexpr double ref_wq(int q) { return gwt(q / 3) * gwt(q % 3); }
-
 // FP32 kernels take the values as immediates; FP64 ones read them from the constant bank (an FP64
 // immediate would be materialised in registers for every use).  Which terms vanish is decided at
-// compile time in both cases (ref_dr / ref_dt above).
+// compile time in both cases (ref_dr / ref_dt of q2_ref.cuh).
 template <typename R> struct CT {
   MW_D static constexpr R dr(int q, int k) { return (R)ref_dr(q, k); }
   MW_D static constexpr R dt(int q, int k) { return (R)ref_dt(q, k); }
@@ -70,33 +46,6 @@ template <> struct CT<double> {
   MW_D static double np(int q, int k) { return c_ref.NP[q * 4 + k]; }
   MW_D static double wq(int q) { return c_ref.wq[q]; }
 };
-
-static void host_ref_tables(RefTables* T) {
-  const double qc[3] = {-std::sqrt(3.0 / 5.0), 0.0, std::sqrt(3.0 / 5.0)};
-  const double qw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
-  int q = 0;
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j, ++q) {
-      double r = qc[i], s = qc[j];
-      T->wq[q] = qw[i] * qw[j];
-      double N[9];
-      q2_basis<double>(r, s, N);
-      for (int k = 0; k < 9; ++k) T->NV[q * 9 + k] = N[k];
-      double dr[9] = {0.5 * (2.0 * r - 1.0) * 0.5 * s * (s - 1), 0.5 * (2.0 * r + 1.0) * 0.5 * s * (s - 1),
-                      0.5 * (2.0 * r + 1.0) * 0.5 * s * (s + 1), 0.5 * (2.0 * r - 1.0) * 0.5 * s * (s + 1),
-                      (-2.0 * r) * 0.5 * s * (s - 1), 0.5 * (2.0 * r + 1.0) * (1.0 - s * s),
-                      (-2.0 * r) * 0.5 * s * (s + 1), 0.5 * (2.0 * r - 1.0) * (1.0 - s * s), (-2.0 * r) * (1.0 - s * s)};
-      double dt[9] = {0.5 * r * (r - 1.0) * 0.5 * (2.0 * s - 1.0), 0.5 * r * (r + 1.0) * 0.5 * (2.0 * s - 1.0),
-                      0.5 * r * (r + 1.0) * 0.5 * (2.0 * s + 1.0), 0.5 * r * (r - 1.0) * 0.5 * (2.0 * s + 1.0),
-                      (1.0 - r * r) * 0.5 * (2.0 * s - 1.0), 0.5 * r * (r + 1.0) * (-2.0 * s),
-                      (1.0 - r * r) * 0.5 * (2.0 * s + 1.0), 0.5 * r * (r - 1.0) * (-2.0 * s), (1.0 - r * r) * (-2.0 * s)};
-      for (int k = 0; k < 9; ++k) { T->dr[q * 9 + k] = dr[k]; T->dt[q * 9 + k] = dt[k]; }
-      T->NP[q * 4 + 0] = 0.25 * (1 - r) * (1 - s);
-      T->NP[q * 4 + 1] = 0.25 * (1 + r) * (1 - s);
-      T->NP[q * 4 + 2] = 0.25 * (1 + r) * (1 + s);
-      T->NP[q * 4 + 3] = 0.25 * (1 - r) * (1 + s);
-    }
-}
 
 static int ensure_ref_tables() {
   if (g_ref_ready) return MW_OK;
@@ -568,7 +517,11 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
     R2 dg{R(0), R(0)}, bb{R(0), R(0)}, dd{R(0), R(0)};
     if (CHEB) dg = pre ? pre_at(1, slot) : reinterpret_cast<const R2*>(a.diag)[n];
     else if (fixed) dg = reinterpret_cast<const R2*>(a.diag)[n];
-    if (fixed && MODE != AM_CHEB_Z) uu = reinterpret_cast<const R2*>(a.u)[n];
+    if (fixed && MODE != AM_CHEB_Z) {                // the fixed components' values (staged as 0);
+      const R2 raw = reinterpret_cast<const R2*>(a.u)[n];   // a free one keeps its staged value,
+      if (ff.x) uu.x = raw.x;                        // which under AM_CHEB_P carries P x_c
+      if (ff.y) uu.y = raw.y;
+    }
     if (MODE != AM_APPLY) bb = pre ? pre_at(0, slot) : reinterpret_cast<const R2*>(a.bV)[n];
     if (MODE == AM_CHEB && c1 != 0.0)                // restart steps never read the old direction
       dd = pre ? pre_at(2, slot) : reinterpret_cast<const R2*>(a.d)[n];
@@ -1848,6 +1801,17 @@ static void launch_tail(Hierarchy<R>& H, int l0, bool first_done, cudaStream_t s
   pdl_launch(k_vtail<R>, TAIL_CLUSTER, tail_threads<R>(), 0, s, A);
 }
 
+// MW_FUSED_PROLONG=0 in the environment (read at the first V-cycle) launches the prolongation on
+// its own (k_prolong_add) before the post-smoothing: the same arithmetic with one launch more per
+// level and V-cycle.
+static bool fused_prolongation() {
+  static const bool on = [] {
+    const char* e = getenv("MW_FUSED_PROLONG");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
 template <typename R>
 static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = false) {
   Level<R>& L = H.L[l];
@@ -1875,6 +1839,12 @@ static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = fal
              L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
              C.x, C.d);
   vcycle(H, l + 1, s, fuse);
+  if (!fused_prolongation()) {                     // x += P x_c as its own launch, then the smoothing
+    pdl_launch(k_prolong_add<R>, dim3((L.g.nnx + PTX - 1) / PTX, (L.g.nnz + PTZ - 1) / PTZ), PTX * PTZ, 0, s, L.g,
+               C.g, (const R*)C.x, L.fix, L.x);
+    smooth(L, L.deg, false, s);
+    return;
+  }
   // x += P x_c folded into the first post-smoothing step (AM_CHEB_P: the restart step, which reads
   // the corrected x only through its staging), then the remaining steps
   {

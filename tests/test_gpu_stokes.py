@@ -163,3 +163,52 @@ def test_coarse_tail_matches_level_launches(precision):
     for k in ("outer_iters", "inner_iters", "refinements"):
         assert i1[k] == i0[k], (k, i1, i0)
     assert np.array_equal(V1, V0) and np.array_equal(P1, P0)
+
+
+_FUSED_SCRIPT = r"""
+import sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+from meeuuw_b200 import _lib
+from meeuuw_b200.stokes import StokesSolver
+nel = 64
+box = _lib.box_of(nel, nel, 1.0, 1.0)
+nn1 = 2 * nel + 1
+X, Z = np.meshgrid(np.arange(nn1), np.arange(nn1))
+fix = np.zeros((nn1 * nn1, 2), dtype=bool)
+fix[:, 0] = ((X == 0) | (X == nn1 - 1)).ravel()            # free slip: one component fixed on each side
+fix[:, 1] = ((Z == 0) | (Z == nn1 - 1)).ravel()
+rng = np.random.default_rng(4)
+etaq = np.exp(np.repeat(rng.uniform(-4.0, 4.0, nel * nel), 9).reshape(nel * nel, 9))
+S = StokesSolver(box, torch.as_tensor(fix.ravel()).cuda(), eta_ref=1.0, L_ref=1.0)
+S.set_viscosity(torch.as_tensor(etaq).cuda(), torch.as_tensor(etaq[:, 0]).cuda())
+g = torch.Generator(device="cuda").manual_seed(9)
+out = {}
+for prec, dt in (("f32", torch.float32), ("f64", torch.float64)):
+    b = torch.randn(S.nv, dtype=dt, device="cuda", generator=g)
+    out["v_" + prec] = S.vcycle(b, precision=prec).cpu().numpy()
+    x, it, rr = S.solve_K(b.double(), precision=prec, rtol=1e-9 if prec == "f64" else 1e-4, maxit=300)
+    out["x_" + prec] = x.cpu().numpy()
+    out["it_" + prec] = np.array([it])
+np.savez(sys.argv[2], **out)
+"""
+
+
+def test_fused_prolongation_matches_separate_launch(tmp_path):
+    """The prolongation folded into the first post-smoothing step (default) and launched on its own
+    (MW_FUSED_PROLONG=0) give the same V-cycle and multigrid-PCG iterates bit for bit, on a mesh with
+    free-slip sides (nodes with one fixed and one free component)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for flag in ("1", "0"):
+        path = str(tmp_path / f"fused{flag}.npz")
+        env = dict(os.environ, MW_FUSED_PROLONG=flag)
+        subprocess.run([sys.executable, "-c", _FUSED_SCRIPT, root, path], env=env, check=True, timeout=600)
+        res[flag] = np.load(path)
+    for k in res["1"].files:
+        assert np.array_equal(res["1"][k], res["0"][k]), k
+    assert res["1"]["it_f64"][0] < 100

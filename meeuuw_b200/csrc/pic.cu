@@ -1,8 +1,8 @@
 // Particle-in-cell kernels for the Cartesian box (sm_100a).
 //
-// Reference: pic_functions.py (locate :108-137, interpolate :85-101 and :18-37, advect :180-292,
-// element projection :603-650, nodal projections :659-1053) and the material hooks
-// experiment0.py:230-264 / experiment1.py:91-113.
+// Reference: pic_functions.py (locate :108-137, element projection :603-650, nodal projections
+// :659-1053, least squares :1061-1285, population control :1621-1812).  Interpolation and
+// advection are in advect.cu.
 //
 // Layout: particles are SoA (x, z, r, t: f64; iel: i32; active: u8), one thread per particle,
 // grid-stride loops sized to a multiple of the SM count.  Projections are atomic-free and
@@ -13,6 +13,7 @@
 #include <cstdlib>
 
 #include "common.cuh"
+#include "pic_common.cuh"
 
 namespace mw {
 
@@ -42,27 +43,6 @@ int grid_for(int64_t n, int threads, int waves) {
   return (int)(need < cap ? need : cap);
 }
 
-// Element containing point (x, z): pic_functions.py:29-31 (int() truncates toward zero).
-// Returns false when the truncated quotient does not fit an int (the reference would index
-// out of bounds there).
-MW_D bool element_of(const mw_box& b, double x, double z, int64_t* e) {
-  double qx = x / b.hx, qz = z / b.hz;
-  if (!(qx > -2147483648.0 && qx < 2147483647.0 && qz > -2147483648.0 && qz < 2147483647.0)) return false;
-  int ielx = (int)qx, ielz = (int)qz;
-  *e = (int64_t)b.nelx * ielz + ielx;
-  return true;
-}
-
-// x_V / z_V of local node 0 of element e: build_velocity_mesh.py:116-117 computes i*hx/2.
-MW_D double xv0(const mw_box& b, int ex) { return ((double)(2 * ex) * b.hx) / 2; }
-MW_D double zv0(const mw_box& b, int ez) { return ((double)(2 * ez) * b.hz) / 2; }
-
-template <typename F>
-MW_D double q2_dot(const double* N, const F& nodal, int ex, int ez, int nnx) {
-  double acc = N[0] * nodal(q2_node(ex, ez, 0, nnx));
-  for (int k = 1; k < 9; ++k) acc = acc + N[k] * nodal(q2_node(ex, ez, k, nnx));
-  return acc;
-}
 
 // ------------------------------------------------------------------------------------------
 __global__ void k_locate(mw_box b, int64_t n, const uint8_t* __restrict__ active,
@@ -88,159 +68,6 @@ __global__ void k_locate(mw_box b, int64_t n, const uint8_t* __restrict__ active
   }
 }
 
-// ------------------------------------------------------------------------------------------
-struct FieldSet {
-  const double* in[MW_MAX_FIELDS];
-  double* out[MW_MAX_FIELDS];
-  int n;
-};
-
-__global__ void k_interp(mw_box b, int64_t n, const uint8_t* __restrict__ active, const double* __restrict__ r,
-                         const double* __restrict__ t, const int32_t* __restrict__ iel, FieldSet fs) {
-  const int nnx = 2 * b.nelx + 1;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    if (!active[i]) {
-      for (int f = 0; f < fs.n; ++f) fs.out[f][i] = 0.0;
-      continue;
-    }
-    double N[9];
-    q2_basis<double>(r[i], t[i], N);
-    int e = iel[i];
-    int ex = e % b.nelx, ez = e / b.nelx;
-    for (int f = 0; f < fs.n; ++f) {
-      const double* phi = fs.in[f];
-      fs.out[f][i] = q2_dot(N, [&](int64_t j) { return __ldg(phi + j); }, ex, ez, nnx);
-    }
-  }
-}
-
-// Interpolation of the five nodal fields the time loop needs (meeuuw.py:1118-1125) fused with
-// the material model (experiment0.py:254-264 / experiment1.py:104-111).
-__global__ void k_interp_material(mw_box b, int64_t n, const uint8_t* __restrict__ active,
-                                  const double* __restrict__ r, const double* __restrict__ t,
-                                  const int32_t* __restrict__ iel, const int8_t* __restrict__ mat,
-                                  mw_nodal5 nodal, mw_material m, mw_swarm_props out) {
-  const int nnx = 2 * b.nelx + 1;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double v[5] = {0, 0, 0, 0, 0};
-    bool act = active[i] != 0;
-    if (act) {
-      double N[9];
-      q2_basis<double>(r[i], t[i], N);
-      int e = iel[i];
-      int ex = e % b.nelx, ez = e / b.nelx;
-      const double* fl[5] = {nodal.exx, nodal.ezz, nodal.exz, nodal.q, nodal.T};
-      for (int f = 0; f < 5; ++f) {
-        if (fl[f] == nullptr) continue;
-        const double* phi = fl[f];
-        v[f] = q2_dot(N, [&](int64_t j) { return __ldg(phi + j); }, ex, ez, nnx);
-      }
-    }
-    if (out.exx) out.exx[i] = v[0];
-    if (out.ezz) out.ezz[i] = v[1];
-    if (out.exz) out.exz[i] = v[2];
-    if (out.p) out.p[i] = v[3];
-    if (out.T) out.T[i] = v[4];
-    double rho, eta, hcond, hcapa, hprod, alpha;
-    if (m.kind == MW_MATERIAL_TWO) {
-      int id = mat ? (int)mat[i] : 0;
-      id = id < 0 ? 0 : (id > 7 ? 7 : id);
-      rho = act ? m.mat_rho[id] : 0.0;
-      eta = act ? m.mat_eta[id] : 0.0;
-      hcond = hcapa = hprod = alpha = 0.0;
-    } else {
-      double T = v[4];
-      rho = m.rho0 * (1 - m.alphaT * T);
-      eta = m.fk_gamma != 0.0 ? exp(-m.fk_gamma * T) : m.eta0;
-      hcond = m.hcond; hcapa = m.hcapa; hprod = m.hprod; alpha = m.alphaT;
-    }
-    out.rho[i] = rho;
-    out.eta[i] = eta;
-    if (out.hcond) out.hcond[i] = hcond;
-    if (out.hcapa) out.hcapa[i] = hcapa;
-    if (out.hprod) out.hprod[i] = hprod;
-    if (out.alpha) out.alpha[i] = alpha;
-  }
-}
-
-// ------------------------------------------------------------------------------------------
-// Velocity at a point: pic_functions.py:18-37.  The element index is the reference's, including
-// the case x == Lx that wraps into the next row; indices outside the mesh set a flag.
-MW_D bool vel_at(const mw_box& b, int64_t nel, int nnx, double xp, double zp, const double* __restrict__ u,
-                 const double* __restrict__ w, double* up, double* wp, int32_t* err) {
-  int64_t e;
-  if (!element_of(b, xp, zp, &e) || e < 0 || e >= nel) {
-    set_flag(err, MW_FLAG_ELEMENT_RANGE);
-    *up = 0.0; *wp = 0.0;
-    return false;
-  }
-  int ex = (int)(e % b.nelx), ez = (int)(e / b.nelx);
-  double rp = ((xp - xv0(b, ex)) / b.hx - 0.5) * 2;
-  double tp = ((zp - zv0(b, ez)) / b.hz - 0.5) * 2;
-  double N[9];
-  q2_basis<double>(rp, tp, N);
-  *up = q2_dot(N, [&](int64_t j) { return __ldg(u + j); }, ex, ez, nnx);
-  *wp = q2_dot(N, [&](int64_t j) { return __ldg(w + j); }, ex, ez, nnx);
-  return true;
-}
-
-MW_D bool outside(const mw_box& b, double x, double z) { return x < 0 || x > b.Lx || z < 0 || z > b.Lz; }
-
-__global__ void k_advect(mw_box b, int rk, double dt_host, const double* __restrict__ dt_dev, int64_t n, double* __restrict__ x, double* __restrict__ z,
-                         uint8_t* __restrict__ active, const double* __restrict__ u, const double* __restrict__ w,
-                         double* __restrict__ up_out, double* __restrict__ wp_out, int32_t* err) {
-  const int64_t nel = (int64_t)b.nelx * b.nelz;
-  const int nnx = 2 * b.nelx + 1;
-  const double dt = dt_dev ? *dt_dev : dt_host;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double su = 0.0, sw = 0.0;
-    bool act = active[i] != 0;
-    if (act) {
-      double xA = x[i], zA = z[i], uA, wA;
-      vel_at(b, nel, nnx, xA, zA, u, w, &uA, &wA, err);
-      if (rk == 1) {                                                  // :220-231
-        su = uA; sw = wA;
-        double xn = xA + uA * dt, zn = zA + wA * dt;
-        x[i] = xn; z[i] = zn;
-        if (outside(b, xn, zn)) act = false;
-      } else {
-        double xB = xA + uA * dt / 2.0, zB = zA + wA * dt / 2.0;      // :239-240
-        if (outside(b, xB, zB)) {
-          act = false;
-        } else {
-          double uB, wB;
-          vel_at(b, nel, nnx, xB, zB, u, w, &uB, &wB, err);
-          if (rk == 2) {                                              // :244-248
-            x[i] = xA + uB * dt; z[i] = zA + wB * dt;
-            su = uB; sw = wB;
-          } else {
-            double xC = xA + uB * dt / 2.0, zC = zA + wB * dt / 2.0;  // :265-266
-            if (outside(b, xC, zC)) {
-              act = false;
-            } else {
-              double uC, wC;
-              vel_at(b, nel, nnx, xC, zC, u, w, &uC, &wC, err);
-              double xD = xA + uC * dt, zD = zA + wC * dt;            // :271-272
-              if (outside(b, xD, zD)) {
-                act = false;
-              } else {
-                double uD, wD;
-                vel_at(b, nel, nnx, xD, zD, u, w, &uD, &wD, err);
-                su = (uA + 2 * uB + 2 * uC + uD) / 6;                 // :277-280
-                sw = (wA + 2 * wB + 2 * wC + wD) / 6;
-                x[i] = xA + su * dt; z[i] = zA + sw * dt;
-              }
-            }
-          }
-        }
-      }
-      if (!act) active[i] = 0;
-    }
-    if (!act) { x[i] = 0.0; z[i] = 0.0; }                              // :287-290
-    if (up_out) up_out[i] = su;
-    if (wp_out) wp_out[i] = sw;
-  }
-}
 
 // ------------------------------------------------------------------------------------------
 // Binning: counts -> exclusive scan -> scatter -> per-bin sort by particle index.
@@ -445,24 +272,27 @@ __global__ void k_project_corners(mw_box b, int flavour, const int32_t* __restri
 // per corner into partials (nel x 4 x (nfield+1) doubles), then each corner node adds the partials
 // of its incident elements in ascending element order and applies the averaging.  The sums agree
 // with the reference's particle-ordered sums to rounding (different association).
+// NF: register capacity for the fields (pf.n <= NF), so that the accumulators of the usual two- or
+// four-field projections do not occupy the registers of eight.
+template <int NF>
 __global__ void k_project_elem_partials(mw_box b, int flavour, const int32_t* __restrict__ offsets,
                                         const int32_t* __restrict__ order, const double* __restrict__ r,
                                         const double* __restrict__ t, ProjFields pf, double* __restrict__ part) {
   const int64_t nel = (int64_t)b.nelx * b.nelz;
   const int nf1 = pf.n + 1;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
-    double acc[4][MW_MAX_FIELDS + 1];
+    double acc[4][NF + 1];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
-      for (int f = 0; f <= MW_MAX_FIELDS; ++f) acc[k][f] = 0.0;
+      for (int f = 0; f <= NF; ++f) acc[k][f] = 0.0;
     const int b0 = offsets[e], b1 = offsets[e + 1];
     for (int j = b0; j < b1; ++j) {
       const int p = order[j];
       const double rp = r[p], tp = t[p];
-      double v[MW_MAX_FIELDS];
+      double v[NF];
 #pragma unroll
-      for (int f = 0; f < MW_MAX_FIELDS; ++f)
+      for (int f = 0; f < NF; ++f)
         if (f < pf.n) v[f] = avg_transform(pf.averaging[f], pf.phi[f][p]);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -470,17 +300,19 @@ __global__ void k_project_elem_partials(mw_box b, int flavour, const int32_t* __
         corner_weight(flavour, k, rp, tp, &use, &w);
         if (!use) continue;
         const bool plain = (flavour == 1 || flavour == 3);
-        acc[k][MW_MAX_FIELDS] = plain ? acc[k][MW_MAX_FIELDS] + 1.0 : acc[k][MW_MAX_FIELDS] + 1 * w;
+        acc[k][NF] = plain ? acc[k][NF] + 1.0 : acc[k][NF] + 1 * w;
 #pragma unroll
-        for (int f = 0; f < MW_MAX_FIELDS; ++f)
+        for (int f = 0; f < NF; ++f)
           if (f < pf.n) acc[k][f] = plain ? acc[k][f] + v[f] : acc[k][f] + v[f] * w;
       }
     }
     double* o = part + e * 4 * nf1;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      for (int f = 0; f < pf.n; ++f) o[k * nf1 + f] = acc[k][f];
-      o[k * nf1 + pf.n] = acc[k][MW_MAX_FIELDS];
+#pragma unroll
+      for (int f = 0; f < NF; ++f)
+        if (f < pf.n) o[k * nf1 + f] = acc[k][f];
+      o[k * nf1 + pf.n] = acc[k][NF];
     }
   }
 }
@@ -920,38 +752,6 @@ int mw_locate_box(mw_box box, int64_t n, const uint8_t* active, const double* x,
   return MW_OK;
 }
 
-int mw_interp_q2(mw_box box, int64_t n, const uint8_t* active, const double* r, const double* t, const int32_t* iel,
-                 int32_t nfield, const double* const* fields, double* const* out, void* stream) {
-  if (!box_ok(box) || n < 0 || nfield < 1 || nfield > MW_MAX_FIELDS) return MW_ERR_BAD_ARG;
-  if (n == 0) return MW_OK;
-  FieldSet fs;
-  fs.n = nfield;
-  for (int f = 0; f < nfield; ++f) { fs.in[f] = fields[f]; fs.out[f] = out[f]; }
-  k_interp<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(box, n, active, r, t, iel, fs);
-  MW_CHECK_LAUNCH();
-  return MW_OK;
-}
-
-int mw_interp_material(mw_box box, int64_t n, const uint8_t* active, const double* r, const double* t,
-                       const int32_t* iel, const int8_t* mat, mw_nodal5 nodal, mw_material m, mw_swarm_props out,
-                       void* stream) {
-  if (!box_ok(box) || n < 0 || !out.rho || !out.eta) return MW_ERR_BAD_ARG;
-  if (n == 0) return MW_OK;
-  k_interp_material<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(box, n, active, r, t, iel, mat, nodal, m, out);
-  MW_CHECK_LAUNCH();
-  return MW_OK;
-}
-
-int mw_advect_box(mw_box box, int32_t rk, double dt, const double* dt_dev, int64_t n, double* x, double* z,
-                  uint8_t* active, const double* u, const double* w, double* up, double* wp, int32_t* err,
-                  void* stream) {
-  if (!box_ok(box) || n < 0 || !(rk == 1 || rk == 2 || rk == 4)) return MW_ERR_BAD_ARG;
-  if (n == 0) return MW_OK;
-  k_advect<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(box, rk, dt, dt_dev, n, x, z, active, u, w, up, wp, err);
-  MW_CHECK_LAUNCH();
-  return MW_OK;
-}
-
 size_t mw_bin_workspace_bytes(int32_t nel) {
   int64_t nb = ((int64_t)nel + 1 + 1023) / 1024;
   return (size_t)((int64_t)nel + 2 * nb + 16) * sizeof(int32_t);
@@ -1012,7 +812,13 @@ int mw_project_nodes(mw_box box, int32_t flavour, int32_t nfield, const int32_t*
   int64_t nc = (int64_t)(box.nelx + 1) * (box.nelz + 1);
   if (work && work_bytes >= mw_project_nodes_workspace_bytes(box, nfield)) {
     int64_t nel = (int64_t)box.nelx * box.nelz;
-    k_project_elem_partials<<<grid_for(nel, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf, (double*)work);
+    if (nfield <= 2)
+      k_project_elem_partials<2><<<grid_for(nel, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf, (double*)work);
+    else if (nfield <= 4)
+      k_project_elem_partials<4><<<grid_for(nel, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf, (double*)work);
+    else
+      k_project_elem_partials<MW_MAX_FIELDS><<<grid_for(nel, 128), 128, 0, s>>>(box, flavour, offsets, order, r, t, pf,
+                                                                               (double*)work);
     MW_CHECK_LAUNCH();
     k_project_corner_finish<<<grid_for(nc, 256), 256, 0, s>>>(box, pf, (const double*)work);
   } else {

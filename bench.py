@@ -205,6 +205,7 @@ def run_ours(args):
     # ---- roofline of the dominant kernel: fine-level operator apply (FP32), CUDA events ----
     roof = roofline_apply(model, torch)
     kroof = kernel_rooflines(model, torch, roof["peak"])
+    unet_tc = unet_throughput(torch)
 
     # ---- plain FP64 path (same problem, same warm start) ----
     plain = None
@@ -266,7 +267,7 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (swarm state ~0.5 GB, fields ~0.2 GB)"},
             "clocks": clk.summary(), "gpu_launches": launches, "kernel_mix_per_step": kernel_mix,
-            "roofline": roof, "kernel_rooflines": kroof, "e2e": e2e, "plain_fp64": plain,
+            "roofline": roof, "kernel_rooflines": kroof, "unet_tensor_cores": unet_tc, "e2e": e2e, "plain_fp64": plain,
             "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
             "last_step": {"vrms": diag["vrms"], "Nu": diag["Nu"], "dt": diag["dt"], "stokes": diag["stokes"],
                           "energy_iters_relres": list(getattr(model, "energy_info", (None, None)))},
@@ -336,6 +337,21 @@ def kernel_rooflines(model, torch, peak_gbs):
     add("k_advect (RK%d)" % m.cfg.RKorder, timed(lambda: ops.advect(b, m.cfg.RKorder, dtv, x, z, act, m.u, m.w, up, wp,
                                                                    m.err), prep_adv),
         50 * n + 2 * 8 * nn, bound_note="FP64 issue (4 stages: element index, reduced coordinates, Q2 basis, 18 gathers)")
+    # the matrix-free energy operator of the last step: y = A x (5 coefficient planes x 9 Gauss
+    # points per element, x and y, the Dirichlet flags) and its set-up (8 Gauss-point input arrays
+    # read, the planes written; per node T, flags and values read, diagonal, flags and rhs written)
+    if m.cfg.solve_T and getattr(m, "energy_op", None) is not None:
+        y = torch.empty_like(m.T)
+        add("k_energy_op_apply", timed(lambda: ops.energy_op_apply(b, m.energy_op, m.T, y)), nel * 360 + nn * 17)
+        qf = m.qf
+        qe = {k: qf[k] for k in ("rhoq", "etaq", "Tq", "uq", "wq", "hcondq", "hcapaq", "alphaq", "hprodq")}
+        qe.update(m.geo)
+        op2, rhs2 = torch.empty_like(m.energy_op), torch.empty_like(m.rhs_T)
+        add("k_energy_op_setup", timed(lambda: ops.energy_op_setup(b, m.T, qe, m.tables, m.bc_fix_T, m.bc_val_T, 0.0,
+                                                                   m.cfg.rho0, m.cfg.formulation, op2, rhs2,
+                                                                   dt_dev=m.dt_out)),
+            nel * (576 + 360) + nn * 34)
+        del op2, rhs2, y
     # FP32 Stokes assembly, the full layout (the drop-in's build_matrix_stokes; the time step's solve
     # is matrix-free and does not assemble)
     q = m.stokes_inputs()
@@ -356,6 +372,66 @@ def kernel_rooflines(model, torch, peak_gbs):
         frac_fp32_peak=flops / (us * 1e-6) / 1e12 / fp32_peak, fp32_peak_tflops=fp32_peak)
     del res
     torch.cuda.empty_cache()
+    return out
+
+
+def unet_throughput(torch):
+    """The learned warm start's network on the tensor cores: the U-Net forward at 128x128 (batch 1,
+    the cold-start inference; batch 16, the training batch) and its largest implicit convolutions,
+    timed with CUDA events (mean of 20 after 3 warm-ups), against MEASURED_PEAKS.json bf16_tflops.
+    FLOPs: 2 M Cout 9 Cin per convolution (M = batch x pixels of the layer's grid)."""
+    from meeuuw_b200 import ops
+    import meeuuw_b200.unet as U
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    wpath = os.path.join(ROOT, "meeuuw_b200", "weights", "unet_fk128.npz")
+    net = U.UNet.load(wpath) if os.path.exists(wpath) else U.UNet(seed=0)
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    def net_flops(B, n):
+        tot, h = 0, n
+        for lvl, (c1, c2) in enumerate(net.enc):
+            tot += 2 * B * h * h * 9 * (c1.cin * c1.cout + c2.cin * c2.cout)
+            if lvl < len(net.enc) - 1:
+                h //= 2
+        for c1, c2 in net.dec:
+            h *= 2
+            tot += 2 * B * h * h * 9 * (c1.cin * c1.cout + c2.cin * c2.cout)
+        return tot + 2 * B * h * h * 9 * net.head.cin * net.head.cout
+
+    out = {"peak_tflops": peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (of measured)" if "bf16_tflops" in peaks
+           else "fallback 1590"}
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for B in (1, 16):
+        X = torch.randn(B, 128, 128, 2, device="cuda", generator=g).to(torch.bfloat16)
+        ms = timed(lambda: net.forward(X, B, 128, 128))
+        fl = net_flops(B, 128)
+        out[f"forward_b{B}"] = {"ms": ms, "gflop": fl / 1e9, "tflops": fl / (ms * 1e-3) / 1e12,
+                                "frac_bf16_peak": fl / (ms * 1e-3) / 1e12 / peak}
+    # single implicit convolutions at the training batch: (B, H, W, Cin, Cout)
+    for B, H, C, N in ((16, 128, 96, 32), (16, 32, 384, 128), (16, 16, 256, 256), (64, 64, 128, 64)):
+        X = torch.randn(B * H * H, C, device="cuda", generator=g).to(torch.bfloat16)
+        Wt = (torch.randn(N, U._kp(C), device="cuda", generator=g) * 0.05).to(torch.bfloat16)
+        y = torch.empty(B * H * H, N, dtype=torch.bfloat16, device="cuda")
+        ms = timed(lambda: ops.conv3x3_bf16(X, B, H, H, C, Wt, out=y, relu=True, out_bf16=True))
+        fl = 2 * B * H * H * N * 9 * C
+        out[f"conv_b{B}_{H}x{H}_{C}to{N}"] = {"ms": ms, "gflop": fl / 1e9, "tflops": fl / (ms * 1e-3) / 1e12,
+                                               "frac_bf16_peak": fl / (ms * 1e-3) / 1e12 / peak}
     return out
 
 

@@ -447,6 +447,23 @@ size_t mw_energy_solve_workspace_bytes(mw_box box);
 int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
                     int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream);
 
+/* Matrix-free form of the same system (no reference counterpart as an interface: it replaces the
+ * pair build_matrix_energy, build_matrix_energy.py:12-141, + spsolve, meeuuw.py:2232-2235, where
+ * the element matrices are not needed).  mw_energy_op_setup takes build_matrix_energy's inputs and
+ * writes into `op` (mw_energy_op_bytes) the Gauss-point coefficients of A = M + (dt/2)(Ka + Kd)
+ * (5 x 9 doubles per element), the summed element diagonals and the Dirichlet flags, and writes rhs
+ * as build_matrix_energy does (:112-130, to rounding); the box's Jacobian is diagonal, so jcbi01q
+ * and jcbi10q are not read and N_T / dNdr_T / dNds_T are the standard Q2 values at the 3x3 Gauss
+ * points.  mw_energy_op_apply: y = A x with the reference's Dirichlet elimination.
+ * mw_energy_op_solve: mw_energy_solve on the matrix-free operator (same iteration, device info
+ * and recording).  The first call on a device loads the reference-element tables (synchronous). */
+size_t mw_energy_op_bytes(mw_box box);
+int mw_energy_op_setup(mw_box box, mw_energy_in in, void* op, size_t op_bytes, double* rhs, void* stream);
+int mw_energy_op_apply(mw_box box, const void* op, const double* x, double* y, void* stream);
+size_t mw_energy_op_solve_workspace_bytes(mw_box box);
+int mw_energy_op_solve(mw_box box, const void* op, const double* rhs, double* T, double rtol, int32_t maxit,
+                       int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream);
+
 /* ======================= learned warm start: tensor-core kernels ======================= */
 /* No reference counterpart: the learned warm start is this build's addition to the method. */
 
@@ -467,6 +484,15 @@ typedef struct {
 size_t mw_gemm_workspace_bytes(int32_t M, int32_t N, int32_t splits);
 int mw_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const void* A, int64_t lda, const void* B, int64_t ldb,
                     mw_gemm_epilogue epi, void* work, size_t work_bytes, int32_t* err, void* stream);
+
+/* 3x3 'same' convolution of NHWC BF16 activations X [B, H, W, C] as an implicit GEMM:
+ * out[B*H*W, N] = im2col(X) * Wt[N, ldw]^T with the im2col layout (K = tap*C + c, tap = 3 dy + dx)
+ * never written: each K block's A tile is loaded from X by a 4D TMA box at the tap's offset.  The
+ * same K blocks and MMAs in the same order as mw_gemm_bf16_tn on im2col(X), so the outputs are
+ * equal.  C a multiple of 32, W <= 128 with 128 % W == 0, H*W a multiple of 128, ldw >= 9 C,
+ * splits = 1; otherwise MW_ERR_BAD_ARG (use mw_unet_im2col + mw_gemm_bf16_tn). */
+int mw_conv3x3_bf16(int32_t B, int32_t H, int32_t W, int32_t C, const void* X, int32_t N, const void* Wt, int64_t ldw,
+                    mw_gemm_epilogue epi, int32_t* err, void* stream);
 
 /* U-Net building blocks (activations NHWC BF16, gradients FP32; conv K index = tap*C + c, zero
  * padded to Kp, a multiple of 64).  transposed=1 writes the im2col matrix as [Kp, ldT] with

@@ -134,6 +134,12 @@ _PROTOS = {
     "mw_energy_device_info": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_energy_solve": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
                                   c_void_p, c_size_t, c_void_p]),
+    "mw_energy_op_bytes": (c_size_t, [MwBox]),
+    "mw_energy_op_setup": (c_int32, [MwBox, MwEnergyIn, c_void_p, c_size_t, c_void_p, c_void_p]),
+    "mw_energy_op_apply": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "mw_energy_op_solve_workspace_bytes": (c_size_t, [MwBox]),
+    "mw_energy_op_solve": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
+                                     c_void_p, c_size_t, c_void_p]),
 }
 
 

@@ -7,6 +7,11 @@
 // matrix applied without forming it -- and the system is solved by Jacobi-preconditioned
 // BiCGSTAB in FP64 to a relative residual tolerance.  The solve first regroups the rows by node
 // class (k_energy_rows) so that every matvec of the iteration reads them coalesced.
+//
+// The time stepper uses the matrix-free form of the same operator instead (mw_energy_op_*): the
+// Gauss-point coefficients of the element matrices stored once per step, the element products
+// formed on the fly in shared-memory tiles, the right-hand side and the Jacobi diagonal formed by
+// the same kernel -- no element matrices are written or read.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -14,6 +19,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "q2_ref.cuh"
 
 namespace mw {
 
@@ -266,6 +272,285 @@ __global__ void k_energy_matvec_rows(mw_box b, RowPlanes P, const double* __rest
   }
 }
 
+// ---------------------------------------------------------------- matrix-free operator
+// A = M + (dt/2)(Ka + Kd) of build_matrix_energy.py:69-114 from its Gauss-point coefficients: per
+// element and Gauss point q, with xv, gr, gs the value and reference-coordinate derivatives of x,
+//   P = cM xv + au gr + aw gs,  Qr = dr gr,  Qs = ds gs,   y_k += N_qk P + dN/dr_qk Qr + dN/ds_qk Qs
+// and the five coefficient planes
+//   cM = rho0 hcapa JxW                                                    (mass, :77)
+//   au = (dt/2) cM u jcbi00,        aw = (dt/2) cM w jcbi11                (advection, :81)
+//   dr = (dt/2) hcond JxW jcbi00^2, ds = (dt/2) hcond JxW jcbi11^2         (diffusion, :79)
+// (the box's Jacobian is diagonal; jcbi01q and jcbi10q are not read).  Dirichlet rows and columns
+// as the reference's elimination (:118-130): fixed entries of x are zeroed before the element
+// products and fixed rows return diag_i x_i, diag the summed element diagonals.  A CTA owns the
+// nodes of an ETX x ETZ tile of elements, recomputes a one-element halo on the left and bottom,
+// and sums every owned node's incident elements in ascending element order from shared memory.
+constexpr int ETX = 16, ETZ = 8;
+constexpr int EEX = ETX + 1, EEZ = ETZ + 1, ENEL = EEX * EEZ;   // 153 element computations
+constexpr int ELX = 2 * ETX + 3, ELZ = 2 * ETZ + 3;           // 35 x 19 staged nodes
+constexpr int E_THREADS = 160;
+constexpr int E_PLANES = 5;
+
+__constant__ RefTables c_eref;
+
+struct EnergyOp {
+  const double* planes;   // [(c * 9 + q) * nel + e], c = cM, au, aw, dr, ds
+  const double* diag;     // summed element diagonals (nn)
+  const uint8_t* fix;     // Dirichlet flags (nn)
+};
+
+inline int64_t eop_plane_doubles(mw_box b) { return (int64_t)E_PLANES * 9 * b.nelx * b.nelz; }
+inline int64_t eop_nodes(mw_box b) { return (int64_t)(2 * b.nelx + 1) * (2 * b.nelz + 1); }
+inline EnergyOp eop_view(mw_box b, const void* op) {
+  EnergyOp o;
+  o.planes = (const double*)op;
+  o.diag = o.planes + eop_plane_doubles(b);
+  o.fix = reinterpret_cast<const uint8_t*>(o.diag + eop_nodes(b));
+  return o;
+}
+
+MW_D double eN(int q, int k) { return c_eref.NV[q * 9 + k]; }
+MW_D double eR(int q, int k) { return c_eref.dr[q * 9 + k]; }
+MW_D double eS(int q, int k) { return c_eref.dt[q * 9 + k]; }
+
+// Gauss point q's contribution to y_k (k = 0..8) of one element from the staged node values: xa
+// feeds the mass term, xb the advection and diffusion terms (the same array for the operator
+// itself); c: the point's five coefficients.  Terms whose basis value vanishes at a Gauss point are
+// dropped at compile time.
+MW_D void energy_point(int q, const double (&c)[E_PLANES], const double* xa, const double* xb, double* y) {
+  double xv = 0.0, gr = 0.0, gs = 0.0;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    if (ref_nv(q, k) != 0.0) xv += eN(q, k) * xa[k];
+    if (ref_dr(q, k) != 0.0) gr += eR(q, k) * xb[k];
+    if (ref_dt(q, k) != 0.0) gs += eS(q, k) * xb[k];
+  }
+  const double P = c[0] * xv + c[1] * gr + c[2] * gs;
+  const double Qr = c[3] * gr, Qs = c[4] * gs;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    if (ref_nv(q, k) != 0.0) y[k] += eN(q, k) * P;
+    if (ref_dr(q, k) != 0.0) y[k] += eR(q, k) * Qr;
+    if (ref_dt(q, k) != 0.0) y[k] += eS(q, k) * Qs;
+  }
+}
+
+// tile geometry of tile t: first owned element (ex0, ez0), owned node ranges [ix0, ix1) x [iz0, iz1)
+struct ETile {
+  int ex0, ez0, ix0, ix1, iz0, iz1, lx0, lz0;
+};
+MW_D ETile etile(const mw_box& b, int64_t t) {
+  const int ntx = (b.nelx + ETX - 1) / ETX;
+  ETile T;
+  T.ex0 = (int)(t % ntx) * ETX;
+  T.ez0 = (int)(t / ntx) * ETZ;
+  T.ix0 = 2 * T.ex0;
+  T.iz0 = 2 * T.ez0;
+  T.ix1 = T.ex0 + ETX >= b.nelx ? 2 * b.nelx + 1 : 2 * (T.ex0 + ETX);
+  T.iz1 = T.ez0 + ETZ >= b.nelz ? 2 * b.nelz + 1 : 2 * (T.ez0 + ETZ);
+  T.lx0 = 2 * T.ex0 - 2;        // staged lattice origin
+  T.lz0 = 2 * T.ez0 - 2;
+  return T;
+}
+
+// sum over the incident elements of node (ix, iz), ascending element order, of the element-local
+// values ye[element][9] of the tile
+MW_D double enode_sum(const mw_box& b, const ETile& T, int ix, int iz, const double* ye) {
+  const bool xo = ix & 1, zo = iz & 1;
+  const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = ix >> 1;
+  const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = iz >> 1;
+  const bool vxa = xa >= 0, vxb = !xo && xb < b.nelx;
+  const bool vza = za >= 0, vzb = !zo && zb < b.nelz;
+  double acc = 0.0;
+  if (vza) {
+    const int lez = za - (T.ez0 - 1);
+    if (vxa) acc += ye[(lez * EEX + xa - (T.ex0 - 1)) * 9 + q2_local_e(ix - 2 * xa, iz - 2 * za)];
+    if (vxb) acc += ye[(lez * EEX + xb - (T.ex0 - 1)) * 9 + q2_local_e(ix - 2 * xb, iz - 2 * za)];
+  }
+  if (vzb) {
+    const int lez = zb - (T.ez0 - 1);
+    if (vxa) acc += ye[(lez * EEX + xa - (T.ex0 - 1)) * 9 + q2_local_e(ix - 2 * xa, iz - 2 * zb)];
+    if (vxb) acc += ye[(lez * EEX + xb - (T.ex0 - 1)) * 9 + q2_local_e(ix - 2 * xb, iz - 2 * zb)];
+  }
+  return acc;
+}
+
+// Set-up: the coefficient planes, the summed element diagonals, the Dirichlet flags and the
+// right-hand side of build_matrix_energy.py:112-130, assembled per node:
+//   rhs_i = dt (heat sources)_i + (M - (dt/2) K) T_old - A x_bc   (free rows; x_bc = bc_val on fixed
+//           nodes, 0 elsewhere: the lifting of the fixed columns)
+//   rhs_i = diag_i bc_val_i                                        (fixed rows)
+// i.e. the element products of mass input T_old - x_bc and stiffness input -(T_old + x_bc).
+__global__ void __launch_bounds__(E_THREADS) k_energy_op_setup(mw_box b, mw_energy_in in, double* __restrict__ planes,
+                                                                double* __restrict__ diag, uint8_t* __restrict__ fix,
+                                                                double* __restrict__ rhs) {
+  pdl_entry();
+  __shared__ double sa[ELZ * ELX], sb[ELZ * ELX];
+  __shared__ double sy[ENEL * 9], sd[ENEL * 9];
+  const int tid = threadIdx.x;
+  const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  const int64_t ntile = (int64_t)((b.nelx + ETX - 1) / ETX) * ((b.nelz + ETZ - 1) / ETZ);
+  const double dt = in.dt_dev ? *in.dt_dev : in.dt;
+  const double h = dt * 0.5;
+  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const ETile T = etile(b, t);
+    for (int i = tid; i < ELZ * ELX; i += E_THREADS) {
+      const int ix = T.lx0 + i % ELX, iz = T.lz0 + i / ELX;
+      double a = 0.0, c = 0.0;
+      if (ix >= 0 && ix < nnx && iz >= 0 && iz < nnz) {
+        const int64_t n = (int64_t)iz * nnx + ix;
+        const double xbc = in.bc_fix_T[n] ? in.bc_val_T[n] : 0.0;
+        a = in.T[n] - xbc;
+        c = -(in.T[n] + xbc);
+      }
+      sa[i] = a;
+      sb[i] = c;
+    }
+    __syncthreads();
+    if (tid < ENEL) {
+      const int lex = tid % EEX, lez = tid / EEX;
+      const int ex = T.ex0 - 1 + lex, ez = T.ez0 - 1 + lez;
+      if (ex >= 0 && ex < b.nelx && ez >= 0 && ez < b.nelz) {
+        const int64_t e = (int64_t)ez * b.nelx + ex;
+        const bool own = lex > 0 && lez > 0;
+        double xa[9], xb[9], y[9], sk[9], dk[9];
+        const int bx = 2 * lex, bz = 2 * lez;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          const int li = (bz + q2_dz(k)) * ELX + bx + q2_dx(k);
+          xa[k] = sa[li];
+          xb[k] = sb[li];
+          y[k] = 0.0; sk[k] = 0.0; dk[k] = 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          const int64_t g = e * 9 + q;
+          const double jxw = in.JxWq[g], j00 = in.jcbi00q[g], j11 = in.jcbi11q[g];
+          const double cM = in.rho0 * in.hcapaq[g] * jxw, cK = h * in.hcondq[g] * jxw;
+          const double c[E_PLANES] = {cM, h * cM * in.uq[g] * j00, h * cM * in.wq[g] * j11, cK * j00 * j00,
+                                      cK * j11 * j11};
+          double sq = in.hprodq[g] * jxw;                                       // :83
+          if (in.formulation == 1) {                                            // :85-110 (EBA)
+            const double exx = in.exxq[g], ezz = in.ezzq[g], exz = in.exzq[g];
+            sq += 2 * in.etaq[g] *
+                  (2.0 / 3.0 * exx * exx + 2.0 / 3.0 * ezz * ezz - 2.0 / 3.0 * exx * ezz + 2 * exz * exz) * jxw;
+            sq += in.alphaq[g] * in.Tq[g] * (-in.wq[g] * in.rho0 * 10) * jxw;
+          }
+          if (own)
+#pragma unroll
+            for (int cc = 0; cc < E_PLANES; ++cc) planes[(int64_t)(cc * 9 + q) * nel + e] = c[cc];
+          energy_point(q, c, xa, xb, y);
+#pragma unroll
+          for (int k = 0; k < 9; ++k) {                 // element diagonal A_kk and heat source
+            if (ref_nv(q, k) != 0.0) {
+              sk[k] += eN(q, k) * sq;
+              double a = c[0] * eN(q, k);
+              if (ref_dr(q, k) != 0.0) a += c[1] * eR(q, k);
+              if (ref_dt(q, k) != 0.0) a += c[2] * eS(q, k);
+              dk[k] += eN(q, k) * a;
+            }
+            if (ref_dr(q, k) != 0.0) dk[k] += c[3] * eR(q, k) * eR(q, k);
+            if (ref_dt(q, k) != 0.0) dk[k] += c[4] * eS(q, k) * eS(q, k);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          sy[tid * 9 + k] = dt * sk[k] + y[k];
+          sd[tid * 9 + k] = dk[k];
+        }
+      }
+    }
+    __syncthreads();
+    const int nox = T.ix1 - T.ix0, noz = T.iz1 - T.iz0;
+    for (int i = tid; i < nox * noz; i += E_THREADS) {
+      const int ix = T.ix0 + i % nox, iz = T.iz0 + i / nox;
+      const int64_t n = (int64_t)iz * nnx + ix;
+      const double d = enode_sum(b, T, ix, iz, sd);
+      const uint8_t f = in.bc_fix_T[n] ? 1 : 0;
+      diag[n] = d;
+      fix[n] = f;
+      rhs[n] = f ? d * in.bc_val_T[n] : enode_sum(b, T, ix, iz, sy);
+    }
+    __syncthreads();
+  }
+}
+
+// y = A x (MODE 0) or y = rhs - A x (MODE 1) on the owned nodes of each tile; ND = 1 also sums
+// (a0, Ax), ND = 2 sums (Ax, a0) and (Ax, Ax), as k_energy_matvec_rows.
+template <int MODE, int ND>
+__global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(mw_box b, EnergyOp op, const double* __restrict__ x,
+                                                                const double* __restrict__ rhs, double* __restrict__ y,
+                                                                const double* __restrict__ a0, double* __restrict__ part,
+                                                                unsigned* __restrict__ counter, double* o0, double* o1) {
+  pdl_entry();
+  __shared__ double sx[ELZ * ELX];
+  __shared__ double sy[ENEL * 9];
+  const int tid = threadIdx.x;
+  const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
+  const int64_t nel = (int64_t)b.nelx * b.nelz;
+  const int64_t ntile = (int64_t)((b.nelx + ETX - 1) / ETX) * ((b.nelz + ETZ - 1) / ETZ);
+  double v[ND > 0 ? ND : 1] = {};
+  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const ETile T = etile(b, t);
+    for (int i = tid; i < ELZ * ELX; i += E_THREADS) {
+      const int ix = T.lx0 + i % ELX, iz = T.lz0 + i / ELX;
+      double a = 0.0;
+      if (ix >= 0 && ix < nnx && iz >= 0 && iz < nnz) {
+        const int64_t n = (int64_t)iz * nnx + ix;
+        a = op.fix[n] ? 0.0 : x[n];
+      }
+      sx[i] = a;
+    }
+    __syncthreads();
+    if (tid < ENEL) {
+      const int lex = tid % EEX, lez = tid / EEX;
+      const int ex = T.ex0 - 1 + lex, ez = T.ez0 - 1 + lez;
+      if (ex >= 0 && ex < b.nelx && ez >= 0 && ez < b.nelz) {
+        const int64_t e = (int64_t)ez * b.nelx + ex;
+        double xe[9], ye[9];
+        const int bx = 2 * lex, bz = 2 * lez;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          xe[k] = sx[(bz + q2_dz(k)) * ELX + bx + q2_dx(k)];
+          ye[k] = 0.0;
+        }
+        const double* pl = op.planes + e;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          double c[E_PLANES];
+#pragma unroll
+          for (int cc = 0; cc < E_PLANES; ++cc) c[cc] = __ldg(pl + (int64_t)(cc * 9 + q) * nel);
+          energy_point(q, c, xe, xe, ye);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sy[tid * 9 + k] = ye[k];
+      }
+    }
+    __syncthreads();
+    const int nox = T.ix1 - T.ix0, noz = T.iz1 - T.iz0;
+    for (int i = tid; i < nox * noz; i += E_THREADS) {
+      const int ix = T.ix0 + i % nox, iz = T.iz0 + i / nox;
+      const int64_t n = (int64_t)iz * nnx + ix;
+      const double acc = op.fix[n] ? op.diag[n] * x[n] : enode_sum(b, T, ix, iz, sy);
+      y[n] = MODE == 1 ? rhs[n] - acc : acc;
+      if (ND == 1) v[0] += a0[n] * acc;
+      if (ND == 2) {
+        v[0] += acc * a0[n];
+        v[ND - 1] += acc * acc;
+      }
+    }
+    __syncthreads();
+  }
+  if (ND == 1) {
+    double* const out[1] = {o0};
+    grid_sums<1>(*reinterpret_cast<double(*)[1]>(v), part, counter, out);
+  } else if (ND == 2) {
+    double* const out[2] = {o0, o1};
+    grid_sums<2>(*reinterpret_cast<double(*)[2]>(v), part, counter, out);
+  }
+}
+
 // Scalar slots of the iteration (sc): 0 rho = (r0, r), 1 rho of the previous iteration, 2 alpha,
 // 3 omega, 4 (r0, v), 5 (t, s), 6 (t, t), 7 (r0, r) of the new residual, 10 (b, b), 11 (r, r),
 // 12 iteration count.  Each iteration is six launches: the direction update, A p^ with (r0, v),
@@ -355,9 +640,16 @@ constexpr int E_NB = 1184;                 // dot-product CTAs (8 per SM); two p
 constexpr int64_t E_SC = 2 * E_NB + 16;    // scalars, after the partials (slot 200: the arrival counter)
 constexpr int64_t E_COEF = E_SC + 256;     // row planes, after the scalars
 
+// The operator of a solve: the element matrices VV_T (row planes built from them in the
+// workspace), or a matrix-free operator from mw_energy_op_setup.
+struct EnergyA {
+  const double* VV;
+  const void* op;
+};
+
 struct EnergyGraph {
   int dev;
-  const void *VV, *rhs, *T, *work;
+  const void *VV, *rhs, *T, *work;   // VV: the operator (VV_T or the matrix-free operator)
   int nelx, nelz, maxit;
   double rtol;
   cudaGraphExec_t exec;
@@ -366,6 +658,21 @@ static std::vector<EnergyGraph> g_energy_graphs;
 static std::mutex g_energy_mutex;
 static cudaStream_t g_energy_stream[64], g_energy_body[64];   // library stream, body-capture stream
 static cudaEvent_t g_energy_ev[64][2];
+static uint64_t g_eref_ready = 0;   // devices whose c_eref is loaded
+
+// The reference-element tables of the matrix-free operator in this device's constant bank (once
+// per device; synchronous, so the first call on a device precedes any stream capture).
+static int ensure_energy_tables() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MW_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_energy_mutex);
+  if (g_eref_ready >> dev & 1u) return MW_OK;
+  RefTables T;
+  host_ref_tables(&T);
+  if (cudaMemcpyToSymbol(c_eref, &T, sizeof(T)) != cudaSuccess) return MW_ERR_CUDA;
+  g_eref_ready |= uint64_t(1) << dev;
+  return MW_OK;
+}
 
 }  // namespace mw
 
@@ -406,10 +713,14 @@ struct EnergyBufs {
   unsigned* counter;
   RowPlanes RP;
   int grid;               // CTAs of the node kernels (at most E_NB: one partial slot each)
+  EnergyA A;
+  EnergyOp op;            // the matrix-free operator's view (A.op set)
+  int grid_op;            // CTAs of the matrix-free apply (tile loop; at most E_NB)
 };
 
-static EnergyBufs energy_bufs(mw_box box, void* work) {
+static EnergyBufs energy_bufs(mw_box box, void* work, EnergyA A) {
   EnergyBufs E;
+  E.A = A;
   E.n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
   double* w = (double*)work;
   const int64_t n = E.n;
@@ -421,17 +732,27 @@ static EnergyBufs energy_bufs(mw_box box, void* work) {
   E.coef = w + 9 * n + E_COEF;
   E.RP = row_planes(box);
   E.grid = std::min(grid_for(n, 256), E_NB);
+  if (A.op) {
+    E.op = eop_view(box, A.op);
+    E.dg = const_cast<double*>(E.op.diag);
+    const int64_t ntile = (int64_t)((box.nelx + ETX - 1) / ETX) * ((box.nelz + ETZ - 1) / ETZ);
+    E.grid_op = (int)std::min<int64_t>(ntile, E_NB);
+  }
   return E;
 }
 
 // Row planes from VV_T, r = b - A T (T holds the initial guess) with diag(A), r0 = r, (b, b) and
 // (r, r) into sc[10], sc[11].
-static void energy_start(const EnergyBufs& E, mw_box box, const double* VV_T, const double* rhs, double* T,
-                         cudaStream_t s) {
+static void energy_start(const EnergyBufs& E, mw_box box, const double* rhs, double* T, cudaStream_t s) {
   cudaMemsetAsync(E.counter, 0, sizeof(unsigned), s);
-  pdl_launch(k_energy_rows, grid_for(E.RP.total / 9, 256), 256, 0, s, box, E.RP, VV_T, E.coef);
-  pdl_launch(k_energy_matvec_rows<0>, E.grid, 256, 0, s, box, E.RP, E.coef, T, rhs, E.r, E.dg, 1, nullptr,
-             nullptr, nullptr, nullptr, nullptr);
+  if (E.A.op) {
+    pdl_launch(k_energy_op_apply<1, 0>, E.grid_op, E_THREADS, 0, s, box, E.op, (const double*)T, rhs, E.r,
+               (const double*)nullptr, (double*)nullptr, (unsigned*)nullptr, (double*)nullptr, (double*)nullptr);
+  } else {
+    pdl_launch(k_energy_rows, grid_for(E.RP.total / 9, 256), 256, 0, s, box, E.RP, E.A.VV, E.coef);
+    pdl_launch(k_energy_matvec_rows<0>, E.grid, 256, 0, s, box, E.RP, E.coef, T, rhs, E.r, E.dg, 1, nullptr,
+               nullptr, nullptr, nullptr, nullptr);
+  }
   cudaMemcpyAsync(E.r0, E.r, sizeof(double) * E.n, cudaMemcpyDeviceToDevice, s);
   const double* a[2] = {rhs, E.r};
   for (int k = 0; k < 2; ++k) {
@@ -445,25 +766,34 @@ static void energy_start(const EnergyBufs& E, mw_box box, const double* VV_T, co
 static void energy_iteration(const EnergyBufs& E, mw_box box, double* T, double rtol, int maxit,
                              cudaGraphConditionalHandle h, int use_h, cudaStream_t s) {
   pdl_launch(k_bicg_p, E.grid, 256, 0, s, E.n, E.sc, E.r, E.v, E.p, E.dg, E.ph);
-  pdl_launch(k_energy_matvec_rows<1>, E.grid, 256, 0, s, box, E.RP, E.coef, E.ph, nullptr, E.v, nullptr, 0, E.r0,
-             E.part, E.counter, E.sc + 4, nullptr);
+  if (E.A.op)
+    pdl_launch(k_energy_op_apply<0, 1>, E.grid_op, E_THREADS, 0, s, box, E.op, (const double*)E.ph,
+               (const double*)nullptr, E.v, (const double*)E.r0, E.part, E.counter, E.sc + 4, (double*)nullptr);
+  else
+    pdl_launch(k_energy_matvec_rows<1>, E.grid, 256, 0, s, box, E.RP, E.coef, E.ph, nullptr, E.v, nullptr, 0, E.r0,
+               E.part, E.counter, E.sc + 4, nullptr);
   pdl_launch(k_bicg_s, E.grid, 256, 0, s, E.n, E.sc, E.r, E.v, E.sv, E.dg, E.sh);
-  pdl_launch(k_energy_matvec_rows<2>, E.grid, 256, 0, s, box, E.RP, E.coef, E.sh, nullptr, E.t, nullptr, 0, E.sv,
-             E.part, E.counter, E.sc + 5, E.sc + 6);
+  if (E.A.op)
+    pdl_launch(k_energy_op_apply<0, 2>, E.grid_op, E_THREADS, 0, s, box, E.op, (const double*)E.sh,
+               (const double*)nullptr, E.t, (const double*)E.sv, E.part, E.counter, E.sc + 5, E.sc + 6);
+  else
+    pdl_launch(k_energy_matvec_rows<2>, E.grid, 256, 0, s, box, E.RP, E.coef, E.sh, nullptr, E.t, nullptr, 0, E.sv,
+               E.part, E.counter, E.sc + 5, E.sc + 6);
   pdl_launch(k_bicg_x, E.grid, 256, 0, s, E.n, E.sc, E.ph, E.sh, E.sv, E.t, E.r0, T, E.r, E.part, E.counter);
   pdl_launch(k_bicg_roll, 1, 32, 0, s, E.sc, rtol, maxit, h, use_h);
 }
 
 // Records the BiCGSTAB solve on the capturing stream s (body captured on b); false on failure.
-static bool energy_record(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int maxit,
-                          void* work, cudaStream_t s, cudaStream_t b);
+static bool energy_record(mw_box box, EnergyA A, const double* rhs, double* T, double rtol, int maxit, void* work,
+                          cudaStream_t s, cudaStream_t b);
 
 // The solve from a graph recorded once per (device, buffers, sizes, rtol, maxit).  A caller's own
 // (non-default) stream is captured and launched on directly, so solves of models on different
 // streams run concurrently; the legacy default stream, which cannot be captured, is served through
 // a library stream ordered after / before it by events.  Returns false when no graph can be used.
-static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol,
-                               int32_t maxit, int32_t* iters, double* relres, void* work, cudaStream_t caller) {
+static bool energy_solve_graph(mw_box box, EnergyA A, const double* rhs, double* T, double rtol, int32_t maxit,
+                               int32_t* iters, double* relres, void* work, cudaStream_t caller) {
+  const void* key = A.op ? A.op : (const void*)A.VV;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
   const bool legacy = caller == nullptr || caller == cudaStreamLegacy || caller == cudaStreamPerThread;
@@ -482,13 +812,13 @@ static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs
     }
     if (legacy) s = g_energy_stream[dev];
     for (auto& e : g_energy_graphs)
-      if (e.dev == dev && e.VV == VV_T && e.rhs == rhs && e.T == T && e.work == work && e.nelx == box.nelx &&
+      if (e.dev == dev && e.VV == key && e.rhs == rhs && e.T == T && e.work == work && e.nelx == box.nelx &&
           e.nelz == box.nelz && e.maxit == maxit && e.rtol == rtol) { exec = e.exec; break; }
     if (!exec) {
       if (g_energy_graphs.size() >= 512) return false;
       cudaStream_t rec = g_energy_stream[dev];   // recording only records: any capturable stream will do
       if (cudaStreamBeginCapture(rec, cudaStreamCaptureModeThreadLocal) != cudaSuccess) { cudaGetLastError(); return false; }
-      bool ok = energy_record(box, VV_T, rhs, T, rtol, maxit, work, rec, g_energy_body[dev]);
+      bool ok = energy_record(box, A, rhs, T, rtol, maxit, work, rec, g_energy_body[dev]);
       cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
       if (cudaStreamIsCapturing(g_energy_body[dev], &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
         cudaGraph_t gb = nullptr;
@@ -499,7 +829,7 @@ static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs
       ok = cudaStreamEndCapture(rec, &g) == cudaSuccess && g && ok && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
       if (g) cudaGraphDestroy(g);
       if (!ok) { cudaGetLastError(); return false; }
-      g_energy_graphs.push_back({dev, VV_T, rhs, T, work, box.nelx, box.nelz, maxit, rtol, exec});
+      g_energy_graphs.push_back({dev, key, rhs, T, work, box.nelx, box.nelz, maxit, rtol, exec});
     }
     if (legacy) {   // the library stream is shared: keep this path serialised
       cudaEventRecord(g_energy_ev[dev][0], caller);
@@ -520,9 +850,10 @@ static bool energy_solve_graph(mw_box box, const double* VV_T, const double* rhs
   return true;
 }
 
-int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
-                    int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream) {
-  if (work_bytes < mw_energy_solve_workspace_bytes(box) || maxit < 1) return MW_ERR_BAD_ARG;
+}  // extern "C"
+
+static int energy_solve(mw_box box, EnergyA A, const double* rhs, double* T, double rtol, int32_t maxit,
+                        int32_t* iters, double* relres, void* work, void* stream) {
   {  // the caller is recording a graph: record the solve into it, results stay on the device
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStream_t cs_stream = (cudaStream_t)stream;
@@ -533,7 +864,7 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
       std::lock_guard<std::mutex> lock(g_energy_mutex);
       if (!g_energy_body[dev] && cudaStreamCreateWithFlags(&g_energy_body[dev], cudaStreamNonBlocking) != cudaSuccess)
         return MW_ERR_CUDA;
-      if (!energy_record(box, VV_T, rhs, T, rtol, maxit, work, cs_stream, g_energy_body[dev])) return MW_ERR_CUDA;
+      if (!energy_record(box, A, rhs, T, rtol, maxit, work, cs_stream, g_energy_body[dev])) return MW_ERR_CUDA;
       if (iters) *iters = 0;
       if (relres) *relres = 0;
       return MW_OK;
@@ -543,7 +874,7 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
   {
     int32_t it = 0;
     double rel = 0;
-    if (energy_solve_graph(box, VV_T, rhs, T, rtol, maxit, &it, &rel, work, (cudaStream_t)stream)) {
+    if (energy_solve_graph(box, A, rhs, T, rtol, maxit, &it, &rel, work, (cudaStream_t)stream)) {
       if (iters) *iters = it;
       if (relres) *relres = rel;
       if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
@@ -551,14 +882,14 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
     }
   }
   cudaStream_t s = (cudaStream_t)stream;
-  const EnergyBufs E = energy_bufs(box, work);
+  const EnergyBufs E = energy_bufs(box, work, A);
   auto rd = [&](const double* d) {
     double h = 0;
     cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
     return h;
   };
-  energy_start(E, box, VV_T, rhs, T, s);
+  energy_start(E, box, rhs, T, s);
   pdl_launch(k_bicg_init, 1, 1, 0, s, E.sc, rtol, maxit, cudaGraphConditionalHandle(0), 0);
   double bb = rd(E.sc + 10);
   double rr = rd(E.sc + 11);
@@ -574,12 +905,66 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
   return std::sqrt(rr / bb) <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
 }
 
+extern "C" {
+
+int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int32_t maxit,
+                    int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream) {
+  if (!VV_T || work_bytes < mw_energy_solve_workspace_bytes(box) || maxit < 1) return MW_ERR_BAD_ARG;
+  return energy_solve(box, EnergyA{VV_T, nullptr}, rhs, T, rtol, maxit, iters, relres, work, stream);
+}
+
+size_t mw_energy_op_bytes(mw_box box) {
+  if (box.nelx <= 0 || box.nelz <= 0) return 0;
+  return (size_t)(eop_plane_doubles(box) + eop_nodes(box)) * sizeof(double) + (size_t)((eop_nodes(box) + 15) / 16) * 16;
+}
+
+int mw_energy_op_setup(mw_box box, mw_energy_in in, void* op, size_t op_bytes, double* rhs, void* stream) {
+  if (box.nelx <= 0 || box.nelz <= 0 || !op || !rhs || op_bytes < mw_energy_op_bytes(box)) return MW_ERR_BAD_ARG;
+  if (!in.T || !in.uq || !in.wq || !in.hcondq || !in.hcapaq || !in.hprodq || !in.JxWq || !in.jcbi00q || !in.jcbi11q ||
+      !in.bc_fix_T || !in.bc_val_T)
+    return MW_ERR_BAD_ARG;
+  if (in.formulation == 1 && (!in.etaq || !in.exxq || !in.ezzq || !in.exzq || !in.alphaq || !in.Tq))
+    return MW_ERR_BAD_ARG;
+  if (ensure_energy_tables() != MW_OK) return MW_ERR_CUDA;
+  double* planes = (double*)op;
+  double* diag = planes + eop_plane_doubles(box);
+  uint8_t* fix = reinterpret_cast<uint8_t*>(diag + eop_nodes(box));
+  const int64_t ntile = (int64_t)((box.nelx + ETX - 1) / ETX) * ((box.nelz + ETZ - 1) / ETZ);
+  pdl_launch(k_energy_op_setup, (int)std::min<int64_t>(ntile, 8 * num_sms()), E_THREADS, 0, (cudaStream_t)stream, box,
+             in, planes, diag, fix, rhs);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_energy_op_apply(mw_box box, const void* op, const double* x, double* y, void* stream) {
+  if (box.nelx <= 0 || box.nelz <= 0 || !op || !x || !y) return MW_ERR_BAD_ARG;
+  if (ensure_energy_tables() != MW_OK) return MW_ERR_CUDA;
+  const int64_t ntile = (int64_t)((box.nelx + ETX - 1) / ETX) * ((box.nelz + ETZ - 1) / ETZ);
+  pdl_launch(k_energy_op_apply<0, 0>, (int)std::min<int64_t>(ntile, E_NB), E_THREADS, 0, (cudaStream_t)stream, box,
+             eop_view(box, op), x, (const double*)nullptr, y, (const double*)nullptr, (double*)nullptr,
+             (unsigned*)nullptr, (double*)nullptr, (double*)nullptr);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+size_t mw_energy_op_solve_workspace_bytes(mw_box box) {
+  int64_t nn = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
+  return (size_t)(9 * nn + E_COEF) * sizeof(double);
+}
+
+int mw_energy_op_solve(mw_box box, const void* op, const double* rhs, double* T, double rtol, int32_t maxit,
+                       int32_t* iters, double* relres, void* work, size_t work_bytes, void* stream) {
+  if (!op || work_bytes < mw_energy_op_solve_workspace_bytes(box) || maxit < 1) return MW_ERR_BAD_ARG;
+  if (ensure_energy_tables() != MW_OK) return MW_ERR_CUDA;
+  return energy_solve(box, EnergyA{nullptr, op}, rhs, T, rtol, maxit, iters, relres, work, stream);
+}
+
 }  // extern "C"
 
-static bool energy_record(mw_box box, const double* VV_T, const double* rhs, double* T, double rtol, int maxit,
-                          void* work, cudaStream_t s, cudaStream_t b) {
-  const EnergyBufs E = energy_bufs(box, work);
-  energy_start(E, box, VV_T, rhs, T, s);
+static bool energy_record(mw_box box, EnergyA A, const double* rhs, double* T, double rtol, int maxit, void* work,
+                          cudaStream_t s, cudaStream_t b) {
+  const EnergyBufs E = energy_bufs(box, work, A);
+  energy_start(E, box, rhs, T, s);
   cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
   cudaGraph_t g = nullptr;
   const cudaGraphNode_t* deps = nullptr;

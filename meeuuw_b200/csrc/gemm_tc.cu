@@ -1,7 +1,9 @@
 // BF16 tensor-core GEMM for sm_100a: D[M, N] = A[M, K] * B[N, K]^T, FP32 accumulation in TMEM.
 //
-// This is the dense-contraction engine of the learned warm start (the U-Net convolutions, as
-// implicit GEMMs over an im2col matrix).  Design:
+// This is the dense-contraction engine of the learned warm start: the U-Net convolutions as
+// implicit GEMMs (k_conv3x3_bf16_tc: the A tiles loaded per tap from the activations by 4D TMA)
+// and the remaining contractions (weight gradients, small-channel layers) over im2col matrices
+// (k_gemm_bf16_tc).  Design:
 //   * one CTA per 128 x BN output tile (BN = 32..256), 128 threads;
 //   * A and B tiles (64 BF16 of K per row = 128 bytes) are brought into shared memory by TMA
 //     (cp.async.bulk.tensor, 128-byte swizzle, this GPU's own memory only) through a 4-stage
@@ -75,6 +77,27 @@ MW_D uint64_t sdesc_sw128(uint32_t saddr) {
   d |= (uint64_t)1 << 46;                    // version
   d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
   return d;
+}
+
+// The same for 64-byte rows with 64-byte swizzle (8-row atoms of 512 bytes): the K blocks of 32
+// BF16 of the implicit convolution over 32-channel tensors.
+MW_D uint64_t sdesc_sw64(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;
+  d |= (uint64_t)(512 >> 4) << 32;
+  d |= (uint64_t)1 << 46;
+  d |= (uint64_t)4 << 61;                    // SWIZZLE_64B
+  return d;
+}
+
+MW_D void tma_load_4d(void* smem_dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+      "[%2];"
+      :
+      : "r"(smem_u32(smem_dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+      : "memory");
 }
 
 // Instruction descriptor: kind::f16, A = B = BF16 (K-major), D = F32, M = 128, N = BN.
@@ -234,6 +257,132 @@ k_gemm_bf16_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
 }
 
+// 3x3 'same' convolution as an implicit GEMM: out[p, co] = sum_{tap, c} X[p + tap, c] W[co, tap C + c]
+// with the A tile of each K block -- 128 pixels (a band of 128 / W full image rows) x KB channels of
+// one tap -- loaded straight from the NHWC activations by a 4D TMA box at the tap's offset (image
+// borders read as zero: the box starts at x = -1 or y = -1, or runs past the last row / column), so
+// no im2col matrix is written.  K block kb covers taps-major K = tap C + c (the im2col layout), so
+// the K blocks, their MMAs and their order are those of the explicit GEMM over im2col(X).  KB = 64
+// (C a multiple of 64): 128-byte rows, 128-byte swizzle; KB = 32: 64-byte rows, 64-byte swizzle.
+struct ConvGeo {
+  int C, W, H;          // input channels, image width and height (W <= 128, 128 % W == 0)
+  int band;             // image rows per 128-pixel tile (128 / W)
+};
+
+template <int BN, int KB>
+__global__ void __launch_bounds__(GT_THREADS, 1)
+k_conv3x3_bf16_tc(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW, ConvGeo cg,
+                  int M, int N, GemmEpi ep, int32_t* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  constexpr int A_BYTES = GT_BM * KB * 2;
+  constexpr int B_BYTES = BN * KB * 2;
+  constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  uint64_t* bars = (uint64_t*)(base + GT_STAGES * STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + GT_STAGES;
+  uint64_t* done = bars + 2 * GT_STAGES;
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * GT_STAGES + 1);
+  __shared__ int abort_flag;
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * GT_BM, n0 = blockIdx.y * BN;
+  const int hw = cg.H * cg.W;
+  const int img = m0 / hw, y0 = (m0 - img * hw) / cg.W;     // tiles never straddle images (hw % 128 == 0)
+  const int cpb = cg.C / KB;                                 // K blocks per tap
+  const int nkb = 9 * cpb;
+
+  if (tid == 0) {
+    abort_flag = 0;
+    for (int s = 0; s < GT_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (tid == 0) {
+    const uint32_t idesc = idesc_bf16(BN);
+    bool ok = true;
+    int produced = 0, consumed = 0;
+    for (int it = 0; it < nkb + GT_STAGES - 1 && ok; ++it) {
+      if (it < nkb) {                                           // produce K block it
+        const int s = it % GT_STAGES;
+        if (it >= GT_STAGES) ok = mbar_wait(&empty[s], (uint32_t)((it / GT_STAGES - 1) & 1));
+        if (!ok) break;
+        unsigned char* sa = base + s * STAGE_BYTES;
+        const int tap = it / cpb, c0 = (it - tap * cpb) * KB;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+        tma_load_4d(sa, &tmX, &full[s], c0, tap % 3 - 1, y0 + tap / 3 - 1, img);
+        tma_load_2d(sa + A_BYTES, &tmW, &full[s], it * KB, n0);
+        produced = it + 1;
+      }
+      const int kc = it - (GT_STAGES - 1);
+      if (kc >= 0 && kc < nkb) {                                // consume K block kc
+        const int s = kc % GT_STAGES;
+        ok = mbar_wait(&full[s], (uint32_t)((kc / GT_STAGES) & 1));
+        if (!ok) break;
+        consumed = kc + 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t sa = smem_u32(base + s * STAGE_BYTES);
+        const uint32_t sb = sa + A_BYTES;
+#pragma unroll
+        for (int k = 0; k < KB / 16; ++k) {
+          const uint64_t da = KB == 64 ? sdesc_sw128(sa + k * 32) : sdesc_sw64(sa + k * 32);
+          const uint64_t db = KB == 64 ? sdesc_sw128(sb + k * 32) : sdesc_sw64(sb + k * 32);
+          mma_bf16(tmem, da, db, idesc, (kc > 0 || k > 0) ? 1u : 0u);
+        }
+        mma_commit(&empty[s]);
+      }
+    }
+    if (!ok) {
+      abort_flag = 1;
+      set_flag(err, MW_FLAG_ITER_LIMIT);
+      for (int k = consumed; k < produced; ++k) mbar_wait(&full[k % GT_STAGES], (uint32_t)((k / GT_STAGES) & 1));
+    }
+    mma_commit(done);
+  }
+  __syncthreads();
+  bool done_ok = mbar_wait(done, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!done_ok) set_flag(err, MW_FLAG_ITER_LIMIT);
+  if (done_ok && !abort_flag) {
+    const int row = m0 + warp * 32 + lane;
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      const int cbase = n0 + c0;
+      if (row >= M) {
+      } else if (ep.mode == MW_GEMM_EPI_F32) {
+        float* o = (float*)ep.out + (int64_t)row * ep.ldo;
+        for (int i = 0; i < 16; ++i) {
+          const int c = cbase + i;
+          if (c < N) o[c] = v[i] + (ep.bias ? ep.bias[c] : 0.f);
+        }
+      } else {
+        __nv_bfloat16* o = (__nv_bfloat16*)ep.out + (int64_t)row * ep.ldo;
+        for (int i = 0; i < 16; ++i) {
+          const int c = cbase + i;
+          if (c >= N) continue;
+          float x = v[i] + (ep.bias ? ep.bias[c] : 0.f);
+          if (ep.relu) x = fmaxf(x, 0.f);
+          o[c] = __float2bfloat16(x);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+}
+
 // out[i] = sum_s part[s * stride + i] (+ bias per column)
 __global__ void k_splitk_reduce(int64_t n, int splits, int64_t stride, int ncols, const float* __restrict__ part,
                                 const float* __restrict__ bias, float* __restrict__ out) {
@@ -259,18 +408,52 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
 
 // 2D row-major BF16 [rows, cols] (cols contiguous), box {64 cols, box_rows rows}, 128B swizzle,
 // out-of-bounds rows/cols read as zero.
-static int make_map(CUtensorMap* m, const void* ptr, int64_t rows, int64_t cols, int box_rows) {
+static int make_map(CUtensorMap* m, const void* ptr, int64_t rows, int64_t cols, int box_rows, int box_k = GT_BK) {
   auto enc = get_encode();
   if (!enc) return MW_ERR_CUDA;
   if (((uintptr_t)ptr & 15) || (cols * 2) % 16) return MW_ERR_BAD_ARG;
   cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)(cols * 2)};
-  cuuint32_t box[2] = {(cuuint32_t)GT_BK, (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, box_k == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? MW_OK : MW_ERR_BAD_ARG;
+}
+
+// NHWC BF16 activations [B, H, W, C] as a 4D map (C innermost), box {KB channels, W, band, 1}:
+// one box is a 128-pixel band of full image rows for one tap; rows and columns outside the image
+// read as zero.
+static int make_map_nhwc(CUtensorMap* m, const void* ptr, int B, int H, int W, int C, int band, int kb) {
+  auto enc = get_encode();
+  if (!enc) return MW_ERR_CUDA;
+  if (((uintptr_t)ptr & 15) || (C * 2) % 16) return MW_ERR_BAD_ARG;
+  cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)C * 2 * W, (cuuint64_t)C * 2 * W * H};
+  cuuint32_t box[4] = {(cuuint32_t)kb, (cuuint32_t)W, (cuuint32_t)band, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(ptr), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, kb == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? MW_OK : MW_ERR_BAD_ARG;
+}
+
+template <int BN, int KB>
+static int launch_conv(const CUtensorMap& tx, const CUtensorMap& tw, ConvGeo cg, int M, int N, GemmEpi ep,
+                       int32_t* err, cudaStream_t s) {
+  dim3 grid((M + GT_BM - 1) / GT_BM, (N + BN - 1) / BN, 1);
+  const size_t smem = 1024 + GT_STAGES * (GT_BM * KB * 2 + BN * KB * 2) + 256;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(k_conv3x3_bf16_tc<BN, KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return MW_ERR_CUDA;
+    attr_set = true;
+  }
+  k_conv3x3_bf16_tc<BN, KB><<<grid, GT_THREADS, smem, s>>>(tx, tw, cg, M, N, ep, err);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
 }
 
 template <int BN>
@@ -348,6 +531,45 @@ int mw_gemm_bf16_tn(int32_t M, int32_t N, int32_t K, const void* A, int64_t lda,
     MW_CHECK_LAUNCH();
   }
   return MW_OK;
+}
+
+int mw_conv3x3_bf16(int32_t B, int32_t H, int32_t W, int32_t C, const void* X, int32_t N, const void* Wt, int64_t ldw,
+                    mw_gemm_epilogue epi, int32_t* err, void* stream) {
+  if (B <= 0 || H <= 0 || W <= 0 || N <= 0 || !X || !Wt) return MW_ERR_BAD_ARG;
+  if (C <= 0 || C % 32 != 0 || W > GT_BM || GT_BM % W != 0 || ((int64_t)H * W) % GT_BM != 0) return MW_ERR_BAD_ARG;
+  if (ldw < 9 * (int64_t)C || epi.splits > 1) return MW_ERR_BAD_ARG;
+  const int KB = C % 64 == 0 ? 64 : 32;
+  ConvGeo cg;
+  cg.C = C; cg.W = W; cg.H = H; cg.band = GT_BM / W;
+  const int M = B * H * W;
+  int BN = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  CUtensorMap tx, tw;
+  int rc = make_map_nhwc(&tx, X, B, H, W, C, cg.band, KB);
+  if (rc) return rc;
+  rc = make_map(&tw, Wt, N, ldw, BN, KB);
+  if (rc) return rc;
+  GemmEpi ep;
+  ep.mode = epi.mode;
+  ep.relu = epi.relu;
+  ep.bias = epi.bias;
+  ep.out = epi.out;
+  ep.ldo = epi.ldo;
+  ep.split_stride = 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (KB == 64) {
+    switch (BN) {
+      case 32: return launch_conv<32, 64>(tx, tw, cg, M, N, ep, err, s);
+      case 64: return launch_conv<64, 64>(tx, tw, cg, M, N, ep, err, s);
+      case 128: return launch_conv<128, 64>(tx, tw, cg, M, N, ep, err, s);
+      default: return launch_conv<256, 64>(tx, tw, cg, M, N, ep, err, s);
+    }
+  }
+  switch (BN) {
+    case 32: return launch_conv<32, 32>(tx, tw, cg, M, N, ep, err, s);
+    case 64: return launch_conv<64, 32>(tx, tw, cg, M, N, ep, err, s);
+    case 128: return launch_conv<128, 32>(tx, tw, cg, M, N, ep, err, s);
+    default: return launch_conv<256, 32>(tx, tw, cg, M, N, ep, err, s);
+  }
 }
 
 size_t mw_gemm_workspace_bytes(int32_t M, int32_t N, int32_t splits) {

@@ -201,6 +201,14 @@ def assemble_stokes(box, blocks, precision, q, tables, bc_fix_V, bc_val_V, eta_r
     return out
 
 
+def _energy_in(T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, dt_dev):
+    keys = ("rhoq", "etaq", "Tq", "uq", "wq", "hcondq", "hcapaq", "alphaq", "hprodq", "exxq", "ezzq", "exzq", "JxWq",
+            "jcbi00q", "jcbi01q", "jcbi10q", "jcbi11q")
+    return L.MwEnergyIn(ptr(T), *[ptr(q.get(k)) for k in keys], ptr(tables["N_V"]), ptr(tables["dNdr_V"]),
+                        ptr(tables["dNdt_V"]), ptr(as_u8(bc_fix_T)), ptr(bc_val_T), float(dt), float(rho0),
+                        ptr(dt_dev), 1 if formulation == "EBA" else 0)
+
+
 def assemble_energy(box, precision, T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, VV=None, rhs=None,
                     dt_dev=None):
     nel = box.nelx * box.nelz
@@ -208,14 +216,28 @@ def assemble_energy(box, precision, T, q, tables, bc_fix_T, bc_val_T, dt, rho0, 
     dty = torch.float32 if precision == 1 else f64
     VV = torch.empty(nel * 81, dtype=dty, device=T.device) if VV is None else VV
     rhs = torch.empty(nn, dtype=f64, device=T.device) if rhs is None else rhs
-    keys = ("rhoq", "etaq", "Tq", "uq", "wq", "hcondq", "hcapaq", "alphaq", "hprodq", "exxq", "ezzq", "exzq", "JxWq",
-            "jcbi00q", "jcbi01q", "jcbi10q", "jcbi11q")
-    ins = L.MwEnergyIn(ptr(T), *[ptr(q.get(k)) for k in keys], ptr(tables["N_V"]), ptr(tables["dNdr_V"]),
-                       ptr(tables["dNdt_V"]), ptr(as_u8(bc_fix_T)), ptr(bc_val_T), float(dt), float(rho0),
-                       ptr(dt_dev), 1 if formulation == "EBA" else 0)
+    ins = _energy_in(T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, dt_dev)
     wp, wb = workspace("asm").get(L.lib().mw_assemble_energy_workspace_bytes(box))
     call("mw_assemble_energy", box, int(precision), ins, ptr(VV), ptr(rhs), wp, wb, stream_ptr())
     return VV, rhs
+
+
+def energy_op_setup(box, T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, op=None, rhs=None, dt_dev=None):
+    """Matrix-free energy operator (Gauss-point coefficients, diagonal, Dirichlet flags) and the
+    right-hand side of build_matrix_energy.  Returns (op, rhs); op is a uint8 device buffer."""
+    nn = (2 * box.nelx + 1) * (2 * box.nelz + 1)
+    nb = L.lib().mw_energy_op_bytes(box)
+    op = torch.empty(nb, dtype=torch.uint8, device=T.device) if op is None else op
+    rhs = torch.empty(nn, dtype=f64, device=T.device) if rhs is None else rhs
+    ins = _energy_in(T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, dt_dev)
+    call("mw_energy_op_setup", box, ins, ptr(op), op.numel(), ptr(rhs), stream_ptr())
+    return op, rhs
+
+
+def energy_op_apply(box, op, x, y=None):
+    y = torch.empty_like(x) if y is None else y
+    call("mw_energy_op_apply", box, ptr(op), ptr(x), ptr(y), stream_ptr())
+    return y
 
 
 # ----------------------------------------------------------------------------- post
@@ -316,11 +338,27 @@ def energy_solve(box, VV, rhs, T, rtol=1e-12, maxit=200):
     return it.value, rr.value
 
 
-def energy_device_info(box):
-    """(iterations, relative residual) of the last energy solve on this stream, from the device."""
+def energy_op_solve(box, op, rhs, T, rtol=1e-12, maxit=200):
+    """energy_solve on the matrix-free operator of energy_op_setup."""
     it = ctypes.c_int32()
     rr = ctypes.c_double()
-    wp, wb = workspace("energy").get(L.lib().mw_energy_solve_workspace_bytes(box))
+    wp, wb = workspace("energy_op").get(L.lib().mw_energy_op_solve_workspace_bytes(box))
+    rc = L.lib().mw_energy_op_solve(box, ptr(op), ptr(rhs), ptr(T), float(rtol), int(maxit), ctypes.byref(it),
+                                    ctypes.byref(rr), wp, wb, stream_ptr())
+    if rc not in (0, 3):
+        raise RuntimeError(f"mw_energy_op_solve returned {L.STATUS.get(rc, rc)}")
+    return it.value, rr.value
+
+
+def energy_device_info(box, op=False):
+    """(iterations, relative residual) of the last energy solve on this stream (op: of the
+    matrix-free one), from the device."""
+    it = ctypes.c_int32()
+    rr = ctypes.c_double()
+    if op:
+        wp, wb = workspace("energy_op").get(L.lib().mw_energy_op_solve_workspace_bytes(box))
+    else:
+        wp, wb = workspace("energy").get(L.lib().mw_energy_solve_workspace_bytes(box))
     call("mw_energy_device_info", box, wp, ctypes.byref(it), ctypes.byref(rr), stream_ptr())
     return it.value, rr.value
 
@@ -349,6 +387,30 @@ L.extra_protos({
 })
 
 EPI_F32, EPI_BF16 = 0, 1
+
+
+L.extra_protos({
+    "mw_conv3x3_bf16": (ctypes.c_int32, [ctypes.c_int32] * 4 + [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                                               ctypes.c_int64, MwGemmEpilogue, ctypes.c_void_p,
+                                                               ctypes.c_void_p]),
+})
+
+
+def conv3x3_ok(C, H, W):
+    """Whether mw_conv3x3_bf16 takes this shape (else im2col + gemm_bf16_tn)."""
+    return C % 32 == 0 and W <= 128 and 128 % W == 0 and (H * W) % 128 == 0
+
+
+def conv3x3_bf16(X, B, H, W, C, Wt, out=None, bias=None, relu=False, out_bf16=False, err=None):
+    """3x3 'same' convolution of NHWC BF16 X [B*H*W, C] with Wt [N, Kp] (K = tap*C + c) as an
+    implicit GEMM on the tensor cores: out [B*H*W, N]."""
+    N = Wt.shape[0]
+    M = B * H * W
+    if out is None:
+        out = torch.empty(M, N, dtype=torch.bfloat16 if out_bf16 else torch.float32, device=X.device)
+    ep = MwGemmEpilogue(EPI_BF16 if out_bf16 else EPI_F32, int(bool(relu)), 1, ptr(bias), ptr(out), out.stride(0))
+    call("mw_conv3x3_bf16", B, H, W, C, ptr(X), N, ptr(Wt), Wt.stride(0), ep, ptr(err), stream_ptr())
+    return out
 
 
 def gemm_bf16_tn(A, B, out=None, bias=None, relu=False, splits=1, out_bf16=False, err=None):

@@ -21,7 +21,7 @@ f64 = torch.float64
 
 class GPUModel:
     def __init__(self, cfg, host=None, stokes="mixed", scheme="cd_u_eta", tol=1e-8, warm_start="previous",
-                 inner_rtol=None, device="cuda"):
+                 inner_rtol=None, energy="matrix_free", device="cuda"):
         L.require_cuda()
         self.cfg = cfg
         host = host if host is not None else configs.build_host_model(cfg)
@@ -39,7 +39,12 @@ class GPUModel:
         # the cold start included: on the 512x512 FK model 1e-9 does (93 ms per warm step, 97 at
         # 1e-10), 1e-8 ... 1e-7 stall at the first step (200 Schur iterations, residual ~1e-8 to
         # 1e-7) although they would be faster on warm steps (86 ... 77 ms) (measured)
-        self.inner_rtol = inner_rtol if inner_rtol is not None else (2e-2 if stokes == "mixed" else 1e-9)
+        # The inexact Schur iteration stalls near its inner solves' accuracy, so a tighter outer
+        # tolerance tightens the FP64 inner one with it (10x below; at an outer 1e-10, inner 1e-9
+        # stalls the 512x512 cold start at 200 iterations)
+        if inner_rtol is None:
+            inner_rtol = 2e-2 if stokes == "mixed" else min(1e-9, 0.1 * tol)
+        self.inner_rtol = inner_rtol
         D = lambda a, dt=None: torch.as_tensor(a, dtype=dt).to(device).contiguous()
         self.tables = fe_tables.device_tables(device)
         self.geo = fe_tables.uniform_geometry(nel, box.hx, box.hz, device)
@@ -74,7 +79,17 @@ class GPUModel:
         self.bc_fix_T, self.bc_val_T = D(host.bc_fix_T, torch.bool), D(host.bc_val_T, f64)
         self.rhs_f, self.rhs_h = E(2 * nn), E(npp)
         self.solV, self.solP = Z(2 * nn), Z(npp)
-        self.VV_T, self.rhs_T = E(nel * 81), E(nn)
+        # energy operator: "matrix_free" (Gauss-point coefficients, 360 B per element, no element
+        # matrices) or "matrices" (the reference's VV_T, 648 B per element, regrouped per solve)
+        if energy not in ("matrix_free", "matrices"):
+            raise ValueError(f"energy must be 'matrix_free' or 'matrices', not {energy!r}")
+        self.energy_form = energy
+        self.rhs_T = E(nn)
+        if energy == "matrix_free":
+            self.VV_T = None
+            self.energy_op = torch.empty(L.lib().mw_energy_op_bytes(box), dtype=torch.uint8, device=device)
+        else:
+            self.VV_T, self.energy_op = E(nel * 81), None
         self.hf = [E(nn) for _ in range(4)]
         # device scalars
         self.dt_state = torch.tensor([1e50, 1e50], dtype=f64, device=device)
@@ -263,9 +278,16 @@ class GPUModel:
             for k in ("exxq", "ezzq", "exzq"):
                 q[k] = qf.get(k)
             q.update(self.geo)
-            ops.assemble_energy(b, 0, self.T, q, tb, self.bc_fix_T, self.bc_val_T, 0.0, c.rho0, c.formulation,
-                                self.VV_T, self.rhs_T, dt_dev=self.dt_out)
-            self.energy_info = ops.energy_solve(b, self.VV_T, self.rhs_T, self.T, rtol=self.energy_rtol, maxit=300)
+            if self.energy_op is not None:
+                ops.energy_op_setup(b, self.T, q, tb, self.bc_fix_T, self.bc_val_T, 0.0, c.rho0, c.formulation,
+                                    self.energy_op, self.rhs_T, dt_dev=self.dt_out)
+                self.energy_info = ops.energy_op_solve(b, self.energy_op, self.rhs_T, self.T, rtol=self.energy_rtol,
+                                                       maxit=300)
+            else:
+                ops.assemble_energy(b, 0, self.T, q, tb, self.bc_fix_T, self.bc_val_T, 0.0, c.rho0, c.formulation,
+                                    self.VV_T, self.rhs_T, dt_dev=self.dt_out)
+                self.energy_info = ops.energy_solve(b, self.VV_T, self.rhs_T, self.T, rtol=self.energy_rtol,
+                                                    maxit=300)
             # heat flux and Nu (meeuuw.py:2259-2308)
             ops.nodal_heat_flux(b, self.T, nd["hcond"], tb, out=self.hf)
             ops.compute_nu(b, self.T, self.hf[0], self.hf[1], nd["hcond"], self.nu_out)
@@ -293,7 +315,7 @@ class GPUModel:
             with ops.workspace_scope(self):
                 self.last_solve = self.solver.device_info(self.tol)
                 if self.cfg.solve_T:
-                    self.energy_info = ops.energy_device_info(self.box)
+                    self.energy_info = ops.energy_device_info(self.box, op=self.energy_op is not None)
             self._replayed = False
         err = int(self.err.item())
         d = dict(istep=self.istep, dt=float(self.dt_out[0].item()), vrms=float(self.gq_out[0].item()),

@@ -1,9 +1,13 @@
 """Learned warm start: a 4-level U-Net mapping (T, log10 eta) to a Stokes initial guess (u, w, p).
 
-Every convolution is an implicit GEMM on this library's tcgen05 BF16 kernel (FP32 accumulation):
+Every convolution is a GEMM on this library's tcgen05 BF16 kernels (FP32 accumulation):
 forward  A = conv(X):   out[M, Cout]  = im2col(X)[M, Kp]    . W[Cout, Kp]^T
 data grad dX:           dX[M, Cin]    = im2col(dZ)[M, Kp']  . Wflip[Cin, Kp']^T
 weight grad dW:         dW[Cout, Kp]  = dZ^T[Cout, M]       . im2col(X)^T[Kp, M]^T   (split-K)
+The first two are implicit GEMMs (mw_conv3x3_bf16: each K block's tile loaded from the NHWC
+activations by TMA at the tap's offset) wherever the input has a multiple of 32 channels; the
+2-channel input layer, the 5-channel head's data gradient and the weight gradients use an
+im2col matrix.
 Activations are NHWC BF16, gradients FP32, master weights FP32 with Adam.  The network's
 arithmetic is the library's kernels; torch allocates buffers and gathers training batches.
 
@@ -21,7 +25,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .ops import gemm_bf16_tn, workspace
+from .ops import conv3x3_bf16, conv3x3_ok, gemm_bf16_tn, workspace
 from ._lib import c_double, c_int32, c_int64, c_void_p, call, ptr, stream_ptr
 
 bf16, f32 = torch.bfloat16, torch.float32
@@ -50,6 +54,11 @@ L.extra_protos({
     "mw_unet_targets": (c_int32, [L.MwBox, c_void_p, c_void_p, c_void_p, c_double, c_double, c_void_p, c_void_p,
                                   c_void_p]),
 })
+
+
+# 3x3 convolutions whose input channels are a multiple of 32 (and images 128-pixel bands) run as
+# implicit GEMMs (ops.conv3x3_bf16, no im2col matrix); False forces im2col + GEMM everywhere
+IMPLICIT = True
 
 
 def _kp(c):
@@ -81,6 +90,8 @@ class Conv:
         return [(self.w, self.gw, self.mw, self.vw, self.w16), (self.b, self.gb, self.mb, self.vb, None)]
 
     def forward(self, X, B, H, W, out_f32=False):
+        if IMPLICIT and conv3x3_ok(self.cin, H, W):
+            return conv3x3_bf16(X, B, H, W, self.cin, self.w16, bias=self.b, relu=self.relu, out_bf16=not out_f32)
         M = B * H * W
         col = _buf(("col", M, self.kp), (M, self.kp), bf16)
         call("mw_unet_im2col", B, H, W, self.cin, self.kp, 0, 0, ptr(X), ptr(col), stream_ptr())
@@ -103,6 +114,8 @@ class Conv:
         if not need_dx:
             return None
         call("mw_unet_weights_bwd", self.cout, self.cin, self.kp, self.kpo, ptr(self.w), ptr(self.wt16), stream_ptr())
+        if IMPLICIT and conv3x3_ok(self.cout, H, W):
+            return conv3x3_bf16(dZ, B, H, W, self.cout, self.wt16)
         colZ = _buf(("colZ", M, self.kpo), (M, self.kpo), bf16)
         call("mw_unet_im2col", B, H, W, self.cout, self.kpo, 0, 0, ptr(dZ), ptr(colZ), stream_ptr())
         return gemm_bf16_tn(colZ, self.wt16)

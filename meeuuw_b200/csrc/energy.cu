@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "q2_ref.cuh"
+#include "tma.cuh"
 
 namespace mw {
 
@@ -297,6 +298,7 @@ struct EnergyOp {
   const double* planes;   // [(c * 9 + q) * nel + e], c = cM, au, aw, dr, ds
   const double* diag;     // summed element diagonals (nn)
   const uint8_t* fix;     // Dirichlet flags (nn)
+  int32_t* flag;          // flag word of standalone applies (after the flags, 16-byte aligned)
 };
 
 inline int64_t eop_plane_doubles(mw_box b) { return (int64_t)E_PLANES * 9 * b.nelx * b.nelz; }
@@ -306,6 +308,7 @@ inline EnergyOp eop_view(mw_box b, const void* op) {
   o.planes = (const double*)op;
   o.diag = o.planes + eop_plane_doubles(b);
   o.fix = reinterpret_cast<const uint8_t*>(o.diag + eop_nodes(b));
+  o.flag = reinterpret_cast<int32_t*>(const_cast<uint8_t*>(o.fix) + (eop_nodes(b) + 15) / 16 * 16);
   return o;
 }
 
@@ -476,23 +479,56 @@ __global__ void __launch_bounds__(E_THREADS) k_energy_op_setup(mw_box b, mw_ener
   }
 }
 
+// Coefficients of one tile for the TMA path: planes [45][nelz][nelx] read as a 3D box of 18 x 9 x
+// 45 starting at element (ex0 - 2, ez0 - 1) -- x even, so the box starts on a 16-byte boundary --
+// into shared memory [45][9][18]; elements off the mesh read as zero.
+constexpr int EBX = ETX + 2, EBZ = EEZ;                 // 18 x 9 elements per box
+constexpr int EP_TILE = E_PLANES * 9 * EBZ * EBX;       // doubles
+constexpr long long E_SPIN = 1LL << 22;                 // mbarrier polls before a tile load is given up
+constexpr size_t E_SMEM_TMA = (size_t)(EP_TILE + ELZ * ELX + ENEL * 9) * sizeof(double) + 16;
+constexpr size_t E_SMEM = (size_t)(ELZ * ELX + ENEL * 9) * sizeof(double);
+
 // y = A x (MODE 0) or y = rhs - A x (MODE 1) on the owned nodes of each tile; ND = 1 also sums
-// (a0, Ax), ND = 2 sums (Ax, a0) and (Ax, Ax), as k_energy_matvec_rows.
-template <int MODE, int ND>
-__global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(mw_box b, EnergyOp op, const double* __restrict__ x,
+// (a0, Ax), ND = 2 sums (Ax, a0) and (Ax, Ax), as k_energy_matvec_rows.  TMA: each tile's
+// coefficients arrive in shared memory by one TMA box (one thread issues it, all wait on an
+// mbarrier while the staging of x runs), so a CTA has its 58 KB of coefficients in flight at once
+// instead of one element's 45 loads at a time; a load not complete after E_SPIN polls sets
+// MW_FLAG_ITER_LIMIT in *flag (when given), waits for it once more (bounded) and stops computing.
+// Without TMA (odd nelx: the planes' rows are not 16-byte multiples) the coefficients are read
+// from global memory.
+template <int MODE, int ND, bool TMA>
+__global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(const __grid_constant__ CUtensorMap tmP, mw_box b,
+                                                                EnergyOp op, const double* __restrict__ x,
                                                                 const double* __restrict__ rhs, double* __restrict__ y,
                                                                 const double* __restrict__ a0, double* __restrict__ part,
-                                                                unsigned* __restrict__ counter, double* o0, double* o1) {
+                                                                unsigned* __restrict__ counter, double* o0, double* o1,
+                                                                int32_t* flag) {
   pdl_entry();
-  __shared__ double sx[ELZ * ELX];
-  __shared__ double sy[ENEL * 9];
+  extern __shared__ __align__(128) double esm[];
+  double* sc = esm;                                     // TMA: the tile's coefficients
+  double* sx = esm + (TMA ? EP_TILE : 0);
+  double* sy = sx + ELZ * ELX;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sy + ENEL * 9);
   const int tid = threadIdx.x;
   const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
   const int64_t nel = (int64_t)b.nelx * b.nelz;
   const int64_t ntile = (int64_t)((b.nelx + ETX - 1) / ETX) * ((b.nelz + ETZ - 1) / ETZ);
   double v[ND > 0 ? ND : 1] = {};
+  if (TMA) {
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
+  uint32_t parity = 0;
   for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x) {
     const ETile T = etile(b, t);
+    if (TMA && tid == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of sc before the copy
+      mbar_expect_tx(bar, (uint32_t)(EP_TILE * sizeof(double)));
+      tma_load_3d(sc, &tmP, bar, T.ex0 - 2, T.ez0 - 1, 0);
+    }
     for (int i = tid; i < ELZ * ELX; i += E_THREADS) {
       const int ix = T.lx0 + i % ELX, iz = T.lz0 + i / ELX;
       double a = 0.0;
@@ -502,7 +538,20 @@ __global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(mw_box b, EnergyO
       }
       sx[i] = a;
     }
-    __syncthreads();
+    if (TMA) {
+      const bool ok = mbar_wait_bounded(bar, parity, E_SPIN);
+      parity ^= 1u;
+      if (__syncthreads_or(!ok)) {                     // give up: flag, drain the copy, stop
+        if (tid == 0) {
+          if (flag) atomicOr(flag, MW_FLAG_ITER_LIMIT);
+          mbar_wait_bounded(bar, parity ^ 1u, E_SPIN);
+        }
+        __syncthreads();
+        break;
+      }
+    } else {
+      __syncthreads();
+    }
     if (tid < ENEL) {
       const int lex = tid % EEX, lez = tid / EEX;
       const int ex = T.ex0 - 1 + lex, ez = T.ez0 - 1 + lez;
@@ -516,11 +565,13 @@ __global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(mw_box b, EnergyO
           ye[k] = 0.0;
         }
         const double* pl = op.planes + e;
+        const double* ps = sc + lez * EBX + lex + 1;
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
           double c[E_PLANES];
 #pragma unroll
-          for (int cc = 0; cc < E_PLANES; ++cc) c[cc] = __ldg(pl + (int64_t)(cc * 9 + q) * nel);
+          for (int cc = 0; cc < E_PLANES; ++cc)
+            c[cc] = TMA ? ps[(cc * 9 + q) * EBZ * EBX] : __ldg(pl + (int64_t)(cc * 9 + q) * nel);
           energy_point(q, c, xe, xe, ye);
         }
 #pragma unroll
@@ -548,6 +599,39 @@ __global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(mw_box b, EnergyO
   } else if (ND == 2) {
     double* const out[2] = {o0, o1};
     grid_sums<2>(*reinterpret_cast<double(*)[2]>(v), part, counter, out);
+  }
+}
+
+// The coefficient-plane map of the TMA path; false when the planes cannot be described (odd nelx).
+static bool eop_plane_map(CUtensorMap* m, mw_box b, const void* op) {
+  auto enc = get_encode();
+  if (!enc || (b.nelx & 1) || ((uintptr_t)op & 15)) return false;
+  cuuint64_t dims[3] = {(cuuint64_t)b.nelx, (cuuint64_t)b.nelz, (cuuint64_t)(E_PLANES * 9)};
+  cuuint64_t strides[2] = {(cuuint64_t)b.nelx * 8, (cuuint64_t)b.nelx * b.nelz * 8};
+  cuuint32_t box[3] = {(cuuint32_t)EBX, (cuuint32_t)EBZ, (cuuint32_t)(E_PLANES * 9)};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void*>(op), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Launches k_energy_op_apply<MODE, ND> on the TMA path when the map could be made.
+template <int MODE, int ND>
+static void launch_eop_apply(bool tma, const CUtensorMap& tm, int grid, cudaStream_t s, mw_box b, const EnergyOp& op,
+                             const double* x, const double* rhs, double* y, const double* a0, double* part,
+                             unsigned* counter, double* o0, double* o1, int32_t* flag) {
+  if (tma) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_energy_op_apply<MODE, ND, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)E_SMEM_TMA);
+      attr = true;
+    }
+    pdl_launch(k_energy_op_apply<MODE, ND, true>, grid, E_THREADS, E_SMEM_TMA, s, tm, b, op, x, rhs, y, a0, part, counter,
+               o0, o1, flag);
+  } else {
+    pdl_launch(k_energy_op_apply<MODE, ND, false>, grid, E_THREADS, E_SMEM, s, tm, b, op, x, rhs, y, a0, part, counter,
+               o0, o1, flag);
   }
 }
 
@@ -689,11 +773,13 @@ int mw_energy_device_info(mw_box box, const void* work, int32_t* iters, double* 
   const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
   const double* sc = (const double*)work + 9 * n + E_SC;
   double q[3];
+  int32_t flag = 0;
   cudaStream_t s = (cudaStream_t)stream;
   cudaMemcpyAsync(q, sc + 10, sizeof(q), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&flag, sc + 202, sizeof(flag), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return MW_ERR_CUDA;
   if (iters) *iters = (int32_t)q[2];
-  if (relres) *relres = std::sqrt(q[1] / q[0]);
+  if (relres) *relres = flag ? NAN : std::sqrt(q[1] / q[0]);     // a tile load given up: no result
   return MW_OK;
 }
 
@@ -716,6 +802,9 @@ struct EnergyBufs {
   EnergyA A;
   EnergyOp op;            // the matrix-free operator's view (A.op set)
   int grid_op;            // CTAs of the matrix-free apply (tile loop; at most E_NB)
+  bool tma;               // coefficient tiles by TMA (the plane map could be made)
+  CUtensorMap tm;
+  int32_t* flag;          // device flag word of the solve (a tile load given up)
 };
 
 static EnergyBufs energy_bufs(mw_box box, void* work, EnergyA A) {
@@ -732,11 +821,15 @@ static EnergyBufs energy_bufs(mw_box box, void* work, EnergyA A) {
   E.coef = w + 9 * n + E_COEF;
   E.RP = row_planes(box);
   E.grid = std::min(grid_for(n, 256), E_NB);
+  E.flag = reinterpret_cast<int32_t*>(E.sc + 202);
+  E.tma = false;
+  memset(&E.tm, 0, sizeof(E.tm));
   if (A.op) {
     E.op = eop_view(box, A.op);
     E.dg = const_cast<double*>(E.op.diag);
     const int64_t ntile = (int64_t)((box.nelx + ETX - 1) / ETX) * ((box.nelz + ETZ - 1) / ETZ);
     E.grid_op = (int)std::min<int64_t>(ntile, E_NB);
+    E.tma = eop_plane_map(&E.tm, box, A.op);
   }
   return E;
 }
@@ -744,10 +837,10 @@ static EnergyBufs energy_bufs(mw_box box, void* work, EnergyA A) {
 // Row planes from VV_T, r = b - A T (T holds the initial guess) with diag(A), r0 = r, (b, b) and
 // (r, r) into sc[10], sc[11].
 static void energy_start(const EnergyBufs& E, mw_box box, const double* rhs, double* T, cudaStream_t s) {
-  cudaMemsetAsync(E.counter, 0, sizeof(unsigned), s);
+  cudaMemsetAsync(E.counter, 0, 4 * sizeof(double), s);        // arrival counter and flag word (slots 200-203)
   if (E.A.op) {
-    pdl_launch(k_energy_op_apply<1, 0>, E.grid_op, E_THREADS, 0, s, box, E.op, (const double*)T, rhs, E.r,
-               (const double*)nullptr, (double*)nullptr, (unsigned*)nullptr, (double*)nullptr, (double*)nullptr);
+    launch_eop_apply<1, 0>(E.tma, E.tm, E.grid_op, s, box, E.op, T, rhs, E.r, nullptr, nullptr, nullptr, nullptr,
+                           nullptr, E.flag);
   } else {
     pdl_launch(k_energy_rows, grid_for(E.RP.total / 9, 256), 256, 0, s, box, E.RP, E.A.VV, E.coef);
     pdl_launch(k_energy_matvec_rows<0>, E.grid, 256, 0, s, box, E.RP, E.coef, T, rhs, E.r, E.dg, 1, nullptr,
@@ -767,15 +860,15 @@ static void energy_iteration(const EnergyBufs& E, mw_box box, double* T, double 
                              cudaGraphConditionalHandle h, int use_h, cudaStream_t s) {
   pdl_launch(k_bicg_p, E.grid, 256, 0, s, E.n, E.sc, E.r, E.v, E.p, E.dg, E.ph);
   if (E.A.op)
-    pdl_launch(k_energy_op_apply<0, 1>, E.grid_op, E_THREADS, 0, s, box, E.op, (const double*)E.ph,
-               (const double*)nullptr, E.v, (const double*)E.r0, E.part, E.counter, E.sc + 4, (double*)nullptr);
+    launch_eop_apply<0, 1>(E.tma, E.tm, E.grid_op, s, box, E.op, E.ph, nullptr, E.v, E.r0, E.part, E.counter, E.sc + 4,
+                           nullptr, E.flag);
   else
     pdl_launch(k_energy_matvec_rows<1>, E.grid, 256, 0, s, box, E.RP, E.coef, E.ph, nullptr, E.v, nullptr, 0, E.r0,
                E.part, E.counter, E.sc + 4, nullptr);
   pdl_launch(k_bicg_s, E.grid, 256, 0, s, E.n, E.sc, E.r, E.v, E.sv, E.dg, E.sh);
   if (E.A.op)
-    pdl_launch(k_energy_op_apply<0, 2>, E.grid_op, E_THREADS, 0, s, box, E.op, (const double*)E.sh,
-               (const double*)nullptr, E.t, (const double*)E.sv, E.part, E.counter, E.sc + 5, E.sc + 6);
+    launch_eop_apply<0, 2>(E.tma, E.tm, E.grid_op, s, box, E.op, E.sh, nullptr, E.t, E.sv, E.part, E.counter, E.sc + 5,
+                           E.sc + 6, E.flag);
   else
     pdl_launch(k_energy_matvec_rows<2>, E.grid, 256, 0, s, box, E.RP, E.coef, E.sh, nullptr, E.t, nullptr, 0, E.sv,
                E.part, E.counter, E.sc + 5, E.sc + 6);
@@ -843,10 +936,12 @@ static bool energy_solve_graph(mw_box box, EnergyA A, const double* rhs, double*
   const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1);
   const double* sc = (const double*)work + 9 * n + E_SC;
   double q[3];
+  int32_t flag = 0;
   cudaMemcpyAsync(q, sc + 10, sizeof(q), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&flag, sc + 202, sizeof(flag), cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) return false;
   if (iters) *iters = (int32_t)q[2];
-  if (relres) *relres = std::sqrt(q[1] / q[0]);
+  if (relres) *relres = flag ? NAN : std::sqrt(q[1] / q[0]);
   return true;
 }
 
@@ -899,10 +994,14 @@ static int energy_solve(mw_box box, EnergyA A, const double* rhs, double* T, dou
     rr = rd(E.sc + 11);
     if (!std::isfinite(rr)) break;
   }
+  int32_t flag = 0;
+  cudaMemcpyAsync(&flag, E.flag, sizeof(flag), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  const double rel = flag ? NAN : std::sqrt(rr / bb);   // a tile load given up: no result
   if (iters) *iters = it - 1;
-  if (relres) *relres = std::sqrt(rr / bb);
+  if (relres) *relres = rel;
   if (cudaGetLastError() != cudaSuccess) return MW_ERR_CUDA;
-  return std::sqrt(rr / bb) <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
+  return rel <= rtol ? MW_OK : MW_ERR_NOT_CONVERGED;
 }
 
 extern "C" {
@@ -915,7 +1014,8 @@ int mw_energy_solve(mw_box box, const double* VV_T, const double* rhs, double* T
 
 size_t mw_energy_op_bytes(mw_box box) {
   if (box.nelx <= 0 || box.nelz <= 0) return 0;
-  return (size_t)(eop_plane_doubles(box) + eop_nodes(box)) * sizeof(double) + (size_t)((eop_nodes(box) + 15) / 16) * 16;
+  return (size_t)(eop_plane_doubles(box) + eop_nodes(box)) * sizeof(double) + (size_t)((eop_nodes(box) + 15) / 16) * 16 +
+         16;
 }
 
 int mw_energy_op_setup(mw_box box, mw_energy_in in, void* op, size_t op_bytes, double* rhs, void* stream) {
@@ -930,6 +1030,7 @@ int mw_energy_op_setup(mw_box box, mw_energy_in in, void* op, size_t op_bytes, d
   double* diag = planes + eop_plane_doubles(box);
   uint8_t* fix = reinterpret_cast<uint8_t*>(diag + eop_nodes(box));
   const int64_t ntile = (int64_t)((box.nelx + ETX - 1) / ETX) * ((box.nelz + ETZ - 1) / ETZ);
+  if (cudaMemsetAsync(eop_view(box, op).flag, 0, 16, (cudaStream_t)stream) != cudaSuccess) return MW_ERR_CUDA;
   pdl_launch(k_energy_op_setup, (int)std::min<int64_t>(ntile, 8 * num_sms()), E_THREADS, 0, (cudaStream_t)stream, box,
              in, planes, diag, fix, rhs);
   MW_CHECK_LAUNCH();
@@ -940,9 +1041,12 @@ int mw_energy_op_apply(mw_box box, const void* op, const double* x, double* y, v
   if (box.nelx <= 0 || box.nelz <= 0 || !op || !x || !y) return MW_ERR_BAD_ARG;
   if (ensure_energy_tables() != MW_OK) return MW_ERR_CUDA;
   const int64_t ntile = (int64_t)((box.nelx + ETX - 1) / ETX) * ((box.nelz + ETZ - 1) / ETZ);
-  pdl_launch(k_energy_op_apply<0, 0>, (int)std::min<int64_t>(ntile, E_NB), E_THREADS, 0, (cudaStream_t)stream, box,
-             eop_view(box, op), x, (const double*)nullptr, y, (const double*)nullptr, (double*)nullptr,
-             (unsigned*)nullptr, (double*)nullptr, (double*)nullptr);
+  CUtensorMap tm;
+  memset(&tm, 0, sizeof(tm));
+  const bool tma = eop_plane_map(&tm, box, op);
+  const EnergyOp o = eop_view(box, op);
+  launch_eop_apply<0, 0>(tma, tm, (int)std::min<int64_t>(ntile, E_NB), (cudaStream_t)stream, box, o, x, nullptr, y,
+                         nullptr, nullptr, nullptr, nullptr, nullptr, o.flag);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }

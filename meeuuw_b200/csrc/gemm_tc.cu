@@ -24,6 +24,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace mw {
 
@@ -33,39 +34,8 @@ constexpr int GT_BK = 64;                 // BF16 elements per K block (128 byte
 constexpr int GT_STAGES = 4;
 constexpr long long GT_SPIN = 1LL << 26;  // wait bound (iterations)
 
-MW_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-MW_D void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-MW_D void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-MW_D bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait; returns false on timeout
-MW_D bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long long i = 0; i < GT_SPIN; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-MW_D void tma_load_2d(void* smem_dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-      :
-      : "r"(smem_u32(smem_dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-      : "memory");
-}
+// wait on an mbarrier phase, bounded by GT_SPIN polls; false on timeout
+MW_D bool mbar_wait(uint64_t* bar, uint32_t parity) { return mbar_wait_bounded(bar, parity, GT_SPIN); }
 
 // Shared-memory matrix descriptor, K-major operand with 128-byte swizzle: rows of 128 bytes,
 // 8-row atoms of 1024 bytes (stride byte offset), descriptor version 1.
@@ -89,15 +59,6 @@ MW_D uint64_t sdesc_sw64(uint32_t saddr) {
   d |= (uint64_t)1 << 46;
   d |= (uint64_t)4 << 61;                    // SWIZZLE_64B
   return d;
-}
-
-MW_D void tma_load_4d(void* smem_dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2, int c3) {
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
-      "[%2];"
-      :
-      : "r"(smem_u32(smem_dst)), "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
-      : "memory");
 }
 
 // Instruction descriptor: kind::f16, A = B = BF16 (K-major), D = F32, M = 128, N = BN.
@@ -394,17 +355,6 @@ __global__ void k_splitk_reduce(int64_t n, int splits, int64_t stride, int ncols
   }
 }
 
-static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
-    cudaDriverEntryPointQueryResult q;
-    void* p = nullptr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-  }
-  return fn;
-}
 
 // 2D row-major BF16 [rows, cols] (cols contiguous), box {64 cols, box_rows rows}, 128B swizzle,
 // out-of-bounds rows/cols read as zero.

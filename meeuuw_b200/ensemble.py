@@ -46,7 +46,12 @@ def sample_configs(n_models=64, seed=0, n_range=(64, 192), Ra_range=(1e4, 1e7), 
 
 
 class Ensemble:
-    """N independent models, each on its own stream, stepped concurrently by `threads` host threads."""
+    """N independent models, each on its own stream, stepped concurrently by `threads` host threads.
+
+    CUDA maps streams onto CUDA_DEVICE_MAX_CONNECTIONS hardware work queues (8 unless the
+    environment says otherwise when CUDA initialises); with more models than queues, streams share
+    queues and their launches serialise.  Set it to 32 before the first CUDA call (bench.py
+    --ensemble does): 88 -> 129 model-steps/s for 64 models (measured)."""
 
     def __init__(self, cfgs, stokes="mixed", threads=8, tol=1e-8, guess=None, graphs=False):
         """graphs=True records each model's whole time step as one CUDA graph (after one eager

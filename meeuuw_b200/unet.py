@@ -423,7 +423,8 @@ class LearnedGuess:
       * ``previous``  - the previous step's solution (the method without the network);
       * ``learned``   - the network's prediction;
       * ``increment`` - previous solution + (network(now) - network(previous step)).
-    The candidate with the smallest Uzawa residual is handed to the solver, so the network can
+    The candidate with the smallest Uzawa residual is handed to the solver -- its pressure with the
+    velocity the judgement computed from it (the previous solution whole) -- so the network can
     never make a solve start from a worse point than the fallback.  With ``judge="cold"`` (the
     default) the network is consulted only when there is no previous solution and the previous
     step's solution is used directly otherwise; ``judge="every"`` weighs all candidates at every
@@ -437,7 +438,13 @@ class LearnedGuess:
         E = lambda t: torch.empty_like(t)
         self.nnV, self.nnP = E(model.solV), E(model.solP)          # network fields, this step
         self.prevV, self.prevP = E(model.solV), E(model.solP)      # network fields, previous step
-        self.candV, self.candP = E(model.solV), E(model.solP)
+        self.candP = E(model.solP)
+        # the velocity K^-1 (f - G P) each candidate's judgement computes: the guess handed to the
+        # solver with a learned, incremental or zero pressure (the network's own velocity is far
+        # less accurate than its pressure: at the 512x512 FK model's first step 6.3x the solution's
+        # norm off against 7e-4 for the pressure; with it the full residual starts at 38x that of
+        # zero and the solve needs 49 Schur iterations, with the consistent velocity 27, from zero 36)
+        self.uzV = {k: E(model.solV) for k in ("zero", "learned", "increment")}
         self.have_prev_nn = False
         self.cold = True
         self.picks = {k: 0 for k in ("previous", "increment", "learned", "zero")}
@@ -453,8 +460,8 @@ class LearnedGuess:
         self.cold = True
         self.have_prev_nn = False
 
-    def _res(self, m, P):
-        return m.solver.uzawa_residual(m.rhs_f, m.rhs_h, P, precision=self.prec, rtol=self.rtol)
+    def _res(self, m, P, V=None):
+        return m.solver.uzawa_residual(m.rhs_f, m.rhs_h, P, precision=self.prec, rtol=self.rtol, V=V)
 
     def __call__(self, m):
         use_nn = self.cold or self.judge == "every"
@@ -468,24 +475,24 @@ class LearnedGuess:
         zeroP = None
         if self.cold:
             zeroP = torch.zeros_like(m.solP)
-            res["zero"] = self._res(m, zeroP)
+            res["zero"] = self._res(m, zeroP, self.uzV["zero"])
         else:
             res["previous"] = self._res(m, m.solP)
             if self.have_prev_nn:
-                torch.add(m.solV, self.nnV - self.prevV, out=self.candV)
                 torch.add(m.solP, self.nnP - self.prevP, out=self.candP)
-                res["increment"] = self._res(m, self.candP)
-        res["learned"] = self._res(m, self.nnP)
+                res["increment"] = self._res(m, self.candP, self.uzV["increment"])
+        res["learned"] = self._res(m, self.nnP, self.uzV["learned"])
         best = min(res, key=lambda k: res[k] if math.isfinite(res[k]) else math.inf)
+        # the pressure of the winner with the velocity its judgement computed (the previous step's
+        # solution is kept whole: its velocity is more accurate than the judgement's solve)
         if best == "learned":
-            m.solV.copy_(self.nnV)
             m.solP.copy_(self.nnP)
         elif best == "increment":
-            m.solV.copy_(self.candV)
             m.solP.copy_(self.candP)
         elif best == "zero":
-            m.solV.zero_()
             m.solP.zero_()
+        if best != "previous":
+            m.solV.copy_(self.uzV[best])
         self.picks[best] += 1
         self.last = dict(res, pick=best)
         self.nnV, self.prevV = self.prevV, self.nnV
@@ -542,6 +549,7 @@ def cold_start_gain(net, cases, steps_before=0, n_net=128, tol=1e-8, log=None):
         V = torch.empty_like(m.solV)
         P = torch.empty_like(m.solP)
         ws.guess(rec.T, rec.eta, V, P)
+        m.solver.uzawa_residual(m.rhs_f, m.rhs_h, P, precision="f32", rtol=1e-3, V=V)   # V = K^-1 (f - G P)
         _, _, i0 = m.solver.solve(m.rhs_f, m.rhs_h, None, None, precision="mixed", tol=tol, inner_rtol=1e-3)
         _, _, i1 = m.solver.solve(m.rhs_f, m.rhs_h, V, P, precision="mixed", tol=tol, inner_rtol=1e-3)
         out.append((cfg.name, i0["outer_iters"], i1["outer_iters"], i0["inner_iters"], i1["inner_iters"]))

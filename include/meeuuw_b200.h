@@ -388,6 +388,11 @@ int mw_stokes_set_viscosity(mw_stokes* S, const double* etaq, const double* eta_
  * u or p may be NULL (treated as zero); yV or yP may be NULL (not computed). */
 int mw_stokes_apply(mw_stokes* S, const double* u, const double* p, double* yV, double* yP, void* stream);
 int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV, float* yP, void* stream);
+/* The G and G^T blocks alone (build_matrix_stokes.py:130-157, Dirichlet rows of G zero and fixed
+ * entries of u ignored, as the eliminated COO): yV = G p, yP = G^T u, as node stencils of the
+ * uniform box's element matrix (what the Schur-complement iterations apply). */
+int mw_stokes_grad(mw_stokes* S, const double* p, double* yV, void* stream);
+int mw_stokes_div(mw_stokes* S, const double* u, double* yP, void* stream);
 
 /* One multigrid V-cycle for K (the inner preconditioner); b, x in the given precision. */
 int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, void* stream);

@@ -14,6 +14,7 @@ struct RefTables {
   double NV[81];           // N_V at the Gauss points
   double NP[36];           // N_P at the Gauss points   [q*4+k]
   double wq[9];            // Gauss weights
+  double GX[36], GZ[36];   // sum_q w_q dN_V/dr (q, k) N_P(q, j) and the same with dN_V/dt  [k*4+j]
 };
 
 // The same reference-element values as compile-time expressions for the operator kernels: inside
@@ -62,6 +63,16 @@ inline void host_ref_tables(RefTables* T) {
       T->NP[q * 4 + 1] = 0.25 * (1 + r) * (1 - s);
       T->NP[q * 4 + 2] = 0.25 * (1 + r) * (1 + s);
       T->NP[q * 4 + 3] = 0.25 * (1 - r) * (1 + s);
+    }
+  for (int k = 0; k < 9; ++k)              // the pressure-gradient element matrix on the reference element
+    for (int j = 0; j < 4; ++j) {
+      double gx = 0.0, gz = 0.0;
+      for (int q2 = 0; q2 < 9; ++q2) {
+        gx += T->wq[q2] * T->dr[q2 * 9 + k] * T->NP[q2 * 4 + j];
+        gz += T->wq[q2] * T->dt[q2 * 9 + k] * T->NP[q2 * 4 + j];
+      }
+      T->GX[k * 4 + j] = gx;
+      T->GZ[k * 4 + j] = gz;
     }
 }
 

@@ -209,6 +209,97 @@ MW_D int q2_local_idx(int dx, int dz) {
   return dx == 0 ? 3 : (dx == 1 ? 6 : 2);
 }
 
+// ---------------------------------------------------------------- G and G^T as node stencils
+// On the uniform box every element's G block is the same 18 x 4 matrix, G_el[2k][j] = cx GX[k][j],
+// G_el[2k+1][j] = cz GZ[k][j] with cx = -s (hx hz / 4)(2 / hx), cz likewise (the pressure terms
+// of build_matrix_stokes.py:130-157: -s B^T N_P JxW summed over the Gauss points), so the
+// Schur-complement iteration's G p and G^T u need no element products: each node gathers its
+// incident elements' entries in ascending element order.  Fixed velocity dofs: zero rows of G,
+// zeroed entries of u for G^T (the reference's Dirichlet elimination).
+__global__ void k_grad_p(LevelGeo g, const double* __restrict__ p, const uint8_t* __restrict__ fix,
+                         const double* __restrict__ b, double* __restrict__ y) {
+  pdl_entry();
+  __shared__ double gx[36], gz[36];
+  if (threadIdx.x < 36) {
+    gx[threadIdx.x] = c_ref.GX[threadIdx.x];
+    gz[threadIdx.x] = c_ref.GZ[threadIdx.x];
+  }
+  __syncthreads();
+  const double jac = g.hx * g.hz / 4.0;
+  const double cx = -g.s * jac * (2.0 / g.hx), cz = -g.s * jac * (2.0 / g.hz);
+  const int64_t nn = (int64_t)g.nnx * g.nnz;
+  const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    const int ix = (int)(n % g.nnx), iz = (int)(n / g.nnx);
+    const bool xo = ix & 1, zo = iz & 1;
+    const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = ix >> 1;
+    const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = iz >> 1;
+    const int exs[2] = {xa, xb}, ezs[2] = {za, zb};
+    const bool vx[2] = {xa >= 0, !xo && xb < g.nx}, vz[2] = {za >= 0, !zo && zb < g.nz};
+    double ax = 0.0, az = 0.0;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        if (!vz[a] || !vx[c]) continue;
+        const int ex = exs[c], ez = ezs[a];
+        const int k = q2_local_idx(ix - 2 * ex, iz - 2 * ez);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double pv = p[q1_node(ex, ez, j, g.nx)];
+          ax += gx[k * 4 + j] * pv;
+          az += gz[k * 4 + j] * pv;
+        }
+      }
+    const uchar2 ff = f2[n];
+    double2 r{ff.x ? 0.0 : cx * ax, ff.y ? 0.0 : cz * az};
+    if (b) {
+      const double2 bb = reinterpret_cast<const double2*>(b)[n];
+      r = double2{bb.x - r.x, bb.y - r.y};
+    }
+    reinterpret_cast<double2*>(y)[n] = r;
+  }
+}
+
+__global__ void k_div_u(LevelGeo g, const double* __restrict__ u, const uint8_t* __restrict__ fix,
+                        double* __restrict__ y) {
+  pdl_entry();
+  __shared__ double gx[36], gz[36];
+  if (threadIdx.x < 36) {
+    gx[threadIdx.x] = c_ref.GX[threadIdx.x];
+    gz[threadIdx.x] = c_ref.GZ[threadIdx.x];
+  }
+  __syncthreads();
+  const double jac = g.hx * g.hz / 4.0;
+  const double cx = -g.s * jac * (2.0 / g.hx), cz = -g.s * jac * (2.0 / g.hz);
+  const int ncx = g.nx + 1;
+  const int64_t np = (int64_t)ncx * (g.nz + 1);
+  const double2* u2 = reinterpret_cast<const double2*>(u);
+  const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x) {
+    const int px = (int)(n % ncx), pz = (int)(n / ncx);
+    // incident elements in ascending order and this node's Q1 index in each
+    const int exs[4] = {px - 1, px, px - 1, px}, ezs[4] = {pz - 1, pz - 1, pz, pz}, js[4] = {2, 3, 1, 0};
+    double acc = 0.0;
+#pragma unroll 1
+    for (int e = 0; e < 4; ++e) {
+      const int ex = exs[e], ez = ezs[e], j = js[e];
+      if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+      double sx = 0.0, sz = 0.0;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const int64_t m = q2_node(ex, ez, k, g.nnx);
+        const double2 uu = u2[m];
+        const uchar2 ff = f2[m];
+        sx += gx[k * 4 + j] * (ff.x ? 0.0 : uu.x);
+        sz += gz[k * 4 + j] * (ff.y ? 0.0 : uu.y);
+      }
+      acc += cx * sx + cz * sz;
+    }
+    y[n] = acc;
+  }
+}
+
 // 1D Q2 prolongation: fine node i from coarse nodes
 MW_D int pw(int i, int* J, double* w) {
   if (!(i & 1)) { J[0] = i / 2; w[0] = 1.0; return 1; }
@@ -1514,6 +1605,16 @@ static void dsum(mw_stokes* S, int64_t n, const double* x, double* out, cudaStre
   pdl_launch(k_dot_final, 1, 256, 0, s, S->red, nb, out);
 }
 
+// y = G p (b == null) or b - G p on the fine level; y = G^T u
+static void grad_p(mw_stokes* S, const double* p, const double* b, double* y, cudaStream_t s) {
+  const int64_t nn = (int64_t)S->fine.nnx * S->fine.nnz;
+  pdl_launch(k_grad_p, grid_for(nn, 256), 256, 0, s, S->fine, p, S->fixV, b, y);
+}
+static void div_u(mw_stokes* S, const double* u, double* y, cudaStream_t s) {
+  const int64_t np = (int64_t)(S->fine.nx + 1) * (S->fine.nz + 1);
+  pdl_launch(k_div_u, grid_for(np, 256), 256, 0, s, S->fine, u, S->fixV, y);
+}
+
 template <typename R>
 static void k_only_apply(const Level<R>& L, const R* x, R* y, cudaStream_t s) {
   ApplyArgs<R> a = args0<R>();
@@ -1801,13 +1902,15 @@ static void launch_tail(Hierarchy<R>& H, int l0, bool first_done, cudaStream_t s
   pdl_launch(k_vtail<R>, TAIL_CLUSTER, tail_threads<R>(), 0, s, A);
 }
 
-// MW_FUSED_PROLONG=0 in the environment (read at the first V-cycle) launches the prolongation on
-// its own (k_prolong_add) before the post-smoothing: the same arithmetic with one launch more per
-// level and V-cycle.
+// The prolongation runs as its own launch (k_prolong_add) before the post-smoothing by default;
+// MW_FUSED_PROLONG=1 in the environment (read at the first V-cycle) folds it into the first
+// smoothing step (AM_CHEB_P) instead: the same arithmetic and results, one launch fewer per level
+// and V-cycle, but the heavier smoothing kernel made the 512x512 FK step slower (26.50 against
+// 26.15 ms, measured).
 static bool fused_prolongation() {
   static const bool on = [] {
     const char* e = getenv("MW_FUSED_PROLONG");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
   }();
   return on;
 }
@@ -2205,21 +2308,12 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
   const double* w = sp.scheme == MW_SCHEME_UZAWA3 ? nullptr : S->etae_w;
   double rel;
   // V = K^-1 (f - G P)
-  {
-    ApplyArgs<double> a = args0<double>();
-    a.p = P; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd; a.bV = f;
-    launch_apply<double, AM_RESID>(g, a, s);                 // Gd = f - G P   (u = null)
-  }
+  grad_p(S, P, f, S->Gd, s);                                // Gd = f - G P
   int inner = solve_K(S, prec, S->Gd, V, sp.inner_rtol, sp.max_inner, &rel, s);
   info->inner_iters += inner;
   // rho = G^T V - h
-  {
-    ApplyArgs<double> a = args0<double>();
-    a.u = V; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64;
-    a.yP = S->rP;
-    launch_apply<double, AM_APPLY>(g, a, s);                 // rP = G^T V (yV not written)
-    if (h) pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
-  }
+  div_u(S, V, S->rP, s);                                    // rP = G^T V
+  if (h) pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
   remove_mean(S, np, S->rP, s);
   mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
   remove_mean(S, np, S->wP, s);
@@ -2231,16 +2325,11 @@ static int uzawa(mw_stokes* S, const mw_solve_params& sp, int prec, const double
   int k;
   for (k = 0; k < sp.max_outer; ++k) {
     // z = K^-1 G d
-    ApplyArgs<double> a = args0<double>();
-    a.p = S->dP; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd;
-    launch_apply<double, AM_APPLY>(g, a, s);
+    grad_p(S, S->dP, nullptr, S->Gd, s);
     inner = solve_K(S, prec, S->Gd, S->z, sp.inner_rtol, sp.max_inner, &rel, s);
     info->inner_iters += inner;
     // G^T z, step length alpha = (rho, w) / (d, G^T z)
-    ApplyArgs<double> b2 = args0<double>();
-    b2.u = S->z; b2.eta = S->etaq64; b2.fix = S->fixV; b2.diag = S->diag64;
-    b2.yP = S->GTz;
-    launch_apply<double, AM_APPLY>(g, b2, s);
+    div_u(S, S->z, S->GTz, s);
     dot<double>(S, np, S->dP, S->GTz, sc + 1, s);
     const bool hist = sp.history && info->outer_iters < sp.history_len;
     if (hist) {                                               // ||d_k||^2, ||z_k||^2 before the updates
@@ -2508,19 +2597,10 @@ static bool uzawa_dev(mw_stokes* S, const mw_solve_params& sp, int prec, const d
   const int64_t nv = 2LL * g.nnx * g.nnz, np = (int64_t)(g.nx + 1) * (g.nz + 1);
   const double* w = sp.scheme == MW_SCHEME_UZAWA3 ? nullptr : S->etae_w;
   double* sc = S->sc;
-  {  // V = K^-1 (f - G P)
-    ApplyArgs<double> a = args0<double>();
-    a.p = P; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd; a.bV = f;
-    launch_apply<double, AM_RESID>(g, a, s);
-  }
+  grad_p(S, P, f, S->Gd, s);                                // V = K^-1 (f - G P)
   if (!solve_K_dev(S, prec, S->Gd, V, sp.inner_rtol, sp.max_inner, s0, depth)) return false;
-  {  // rho = G^T V - h
-    ApplyArgs<double> a = args0<double>();
-    a.u = V; a.eta = S->etaq64; a.fix = S->fixV; a.diag = S->diag64;
-    a.yP = S->rP;
-    launch_apply<double, AM_APPLY>(g, a, s);
-    if (h) pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
-  }
+  div_u(S, V, S->rP, s);                                    // rho = G^T V - h
+  if (h) pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
   remove_mean(S, np, S->rP, s);
   mass_solve(S, w, S->rP, S->wP, sp.mass_iters, s);
   remove_mean(S, np, S->wP, s);
@@ -2531,18 +2611,9 @@ static bool uzawa_dev(mw_stokes* S, const mw_solve_params& sp, int prec, const d
   if (!cond_handle(s, &hw)) return false;
   pdl_launch(k_dev_uz_init, 1, 1, 0, s, sc, sp.max_outer, hw);
   if (!cond_node(s, b1, cudaGraphCondTypeWhile, hw)) return false;
-  {
-    ApplyArgs<double> a = args0<double>();
-    a.p = S->dP; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd;
-    launch_apply<double, AM_APPLY>(g, a, b1);
-  }
+  grad_p(S, S->dP, nullptr, S->Gd, b1);
   if (!solve_K_dev(S, prec, S->Gd, S->z, sp.inner_rtol, sp.max_inner, s0, depth + 1)) return false;
-  {
-    ApplyArgs<double> b2 = args0<double>();
-    b2.u = S->z; b2.eta = S->etaq64; b2.fix = S->fixV; b2.diag = S->diag64;
-    b2.yP = S->GTz;
-    launch_apply<double, AM_APPLY>(g, b2, b1);
-  }
+  div_u(S, S->z, S->GTz, b1);
   dot<double>(S, np, S->dP, S->GTz, sc + U_DSD, b1);
   const bool hist = sp.history && sp.history_len > 0;
   if (hist) {
@@ -2745,6 +2816,20 @@ int mw_stokes_apply(mw_stokes* S, const double* u, const double* p, double* yV, 
   return MW_OK;
 }
 
+int mw_stokes_grad(mw_stokes* S, const double* p, double* yV, void* stream) {
+  if (!p || !pair_aligned(yV, 16)) return MW_ERR_BAD_ARG;
+  grad_p(S, p, nullptr, yV, (cudaStream_t)stream);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_div(mw_stokes* S, const double* u, double* yP, void* stream) {
+  if (!pair_aligned(u, 16) || !yP) return MW_ERR_BAD_ARG;
+  div_u(S, u, yP, (cudaStream_t)stream);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
 int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV, float* yP, void* stream) {
   if (!S->has32 || !pair_aligned(u, 8) || !pair_aligned(yV, 8)) return MW_ERR_BAD_ARG;
   if (ensure_hierarchy(S, MW_F32, (cudaStream_t)stream)) return MW_ERR_CUDA;
@@ -2804,15 +2889,11 @@ int mw_stokes_uzawa_residual(mw_stokes* S, int32_t precision, const double* f, c
   if (!rc) {
     const LevelGeo& g = S->fine;
     const int64_t np = (int64_t)(g.nx + 1) * (g.nz + 1);
-    ApplyArgs<double> a = args0<double>();
-    a.p = P; a.eta = S->etaq64; a.fix = S->fixV; a.yV = S->Gd; a.bV = f;
-    launch_apply<double, AM_RESID>(g, a, s);                 // Gd = f - G P
+    grad_p(S, P, f, S->Gd, s);                              // Gd = f - G P
     double rr = 0;
     double* Vo = V ? V : S->z;
     solve_K(S, precision, S->Gd, Vo, rtol, maxit, &rr, s);
-    ApplyArgs<double> b = args0<double>();
-    b.u = Vo; b.eta = S->etaq64; b.fix = S->fixV; b.diag = S->diag64; b.yP = S->rP;
-    launch_apply<double, AM_APPLY>(g, b, s);                 // rP = G^T V
+    div_u(S, Vo, S->rP, s);                                 // rP = G^T V
     pdl_launch(k_axpy<double>, grid_for(np, 256), 256, 0, s, np, -1.0, h, S->rP);
     remove_mean(S, np, S->rP, s);
     dot<double>(S, np, S->rP, S->rP, S->sc + 54, s);

@@ -46,6 +46,8 @@ L.extra_protos({
     "mw_stokes_set_viscosity": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_stokes_apply": (c_int32, [c_void_p] * 6),
     "mw_stokes_apply_f32": (c_int32, [c_void_p] * 6),
+    "mw_stokes_grad": (c_int32, [c_void_p] * 4),
+    "mw_stokes_div": (c_int32, [c_void_p] * 4),
     "mw_stokes_vcycle": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "mw_stokes_solve_K": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_double, c_int32,
                                     ctypes.POINTER(c_int32), ctypes.POINTER(c_double), c_void_p]),
@@ -101,6 +103,18 @@ class StokesSolver:
         name = "mw_stokes_apply_f32" if precision == "f32" else "mw_stokes_apply"
         call(name, self.h, ptr(u), ptr(p), ptr(yV), ptr(yP), stream_ptr())
         return yV, yP
+
+    def grad(self, p, yV=None):
+        """yV = G p (the Schur iterations' stencil form of the G block)."""
+        yV = torch.empty(self.nv, dtype=torch.float64, device="cuda") if yV is None else yV
+        call("mw_stokes_grad", self.h, ptr(p), ptr(yV), stream_ptr())
+        return yV
+
+    def div(self, u, yP=None):
+        """yP = G^T u (fixed velocity entries ignored)."""
+        yP = torch.empty(self.np, dtype=torch.float64, device="cuda") if yP is None else yP
+        call("mw_stokes_div", self.h, ptr(u), ptr(yP), stream_ptr())
+        return yP
 
     def solve_K(self, b, precision="f64", rtol=1e-10, maxit=500):
         x = torch.empty_like(b)

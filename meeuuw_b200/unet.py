@@ -430,10 +430,16 @@ class LearnedGuess:
     step's solution is used directly otherwise; ``judge="every"`` weighs all candidates at every
     step (one extra inner solve per candidate)."""
 
-    def __init__(self, model, net, n_net=128, judge="cold", rtol=1e-3):
+    def __init__(self, model, net, n_net=128, judge="cold", rtol=None):
         c = model.cfg
         self.ws = WarmStart(net, model.box, c.Ra, c.alphaT, model.bc_fix_V, n_net, c.rho0, c.eta_ref / model.L_ref)
-        self.judge, self.rtol = judge, rtol
+        # inner tolerance of the judgement's velocity solves: at a cold start the candidates' residuals
+        # differ by orders of magnitude and 2e-2 (the mixed solver's own inner tolerance) separates
+        # them (512x512 first step: 53.9 ms with 2e-2, 79.1 with 1e-3, 57.3 from zero; 27 Schur
+        # iterations either way, measured); weighing the previous solution against the network's
+        # increment at every step needs 1e-3
+        self.judge = judge
+        self.rtol = rtol if rtol is not None else (1e-3 if judge == "every" else 2e-2)
         self.prec = "f64" if model.stokes_precision == "f64" else "f32"
         E = lambda t: torch.empty_like(t)
         self.nnV, self.nnP = E(model.solV), E(model.solP)          # network fields, this step

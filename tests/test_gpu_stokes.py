@@ -68,6 +68,11 @@ def test_apply_matches_assembled_coo(shape):
     yV32, yP32 = S.apply(torch.as_tensor(u).float().cuda(), torch.as_tensor(p).float().cuda(), precision="f32")
     assert rel_err(yV32.double().cpu().numpy(), yref[:m.Nfem_V]) < 1e-5
     assert rel_err(yP32.double().cpu().numpy(), yref[m.Nfem_V:]) < 1e-5
+    # the G and G^T blocks alone, as the Schur iterations apply them (node stencils)
+    A = c["A"]
+    G, GT = A[:m.Nfem_V, m.Nfem_V:], A[m.Nfem_V:, :m.Nfem_V]
+    assert rel_err(S.grad(torch.as_tensor(p).cuda()).cpu().numpy(), G @ p) < 1e-12
+    assert rel_err(S.div(torch.as_tensor(u).cuda()).cpu().numpy(), GT @ u) < 1e-12
 
 
 @pytest.mark.parametrize("precision,tol,true_tol", [("f64", 1e-10, 3e-10), ("f32", 1e-4, 2e-3)])
@@ -196,9 +201,9 @@ np.savez(sys.argv[2], **out)
 
 
 def test_fused_prolongation_matches_separate_launch(tmp_path):
-    """The prolongation folded into the first post-smoothing step (default) and launched on its own
-    (MW_FUSED_PROLONG=0) give the same V-cycle and multigrid-PCG iterates bit for bit, on a mesh with
-    free-slip sides (nodes with one fixed and one free component)."""
+    """The prolongation folded into the first post-smoothing step (MW_FUSED_PROLONG=1) and launched
+    on its own (the default) give the same V-cycle and multigrid-PCG iterates bit for bit, on a mesh
+    with free-slip sides (nodes with one fixed and one free component)."""
     import os
     import subprocess
     import sys

@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--no-profile", action="store_true", help="skip the torch-profiler launch count")
     ap.add_argument("--roofline-only", action="store_true", help="set up the model, time the operator apply, exit")
     ap.add_argument("--kernels-only", action="store_true",
-                    help="set up the model, run the warm-up steps, time the particle kernels and the FP32 assembly, exit")
+                    help="set up the model, run the warm-up steps, time the particle and energy kernels, the FP32 "
+                         "assembly and the U-Net convolutions, exit")
     ap.add_argument("--host-loops", action="store_true",
                     help="solver loops driven from the host (same kernels; lets a kernel profiler list every launch)")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -161,8 +162,8 @@ def run_ours(args):
             model.step()
         model.check()
         roof = roofline_apply(model, torch)
-        print(json.dumps({"roofline": roof, "kernel_rooflines": kernel_rooflines(model, torch, roof["peak"])}),
-              flush=True)
+        print(json.dumps({"roofline": roof, "kernel_rooflines": kernel_rooflines(model, torch, roof["peak"]),
+                          "unet_tensor_cores": unet_throughput(torch)}), flush=True)
         return
     dev_index = torch.cuda.current_device()
     with ClockSampler(dev_index) as clk:

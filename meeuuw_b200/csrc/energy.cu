@@ -529,14 +529,27 @@ __global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(const __grid_cons
       mbar_expect_tx(bar, (uint32_t)(EP_TILE * sizeof(double)));
       tma_load_3d(sc, &tmP, bar, T.ex0 - 2, T.ez0 - 1, 0);
     }
-    for (int i = tid; i < ELZ * ELX; i += E_THREADS) {
-      const int ix = T.lx0 + i % ELX, iz = T.lz0 + i / ELX;
-      double a = 0.0;
-      if (ix >= 0 && ix < nnx && iz >= 0 && iz < nnz) {
-        const int64_t n = (int64_t)iz * nnx + ix;
-        a = op.fix[n] ? 0.0 : x[n];
+    {  // stage x (fixed entries zeroed): every load issued before any store, one round trip
+      constexpr int NS = (ELZ * ELX + E_THREADS - 1) / E_THREADS;
+      double xv[NS];
+      uint8_t fv[NS];
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const int i = tid + k * E_THREADS;
+        const int ix = T.lx0 + i % ELX, iz = T.lz0 + i / ELX;
+        xv[k] = 0.0;
+        fv[k] = 1;
+        if (i < ELZ * ELX && ix >= 0 && ix < nnx && iz >= 0 && iz < nnz) {
+          const int64_t n = (int64_t)iz * nnx + ix;
+          fv[k] = op.fix[n];
+          xv[k] = x[n];
+        }
       }
-      sx[i] = a;
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        const int i = tid + k * E_THREADS;
+        if (i < ELZ * ELX) sx[i] = fv[k] ? 0.0 : xv[k];
+      }
     }
     if (TMA) {
       const bool ok = mbar_wait_bounded(bar, parity, E_SPIN);
@@ -579,16 +592,40 @@ __global__ void __launch_bounds__(E_THREADS) k_energy_op_apply(const __grid_cons
       }
     }
     __syncthreads();
-    const int nox = T.ix1 - T.ix0, noz = T.iz1 - T.iz0;
-    for (int i = tid; i < nox * noz; i += E_THREADS) {
-      const int ix = T.ix0 + i % nox, iz = T.iz0 + i / nox;
-      const int64_t n = (int64_t)iz * nnx + ix;
-      const double acc = op.fix[n] ? op.diag[n] * x[n] : enode_sum(b, T, ix, iz, sy);
-      y[n] = MODE == 1 ? rhs[n] - acc : acc;
-      if (ND == 1) v[0] += a0[n] * acc;
-      if (ND == 2) {
-        v[0] += acc * a0[n];
-        v[ND - 1] += acc * acc;
+    {  // owned nodes: the loads of every node first, then the (rare) fixed rows, then the stores
+      const int nox = T.ix1 - T.ix0, noz = T.iz1 - T.iz0;
+      constexpr int NO = ((2 * ETX + 1) * (2 * ETZ + 1) + E_THREADS - 1) / E_THREADS;
+      int64_t nk[NO];
+      uint8_t fk[NO];
+      double acc[NO], bk[NO], ak[NO];
+#pragma unroll
+      for (int k = 0; k < NO; ++k) {
+        const int i = tid + k * E_THREADS;
+        nk[k] = -1;
+        fk[k] = 0;
+        acc[k] = bk[k] = ak[k] = 0.0;
+        if (i < nox * noz) {
+          const int ix = T.ix0 + i % nox, iz = T.iz0 + i / nox;
+          const int64_t n = (int64_t)iz * nnx + ix;
+          nk[k] = n;
+          fk[k] = op.fix[n];
+          if (MODE == 1) bk[k] = rhs[n];
+          if (ND > 0) ak[k] = a0[n];
+          acc[k] = enode_sum(b, T, ix, iz, sy);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < NO; ++k)
+        if (nk[k] >= 0 && fk[k]) acc[k] = op.diag[nk[k]] * x[nk[k]];
+#pragma unroll
+      for (int k = 0; k < NO; ++k) {
+        if (nk[k] < 0) continue;
+        y[nk[k]] = MODE == 1 ? bk[k] - acc[k] : acc[k];
+        if (ND == 1) v[0] += ak[k] * acc[k];
+        if (ND == 2) {
+          v[0] += acc[k] * ak[k];
+          v[ND - 1] += acc[k] * acc[k];
+        }
       }
     }
     __syncthreads();

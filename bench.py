@@ -521,9 +521,26 @@ def roofline_apply(model, torch):
     # DRAM bytes (read + write) of one launch at 512x512 from an ncu capture of this kernel
     # (profiles/k_apply_fp32_fk512.txt); other sizes scale with the element count
     traffic = int(20162560 * nel / 262144)
+    # the Chebyshev smoothing step (mode CHEB, the kernel the V-cycle launches most): reads x, b,
+    # diag, d (2nn f32 each), eta, mask; writes d and x_out (2nn f32 each); no pressure
+    b = torch.randn(nv, dtype=torch.float32, device="cuda")
+    d = torch.zeros_like(b)
+    xo = torch.empty_like(b)
+    for _ in range(5):
+        S.cheb_step_f32(b, u, xo, d, 1)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        S.cheb_step_f32(b, u, xo, d, 1)
+    e.record()
+    torch.cuda.synchronize()
+    us_c = s.elapsed_time(e) * 1000.0 / reps
+    algo_c = 4 * 2 * nn * 4 + 4 * 9 * nel + 2 * nn + 4 * 2 * nn * 2
+    cheb = {"kernel": "mw::k_apply<float, AM_CHEB> (fine level)", "us_per_launch": us_c, "algorithmic_bytes": algo_c,
+            "achieved": algo_c / (us_c * 1e-6) / 1e9, "frac": algo_c / (us_c * 1e-6) / 1e9 / peak}
     return {"kernel": "mw::k_apply<float, AM_APPLY> (fine level, 512x512)", "bound": "hbm", "achieved": achieved,
             "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "us_per_launch": us,
-            "algorithmic_bytes": algo,
+            "algorithmic_bytes": algo, "cheb_mode": cheb,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if "hbm_gbs" in peaks else "fallback 6650"}
 
 

@@ -392,6 +392,11 @@ int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV,
  * entries of u ignored, as the eliminated COO): yV = G p, yP = G^T u, as node stencils of the
  * uniform box's element matrix (what the Schur-complement iterations apply). */
 int mw_stokes_grad(mw_stokes* S, const double* p, double* yV, void* stream);
+/* One Chebyshev smoothing step of the FP32 multigrid's finest level (the kernel the V-cycle
+ * launches most): d = c1 d + c2 D^-1 (b - K x), xo = x + d with the level's coefficient pair
+ * `step` (0: the restart step, d not read).  For measurement and tests. */
+int mw_stokes_cheb_step_f32(mw_stokes* S, const float* b, const float* x, float* xo, float* d, int32_t step,
+                            void* stream);
 int mw_stokes_div(mw_stokes* S, const double* u, double* yP, void* stream);
 
 /* One multigrid V-cycle for K (the inner preconditioner); b, x in the given precision. */

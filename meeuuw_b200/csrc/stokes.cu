@@ -227,10 +227,11 @@ __global__ void k_grad_p(LevelGeo g, const double* __restrict__ p, const uint8_t
   __syncthreads();
   const double jac = g.hx * g.hz / 4.0;
   const double cx = -g.s * jac * (2.0 / g.hx), cz = -g.s * jac * (2.0 / g.hz);
-  const int64_t nn = (int64_t)g.nnx * g.nnz;
   const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(n % g.nnx), iz = (int)(n / g.nnx);
+  // one lattice row per blockIdx.y: no index division
+  for (int iz = blockIdx.y; iz < g.nnz; iz += gridDim.y)
+  for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < g.nnx; ix += gridDim.x * blockDim.x) {
+    const int64_t n = (int64_t)iz * g.nnx + ix;
     const bool xo = ix & 1, zo = iz & 1;
     const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = ix >> 1;
     const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = iz >> 1;
@@ -273,11 +274,12 @@ __global__ void k_div_u(LevelGeo g, const double* __restrict__ u, const uint8_t*
   const double jac = g.hx * g.hz / 4.0;
   const double cx = -g.s * jac * (2.0 / g.hx), cz = -g.s * jac * (2.0 / g.hz);
   const int ncx = g.nx + 1;
-  const int64_t np = (int64_t)ncx * (g.nz + 1);
   const double2* u2 = reinterpret_cast<const double2*>(u);
   const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x) {
-    const int px = (int)(n % ncx), pz = (int)(n / ncx);
+  // one pressure-node row per blockIdx.y: no index division
+  for (int pz = blockIdx.y; pz <= g.nz; pz += gridDim.y)
+  for (int px = blockIdx.x * blockDim.x + threadIdx.x; px < ncx; px += gridDim.x * blockDim.x) {
+    const int64_t n = (int64_t)pz * ncx + px;
     // incident elements in ascending order and this node's Q1 index in each
     const int exs[4] = {px - 1, px, px - 1, px}, ezs[4] = {pz - 1, pz - 1, pz, pz}, js[4] = {2, 3, 1, 0};
     double acc = 0.0;
@@ -1607,12 +1609,14 @@ static void dsum(mw_stokes* S, int64_t n, const double* x, double* out, cudaStre
 
 // y = G p (b == null) or b - G p on the fine level; y = G^T u
 static void grad_p(mw_stokes* S, const double* p, const double* b, double* y, cudaStream_t s) {
-  const int64_t nn = (int64_t)S->fine.nnx * S->fine.nnz;
-  pdl_launch(k_grad_p, grid_for(nn, 256), 256, 0, s, S->fine, p, S->fixV, b, y);
+  const LevelGeo& g = S->fine;
+  dim3 grid((g.nnx + 127) / 128, std::min(g.nnz, 65535));
+  pdl_launch(k_grad_p, grid, 128, 0, s, g, p, S->fixV, b, y);
 }
 static void div_u(mw_stokes* S, const double* u, double* y, cudaStream_t s) {
-  const int64_t np = (int64_t)(S->fine.nx + 1) * (S->fine.nz + 1);
-  pdl_launch(k_div_u, grid_for(np, 256), 256, 0, s, S->fine, u, S->fixV, y);
+  const LevelGeo& g = S->fine;
+  dim3 grid((g.nx + 1 + 127) / 128, std::min(g.nz + 1, 65535));
+  pdl_launch(k_div_u, grid, 128, 0, s, g, u, S->fixV, y);
 }
 
 template <typename R>
@@ -1906,7 +1910,8 @@ static void launch_tail(Hierarchy<R>& H, int l0, bool first_done, cudaStream_t s
 // MW_FUSED_PROLONG=1 in the environment (read at the first V-cycle) folds it into the first
 // smoothing step (AM_CHEB_P) instead: the same arithmetic and results, one launch fewer per level
 // and V-cycle, but the heavier smoothing kernel made the 512x512 FK step slower (26.50 against
-// 26.15 ms, measured).
+// 26.15 ms; on the levels of at most 128^2 or 256^2 elements only: 24.84 / 24.86 against 24.76 ms,
+// measured).
 static bool fused_prolongation() {
   static const bool on = [] {
     const char* e = getenv("MW_FUSED_PROLONG");
@@ -2836,6 +2841,21 @@ int mw_stokes_apply_f32(mw_stokes* S, const float* u, const float* p, float* yV,
   ApplyArgs<float> a = args0<float>();
   a.u = u; a.p = p; a.eta = S->etaq32; a.fix = S->fixV; a.diag = S->H32.L[0].diag; a.yV = yV; a.yP = yP;
   launch_apply<float, AM_APPLY>(S->fine, a, (cudaStream_t)stream);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_cheb_step_f32(mw_stokes* S, const float* b, const float* x, float* xo, float* d, int32_t step,
+                            void* stream) {
+  if (!S->has32 || !b || !pair_aligned(x, 8) || !pair_aligned(xo, 8) || !d || step < 0 || step >= MAXDEG)
+    return MW_ERR_BAD_ARG;
+  if (ensure_hierarchy(S, MW_F32, (cudaStream_t)stream)) return MW_ERR_CUDA;
+  Level<float>& L = S->H32.L[0];
+  if (step >= L.deg && step > 0) return MW_ERR_BAD_ARG;
+  ApplyArgs<float> a = args0<float>();
+  a.u = x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = d; a.bV = b; a.d = d; a.xo = xo;
+  a.cheb = L.cheb + 2 * step;
+  launch_apply<float, AM_CHEB>(L.g, a, (cudaStream_t)stream);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }

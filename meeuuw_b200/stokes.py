@@ -47,6 +47,7 @@ L.extra_protos({
     "mw_stokes_apply": (c_int32, [c_void_p] * 6),
     "mw_stokes_apply_f32": (c_int32, [c_void_p] * 6),
     "mw_stokes_grad": (c_int32, [c_void_p] * 4),
+    "mw_stokes_cheb_step_f32": (c_int32, [c_void_p] * 5 + [c_int32, c_void_p]),
     "mw_stokes_div": (c_int32, [c_void_p] * 4),
     "mw_stokes_vcycle": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p]),
     "mw_stokes_solve_K": (c_int32, [c_void_p, c_int32, c_void_p, c_void_p, c_double, c_int32,
@@ -103,6 +104,11 @@ class StokesSolver:
         name = "mw_stokes_apply_f32" if precision == "f32" else "mw_stokes_apply"
         call(name, self.h, ptr(u), ptr(p), ptr(yV), ptr(yP), stream_ptr())
         return yV, yP
+
+    def cheb_step_f32(self, b, x, xo, d, step=1):
+        """One Chebyshev smoothing step of the FP32 finest level (coefficient pair `step`)."""
+        call("mw_stokes_cheb_step_f32", self.h, ptr(b), ptr(x), ptr(xo), ptr(d), int(step), stream_ptr())
+        return xo
 
     def grad(self, p, yV=None):
         """yV = G p (the Schur iterations' stencil form of the G block)."""

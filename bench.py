@@ -694,8 +694,9 @@ def run_ensemble(args):
         ens.close()
         del ens
         torch.cuda.empty_cache()
-        # recorded steps; every model's cold first step runs eagerly with its learned guess (models whose
-        # grid the network cannot take start from zero), then the step is recorded
+        # recorded steps; every model's cold first step runs eagerly with its learned guess (the network
+        # runs on the model's grid padded to multiples of 8; a mesh its pooling factor does not divide
+        # starts from zero), then the step is recorded
         guess, nguess = None, [0]
         wpath = os.path.join(ROOT, "meeuuw_b200", "weights", "unet_fk128.npz")
         if os.path.exists(wpath):

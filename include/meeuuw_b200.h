@@ -544,6 +544,13 @@ int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e
  * in the solver's pressure units).  scales (device, 2 doubles) receives the predicted (sv, sp). */
 int mw_unet_to_fields(mw_box box, int32_t f, const float* Y, const double* stats, double pscale, double ghyd,
                       double* scales, const uint8_t* bc_fix_V, double* solV, double* solP, void* stream);
+/* The same two on a network grid gzp x gxp at least nelz/f x nelx/f (the network needs multiples
+ * of 8): the features repeat the last cell row and column, the guess reads the mesh's cells only. */
+int mw_unet_features_padded(mw_box box, int32_t f, int32_t gxp, int32_t gzp, const double* T, const double* eta_e,
+                            double Ra, double* stats, void* X, void* stream);
+int mw_unet_to_fields_padded(mw_box box, int32_t f, int32_t gxp, const float* Y, const double* stats, double pscale,
+                             double ghyd, double* scales, const uint8_t* bc_fix_V, double* solV, double* solP,
+                             void* stream);
 /* training targets [nelz, nelx, 5] from a solution (inverse of mw_unet_to_fields at the element
  * centres); scales (device, 2 doubles) receives the solution's (sv, sp) */
 int mw_unet_targets(mw_box box, const double* solV, const double* solP, const double* stats, double pscale,

@@ -236,16 +236,18 @@ __global__ void k_feature_stats(int64_t nel, const double* __restrict__ eta_e, d
   }
 }
 
-// features [nelz/f, nelx/f, 2] bf16 on the network grid (f x f elements per cell, averaged):
-// T at the element centre nodes, (log10 eta_e - mean) / 2.5
-__global__ void k_features(mw_box b, int f, const double* __restrict__ T, const double* __restrict__ eta_e,
-                           const double* __restrict__ stats, bf16* __restrict__ X) {
+// features [gzp, gxp, 2] bf16 on the network grid (f x f elements per cell, averaged):
+// T at the element centre nodes, (log10 eta_e - mean) / 2.5.  The grid of the mesh is nelz/f x
+// nelx/f; a network grid gzp x gxp larger than that (the network needs multiples of 8) repeats the
+// last row and column (replicate padding).
+__global__ void k_features(mw_box b, int f, int gxp, int gzp, const double* __restrict__ T,
+                           const double* __restrict__ eta_e, const double* __restrict__ stats, bf16* __restrict__ X) {
   const int gx = b.nelx / f, gz = b.nelz / f;
-  const int64_t ncell = (int64_t)gx * gz;
+  const int64_t ncell = (int64_t)gxp * gzp;
   const int nnx = 2 * b.nelx + 1;
   const double inv = 1.0 / ((double)f * f);
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncell; c += (int64_t)gridDim.x * blockDim.x) {
-    const int cx = (int)(c % gx), cz = (int)(c / gx);
+    const int cx = min((int)(c % gxp), gx - 1), cz = min((int)(c / gxp), gz - 1);
     double st = 0, se = 0;
     for (int a = 0; a < f; ++a)
       for (int d = 0; d < f; ++d) {
@@ -328,11 +330,17 @@ __global__ void k_targets(mw_box b, const double* __restrict__ solV, const doubl
   }
 }
 
-// predicted scales from channels 3, 4: scales = 10^mean over the network grid (one block)
-__global__ void k_pred_scales(int64_t ncell, const float* __restrict__ Y, double* __restrict__ scales) {
+// predicted scales from channels 3, 4: scales = 10^mean over the mesh's cells gx x gz of the
+// network grid (row length gxp) (one block)
+__global__ void k_pred_scales(int gx, int gz, int gxp, const float* __restrict__ Y, double* __restrict__ scales) {
   __shared__ double sh[64];
   double a = 0, c = 0;
-  for (int64_t i = threadIdx.x; i < ncell; i += blockDim.x) { a += Y[NC * i + 3]; c += Y[NC * i + 4]; }
+  const int64_t ncell = (int64_t)gx * gz;
+  for (int64_t k = threadIdx.x; k < ncell; k += blockDim.x) {
+    const int64_t i = (k / gx) * gxp + k % gx;
+    a += Y[NC * i + 3];
+    c += Y[NC * i + 4];
+  }
   for (int o = 16; o > 0; o >>= 1) { a += __shfl_down_sync(0xffffffffu, a, o); c += __shfl_down_sync(0xffffffffu, c, o); }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (lane == 0) { sh[wid] = a; sh[32 + wid] = c; }
@@ -348,18 +356,18 @@ __global__ void k_pred_scales(int64_t ncell, const float* __restrict__ Y, double
 // prediction [nelz/f, nelx/f, NC] -> Stokes initial guess: solV (interleaved u, w on the Q2
 // lattice, bilinear between network-cell centres, fixed dofs 0) and solP (Q1 nodes, bilinear
 // dynamic pressure + hydrostatic pressure); scales = (sv, sp)
-__global__ void k_to_fields(mw_box b, int f, const float* __restrict__ Y, const double* __restrict__ stats,
+__global__ void k_to_fields(mw_box b, int f, int gxp, const float* __restrict__ Y, const double* __restrict__ stats,
                             double pscale, double ghyd, const double* __restrict__ scales,
                             const uint8_t* __restrict__ fix, double* __restrict__ solV, double* __restrict__ solP) {
   const int nnx = 2 * b.nelx + 1, nnz = 2 * b.nelz + 1;
-  const int gxn = b.nelx / f, gzn = b.nelz / f;          // network grid
+  const int gxn = b.nelx / f, gzn = b.nelz / f;          // the mesh's cells of the network grid (rows gxp long)
   const int64_t nn = (int64_t)nnx * nnz;
   const int64_t np = (int64_t)(b.nelx + 1) * (b.nelz + 1);
   const double vs = stats[1] * scales[0], ps = pscale * scales[1];
   auto at = [&](int cx, int cz, int ch) -> double {
     cx = cx < 0 ? 0 : (cx >= gxn ? gxn - 1 : cx);
     cz = cz < 0 ? 0 : (cz >= gzn ? gzn - 1 : cz);
-    return (double)Y[((int64_t)cz * gxn + cx) * NC + ch];
+    return (double)Y[((int64_t)cz * gxp + cx) * NC + ch];
   };
   auto bilin = [&](double gx, double gz, int ch) -> double {
     const int x0 = (int)floor(gx), z0 = (int)floor(gz);
@@ -485,27 +493,39 @@ int mw_unet_adam(int64_t n, float* w, float* m, float* v, const float* g, float 
   return MW_OK;
 }
 
-int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e, double Ra, double* stats, void* X,
-                     void* stream) {
-  if (f < 1 || box.nelx % f || box.nelz % f) return MW_ERR_BAD_ARG;
+int mw_unet_features_padded(mw_box box, int32_t f, int32_t gxp, int32_t gzp, const double* T, const double* eta_e,
+                            double Ra, double* stats, void* X, void* stream) {
+  if (f < 1 || box.nelx % f || box.nelz % f || gxp < box.nelx / f || gzp < box.nelz / f) return MW_ERR_BAD_ARG;
   const int64_t nel = (int64_t)box.nelx * box.nelz;
   k_feature_stats<<<1, 1024, 0, (cudaStream_t)stream>>>(nel, eta_e, Ra, stats);
   MW_CHECK_LAUNCH();
-  k_features<<<MW_GRID(nel / ((int64_t)f * f))>>>(box, f, T, eta_e, stats, (bf16*)X);
+  k_features<<<MW_GRID((int64_t)gxp * gzp)>>>(box, f, gxp, gzp, T, eta_e, stats, (bf16*)X);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_unet_features(mw_box box, int32_t f, const double* T, const double* eta_e, double Ra, double* stats, void* X,
+                     void* stream) {
+  if (f < 1) return MW_ERR_BAD_ARG;
+  return mw_unet_features_padded(box, f, box.nelx / f, box.nelz / f, T, eta_e, Ra, stats, X, stream);
+}
+
+int mw_unet_to_fields_padded(mw_box box, int32_t f, int32_t gxp, const float* Y, const double* stats, double pscale,
+                             double ghyd, double* scales, const uint8_t* bc_fix_V, double* solV, double* solP,
+                             void* stream) {
+  if (f < 1 || box.nelx % f || box.nelz % f || !scales || gxp < box.nelx / f) return MW_ERR_BAD_ARG;
+  k_pred_scales<<<1, 1024, 0, (cudaStream_t)stream>>>(box.nelx / f, box.nelz / f, gxp, Y, scales);
+  MW_CHECK_LAUNCH();
+  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1) + (int64_t)(box.nelx + 1) * (box.nelz + 1);
+  k_to_fields<<<MW_GRID(n)>>>(box, f, gxp, Y, stats, pscale, ghyd, scales, bc_fix_V, solV, solP);
   MW_CHECK_LAUNCH();
   return MW_OK;
 }
 
 int mw_unet_to_fields(mw_box box, int32_t f, const float* Y, const double* stats, double pscale, double ghyd,
                       double* scales, const uint8_t* bc_fix_V, double* solV, double* solP, void* stream) {
-  if (f < 1 || box.nelx % f || box.nelz % f || !scales) return MW_ERR_BAD_ARG;
-  const int64_t ncell = (int64_t)(box.nelx / f) * (box.nelz / f);
-  k_pred_scales<<<1, 1024, 0, (cudaStream_t)stream>>>(ncell, Y, scales);
-  MW_CHECK_LAUNCH();
-  const int64_t n = (int64_t)(2 * box.nelx + 1) * (2 * box.nelz + 1) + (int64_t)(box.nelx + 1) * (box.nelz + 1);
-  k_to_fields<<<MW_GRID(n)>>>(box, f, Y, stats, pscale, ghyd, scales, bc_fix_V, solV, solP);
-  MW_CHECK_LAUNCH();
-  return MW_OK;
+  if (f < 1) return MW_ERR_BAD_ARG;
+  return mw_unet_to_fields_padded(box, f, box.nelx / f, Y, stats, pscale, ghyd, scales, bc_fix_V, solV, solP, stream);
 }
 
 int mw_unet_targets(mw_box box, const double* solV, const double* solP, const double* stats, double pscale,

@@ -49,6 +49,10 @@ L.extra_protos({
     "mw_unet_adam": (c_int32, [c_int64, c_void_p, c_void_p, c_void_p, c_void_p] + [ctypes.c_float] * 6 +
                      [c_void_p, c_void_p]),
     "mw_unet_features": (c_int32, [L.MwBox, c_int32, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p]),
+    "mw_unet_features_padded": (c_int32, [L.MwBox, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_double, c_void_p,
+                                          c_void_p, c_void_p]),
+    "mw_unet_to_fields_padded": (c_int32, [L.MwBox, c_int32, c_int32, c_void_p, c_void_p, c_double, c_double,
+                                           c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_unet_to_fields": (c_int32, [L.MwBox, c_int32, c_void_p, c_void_p, c_double, c_double, c_void_p, c_void_p,
                                     c_void_p, c_void_p, c_void_p]),
     "mw_unet_targets": (c_int32, [L.MwBox, c_void_p, c_void_p, c_void_p, c_double, c_double, c_void_p, c_void_p,
@@ -387,28 +391,28 @@ def train(net, Xs, Ys, epochs=20, batch=16, lr=1e-3, seed=0, log=None):
 
 class WarmStart:
     """Stokes initial guess from the trained network at the network resolution `n_net` (the model
-    grid is pooled by f = nelx / n_net and the prediction interpolated back)."""
+    grid is pooled by f = nelx / n_net and the prediction interpolated back).  The network halves
+    its grid three times, so the pooled grid is padded up to multiples of 8 (the last cell row and
+    column repeated) and the prediction is read on the mesh's cells only."""
 
     def __init__(self, net, box, Ra, alphaT, bc_fix_V, n_net=128, rho0=1.0, s=1.0):
         self.net, self.box, self.Ra = net, box, float(Ra)
         self.pscale, self.ghyd = pressure_scales(Ra, alphaT, rho0, s)
         self.f = max(1, box.nelx // n_net)
+        if box.nelx % self.f or box.nelz % self.f:
+            raise ValueError(f"the pooling factor {self.f} does not divide the {box.nelx}x{box.nelz} mesh")
         self.gx, self.gz = box.nelx // self.f, box.nelz // self.f
-        # the network halves the grid three times and concatenates the skips after upsampling, so
-        # the grid it sees must divide by 8; the pooling factor must divide the mesh
-        if box.nelx % self.f or box.nelz % self.f or self.gx % 8 or self.gz % 8:
-            raise ValueError(f"a {box.nelx}x{box.nelz} mesh maps to a {self.gx}x{self.gz} network grid; the "
-                             f"network needs multiples of 8 (and the pooling factor {self.f} to divide the mesh)")
+        self.gxp, self.gzp = -(-self.gx // 8) * 8, -(-self.gz // 8) * 8
         self.fix = bc_fix_V.view(torch.uint8) if bc_fix_V.dtype == torch.bool else bc_fix_V
         self.stats = torch.empty(2, dtype=torch.float64, device="cuda")
         self.scales = torch.empty(2, dtype=torch.float64, device="cuda")
-        self.X = torch.empty(1, self.gz, self.gx, 2, dtype=bf16, device="cuda")
+        self.X = torch.empty(1, self.gzp, self.gxp, 2, dtype=bf16, device="cuda")
 
     def guess(self, T, eta_e, solV, solP):
-        call("mw_unet_features", self.box, self.f, ptr(T), ptr(eta_e), self.Ra, ptr(self.stats), ptr(self.X),
-             stream_ptr())
-        y = self.net.forward(self.X, 1, self.gz, self.gx)
-        call("mw_unet_to_fields", self.box, self.f, ptr(y), ptr(self.stats), self.pscale, self.ghyd,
+        call("mw_unet_features_padded", self.box, self.f, self.gxp, self.gzp, ptr(T), ptr(eta_e), self.Ra,
+             ptr(self.stats), ptr(self.X), stream_ptr())
+        y = self.net.forward(self.X, 1, self.gzp, self.gxp)
+        call("mw_unet_to_fields_padded", self.box, self.f, self.gxp, ptr(y), ptr(self.stats), self.pscale, self.ghyd,
              ptr(self.scales), ptr(self.fix), ptr(solV), ptr(solP), stream_ptr())
         return solV, solP
 

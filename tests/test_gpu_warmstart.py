@@ -81,3 +81,55 @@ def test_learned_cold_start_512_from_128_network():
             assert m.guess.last["pick"] == "learned", m.guess.last
         del m
     assert outer["learned"] < outer["zero"], outer
+
+
+def test_warm_start_on_meshes_not_multiple_of_eight():
+    """Meshes whose network grid is not a multiple of 8 (66x66, 100x60) run the network on a
+    replicate-padded grid; the guess is finite, its fixed velocity dofs are zero, and the gated
+    cold start converges (the ensemble's uneven members all get a learned guess)."""
+    import torch
+    from dataclasses import replace
+    from meeuuw_b200 import configs
+    from meeuuw_b200.timestep import GPUModel
+    from meeuuw_b200.unet import LearnedGuess, UNet, WarmStart, _Recorder
+    net = UNet.load(WEIGHTS)
+    for nx, nz in ((66, 66), (100, 60)):
+        cfg = replace(configs.fk_convection(nx), nelz=nz, Lz=nz / nx, name=f"pad{nx}x{nz}")
+        host = configs.build_host_model(cfg)
+        m = GPUModel(cfg, host, stokes="mixed")
+        rec = _Recorder(m)                  # the state (T, element viscosity) a step's Stokes solve sees
+        m.guess = rec
+        m.step()
+        ws = WarmStart(net, m.box, cfg.Ra, cfg.alphaT, m.bc_fix_V, 128, cfg.rho0, cfg.eta_ref / m.L_ref)
+        assert (ws.gxp, ws.gzp) == (-(-nx // 8) * 8, -(-nz // 8) * 8)
+        V, P = torch.empty_like(m.solV), torch.empty_like(m.solP)
+        ws.guess(rec.T, rec.eta, V, P)
+        assert bool(torch.isfinite(V).all()) and bool(torch.isfinite(P).all())
+        assert float(V[m.bc_fix_V].abs().max()) == 0.0
+        m = GPUModel(cfg, host, stokes="mixed")
+        m.guess = LearnedGuess(m, net)
+        m.step()
+        assert m.last_solve["converged"] == 1, m.last_solve
+        assert m.guess.last["pick"] in ("learned", "zero")
+
+
+def test_padded_features_equal_unpadded_on_multiples_of_eight():
+    import torch
+    from meeuuw_b200 import configs
+    from meeuuw_b200._lib import call, ptr, stream_ptr
+    from meeuuw_b200.timestep import GPUModel
+    from meeuuw_b200.unet import _Recorder
+    cfg = configs.fk_convection(64)
+    m = GPUModel(cfg, configs.build_host_model(cfg), stokes="mixed")
+    rec = _Recorder(m)
+    m.guess = rec
+    m.step()
+    stats = torch.empty(2, dtype=torch.float64, device="cuda")
+    X0 = torch.empty(64, 64, 2, dtype=torch.bfloat16, device="cuda")
+    X1 = torch.empty(72, 72, 2, dtype=torch.bfloat16, device="cuda")
+    call("mw_unet_features", m.box, 1, ptr(rec.T), ptr(rec.eta), float(cfg.Ra), ptr(stats), ptr(X0), stream_ptr())
+    call("mw_unet_features_padded", m.box, 1, 72, 72, ptr(rec.T), ptr(rec.eta), float(cfg.Ra), ptr(stats), ptr(X1),
+         stream_ptr())
+    assert bool(torch.isfinite(X0.float()).all())
+    assert torch.equal(X1[:64, :64], X0)
+    assert torch.equal(X1[64:, :64], X0[63:64].expand(8, 64, 2)) and torch.equal(X1[:64, 64:], X0[:, 63:64].expand(64, 8, 2))

@@ -441,6 +441,33 @@ int mw_split_solution(int64_t nn_V, int64_t nn_P, const double* solV, const doub
 /* "elemental" qpoint fields (meeuuw.py:1512-1514, :1545-1547): aq[e, :] = a[e] (b, bq optional). */
 int mw_elemental_to_qpoints(int64_t nel, const double* a, const double* b, double* aq, double* bq, void* stream);
 
+/* ======================= sparse patterns ======================= */
+
+/* The reference's COO index arrays (meeuuw.py:874-1017) for the uniform box, in its element order:
+ * kind 0 the full Stokes matrix (nel*468 entries, pressure indices offset by Nfem_V), 1 K (nel*324),
+ * 2 G (nel*72), 3 G^T (nel*72), 4 the Q1 pressure mass matrix M_P (nel*16), 5 the Q2 temperature
+ * matrix (nel*81) -- the triplets the assembly's VV layouts pair with. */
+#define MW_COO_STOKES 0
+#define MW_COO_K 1
+#define MW_COO_G 2
+#define MW_COO_GT 3
+#define MW_COO_MP 4
+#define MW_COO_T 5
+int64_t mw_coo_length(mw_box box, int32_t kind);
+int mw_coo_pattern(mw_box box, int32_t kind, int32_t* II, int32_t* JJ, void* stream);
+/* The summed matrix coo_matrix((VV, (II, JJ))).tocsr() of meeuuw.py:1784-1800 / :2232 in CSR form on
+ * the device: mw_csr_pattern writes the row pointers (rows + 1, int64) and returns nnz (synchronises;
+ * workspace mw_csr_workspace_bytes), mw_csr_columns the sorted column indices (nnz, int32),
+ * mw_csr_values the values from a VV of the same kind (duplicates summed in ascending element
+ * order).  The pattern is constant: build it once, refresh the values every step. */
+int64_t mw_csr_rows(mw_box box, int32_t kind);
+size_t mw_csr_workspace_bytes(mw_box box, int32_t kind);
+int mw_csr_pattern(mw_box box, int32_t kind, int64_t* row_ptr, int64_t* nnz, void* work, size_t work_bytes,
+                   void* stream);
+int mw_csr_columns(mw_box box, int32_t kind, const int64_t* row_ptr, int32_t* col, void* stream);
+int mw_csr_values(mw_box box, int32_t kind, const double* VV, const int64_t* row_ptr, const int32_t* col, double* val,
+                  void* stream);
+
 /* ======================= energy solve ======================= */
 
 /* y = A x with A the summed element matrices VV_T (nel*81, build_matrix_energy.py:133-137). */

@@ -134,6 +134,13 @@ _PROTOS = {
     "mw_energy_device_info": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_energy_solve": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_double, c_int32, c_void_p, c_void_p,
                                   c_void_p, c_size_t, c_void_p]),
+    "mw_coo_length": (c_int64, [MwBox, c_int32]),
+    "mw_coo_pattern": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p]),
+    "mw_csr_rows": (c_int64, [MwBox, c_int32]),
+    "mw_csr_workspace_bytes": (c_size_t, [MwBox, c_int32]),
+    "mw_csr_pattern": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "mw_csr_columns": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p]),
+    "mw_csr_values": (c_int32, [MwBox, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "mw_energy_op_bytes": (c_size_t, [MwBox]),
     "mw_energy_op_setup": (c_int32, [MwBox, MwEnergyIn, c_void_p, c_size_t, c_void_p, c_void_p]),
     "mw_energy_op_apply": (c_int32, [MwBox, c_void_p, c_void_p, c_void_p, c_void_p]),

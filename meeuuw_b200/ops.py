@@ -222,6 +222,47 @@ def assemble_energy(box, precision, T, q, tables, bc_fix_T, bc_val_T, dt, rho0, 
     return VV, rhs
 
 
+# ----------------------------------------------------------------------------- sparse patterns
+COO_KINDS = {"stokes": 0, "K": 1, "G": 2, "GT": 3, "MP": 4, "T": 5}
+
+
+def coo_pattern(box, kind, device="cuda"):
+    """The reference's (II, JJ) of matrix `kind` (meeuuw.py:874-1017), int32 device tensors."""
+    k = COO_KINDS[kind]
+    n = L.lib().mw_coo_length(box, k)
+    II = torch.empty(n, dtype=torch.int32, device=device)
+    JJ = torch.empty(n, dtype=torch.int32, device=device)
+    call("mw_coo_pattern", box, k, ptr(II), ptr(JJ), stream_ptr())
+    return II, JJ
+
+
+class CsrPattern:
+    """Row pointers and sorted column indices of the summed matrix `kind`, built once on the
+    device; values(VV) sums an assembled VV of the same kind into them (coo_matrix((VV, (II, JJ)))
+    .tocsr() of meeuuw.py:1784-1800, without leaving the device)."""
+
+    def __init__(self, box, kind, device="cuda"):
+        self.box, self.kind = box, COO_KINDS[kind]
+        self.rows = L.lib().mw_csr_rows(box, self.kind)
+        self.row_ptr = torch.empty(self.rows + 1, dtype=torch.int64, device=device)
+        nnz = ctypes.c_int64()
+        wp, wb = workspace("csr").get(L.lib().mw_csr_workspace_bytes(box, self.kind))
+        call("mw_csr_pattern", box, self.kind, ptr(self.row_ptr), ctypes.byref(nnz), wp, wb, stream_ptr())
+        self.nnz = nnz.value
+        self.col = torch.empty(self.nnz, dtype=torch.int32, device=device)
+        call("mw_csr_columns", box, self.kind, ptr(self.row_ptr), ptr(self.col), stream_ptr())
+
+    def values(self, VV, out=None):
+        out = torch.empty(self.nnz, dtype=f64, device=VV.device) if out is None else out
+        call("mw_csr_values", self.box, self.kind, ptr(VV), ptr(self.row_ptr), ptr(self.col), ptr(out), stream_ptr())
+        return out
+
+    def tensor(self, VV, ncols):
+        """torch.sparse_csr_tensor of the summed matrix (ncols columns)."""
+        return torch.sparse_csr_tensor(self.row_ptr, self.col.to(torch.int64), self.values(VV),
+                                       size=(self.rows, ncols), check_invariants=False)
+
+
 def energy_op_setup(box, T, q, tables, bc_fix_T, bc_val_T, dt, rho0, formulation, op=None, rhs=None, dt_dev=None):
     """Matrix-free energy operator (Gauss-point coefficients, diagonal, Dirichlet flags) and the
     right-hand side of build_matrix_energy.  Returns (op, rhs); op is a uint8 device buffer."""

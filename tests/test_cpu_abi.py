@@ -11,7 +11,8 @@ def header_symbols():
     for f in os.listdir(os.path.join(ROOT, "include")):
         if f.endswith(".h"):
             txt = open(os.path.join(ROOT, "include", f)).read()
-            names |= set(re.findall(r"^\s*(?:int|size_t|void|const char\s*\*)\s+(mw_\w+)\s*\(", txt, re.M))
+            names |= set(re.findall(r"^\s*(?:int|int32_t|int64_t|size_t|void|const char\s*\*)\s+(mw_\w+)\s*\(", txt,
+                                    re.M))
     return names
 
 

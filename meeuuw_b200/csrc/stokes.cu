@@ -1666,6 +1666,15 @@ struct TailArgs {
   int dense, nd;       // coarsest level: dense inverse Ainv (nd unknowns), else MAXDEG smoothing
   const double* Ainv;
   R* ye;               // element products (global scratch, 18 per element of the largest level)
+  R* out_x;            // shared-memory tail: where the first level's final x goes (the buffer the
+                       // host's record of the pointer swaps names)
+};
+
+struct ClusterBarrier {
+  MW_D void operator()() const { cluster_barrier(); }
+};
+struct BlockBarrier {
+  MW_D void operator()() const { __syncthreads(); }
 };
 
 template <typename R>
@@ -1674,8 +1683,9 @@ constexpr int tail_threads() { return sizeof(R) == 4 ? 512 : 256; }
 // One operator apply of tail level L on u: AM_RESID writes r = b - K u, AM_CHEB the Chebyshev
 // step (d, xo) with coefficient pair cheb.  Element products go through the global scratch sye;
 // this is thread t0 of the nt threads of the cluster.
-template <typename R, int MODE>
-MW_D void tail_apply(const TailLevel<R>& L, const R* u, R* xo, const double* cheb, R* sye, int t0, int nt) {
+template <typename R, int MODE, typename B>
+MW_D void tail_apply(const TailLevel<R>& L, const R* u, R* xo, const double* cheb, R* sye, int t0, int nt,
+                     const B& barrier) {
   typedef typename Vec2<R>::T R2;
   const LevelGeo& g = L.g;
   const int nel = g.nx * g.nz;
@@ -1696,7 +1706,7 @@ MW_D void tail_apply(const TailLevel<R>& L, const R* u, R* xo, const double* che
 #pragma unroll
     for (int k = 0; k < 18; ++k) sye[e * 18 + k] = ye[k];
   }
-  cluster_barrier();
+  barrier();
   const int64_t nn = (int64_t)g.nnx * g.nnz;
   for (int64_t n = t0; n < nn; n += nt) {
     const int ix = (int)(n % g.nnx), iz = (int)(n / g.nnx);
@@ -1746,25 +1756,18 @@ MW_D void tail_apply(const TailLevel<R>& L, const R* u, R* xo, const double* che
       reinterpret_cast<R2*>(xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
     }
   }
-  cluster_barrier();
+  barrier();
 }
 
-template <typename R>
-__global__ void __cluster_dims__(TAIL_CLUSTER, 1, 1) __launch_bounds__(tail_threads<R>(), 1)
-k_vtail(TailArgs<R> A) {
-  pdl_entry();
-  R* sye = A.ye;
-  const int t0 = (int)(cluster_rank() * blockDim.x + threadIdx.x), nt = (int)(TAIL_CLUSTER * blockDim.x);
-  __shared__ TailLevel<R> sL[MAX_TAIL];
-#pragma unroll
-  for (int l = 0; l < MAX_TAIL; ++l)
-    if (threadIdx.x == l && l < A.n) sL[l] = A.L[l];
-  __syncthreads();
+// The tail's V-cycle (levels sL[0 .. A.n-1], the last the coarsest) by the t0-th of nt threads, the
+// phases separated by `barrier`; returns where level 0's final x is (the x/t ping-pong).
+template <typename R, typename B>
+MW_D R* tail_vcycle(const TailLevel<R>* sL, const TailArgs<R>& A, R* sye, int t0, int nt, const B& barrier) {
   R* xs[MAX_TAIL];
   R* ts[MAX_TAIL];
   for (int l = 0; l < A.n; ++l) { xs[l] = sL[l].x; ts[l] = sL[l].t; }
   auto cheb_step = [&](int l, int k) {             // Chebyshev step k: x_out in t, then swap
-    tail_apply<R, AM_CHEB>(sL[l], xs[l], ts[l], sL[l].cheb + 2 * k, sye, t0, nt);
+    tail_apply<R, AM_CHEB>(sL[l], xs[l], ts[l], sL[l].cheb + 2 * k, sye, t0, nt, barrier);
     R* tmp = xs[l]; xs[l] = ts[l]; ts[l] = tmp;
   };
   auto smooth_tail = [&](int l, int degree, bool zero_start, bool first_done) {
@@ -1778,7 +1781,7 @@ k_vtail(TailArgs<R> A) {
         R v = c * L.b[i] / L.diag[i];
         xs[l][i] = v; L.d[i] = v;
       }
-      cluster_barrier();
+      barrier();
     } else {
       cheb_step(l, 0);
     }
@@ -1788,7 +1791,7 @@ k_vtail(TailArgs<R> A) {
   for (int l = 0; l + 1 < A.n; ++l) {
     const bool fd = l == 0 ? A.first_done != 0 : true;
     smooth_tail(l, sL[l].deg, !fd, fd);
-    tail_apply<R, AM_RESID>(sL[l], xs[l], nullptr, nullptr, sye, t0, nt);
+    tail_apply<R, AM_RESID>(sL[l], xs[l], nullptr, nullptr, sye, t0, nt, barrier);
     const TailLevel<R>& F = sL[l];
     const TailLevel<R>& C = sL[l + 1];
     const bool fuse = !(l + 2 == A.n && A.dense);
@@ -1796,7 +1799,7 @@ k_vtail(TailArgs<R> A) {
     const int64_t ncn = (int64_t)C.g.nnx * C.g.nnz;
     for (int64_t n = t0; n < ncn; n += nt)
       restrict_node(F.g, C.g, F.r, C.fix, C.b, c0, fuse, C.diag, xs[l + 1], C.d, n);
-    cluster_barrier();
+    barrier();
   }
   {  // coarsest level
     const int l = A.n - 1;
@@ -1809,7 +1812,7 @@ k_vtail(TailArgs<R> A) {
         for (int o = 16; o > 0; o >>= 1) sacc += __shfl_down_sync(0xffffffffu, sacc, o);
         if (lane == 0) xs[l][row] = (R)sacc;
       }
-      cluster_barrier();
+      barrier();
     } else {
       const bool fd = A.n == 1 ? A.first_done != 0 : true;
       smooth_tail(l, MAXDEG, !fd, fd);
@@ -1821,12 +1824,98 @@ k_vtail(TailArgs<R> A) {
     const TailLevel<R>& C = sL[l + 1];
     const int64_t nfn = (int64_t)F.g.nnx * F.g.nnz;
     for (int64_t n = t0; n < nfn; n += nt) prolong_node(F.g, C.g, xs[l + 1], F.fix, xs[l], n);
-    cluster_barrier();
+    barrier();
     smooth_tail(l, sL[l].deg, false, false);
   }
+  return xs[0];
 }
 
+template <typename R>
+__global__ void __cluster_dims__(TAIL_CLUSTER, 1, 1) __launch_bounds__(tail_threads<R>(), 1)
+k_vtail(TailArgs<R> A) {
+  pdl_entry();
+  const int t0 = (int)(cluster_rank() * blockDim.x + threadIdx.x), nt = (int)(TAIL_CLUSTER * blockDim.x);
+  __shared__ TailLevel<R> sL[MAX_TAIL];
+#pragma unroll
+  for (int l = 0; l < MAX_TAIL; ++l)
+    if (threadIdx.x == l && l < A.n) sL[l] = A.L[l];
+  __syncthreads();
+  tail_vcycle<R>(sL, A, A.ye, t0, nt, ClusterBarrier());
+}
 
+// The same tail in one CTA with every level's vectors, viscosities, diagonals, masks and the
+// element products in shared memory: each phase is a shared-memory round trip and a block
+// barrier instead of a launch or a round trip through L2.  Reads the first level's b (and x, d
+// when the restriction did the first Chebyshev step) and every level's eta, mask and diagonal,
+// writes the first level's final x to A.out_x.  Same phases, same arithmetic, same order as the
+// multi-launch V-cycle.
+template <typename R>
+__global__ void __launch_bounds__(tail_threads<R>(), 1) k_vtail_smem(TailArgs<R> A) {
+  pdl_entry();
+  extern __shared__ __align__(16) unsigned char tsm[];
+  __shared__ TailLevel<R> sL[MAX_TAIL];
+  const int t0 = threadIdx.x, nt = blockDim.x;
+  if (threadIdx.x == 0) {                       // carve the shared memory (the host sized it alike)
+    size_t off = 0;
+    auto take = [&](size_t bytes) { void* p = tsm + off; off += (bytes + 15) & ~size_t(15); return p; };
+    for (int l = 0; l < A.n; ++l) {
+      TailLevel<R> L = A.L[l];
+      const int64_t nd = 2LL * L.g.nnx * L.g.nnz, ne = (int64_t)L.g.nx * L.g.nz;
+      L.eta = (const R*)take(sizeof(R) * ne * 9);
+      L.diag = (const R*)take(sizeof(R) * nd);
+      L.fix = (const uint8_t*)take(nd);
+      L.x = (R*)take(sizeof(R) * nd);
+      L.t = (R*)take(sizeof(R) * nd);
+      L.b = (R*)take(sizeof(R) * nd);
+      L.r = (R*)take(sizeof(R) * nd);
+      L.d = (R*)take(sizeof(R) * nd);
+      sL[l] = L;
+    }
+  }
+  __syncthreads();
+  R* sye = nullptr;
+  {
+    size_t off = 0;                             // the element products after the levels
+    for (int l = 0; l < A.n; ++l) {
+      const int64_t nd = 2LL * A.L[l].g.nnx * A.L[l].g.nnz, ne = (int64_t)A.L[l].g.nx * A.L[l].g.nz;
+      off += ((sizeof(R) * ne * 9 + 15) & ~size_t(15)) + ((sizeof(R) * nd + 15) & ~size_t(15)) + ((nd + 15) & ~size_t(15)) +
+             5 * ((sizeof(R) * nd + 15) & ~size_t(15));
+    }
+    sye = reinterpret_cast<R*>(tsm + off);
+  }
+  for (int l = 0; l < A.n; ++l) {               // stage the inputs
+    const TailLevel<R>& G = A.L[l];
+    const TailLevel<R>& S = sL[l];
+    const int64_t nd = 2LL * G.g.nnx * G.g.nnz, ne = (int64_t)G.g.nx * G.g.nz;
+    for (int64_t i = t0; i < ne * 9; i += nt) const_cast<R*>(S.eta)[i] = G.eta[i];
+    for (int64_t i = t0; i < nd; i += nt) {
+      const_cast<R*>(S.diag)[i] = G.diag[i];
+      const_cast<uint8_t*>(S.fix)[i] = G.fix[i];
+      if (l == 0) {
+        S.b[i] = G.b[i];
+        if (A.first_done) { S.x[i] = G.x[i]; S.d[i] = G.d[i]; }
+      }
+    }
+  }
+  __syncthreads();
+  const R* xf = tail_vcycle<R>(sL, A, sye, t0, nt, BlockBarrier());
+  const int64_t nd0 = 2LL * A.L[0].g.nnx * A.L[0].g.nnz;
+  for (int64_t i = t0; i < nd0; i += nt) A.out_x[i] = xf[i];
+}
+
+// shared memory of the one-CTA tail over levels L[0 .. n-1] (the carving of k_vtail_smem)
+template <typename R>
+static size_t tail_smem_bytes(const TailArgs<R>& A) {
+  size_t off = 0;
+  auto r16 = [](size_t b) { return (b + 15) & ~size_t(15); };
+  int64_t maxe = 0;
+  for (int l = 0; l < A.n; ++l) {
+    const int64_t nd = 2LL * A.L[l].g.nnx * A.L[l].g.nnz, ne = (int64_t)A.L[l].g.nx * A.L[l].g.nz;
+    off += r16(sizeof(R) * ne * 9) + r16(sizeof(R) * nd) + r16(nd) + 5 * r16(sizeof(R) * nd);
+    maxe = std::max(maxe, ne);
+  }
+  return off + sizeof(R) * maxe * 18;
+}
 
 // Chebyshev smoothing of level L: x (in/out) with rhs b, `steps` steps; zero_start -> x = 0 on entry.
 template <typename R>
@@ -1903,7 +1992,32 @@ static void launch_tail(Hierarchy<R>& H, int l0, bool first_done, cudaStream_t s
   A.nd = H.nd;
   A.Ainv = H.Ainv;
   A.ye = H.tail_ye;
+  // the one-CTA shared-memory tail when every tail level fits (MW_TAIL_SMEM=0 in the environment:
+  // the cluster tail through global memory)
+  static const bool smem_on = [] {
+    const char* e = getenv("MW_TAIL_SMEM");
+    return !(e && e[0] == '0');
+  }();
+  const size_t sm = tail_smem_bytes(A);
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t limit = (size_t)optin > 1024 ? (size_t)optin - 1024 : 0;   // static TailLevel copies
+  if (smem_on && sm <= limit) {
+    static size_t attr_set = 0;
+    if (sm > attr_set &&
+        cudaFuncSetAttribute(k_vtail_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit) == cudaSuccess)
+      attr_set = limit;
+    if (sm <= attr_set) {
+      tail_swaps(H, l0, first_done);          // the host's record of where level l0's x ends up
+      A.out_x = H.L[l0].x;
+      pdl_launch(k_vtail_smem<R>, 1, tail_threads<R>(), sm, s, A);
+      return;
+    }
+    cudaGetLastError();
+  }
   pdl_launch(k_vtail<R>, TAIL_CLUSTER, tail_threads<R>(), 0, s, A);
+  tail_swaps(H, l0, first_done);
 }
 
 // The prolongation runs as its own launch (k_prolong_add) before the post-smoothing by default;
@@ -1924,8 +2038,7 @@ template <typename R>
 static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = false) {
   Level<R>& L = H.L[l];
   if (H.tail0 > 0 && l == H.tail0) {               // the coarse levels in one launch
-    launch_tail(H, l, first_done, s);
-    tail_swaps(H, l, first_done);
+    launch_tail(H, l, first_done, s);        // records the tail's pointer swaps too
     return;
   }
   if (l == H.nlev - 1) {

@@ -146,23 +146,26 @@ def test_device_loops_reproduce_host_loops(precision):
         assert rel_err(Vd, Vh) < 1e-12 and rel_err(Pd, Ph) < 1e-12
 
 
+@pytest.mark.parametrize("tail_nel", [1024, 256])
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
-def test_coarse_tail_matches_level_launches(precision):
-    """The coarse multigrid levels run as one CTA per V-cycle (tail_nel) repeat the multi-launch
-    V-cycle bit for bit: same V-cycle output, same solve iterates and counts."""
+def test_coarse_tail_matches_level_launches(precision, tail_nel):
+    """The coarse multigrid levels run as one launch per V-cycle (tail_nel: levels of at most 1024
+    elements as an 8-CTA cluster through global memory; of at most 256 as one CTA with every
+    vector in shared memory) repeat the multi-launch V-cycle bit for bit: same V-cycle output, same
+    solve iterates and counts."""
     c = make_case(64, 64, contrast=1e4, seed=3)
     f, h = torch.as_tensor(c["f"]).cuda(), torch.as_tensor(c["h"]).cuda()
     hier = "f32" if precision == "mixed" else "f64"
     dt = torch.float32 if hier == "f32" else torch.float64
     g = torch.Generator(device="cuda").manual_seed(5)
     out = {}
-    for tail in (1024, 0):
+    for tail in (tail_nel, 0):
         S = solver_for(c, tail_nel=tail)
         b = torch.randn(S.nv, dtype=dt, device="cuda", generator=g) if tail else b
         x = S.vcycle(b, precision=hier)
         V, P, info = S.solve(f, h, precision=precision, tol=1e-8)
         out[tail] = (x.cpu().numpy(), V.cpu().numpy(), P.cpu().numpy(), info)
-    (x1, V1, P1, i1), (x0, V0, P0, i0) = out[1024], out[0]
+    (x1, V1, P1, i1), (x0, V0, P0, i0) = out[tail_nel], out[0]
     assert np.array_equal(x1, x0)
     assert i1["converged"] == 1 and i0["converged"] == 1
     for k in ("outer_iters", "inner_iters", "refinements"):

@@ -434,6 +434,22 @@ int mw_stokes_residual(mw_stokes* S, const double* V, const double* P, const dou
 int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV, double* solP, mw_solve_params sp,
                     mw_solve_info* info, void* stream);
 
+/* Ensembles: the Stokes solves of many models in one launch, one thread-block cluster per model
+ * running that model's whole mixed-precision solve (MW_F32: FP64 refinement, Schur-complement CG,
+ * FP32 multigrid-PCG inner solves) with its own hierarchy, iteration counts and convergence tests.
+ * mw_stokes_ensemble_create binds n solvers (each created with the FP32 hierarchy) to their
+ * right-hand sides f, h and solutions V, P (device arrays that stay in place; V 16-byte aligned);
+ * before each ensemble solve, every model's viscosity is set (mw_stokes_set_viscosity) and its
+ * hierarchy prepared (mw_stokes_prepare, on a stream ordered before the solve).  The solve takes
+ * precision MW_F32 and no history; each model's outcome is read with mw_stokes_device_info.
+ * Replaces, for an ensemble, the per-model mw_stokes_solve calls (one per model and step). */
+typedef struct mw_stokes_ensemble mw_stokes_ensemble;
+int mw_stokes_prepare(mw_stokes* S, int32_t precision, void* stream);
+int mw_stokes_ensemble_create(mw_stokes* const* S, const double* const* f, const double* const* h,
+                              double* const* V, double* const* P, int32_t n, mw_stokes_ensemble** out);
+int mw_stokes_ensemble_solve(mw_stokes_ensemble* E, mw_solve_params sp, void* stream);
+int mw_stokes_ensemble_destroy(mw_stokes_ensemble* E);
+
 /* u, w from the interleaved solution and p = solP * scale (meeuuw.py:1846-1851). */
 int mw_split_solution(int64_t nn_V, int64_t nn_P, const double* solV, const double* solP, double scale, double* u,
                       double* w, double* p, void* stream);

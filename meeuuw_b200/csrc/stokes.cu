@@ -216,6 +216,72 @@ MW_D int q2_local_idx(int dx, int dz) {
 // Schur-complement iteration's G p and G^T u need no element products: each node gathers its
 // incident elements' entries in ascending element order.  Fixed velocity dofs: zero rows of G,
 // zeroed entries of u for G^T (the reference's Dirichlet elimination).
+// G p at velocity node (ix, iz) (f - G p with b): gx, gz are the GX, GZ tables, cx, cz the scalings.
+MW_D void grad_node(const LevelGeo& g, const double* p, const uint8_t* fix, const double* b, double* y, int ix,
+                    int iz, const double* gx, const double* gz, double cx, double cz) {
+  const int64_t n = (int64_t)iz * g.nnx + ix;
+  const bool xo = ix & 1, zo = iz & 1;
+  const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = ix >> 1;
+  const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = iz >> 1;
+  const int exs[2] = {xa, xb}, ezs[2] = {za, zb};
+  const bool vx[2] = {xa >= 0, !xo && xb < g.nx}, vz[2] = {za >= 0, !zo && zb < g.nz};
+  double ax = 0.0, az = 0.0;
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      if (!vz[a] || !vx[c]) continue;
+      const int ex = exs[c], ez = ezs[a];
+      const int k = q2_local_idx(ix - 2 * ex, iz - 2 * ez);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double pv = p[q1_node(ex, ez, j, g.nx)];
+        ax += gx[k * 4 + j] * pv;
+        az += gz[k * 4 + j] * pv;
+      }
+    }
+  const uchar2 ff = reinterpret_cast<const uchar2*>(fix)[n];
+  double2 r{ff.x ? 0.0 : cx * ax, ff.y ? 0.0 : cz * az};
+  if (b) {
+    const double2 bb = reinterpret_cast<const double2*>(b)[n];
+    r = double2{bb.x - r.x, bb.y - r.y};
+  }
+  reinterpret_cast<double2*>(y)[n] = r;
+}
+
+// G^T u at pressure node (px, pz)
+MW_D double div_node(const LevelGeo& g, const double* u, const uint8_t* fix, int px, int pz, const double* gx,
+                     const double* gz, double cx, double cz) {
+  const double2* u2 = reinterpret_cast<const double2*>(u);
+  const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
+  // incident elements in ascending order and this node's Q1 index in each
+  const int exs[4] = {px - 1, px, px - 1, px}, ezs[4] = {pz - 1, pz - 1, pz, pz}, js[4] = {2, 3, 1, 0};
+  double acc = 0.0;
+#pragma unroll 1
+  for (int e = 0; e < 4; ++e) {
+    const int ex = exs[e], ez = ezs[e], j = js[e];
+    if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+    double sx = 0.0, sz = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      const int64_t m = q2_node(ex, ez, k, g.nnx);
+      const double2 uu = u2[m];
+      const uchar2 ff = f2[m];
+      sx += gx[k * 4 + j] * (ff.x ? 0.0 : uu.x);
+      sz += gz[k * 4 + j] * (ff.y ? 0.0 : uu.y);
+    }
+    acc += cx * sx + cz * sz;
+  }
+  return acc;
+}
+
+// the element scalings of G: cx = -s (hx hz / 4)(2 / hx), cz = -s (hx hz / 4)(2 / hz)
+MW_D void grad_scales(const LevelGeo& g, double* cx, double* cz) {
+  const double jac = g.hx * g.hz / 4.0;
+  *cx = -g.s * jac * (2.0 / g.hx);
+  *cz = -g.s * jac * (2.0 / g.hz);
+}
+
 __global__ void k_grad_p(LevelGeo g, const double* __restrict__ p, const uint8_t* __restrict__ fix,
                          const double* __restrict__ b, double* __restrict__ y) {
   pdl_entry();
@@ -225,41 +291,12 @@ __global__ void k_grad_p(LevelGeo g, const double* __restrict__ p, const uint8_t
     gz[threadIdx.x] = c_ref.GZ[threadIdx.x];
   }
   __syncthreads();
-  const double jac = g.hx * g.hz / 4.0;
-  const double cx = -g.s * jac * (2.0 / g.hx), cz = -g.s * jac * (2.0 / g.hz);
-  const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
+  double cx, cz;
+  grad_scales(g, &cx, &cz);
   // one lattice row per blockIdx.y: no index division
   for (int iz = blockIdx.y; iz < g.nnz; iz += gridDim.y)
-  for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < g.nnx; ix += gridDim.x * blockDim.x) {
-    const int64_t n = (int64_t)iz * g.nnx + ix;
-    const bool xo = ix & 1, zo = iz & 1;
-    const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = ix >> 1;
-    const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = iz >> 1;
-    const int exs[2] = {xa, xb}, ezs[2] = {za, zb};
-    const bool vx[2] = {xa >= 0, !xo && xb < g.nx}, vz[2] = {za >= 0, !zo && zb < g.nz};
-    double ax = 0.0, az = 0.0;
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        if (!vz[a] || !vx[c]) continue;
-        const int ex = exs[c], ez = ezs[a];
-        const int k = q2_local_idx(ix - 2 * ex, iz - 2 * ez);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const double pv = p[q1_node(ex, ez, j, g.nx)];
-          ax += gx[k * 4 + j] * pv;
-          az += gz[k * 4 + j] * pv;
-        }
-      }
-    const uchar2 ff = f2[n];
-    double2 r{ff.x ? 0.0 : cx * ax, ff.y ? 0.0 : cz * az};
-    if (b) {
-      const double2 bb = reinterpret_cast<const double2*>(b)[n];
-      r = double2{bb.x - r.x, bb.y - r.y};
-    }
-    reinterpret_cast<double2*>(y)[n] = r;
-  }
+    for (int ix = blockIdx.x * blockDim.x + threadIdx.x; ix < g.nnx; ix += gridDim.x * blockDim.x)
+      grad_node(g, p, fix, b, y, ix, iz, gx, gz, cx, cz);
 }
 
 __global__ void k_div_u(LevelGeo g, const double* __restrict__ u, const uint8_t* __restrict__ fix,
@@ -271,35 +308,13 @@ __global__ void k_div_u(LevelGeo g, const double* __restrict__ u, const uint8_t*
     gz[threadIdx.x] = c_ref.GZ[threadIdx.x];
   }
   __syncthreads();
-  const double jac = g.hx * g.hz / 4.0;
-  const double cx = -g.s * jac * (2.0 / g.hx), cz = -g.s * jac * (2.0 / g.hz);
+  double cx, cz;
+  grad_scales(g, &cx, &cz);
   const int ncx = g.nx + 1;
-  const double2* u2 = reinterpret_cast<const double2*>(u);
-  const uchar2* f2 = reinterpret_cast<const uchar2*>(fix);
   // one pressure-node row per blockIdx.y: no index division
   for (int pz = blockIdx.y; pz <= g.nz; pz += gridDim.y)
-  for (int px = blockIdx.x * blockDim.x + threadIdx.x; px < ncx; px += gridDim.x * blockDim.x) {
-    const int64_t n = (int64_t)pz * ncx + px;
-    // incident elements in ascending order and this node's Q1 index in each
-    const int exs[4] = {px - 1, px, px - 1, px}, ezs[4] = {pz - 1, pz - 1, pz, pz}, js[4] = {2, 3, 1, 0};
-    double acc = 0.0;
-#pragma unroll 1
-    for (int e = 0; e < 4; ++e) {
-      const int ex = exs[e], ez = ezs[e], j = js[e];
-      if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
-      double sx = 0.0, sz = 0.0;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        const int64_t m = q2_node(ex, ez, k, g.nnx);
-        const double2 uu = u2[m];
-        const uchar2 ff = f2[m];
-        sx += gx[k * 4 + j] * (ff.x ? 0.0 : uu.x);
-        sz += gz[k * 4 + j] * (ff.y ? 0.0 : uu.y);
-      }
-      acc += cx * sx + cz * sz;
-    }
-    y[n] = acc;
-  }
+    for (int px = blockIdx.x * blockDim.x + threadIdx.x; px < ncx; px += gridDim.x * blockDim.x)
+      y[(int64_t)pz * ncx + px] = div_node(g, u, fix, px, pz, gx, gz, cx, cz);
 }
 
 // 1D Q2 prolongation: fine node i from coarse nodes
@@ -354,27 +369,45 @@ MW_D void cp_async_pair(void* dst, const void* src) {
 }
 MW_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// Shared memory of one operator-apply tile (the arrays of apply_tile).  Node vectors the epilogue
+// reads for the four nodes each owned element emits (b; b, diag, d) are fetched asynchronously
+// while the element products run (FP32 only: the FP64 tile's shared memory stays under the 48 KB
+// static limit without them).
 template <typename R, int MODE>
-__global__ void __launch_bounds__(APPLY_THREADS, sizeof(R) == 4 ? MW_APPLY_MINB : 1)
-k_apply(LevelGeo g, ApplyArgs<R> a) {
-  pdl_entry();
+struct ApplySmem {
   typedef typename Vec2<R>::T R2;
-  // node vectors the epilogue reads for the four nodes each owned element emits (b; b, diag, d),
-  // fetched asynchronously while the element products run (FP32; the FP64 kernel's shared memory
-  // is already at the 48 KB static limit)
-  constexpr bool CHEB = MODE == AM_CHEB || MODE == AM_CHEB_Z || MODE == AM_CHEB_P;
-  constexpr bool PRO = MODE == AM_CHEB_P;
-  constexpr int NPRE = sizeof(R) == 8 ? 0 : (CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
-  __shared__ __align__(16) R su[LZ * LX * 2];
-  __shared__ __align__(16) R2 spre[(NPRE ? NPRE : 1) * 4 * TX * TZ];
-  constexpr int NJ = APPLY_THREADS - TX * TZ;         // spare threads: right column and top row nodes
+  static constexpr bool CHEB = MODE == AM_CHEB || MODE == AM_CHEB_Z || MODE == AM_CHEB_P;
+  static constexpr bool PRO = MODE == AM_CHEB_P;
+  static constexpr int NPRE = sizeof(R) == 8 ? 0 : (CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
+  static constexpr int NJ = APPLY_THREADS - TX * TZ;  // spare threads: right column and top row nodes
+  __align__(16) R su[LZ * LX * 2];
+  __align__(16) R2 spre[NPRE ? NPRE * 4 * TX * TZ : 1];
+  __align__(16) R2 sspare[NPRE ? NPRE * 2 * NJ : 1];
+  R sp[PZ * PX];
+  R sye[NEL_T * 22];
+  uchar2 sfix[LZ * LX];                              // Dirichlet flags of the staged nodes
+  __align__(16) R2 scx[PRO ? CLZ * CLX : 1];         // AM_CHEB_P: the coarse correction tile
+};
+
+// One operator apply over element tile (bx, bz) by the APPLY_THREADS threads of a CTA, in the
+// shared memory sm.  A CTA that runs several tiles one after another separates them with a
+// __syncthreads() (the next tile's staging overwrites what this one's epilogue reads).
+template <typename R, int MODE>
+MW_D void apply_tile(const LevelGeo g, const ApplyArgs<R> a, int bx, int bz, ApplySmem<R, MODE>& sm) {
+  typedef typename Vec2<R>::T R2;
+  constexpr bool CHEB = ApplySmem<R, MODE>::CHEB;
+  constexpr bool PRO = ApplySmem<R, MODE>::PRO;
+  constexpr int NPRE = ApplySmem<R, MODE>::NPRE;
+  constexpr int NJ = ApplySmem<R, MODE>::NJ;
   static_assert(2 * TZ + 1 + 2 * TX <= 2 * NJ, "the spare threads take at most two boundary nodes each");
-  __shared__ __align__(16) R2 sspare[(NPRE ? NPRE : 1) * 2 * NJ];
-  __shared__ R sp[PZ * PX];
-  __shared__ R sye[NEL_T * 22];
-  __shared__ uchar2 sfix[LZ * LX];          // Dirichlet flags of the staged nodes
-  __shared__ __align__(16) R2 scx[PRO ? CLZ * CLX : 1];   // AM_CHEB_P: the coarse correction tile
-  const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
+  auto& su = sm.su;
+  auto& spre = sm.spre;
+  auto& sspare = sm.sspare;
+  auto& sp = sm.sp;
+  auto& sye = sm.sye;
+  auto& sfix = sm.sfix;
+  auto& scx = sm.scx;
+  const int ex0 = bx * TX, ez0 = bz * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
   const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
@@ -749,6 +782,14 @@ k_apply(LevelGeo g, ApplyArgs<R> a) {
       }
     }
   }
+}
+
+template <typename R, int MODE>
+__global__ void __launch_bounds__(APPLY_THREADS, sizeof(R) == 4 ? MW_APPLY_MINB : 1)
+k_apply(LevelGeo g, ApplyArgs<R> a) {
+  pdl_entry();
+  __shared__ ApplySmem<R, MODE> sm;
+  apply_tile<R, MODE>(g, a, blockIdx.x, blockIdx.y, sm);
 }
 
 // diag(K): sum over incident elements of the element diagonal, ascending element order.
@@ -1255,46 +1296,53 @@ __global__ void k_mass_diag(LevelGeo g, const double* __restrict__ w, double* __
   }
 }
 
+// the Q1 element mass matrix of the uniform box, Me[a * 4 + c] = sum_q N_a N_c JxW
+MW_D double mass_entry(const LevelGeo& g, int a, int c) {
+  const double jac = g.hx * g.hz / 4.0;
+  double m = 0;
+  for (int q = 0; q < 9; ++q) m += c_ref.NP[q * 4 + a] * c_ref.NP[q * 4 + c] * jac * c_ref.wq[q];
+  return m;
+}
+
 // One fused Chebyshev-Jacobi step for M_w x = b:  r = b - M_w x_in ; d = c1 d + c2 D^-1 r ;
 // x_out = x_in + d.  `first` means x_in = 0 (no product, no old direction).  For Q1 mass matrices
 // with positive element weights, lambda(D^-1 M_w) lies in [0.25, 2.25] whatever the weights
 // (element-by-element bound; the exactly integrated bilinear element matrix has D_e^-1 M_e eigenvalues
 // 9/4, 3/4, 3/4, 1/4), so the coefficients are fixed and need no dot products.
+// (the step at pressure node n; Me: the element mass matrix)
+MW_D void mass_cheb_node(const LevelGeo& g, const double* w, const double* b, const double* xin, double* xout,
+                         double* d, const double* dg, double c1, double c2, int first, const double* Me, int64_t n) {
+  const int ncx = g.nx + 1;
+  double y = 0;
+  if (!first) {
+    const int i = (int)(n % ncx), j = (int)(n / ncx);
+    // incident elements (j-1,i-1) k=2, (j-1,i) k=3, (j,i-1) k=1, (j,i) k=0
+    for (int s = 0; s < 4; ++s) {
+      const int ex = (s & 1) ? i : i - 1, ez = (s & 2) ? j : j - 1;
+      if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
+      const int kl = s == 0 ? 2 : (s == 1 ? 3 : (s == 2 ? 1 : 0));
+      const int64_t e = (int64_t)ez * g.nx + ex;
+      double v = 0;
+      for (int k2 = 0; k2 < 4; ++k2) v += Me[kl * 4 + k2] * xin[q1_node(ex, ez, k2, g.nx)];
+      y += (w ? w[e] : 1.0) * v;
+    }
+  }
+  const double r = b[n] - y;
+  const double dn = first ? c2 * r / dg[n] : c1 * d[n] + c2 * r / dg[n];
+  d[n] = dn;
+  xout[n] = (first ? 0.0 : xin[n]) + dn;
+}
+
 __global__ void k_mass_cheb(LevelGeo g, const double* __restrict__ w, const double* __restrict__ b,
                             const double* __restrict__ xin, double* __restrict__ xout, double* __restrict__ d,
                             const double* __restrict__ dg, double c1, double c2, int first) {
   pdl_entry();
   __shared__ double Me[16];
-  if (threadIdx.x < 16) {
-    const double jac = g.hx * g.hz / 4.0;
-    int a = threadIdx.x / 4, c = threadIdx.x % 4;
-    double m = 0;
-    for (int q = 0; q < 9; ++q) m += c_ref.NP[q * 4 + a] * c_ref.NP[q * 4 + c] * jac * c_ref.wq[q];
-    Me[threadIdx.x] = m;
-  }
+  if (threadIdx.x < 16) Me[threadIdx.x] = mass_entry(g, threadIdx.x / 4, threadIdx.x % 4);
   __syncthreads();
-  const int ncx = g.nx + 1;
-  const int64_t np = (int64_t)ncx * (g.nz + 1);
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x) {
-    double y = 0;
-    if (!first) {
-      const int i = (int)(n % ncx), j = (int)(n / ncx);
-      // incident elements (j-1,i-1) k=2, (j-1,i) k=3, (j,i-1) k=1, (j,i) k=0
-      for (int s = 0; s < 4; ++s) {
-        const int ex = (s & 1) ? i : i - 1, ez = (s & 2) ? j : j - 1;
-        if (ex < 0 || ex >= g.nx || ez < 0 || ez >= g.nz) continue;
-        const int kl = s == 0 ? 2 : (s == 1 ? 3 : (s == 2 ? 1 : 0));
-        const int64_t e = (int64_t)ez * g.nx + ex;
-        double v = 0;
-        for (int k2 = 0; k2 < 4; ++k2) v += Me[kl * 4 + k2] * xin[q1_node(ex, ez, k2, g.nx)];
-        y += (w ? w[e] : 1.0) * v;
-      }
-    }
-    const double r = b[n] - y;
-    const double dn = first ? c2 * r / dg[n] : c1 * d[n] + c2 * r / dg[n];
-    d[n] = dn;
-    xout[n] = (first ? 0.0 : xin[n]) + dn;
-  }
+  const int64_t np = (int64_t)(g.nx + 1) * (g.nz + 1);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < np; n += (int64_t)gridDim.x * blockDim.x)
+    mass_cheb_node(g, w, b, xin, xout, d, dg, c1, c2, first, Me, n);
 }
 
 // The grid-wide sum of one value per thread, finished in the same launch: block partials in
@@ -3291,3 +3339,6 @@ static int stokes_solve_host(mw_stokes* S, const double* f, const double* h, dou
 }
 
 }  // extern "C"
+
+// the Stokes solves of an ensemble of models in one launch (one cluster per model)
+#include "stokes_ensemble.cuh"

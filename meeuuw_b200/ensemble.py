@@ -11,6 +11,11 @@ Stokes solver (its own stream and recorded CUDA graphs), so nothing is shared be
 ``Autotuner`` picks the number of host threads (the concurrency level) by timing ensemble steps,
 and caches the choice per GPU and ensemble shape.
 
+``BatchedEnsemble`` runs the Stokes solves of all models in one launch instead (one thread-block
+cluster per model running that model's whole mixed-precision solve,
+``stokes.StokesEnsembleSolve``), between the models' other phases on their own streams; the whole
+ensemble step is recorded as one CUDA graph.
+
 Many streams share the GPU's hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default): a
 process running a large ensemble should set it higher (up to 32) before CUDA is initialised, so
 that one model's device-side solver loop does not hold up the models queued behind it.
@@ -25,7 +30,8 @@ from dataclasses import replace
 import numpy as np
 import torch
 
-from . import configs
+from . import configs, ops
+from .stokes import StokesEnsembleSolve
 from .timestep import GPUModel
 
 
@@ -161,6 +167,128 @@ class Ensemble:
         if self.pool is not None:
             self.pool.shutdown(wait=True)
             self.pool = None
+
+
+class BatchedEnsemble:
+    """N independent models whose Stokes solves run in one launch.
+
+    A step: every model's phases up to the solve (particles, projections, right-hand side,
+    viscosity, multigrid hierarchy) on its own stream; then one launch in which a thread-block
+    cluster per model runs that model's whole solve (its own hierarchy, iteration counts and
+    convergence tests, no waiting between clusters); then every model's phases after the solve
+    (energy, Nu, vrms, advection, locate) on its own stream.  After each model's cold first step
+    (eager, with the guess hook if one is given), the whole step is recorded as one CUDA graph and
+    replayed.  A model whose device flags are set is retired with the reference's message and the
+    step is recorded again without it."""
+
+    def __init__(self, cfgs, tol=1e-8, guess=None, record=True):
+        self.cfgs = list(cfgs)
+        self.models, self.streams = [], []
+        self.first_step_info = []
+        for cfg in self.cfgs:
+            st = torch.cuda.Stream()
+            with torch.cuda.stream(st):
+                m = GPUModel(cfg, stokes="mixed", tol=tol)
+                if guess is not None:
+                    m.guess = guess(m)
+                m.step()                          # the cold start: per-model solve (and hook)
+                self.first_step_info.append(dict(m.last_solve))
+                if m.guess is not None and not m._guess_idle():
+                    raise ValueError("the guess hook must be idle after the first step")
+            self.models.append(m)
+            self.streams.append(st)
+        torch.cuda.synchronize()
+        self.active = [True] * len(self.models)
+        self.retired = {}
+        self.steps_done = len(self.models)
+        self.record = bool(record)
+        self.main = torch.cuda.Stream()
+        self._bind()
+
+    def _bind(self):
+        idx = [i for i in range(len(self.models)) if self.active[i]]
+        self.idx = idx
+        ms = [self.models[i] for i in idx]
+        self.solve = StokesEnsembleSolve([m.solver for m in ms], [m.rhs_f for m in ms], [m.rhs_h for m in ms],
+                                         [m.solV for m in ms], [m.solP for m in ms]) if ms else None
+        self.graph = None
+
+    def _body(self):
+        main = torch.cuda.current_stream()
+        for i in self.idx:
+            m, st = self.models[i], self.streams[i]
+            st.wait_stream(main)
+            with torch.cuda.stream(st), ops.workspace_scope(m):
+                m._step_pre()
+                m.solver.prepare("mixed")
+            main.wait_stream(st)
+        m0 = self.models[self.idx[0]]
+        kw = m0.stokes_solve_kw()
+        kw.pop("precision")
+        self.solve.solve(use_guess=True, **kw)
+        for i in self.idx:
+            m, st = self.models[i], self.streams[i]
+            st.wait_stream(main)
+            with torch.cuda.stream(st), ops.workspace_scope(m):
+                m._step_post()
+            main.wait_stream(st)
+
+    def step(self):
+        """One time step of every active model."""
+        if not self.idx:
+            return
+        self.main.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(self.main):
+            if self.record and self.graph is None:
+                g = torch.cuda.CUDAGraph()
+                for i in self.idx:
+                    self.models[i]._capturing = True
+                try:
+                    with torch.cuda.graph(g, stream=self.main, capture_error_mode="thread_local"):
+                        self._body()
+                finally:
+                    for i in self.idx:
+                        self.models[i]._capturing = False
+                        self.models[i].istep -= 1          # the capture recorded the step; nothing ran
+                self.graph = g
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._body()
+        torch.cuda.current_stream().wait_stream(self.main)
+        for i in self.idx:
+            self.models[i]._replayed = True                # outcomes are on the device
+            if self.graph is not None:
+                self.models[i].istep += 1
+        self.steps_done += len(self.idx)
+        self._retire_flagged()
+
+    def _retire_flagged(self):
+        changed = False
+        for i in self.idx:
+            m = self.models[i]
+            flags = int(m.err.item())
+            if flags:
+                try:
+                    m.check()
+                    self.retired[i] = f"device flags {flags}"
+                except SystemExit as e:
+                    self.retired[i] = str(e)
+                self.active[i] = False
+                changed = True
+        if changed:
+            self._bind()
+
+    def synchronize(self):
+        torch.cuda.synchronize()
+
+    def diagnostics(self):
+        return [m.diagnostics() for m in self.models]
+
+    def check(self):
+        for i, m in enumerate(self.models):
+            if self.active[i]:
+                m.check()
 
 
 class Autotuner:

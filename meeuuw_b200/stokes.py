@@ -55,6 +55,10 @@ L.extra_protos({
     "mw_stokes_residual": (c_int32, [c_void_p] * 7 + [c_void_p, c_void_p]),
     "mw_stokes_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, MwSolveParams, c_void_p,
                                   c_void_p]),
+    "mw_stokes_prepare": (c_int32, [c_void_p, c_int32, c_void_p]),
+    "mw_stokes_ensemble_create": (c_int32, [c_void_p] * 5 + [c_int32, c_void_p]),
+    "mw_stokes_ensemble_solve": (c_int32, [c_void_p, MwSolveParams, c_void_p]),
+    "mw_stokes_ensemble_destroy": (c_int32, [c_void_p]),
 })
 
 SCHEME = {"cd_u_eta": 0, "uzawa3": 1}
@@ -94,6 +98,12 @@ class StokesSolver:
     def set_viscosity(self, etaq, eta_e=None):
         self._eta = etaq
         call("mw_stokes_set_viscosity", self.h, ptr(etaq), ptr(eta_e), stream_ptr())
+
+    def prepare(self, precision="mixed"):
+        """Set up the multigrid hierarchy for the current viscosity (coarse viscosities, diagonals,
+        Chebyshev intervals, the coarsest inverse) on the current stream; a solve does this itself,
+        an ensemble solve (StokesEnsembleSolve) needs it done per model first."""
+        call("mw_stokes_prepare", self.h, PREC[precision], stream_ptr())
 
     def apply(self, u=None, p=None, yV=None, yP=None, precision="f64"):
         dt = torch.float32 if precision == "f32" else torch.float64
@@ -186,3 +196,44 @@ class StokesSolver:
         if rc not in (0, 3) or (raise_on_fail and rc != 0):
             raise RuntimeError(f"mw_stokes_solve returned {out['status']} ({out})")
         return V, P, out
+
+
+def solve_params(scheme="cd_u_eta", precision="f64", tol=1e-8, use_guess=True, **kw):
+    sp = MwSolveParams()
+    L.lib().mw_solve_default_params(ctypes.byref(sp))
+    sp.scheme, sp.precision, sp.tol = SCHEME[scheme], PREC[precision], float(tol)
+    sp.use_guess = 1 if use_guess else 0
+    for k, v in kw.items():
+        setattr(sp, k, v)
+    return sp
+
+
+class StokesEnsembleSolve:
+    """The Stokes solves of many models in one launch: one thread-block cluster per model runs that
+    model's whole mixed-precision solve (FP64 refinement, Schur-complement CG, FP32 multigrid-PCG)
+    with its own hierarchy and convergence tests.  Binds each solver to its right-hand side (f, h)
+    and solution (V, P) tensors, which must stay in place.  Before solve(), every model's viscosity
+    is set and its hierarchy prepared (StokesSolver.prepare) on streams the current stream waits for;
+    the outcomes are read per model with StokesSolver.device_info."""
+
+    def __init__(self, solvers, f, h, V, P):
+        n = len(solvers)
+        if not (n == len(f) == len(h) == len(V) == len(P)) or n == 0:
+            raise ValueError("one (f, h, V, P) per solver")
+        self.solvers = list(solvers)
+        self._keep = (list(f), list(h), list(V), list(P))     # the bound tensors stay alive
+        arr = lambda xs: (c_void_p * n)(*[x.data_ptr() for x in xs])
+        hs = (c_void_p * n)(*[s.h.value for s in self.solvers])
+        e = c_void_p()
+        call("mw_stokes_ensemble_create", hs, arr(f), arr(h), arr(V), arr(P), n, ctypes.byref(e))
+        self.h = e
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and L._lib is not None:
+            L.lib().mw_stokes_ensemble_destroy(self.h)
+            self.h = None
+
+    def solve(self, scheme="cd_u_eta", tol=1e-8, use_guess=True, **kw):
+        sp = solve_params(scheme, "mixed", tol, use_guess, **kw)
+        call("mw_stokes_ensemble_solve", self.h, sp, stream_ptr())
+

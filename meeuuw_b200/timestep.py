@@ -206,6 +206,19 @@ class GPUModel:
             self._step_body()
 
     def _step_body(self):
+        self._step_pre()
+        _, _, info = self.solver.solve(self.rhs_f, self.rhs_h, self.solV, self.solP, **self.stokes_solve_kw())
+        self.last_solve = info
+        self._step_post()
+
+    def stokes_solve_kw(self):
+        """The Stokes solve's settings (StokesSolver.solve keywords)."""
+        return dict(scheme=self.scheme, precision=self.stokes_precision, tol=self.tol, inner_rtol=self.inner_rtol,
+                    **self.solve_kw)
+
+    def _step_pre(self):
+        """The step up to the Stokes solve: particles, projections, qpoint fields, the Stokes
+        right-hand side (rhs_f, rhs_h) and viscosity, the guess (solV, solP)."""
         c, b, tb = self.cfg, self.box, self.tables
         P = self.props
         self._mark("particles+projections")
@@ -257,10 +270,13 @@ class GPUModel:
         elif self.warm_start != "previous":
             self.solV.zero_()
             self.solP.zero_()
-        _, _, info = self.solver.solve(self.rhs_f, self.rhs_h, self.solV, self.solP, scheme=self.scheme,
-                                       precision=self.stokes_precision, tol=self.tol, inner_rtol=self.inner_rtol,
-                                       **self.solve_kw)
-        self.last_solve = info
+
+    def _step_post(self):
+        """The step after the Stokes solve: velocity and pressure fields, dt, energy, Nu, strain
+        rate, vrms, advection and locate."""
+        c, b, tb = self.cfg, self.box, self.tables
+        P = self.props
+        qf, nd = self.qf, self.nodal
         ops.split_solution(self.solV, self.solP, c.eta_ref / self.L_ref, self.u, self.w, self.p)
         self._mark("post+dt")
         # pressure normalisation and nodal pressure (meeuuw.py:1958-2051)

@@ -650,15 +650,23 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _ensemble_state(ens):
+    """(vrms per model, active flags, models converged, retired) of an ensemble after its steps."""
+    diag = ens.diagnostics()
+    conv = sum(1 for i, d in enumerate(diag) if ens.active[i] and d["stokes"]["converged"] == 1)
+    return [d["vrms"] for d in diag], list(ens.active), conv, dict(ens.retired)
+
+
 def run_ensemble(args):
     """Uneven ensemble (n ~ U[64,192], Ra ~ logU[1e4,1e7], contrast ~ logU[1,1e4], 16 particles per
-    element): aggregate model-timesteps/s of the mixed-precision ensemble in its two modes -- every
-    model's step recorded as one CUDA graph (one launch per model per step), and the thread pool
-    with autotuned concurrency -- each timed with CUDA events; `value` is the faster mode.  Each
-    model's vrms is compared with the same model run with the FP64 solver."""
+    element): aggregate model-timesteps/s of the mixed-precision ensemble in its three modes -- the
+    thread pool with autotuned concurrency, every model's step recorded as one CUDA graph (one launch
+    per model per step), and every model's Stokes solve in one shared launch (one thread-block
+    cluster per model) inside one recorded ensemble step -- each timed with CUDA events; `value` is
+    the fastest mode.  Each model's vrms is compared with the same model run with the FP64 solver."""
     import torch
     from meeuuw_b200 import replicas
-    from meeuuw_b200.ensemble import Autotuner, Ensemble, sample_configs
+    from meeuuw_b200.ensemble import Autotuner, BatchedEnsemble, Ensemble, sample_configs
     world, rank, local = replicas.world()
     torch.cuda.set_device(local)
     replicas.init("nccl")
@@ -714,16 +722,20 @@ def run_ensemble(args):
         cold_learned = ens.first_step_info
         ms, n = timed(ens)
         modes["graphs"] = {"model_steps_per_s": n / (ms / 1000.0), "ms_per_step": ms / args.steps}
-    diag = ens.diagnostics()
-    mixed = [d["vrms"] for d in diag]
-    have_guess = [m.guess is not None for m in ens.models]
-    converged = sum(1 for i, d in enumerate(diag) if ens.active[i] and d["stokes"]["converged"] == 1)
-    active = list(ens.active)
-    retired = dict(ens.retired)
+        states = {"graphs": _ensemble_state(ens)}
+        have_guess = [m.guess is not None for m in ens.models]
+        ens.close()
+        del ens
+        torch.cuda.empty_cache()
+        # every model's Stokes solve in one launch (one thread-block cluster per model), the whole
+        # ensemble step recorded as one graph; the cold first steps as in the graphs mode
+        ens = BatchedEnsemble(cfgs, guess=guess)
+        ms, n = timed(ens)
+        modes["batched"] = {"model_steps_per_s": n / (ms / 1000.0), "ms_per_step": ms / args.steps}
+        states["batched"] = _ensemble_state(ens)
+        del ens
+        torch.cuda.empty_cache()
     nsteps_done = 1 + args.warmup + args.steps
-    ens.close()
-    del ens
-    torch.cuda.empty_cache()
     # FP64 runs of the same models for the same number of steps: at the benchmark's 1e-8 and at 1e-10
     # (the reference both are measured against; FP64 at 1e-8 against it is the floor the tolerance
     # itself sets)
@@ -750,9 +762,17 @@ def run_ensemble(args):
             "pcg_iters_zero": sum(cold_zero[i]["inner_iters"] for i in sel)}
     fp64, act64 = fp64_run(1e-8)
     tight, act_t = fp64_run(1e-10)
+    best = max(modes, key=lambda k: modes[k]["model_steps_per_s"])
+    # the accuracy figures below are the fastest recorded mode's (the thread pool's models are
+    # the graphs mode's, stepped from host threads)
+    mixed, active, converged, retired = states[best if best in states else "graphs"]
     both = [i for i in range(len(cfgs)) if active[i] and act64[i] and act_t[i]]
     err = [abs(mixed[i] - tight[i]) / abs(tight[i]) for i in both]
     floor = sorted(abs(fp64[i] - tight[i]) / abs(tight[i]) for i in both)
+    err_modes = {}
+    for k, (mx, ac, _, _) in states.items():
+        e = sorted(abs(mx[i] - tight[i]) / abs(tight[i]) for i in range(len(cfgs)) if ac[i] and act64[i] and act_t[i])
+        err_modes[k] = {"max": e[-1] if e else None, "median": e[len(e) // 2] if e else None}
     retired = {cfgs[i].name: why for i, why in retired.items()}
     if world > 1:                            # gather the per-model figures on rank 0
         import torch.distributed as dist
@@ -763,7 +783,6 @@ def run_ensemble(args):
         converged = sum(g[2] for g in got)
         floor = sorted(x for g in got for x in g[3])
     err = sorted(err)
-    best = max(modes, key=lambda k: modes[k]["model_steps_per_s"])
     line = {"metric": "aggregate model-timesteps/s, uneven ensemble (64..192 squared, 16 particles/element)",
             "value": modes[best]["model_steps_per_s"], "unit": "model-timesteps/s",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": modes[best]["ms_per_step"],
@@ -779,6 +798,7 @@ def run_ensemble(args):
             "vrms_rel_err_vs_fp64_1e-10": {"models": len(err), "max": err[-1] if err else None,
                                            "median": err[len(err) // 2] if err else None,
                                            "p90": err[int(0.9 * (len(err) - 1))] if err else None},
+            "vrms_rel_err_by_mode": err_modes,
             "vrms_floor_fp64_1e-8_vs_1e-10": {"max": floor[-1] if floor else None,
                                               "median": floor[len(floor) // 2] if floor else None,
                                               "p90": floor[int(0.9 * (len(floor) - 1))] if floor else None},

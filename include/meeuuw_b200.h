@@ -339,6 +339,9 @@ typedef struct {
   int32_t tail_nel;       /* levels with at most this many elements run each V-cycle as one launch of
                              one cluster (0: a launch per smoothing step, residual and transfer)    */
   int32_t cheb_degree_coarse; /* Chebyshev steps per sweep below the finest level (0: cheb_degree)   */
+  int32_t coarsen_odd;    /* 1: an odd element count coarsens to ceil(n/2) elements over the same box
+                             (a grid not nested in the fine one, Q2 interpolation as the transfer);
+                             0: coarsening stops at the first odd count                           */
 } mw_stokes_params;
 
 typedef struct {
@@ -401,6 +404,12 @@ int mw_stokes_div(mw_stokes* S, const double* u, double* yP, void* stream);
 
 /* One multigrid V-cycle for K (the inner preconditioner); b, x in the given precision. */
 int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, void* stream);
+/* Grid transfer between multigrid levels `level` (fine) and level + 1 (coarse) of the current
+ * hierarchy: restrict_dir = 1: out (coarse) = P^T in (fine), fixed coarse dofs zero; 0: out (fine)
+ * += P in (coarse) on the free fine dofs.  Element counts of a level: mw_stokes_level_shape. */
+int mw_stokes_transfer(mw_stokes* S, int32_t precision, int32_t level, int32_t restrict_dir, const void* in,
+                       void* out, void* stream);
+int mw_stokes_level_shape(const mw_stokes* S, int32_t precision, int32_t level, int32_t* nx, int32_t* nz);
 
 /* K x = b by multigrid-preconditioned CG (replaces splu(K).solve, uzawa3_solver_L2.py:37-38). */
 int mw_stokes_solve_K(mw_stokes* S, int32_t precision, const double* b, double* x, double rtol, int32_t maxit,

@@ -351,6 +351,62 @@ MW_D void prolong_taps(int ix, int iz, const V& coarse, double* s0, double* s1) 
   *s1 = a1;
 }
 
+// Levels whose element count is odd coarsen onto a uniform grid of ceil(n/2) elements over the same
+// box (element size n h / ceil(n/2)), which is not nested in the fine one.  The prolongation
+// there evaluates the coarse Q2 function at each fine node: fine lattice node i (position
+// i L / (2 nf)) lies in coarse element E = floor(i nc / (2 nf)) (the last one at the far end) at
+// local coordinate xi = (i nc - 2 nf E - nf) / nf, and takes the 1D Q2 basis values
+// xi (xi - 1) / 2, (1 - xi)(1 + xi), xi (xi + 1) / 2 of coarse nodes 2E, 2E + 1, 2E + 2; the
+// restriction is its exact transpose.  Nested dimensions (nf = 2 nc) keep the taps above.
+MW_HD bool nested_1d(int nf, int nc) { return nf == 2 * nc; }
+MW_HD bool nested_levels(const LevelGeo& gf, const LevelGeo& gc) {
+  return nested_1d(gf.nx, gc.nx) && nested_1d(gf.nz, gc.nz);
+}
+
+MW_D int q2_weights_1d(int i, int nf, int nc, double* w) {
+  int E = (int)(((int64_t)i * nc) / (2LL * nf));
+  if (E > nc - 1) E = nc - 1;
+  const double xi = (double)((int64_t)i * nc - 2LL * nf * E - nf) / (double)nf;
+  w[0] = 0.5 * xi * (xi - 1.0);
+  w[1] = (1.0 - xi) * (1.0 + xi);
+  w[2] = 0.5 * xi * (xi + 1.0);
+  return E;
+}
+
+// 1D prolongation taps of fine node i: count, coarse nodes J, weights w (nested or not)
+MW_D int pw_g(int i, int nf, int nc, int* J, double* w) {
+  if (nested_1d(nf, nc)) return pw(i, J, w);
+  const int E = q2_weights_1d(i, nf, nc, w);
+  J[0] = 2 * E; J[1] = 2 * E + 1; J[2] = 2 * E + 2;
+  return 3;
+}
+
+// (P x_c) at fine node (ix, iz) between levels gf and gc: prolong_taps when both dimensions are
+// nested, else the same sums over the general taps
+template <typename G, typename V>
+MW_D void prolong_taps_g(const G& gf, const G& gc, int ix, int iz, const V& coarse, double* s0, double* s1) {
+  if (nested_1d(gf.nx, gc.nx) && nested_1d(gf.nz, gc.nz)) {
+    prolong_taps(ix, iz, coarse, s0, s1);
+    return;
+  }
+  int Jx[3] = {0, 0, 0}, Jz[3] = {0, 0, 0};
+  double wx[3] = {0, 0, 0}, wz[3] = {0, 0, 0};
+  const int nxw = pw_g(ix, gf.nx, gc.nx, Jx, wx), nzw = pw_g(iz, gf.nz, gc.nz, Jz, wz);
+  double a0 = 0, a1 = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      if (a < nzw && b < nxw) {
+        const auto v = coarse(Jz[a], Jx[b]);
+        const double w = wz[a] * wx[b];
+        a0 = fma(w, (double)v.x, a0);
+        a1 = fma(w, (double)v.y, a1);
+      }
+  *s0 = a0;
+  *s1 = a1;
+}
+
 // the coarse-correction tile the AM_CHEB_P staging reads: coarse lattice nodes [ex0 - 2, ex0 + 17]
 // x [ez0 - 2, ez0 + 9] cover every tap of the staged fine nodes [2 ex0 - 2, 2 ex0 + 32] x
 // [2 ez0 - 2, 2 ez0 + 16]
@@ -824,19 +880,53 @@ __global__ void k_diag(LevelGeo g, const R* __restrict__ eta, R* __restrict__ di
 
 // coarse viscosity: mean of the 36 fine qpoint values of the 2x2 children (element constant)
 template <typename R>
-__global__ void k_coarsen_eta(LevelGeo gc, const R* __restrict__ fine, R* __restrict__ coarse) {
+__global__ void k_coarsen_eta(LevelGeo gf, LevelGeo gc, const R* __restrict__ fine, R* __restrict__ coarse) {
   pdl_entry();
   const int64_t nel = (int64_t)gc.nx * gc.nz;
-  const int fnx = 2 * gc.nx;
+  const int fnx = gf.nx;
+  const bool nested = nested_levels(gf, gc);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
     int ex = (int)(e % gc.nx), ez = (int)(e / gc.nx);
     double s = 0;
-    for (int a = 0; a < 2; ++a)
-      for (int b = 0; b < 2; ++b) {
-        const R* f = fine + ((int64_t)(2 * ez + a) * fnx + (2 * ex + b)) * 9;
-        for (int q = 0; q < 9; ++q) s += (double)f[q];
+    if (nested) {
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          const R* f = fine + ((int64_t)(2 * ez + a) * fnx + (2 * ex + b)) * 9;
+          for (int q = 0; q < 9; ++q) s += (double)f[q];
+        }
+      s /= 36.0;
+    } else {
+      // the mean over the coarse element of the fine elements' qpoint means, each weighted by its
+      // overlap (coarse edges at e nf, fine edges at f nc, in units of L / (nf nc))
+      auto range = [](int e, int nf, int nc, int* f0, int* f1) {
+        *f0 = (int)(((int64_t)e * nf) / nc);
+        *f1 = (int)(((int64_t)(e + 1) * nf + nc - 1) / nc) - 1;
+        if (*f1 > nf - 1) *f1 = nf - 1;
+      };
+      auto overlap = [](int e, int f, int nf, int nc) {
+        const int64_t a = std::max<int64_t>((int64_t)e * nf, (int64_t)f * nc);
+        const int64_t b = std::min<int64_t>((int64_t)(e + 1) * nf, (int64_t)(f + 1) * nc);
+        return b > a ? (double)(b - a) : 0.0;
+      };
+      int x0, x1, z0, z1;
+      range(ex, gf.nx, gc.nx, &x0, &x1);
+      range(ez, gf.nz, gc.nz, &z0, &z1);
+      double wsum = 0;
+      for (int fz = z0; fz <= z1; ++fz) {
+        const double wz = overlap(ez, fz, gf.nz, gc.nz);
+        for (int fx = x0; fx <= x1; ++fx) {
+          const double w = wz * overlap(ex, fx, gf.nx, gc.nx);
+          if (w == 0.0) continue;
+          const R* f = fine + ((int64_t)fz * fnx + fx) * 9;
+          double m = 0;
+          for (int q = 0; q < 9; ++q) m += (double)f[q];
+          s += w * (m / 9.0);
+          wsum += w;
+        }
       }
-    R v = (R)(s / 36.0);
+      s /= wsum;
+    }
+    R v = (R)s;
     for (int q = 0; q < 9; ++q) coarse[e * 9 + q] = v;
   }
 }
@@ -900,6 +990,59 @@ MW_D void restrict_core(const LevelGeo& gf, const LevelGeo& gc, Fetch fetch, con
   }
 }
 
+// 1D restriction taps of coarse node J (the transpose of pw_g): fine nodes idx with weights w,
+// at most 10 (the fine nodes within the support of J's basis function, nf / nc <= 2)
+constexpr int RMAXT = 10;
+MW_D int restrict_taps_1d(int J, int nf, int nc, int* idx, double* w) {
+  int k = 0;
+  if (nested_1d(nf, nc)) {
+    const int OFF[5] = {-3, -1, 0, 1, 3};
+    for (int t = 0; t < 5; ++t) {
+      const int i = 2 * J + OFF[t];
+      const double v = rw(J, OFF[t]);
+      if (v != 0.0 && i >= 0 && i <= 2 * nf) { idx[k] = i; w[k] = v; ++k; }
+    }
+    return k;
+  }
+  const int lo = J >= 2 ? (int)(((int64_t)(J - 2) * nf) / nc) : 0;
+  int hi = (int)(((int64_t)(J + 2) * nf + nc - 1) / nc);
+  if (hi > 2 * nf) hi = 2 * nf;
+  for (int i = lo; i <= hi && k < RMAXT; ++i) {
+    double q[3];
+    const int E = q2_weights_1d(i, nf, nc, q);
+    const int o = J - 2 * E;
+    if (o >= 0 && o <= 2 && q[o] != 0.0) { idx[k] = i; w[k] = q[o]; ++k; }
+  }
+  return k;
+}
+
+// The restriction at coarse node n when a dimension is not nested: the same epilogue as
+// restrict_core, the fine residual summed over the general taps (z outer, x inner)
+template <typename R, typename Fetch>
+MW_D void restrict_core_g(const LevelGeo& gf, const LevelGeo& gc, Fetch fetch, const uint8_t* fixc, R* bc, double c0,
+                          bool cheb, const R* diag_c, R* xc, R* dc, int64_t n) {
+  const int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
+  int ix[RMAXT], iz[RMAXT];
+  double wx[RMAXT], wz[RMAXT];
+  const int nx = restrict_taps_1d(I, gf.nx, gc.nx, ix, wx), nz = restrict_taps_1d(J, gf.nz, gc.nz, iz, wz);
+  double s0 = 0, s1 = 0;
+  for (int a = 0; a < nz; ++a)
+    for (int b = 0; b < nx; ++b) {
+      R v0, v1;
+      fetch(iz[a], ix[b], &v0, &v1);
+      s0 += wz[a] * wx[b] * (double)v0;
+      s1 += wz[a] * wx[b] * (double)v1;
+    }
+  const R b0 = fixc[2 * n] ? R(0) : (R)s0, b1 = fixc[2 * n + 1] ? R(0) : (R)s1;
+  bc[2 * n] = b0;
+  bc[2 * n + 1] = b1;
+  if (cheb) {
+    const R x0 = R(c0) * b0 / diag_c[2 * n], x1 = R(c0) * b1 / diag_c[2 * n + 1];
+    xc[2 * n] = x0; dc[2 * n] = x0;
+    xc[2 * n + 1] = x1; dc[2 * n + 1] = x1;
+  }
+}
+
 template <typename R>
 MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, const uint8_t* fixc, R* bc, double c0,
                         bool cheb, const R* diag_c, R* xc, R* dc, int64_t n) {
@@ -908,7 +1051,20 @@ MW_D void restrict_node(const LevelGeo& gf, const LevelGeo& gc, const R* rf, con
     *a0 = rf[2 * m];
     *a1 = rf[2 * m + 1];
   };
-  restrict_core(gf, gc, fetch, fixc, bc, c0, cheb, diag_c, xc, dc, n);
+  if (nested_levels(gf, gc)) restrict_core(gf, gc, fetch, fixc, bc, c0, cheb, diag_c, xc, dc, n);
+  else restrict_core_g(gf, gc, fetch, fixc, bc, c0, cheb, diag_c, xc, dc, n);
+}
+
+// the restriction between levels that are not nested, one coarse node per thread
+template <typename R>
+__global__ void k_restrict_g(LevelGeo gf, LevelGeo gc, const R* __restrict__ rf, const uint8_t* __restrict__ fixc,
+                             R* __restrict__ bc, const double* __restrict__ cheb_c, const R* __restrict__ diag_c,
+                             R* __restrict__ xc, R* __restrict__ dc) {
+  pdl_entry();
+  const double c0 = cheb_c ? cheb_c[1] : 0.0;
+  const int64_t nn = (int64_t)gc.nnx * gc.nnz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x)
+    restrict_node(gf, gc, rf, fixc, bc, c0, cheb_c != nullptr, diag_c, xc, dc, n);
 }
 
 // The restriction over a tile of RTX x RTZ coarse nodes (one per thread): the fine residual the
@@ -964,10 +1120,20 @@ MW_D void prolong_node(const LevelGeo& gf, const LevelGeo& gc, const R* xc, cons
   typedef typename Vec2<R>::T R2;
   const int ix = (int)(n % gf.nnx), iz = (int)(n / gf.nnx);
   double s0, s1;
-  prolong_taps(ix, iz, [&](int jz, int jx) { return reinterpret_cast<const R2*>(xc)[(int64_t)jz * gc.nnx + jx]; },
-               &s0, &s1);
+  prolong_taps_g(gf, gc, ix, iz,
+                 [&](int jz, int jx) { return reinterpret_cast<const R2*>(xc)[(int64_t)jz * gc.nnx + jx]; }, &s0, &s1);
   if (!fixf[2 * n]) xf[2 * n] += (R)s0;
   if (!fixf[2 * n + 1]) xf[2 * n + 1] += (R)s1;
+}
+
+// the prolongation between levels that are not nested, one fine node per thread
+template <typename R>
+__global__ void k_prolong_g(LevelGeo gf, LevelGeo gc, const R* __restrict__ xc, const uint8_t* __restrict__ fixf,
+                            R* __restrict__ xf) {
+  pdl_entry();
+  const int64_t nn = (int64_t)gf.nnx * gf.nnz;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x)
+    prolong_node(gf, gc, xc, fixf, xf, n);
 }
 
 // The prolongation over a tile of PTX x PTZ fine nodes (one per thread): the coarse values the tile
@@ -1008,13 +1174,18 @@ __global__ void __launch_bounds__(PTX * PTZ) k_prolong_add(LevelGeo gf, LevelGeo
 }
 
 template <typename R>
-__global__ void k_fix_coarse(LevelGeo gc, const uint8_t* __restrict__ fixf, int fnnx, uint8_t* __restrict__ fixc) {
+__global__ void k_fix_coarse(LevelGeo gf, LevelGeo gc, const uint8_t* __restrict__ fixf, uint8_t* __restrict__ fixc) {
   pdl_entry();
-  // a coarse dof is fixed when the coincident fine dof is fixed (same boundaries)
+  // a coarse dof is fixed when the coincident fine dof is fixed (same boundaries); on a level that
+  // is not nested, the fine node nearest to the coarse one (on the same side of the box: box
+  // conditions depend only on the side)
   const int64_t nn = (int64_t)gc.nnx * gc.nnz;
+  const int fnnx = gf.nnx;
   for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
     int I = (int)(n % gc.nnx), J = (int)(n / gc.nnx);
-    int64_t m = (int64_t)(2 * J) * fnnx + 2 * I;
+    const int fi = nested_1d(gf.nx, gc.nx) ? 2 * I : (int)(((int64_t)I * gf.nx + gc.nx / 2) / gc.nx);
+    const int fj = nested_1d(gf.nz, gc.nz) ? 2 * J : (int)(((int64_t)J * gf.nz + gc.nz / 2) / gc.nz);
+    int64_t m = (int64_t)fj * fnnx + fi;
     fixc[2 * n] = fixf[2 * m];
     fixc[2 * n + 1] = fixf[2 * m + 1];
   }
@@ -1561,11 +1732,18 @@ static void plan_levels(Hierarchy<R>& H, const LevelGeo& fine, const mw_stokes_p
     l.g = g;
     l.deg = (H.nlev == 1 || prm.cheb_degree_coarse <= 0) ? prm.cheb_degree : prm.cheb_degree_coarse;
     l.nn = (int64_t)g.nnx * g.nnz; l.ndof = 2 * l.nn; l.nel = (int64_t)g.nx * g.nz;
-    bool can = (g.nx % 2 == 0) && (g.nz % 2 == 0) && (g.nx / 2 >= prm.coarse_min) && (g.nz / 2 >= prm.coarse_min) &&
+    // even element counts halve (nested levels); odd ones, with coarsen_odd, go to ceil(n / 2)
+    // elements over the same box (a level that is not nested in this one)
+    const bool odd_ok = prm.coarsen_odd != 0;
+    const int cx = (g.nx % 2 == 0) ? g.nx / 2 : (odd_ok ? (g.nx + 1) / 2 : 0);
+    const int cz = (g.nz % 2 == 0) ? g.nz / 2 : (odd_ok ? (g.nz + 1) / 2 : 0);
+    bool can = cx > 0 && cz > 0 && cx < g.nx && cz < g.nz && cx >= prm.coarse_min && cz >= prm.coarse_min &&
                H.nlev < MAXLEV && (l.nel > (int64_t)prm.coarse_min * prm.coarse_min);
     if (!can) break;
     LevelGeo c = g;
-    c.nx = g.nx / 2; c.nz = g.nz / 2; c.nnx = 2 * c.nx + 1; c.nnz = 2 * c.nz + 1; c.hx = 2 * g.hx; c.hz = 2 * g.hz;
+    c.nx = cx; c.nz = cz; c.nnx = 2 * c.nx + 1; c.nnz = 2 * c.nz + 1;
+    c.hx = g.nx == 2 * cx ? 2 * g.hx : g.hx * g.nx / cx;
+    c.hz = g.nz == 2 * cz ? 2 * g.hz : g.hz * g.nz / cz;
     g = c;
   }
   const Level<R>& lc = H.L[H.nlev - 1];
@@ -2104,13 +2282,21 @@ static void vcycle(Hierarchy<R>& H, int l, cudaStream_t s, bool first_done = fal
   a.u = L.x; a.eta = L.eta; a.fix = L.fix; a.diag = L.diag; a.yV = L.r; a.bV = L.b;
   launch_apply<R, AM_RESID>(L.g, a, s);
   const bool fuse = !(l + 1 == H.nlev - 1 && H.dense);
-  pdl_launch(k_restrict<R>, dim3((C.g.nnx + RTX - 1) / RTX, (C.g.nnz + RTZ - 1) / RTZ), RTX * RTZ, 0, s, L.g, C.g,
-             L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
-             C.x, C.d);
+  const bool nested = nested_levels(L.g, C.g);
+  if (nested)
+    pdl_launch(k_restrict<R>, dim3((C.g.nnx + RTX - 1) / RTX, (C.g.nnz + RTZ - 1) / RTZ), RTX * RTZ, 0, s, L.g, C.g,
+               L.r, C.fix, C.b, fuse ? C.cheb : nullptr, C.diag,
+               C.x, C.d);
+  else
+    pdl_launch(k_restrict_g<R>, grid_for(C.nn, 256), 256, 0, s, L.g, C.g, L.r, C.fix, C.b, fuse ? C.cheb : nullptr,
+               C.diag, C.x, C.d);
   vcycle(H, l + 1, s, fuse);
-  if (!fused_prolongation()) {                     // x += P x_c as its own launch, then the smoothing
-    pdl_launch(k_prolong_add<R>, dim3((L.g.nnx + PTX - 1) / PTX, (L.g.nnz + PTZ - 1) / PTZ), PTX * PTZ, 0, s, L.g,
-               C.g, (const R*)C.x, L.fix, L.x);
+  if (!fused_prolongation() || !nested) {          // x += P x_c as its own launch, then the smoothing
+    if (nested)
+      pdl_launch(k_prolong_add<R>, dim3((L.g.nnx + PTX - 1) / PTX, (L.g.nnz + PTZ - 1) / PTZ), PTX * PTZ, 0, s, L.g,
+                 C.g, (const R*)C.x, L.fix, L.x);
+    else
+      pdl_launch(k_prolong_g<R>, grid_for(L.nn, 256), 256, 0, s, L.g, C.g, (const R*)C.x, L.fix, L.x);
     smooth(L, L.deg, false, s);
     return;
   }
@@ -2239,8 +2425,8 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
     Level<R>& L = H.L[l];
     if (l > 0) {
       Level<R>& F = H.L[l - 1];
-      pdl_launch(k_coarsen_eta<R>, grid_for(L.nel, 256), 256, 0, s, L.g, F.eta, L.eta);
-      pdl_launch(k_fix_coarse<R>, grid_for(L.nn, 256), 256, 0, s, L.g, F.fix, F.g.nnx, L.fix);
+      pdl_launch(k_coarsen_eta<R>, grid_for(L.nel, 256), 256, 0, s, F.g, L.g, F.eta, L.eta);
+      pdl_launch(k_fix_coarse<R>, grid_for(L.nn, 256), 256, 0, s, F.g, L.g, F.fix, L.fix);
     }
     pdl_launch(k_diag<R>, grid_for(L.nn, 128), 128, 0, s, L.g, L.eta, L.diag);
   }
@@ -2845,6 +3031,21 @@ static bool stokes_solve_record(mw_stokes* S, const double* f, const double* h, 
 }
 
 template <typename R>
+static int transfer_level(Hierarchy<R>& H, int level, int restrict_dir, const void* in, void* out, cudaStream_t s) {
+  if (level < 0 || level + 1 >= H.nlev) return MW_ERR_BAD_ARG;
+  const Level<R>& F = H.L[level];
+  const Level<R>& C = H.L[level + 1];
+  if (restrict_dir)
+    pdl_launch(k_restrict_g<R>, grid_for(C.nn, 256), 256, 0, s, F.g, C.g, (const R*)in, (const uint8_t*)C.fix,
+               (R*)out, (const double*)nullptr, (const R*)nullptr, (R*)nullptr, (R*)nullptr);
+  else
+    pdl_launch(k_prolong_g<R>, grid_for(F.nn, 256), 256, 0, s, F.g, C.g, (const R*)in, (const uint8_t*)F.fix,
+               (R*)out);
+  MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+template <typename R>
 __global__ void k_cast(int64_t n, const double* __restrict__ a, R* __restrict__ b) {
   pdl_entry();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -2887,6 +3088,7 @@ void mw_stokes_default_params(mw_stokes_params* p) {
   p->power_iters = 40;
   p->power_iters_warm = 3;
   p->tail_nel = 0;
+  p->coarsen_odd = 1;
 }
 
 void mw_solve_default_params(mw_solve_params* p) {
@@ -3036,6 +3238,25 @@ int mw_stokes_vcycle(mw_stokes* S, int32_t precision, const void* b, void* x, vo
     pdl_launch(k_copy<double, double>, grid_for(L.ndof, 256), 256, 0, s, L.ndof, L.x, (double*)x);
   }
   MW_CHECK_LAUNCH();
+  return MW_OK;
+}
+
+int mw_stokes_transfer(mw_stokes* S, int32_t precision, int32_t level, int32_t restrict_dir, const void* in,
+                       void* out, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!S || !in || !out) return MW_ERR_BAD_ARG;
+  if (int rc = ensure_hierarchy(S, precision, s)) return rc;
+  return precision == MW_F32 ? transfer_level(S->H32, level, restrict_dir, in, out, s)
+                             : transfer_level(S->H64, level, restrict_dir, in, out, s);
+}
+
+int mw_stokes_level_shape(const mw_stokes* S, int32_t precision, int32_t level, int32_t* nx, int32_t* nz) {
+  const auto& H32 = S->H32;
+  const auto& H64 = S->H64;
+  const int nlev = precision == MW_F32 ? H32.nlev : H64.nlev;
+  if (!nx || !nz || level < 0 || level >= nlev) return MW_ERR_BAD_ARG;
+  *nx = precision == MW_F32 ? H32.L[level].g.nx : H64.L[level].g.nx;
+  *nz = precision == MW_F32 ? H32.L[level].g.nz : H64.L[level].g.nz;
   return MW_OK;
 }
 

@@ -467,6 +467,8 @@ k_ens_stokes(const EnsMember* __restrict__ members, const int* __restrict__ orde
     nref += 1;
     go = isfinite(rel) && rel > prm.tol && nref < (double)prm.max_refine && status == 0;
   }
+  // no CTA leaves while another may still read its shared memory (the last ens_sum's remote loads)
+  cluster_barrier();
   if (c.rank == 0 && threadIdx.x == 0) {
     double* sc = M.sc;
     sc[S_BB] = v2[0]; sc[S_BH] = v2[1]; sc[S_BNORM] = bnorm;

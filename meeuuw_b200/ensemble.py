@@ -11,10 +11,10 @@ Stokes solver (its own stream and recorded CUDA graphs), so nothing is shared be
 ``Autotuner`` picks the number of host threads (the concurrency level) by timing ensemble steps,
 and caches the choice per GPU and ensemble shape.
 
-``BatchedEnsemble`` runs the Stokes solves of all models in one launch instead (one thread-block
+``BatchedEnsemble`` runs the Stokes solves of the models in one launch instead (one thread-block
 cluster per model running that model's whole mixed-precision solve,
-``stokes.StokesEnsembleSolve``), between the models' other phases on their own streams; the whole
-ensemble step is recorded as one CUDA graph.
+``stokes.StokesEnsembleSolve``), between the models' other phases, which replay from recorded
+graphs on the models' own streams.
 
 Many streams share the GPU's hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS, 8 by default): a
 process running a large ensemble should set it higher (up to 32) before CUDA is initialised, so
@@ -173,15 +173,17 @@ class BatchedEnsemble:
     """N independent models whose Stokes solves run in one launch.
 
     A step: every model's phases up to the solve (particles, projections, right-hand side,
-    viscosity, multigrid hierarchy) on its own stream; then one launch in which a thread-block
-    cluster per model runs that model's whole solve (its own hierarchy, iteration counts and
-    convergence tests, no waiting between clusters); then every model's phases after the solve
-    (energy, Nu, vrms, advection, locate) on its own stream.  After each model's cold first step
-    (eager, with the guess hook if one is given), the whole step is recorded as one CUDA graph and
-    replayed.  A model whose device flags are set is retired with the reference's message and the
-    step is recorded again without it."""
+    viscosity, multigrid hierarchy) replayed from the model's own recorded graph on its own stream;
+    then one launch in which a thread-block cluster per model runs that model's whole solve (its
+    own hierarchy, iteration counts and convergence tests, no waiting between clusters); then every
+    model's phases after the solve (energy, Nu, vrms, advection, locate), again one recorded graph
+    per model on its stream.  Models with more than `cluster_max_nel` elements (None: no limit)
+    instead replay their whole step as one graph on their own stream, concurrently, since one
+    cluster (8 CTAs) works through a large model's solve more slowly than the whole GPU does.
+    Every model's cold first step runs eagerly (with the guess hook, if one is given).  A model
+    whose device flags are set is retired with the reference's message."""
 
-    def __init__(self, cfgs, tol=1e-8, guess=None, record=True):
+    def __init__(self, cfgs, tol=1e-8, guess=None, cluster_max_nel=None):
         self.cfgs = list(cfgs)
         self.models, self.streams = [], []
         self.first_step_info = []
@@ -201,65 +203,83 @@ class BatchedEnsemble:
         self.active = [True] * len(self.models)
         self.retired = {}
         self.steps_done = len(self.models)
-        self.record = bool(record)
+        self.cluster_max_nel = cluster_max_nel
         self.main = torch.cuda.Stream()
+        self.graphs = {}                          # model index -> (pre, post) or whole-step graph
         self._bind()
 
+    def _in_cluster(self, i):
+        return self.cluster_max_nel is None or self.models[i].nel <= self.cluster_max_nel
+
     def _bind(self):
-        idx = [i for i in range(len(self.models)) if self.active[i]]
-        self.idx = idx
-        ms = [self.models[i] for i in idx]
+        self.idx = [i for i in range(len(self.models)) if self.active[i]]
+        self.batched = [i for i in self.idx if self._in_cluster(i)]
+        self.alone = [i for i in self.idx if not self._in_cluster(i)]
+        ms = [self.models[i] for i in self.batched]
         self.solve = StokesEnsembleSolve([m.solver for m in ms], [m.rhs_f for m in ms], [m.rhs_h for m in ms],
                                          [m.solV for m in ms], [m.solP for m in ms]) if ms else None
-        self.graph = None
 
-    def _body(self):
-        main = torch.cuda.current_stream()
-        for i in self.idx:
-            m, st = self.models[i], self.streams[i]
-            st.wait_stream(main)
-            with torch.cuda.stream(st), ops.workspace_scope(m):
-                m._step_pre()
-                m.solver.prepare("mixed")
-            main.wait_stream(st)
-        m0 = self.models[self.idx[0]]
-        kw = m0.stokes_solve_kw()
-        kw.pop("precision")
-        self.solve.solve(use_guess=True, **kw)
-        for i in self.idx:
-            m, st = self.models[i], self.streams[i]
-            st.wait_stream(main)
-            with torch.cuda.stream(st), ops.workspace_scope(m):
-                m._step_post()
-            main.wait_stream(st)
+    def _record(self, i):
+        """The model's recorded graphs: (pre, post) around the shared solve, or its whole step."""
+        if i in self.graphs:
+            return self.graphs[i]
+        m, st = self.models[i], self.streams[i]
+        torch.cuda.synchronize()
+        if not self._in_cluster(i):
+            with torch.cuda.stream(st):
+                m.capture_step()
+            self.graphs[i] = m.graph
+            return m.graph
+        gs = []
+        for body in (lambda: (m._step_pre(), m.solver.prepare("mixed")), m._step_post):
+            g = torch.cuda.CUDAGraph()
+            m._capturing = True
+            try:
+                with torch.cuda.stream(st), ops.workspace_scope(m):
+                    with torch.cuda.graph(g, stream=st, capture_error_mode="thread_local"):
+                        body()
+            finally:
+                m._capturing = False
+            gs.append(g)
+        m.istep -= 1                              # the post capture counted a step; nothing ran
+        self.graphs[i] = tuple(gs)
+        return self.graphs[i]
 
     def step(self):
         """One time step of every active model."""
         if not self.idx:
             return
-        self.main.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(self.main):
-            if self.record and self.graph is None:
-                g = torch.cuda.CUDAGraph()
-                for i in self.idx:
-                    self.models[i]._capturing = True
-                try:
-                    with torch.cuda.graph(g, stream=self.main, capture_error_mode="thread_local"):
-                        self._body()
-                finally:
-                    for i in self.idx:
-                        self.models[i]._capturing = False
-                        self.models[i].istep -= 1          # the capture recorded the step; nothing ran
-                self.graph = g
-            if self.graph is not None:
-                self.graph.replay()
-            else:
-                self._body()
-        torch.cuda.current_stream().wait_stream(self.main)
+        rec = {i: self._record(i) for i in self.idx}
+        main = self.main
+        main.wait_stream(torch.cuda.current_stream())
+        for i in self.alone:                      # whole steps, concurrently with the rest
+            st = self.streams[i]
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                self.models[i].step()
+        for i in self.batched:
+            st = self.streams[i]
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                rec[i][0].replay()
+            main.wait_stream(st)
+        if self.batched:
+            m0 = self.models[self.batched[0]]
+            kw = m0.stokes_solve_kw()
+            kw.pop("precision")
+            with torch.cuda.stream(main):
+                self.solve.solve(use_guess=True, **kw)
+        for i in self.batched:
+            st = self.streams[i]
+            st.wait_stream(main)
+            with torch.cuda.stream(st):
+                rec[i][1].replay()
+            m = self.models[i]
+            m._replayed = True                    # outcomes are on the device
+            m.istep += 1
+        cur = torch.cuda.current_stream()
         for i in self.idx:
-            self.models[i]._replayed = True                # outcomes are on the device
-            if self.graph is not None:
-                self.models[i].istep += 1
+            cur.wait_stream(self.streams[i])
         self.steps_done += len(self.idx)
         self._retire_flagged()
 
@@ -267,7 +287,8 @@ class BatchedEnsemble:
         changed = False
         for i in self.idx:
             m = self.models[i]
-            flags = int(m.err.item())
+            with torch.cuda.stream(self.streams[i]):
+                flags = int(m.err.item())
             if flags:
                 try:
                     m.check()

@@ -16,7 +16,7 @@ class MwStokesParams(ctypes.Structure):
     _fields_ = [("eta_ref", c_double), ("L_ref", c_double), ("precisions", c_int32), ("coarse_min", c_int32),
                 ("dense_max", c_int32), ("cheb_degree", c_int32), ("cheb_ratio", c_double),
                 ("cheb_safety", c_double), ("power_iters", c_int32), ("power_iters_warm", c_int32),
-                ("tail_nel", c_int32), ("cheb_degree_coarse", c_int32)]
+                ("tail_nel", c_int32), ("cheb_degree_coarse", c_int32), ("coarsen_odd", c_int32)]
 
 
 class MwSolveParams(ctypes.Structure):
@@ -56,6 +56,9 @@ L.extra_protos({
     "mw_stokes_solve": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, MwSolveParams, c_void_p,
                                   c_void_p]),
     "mw_stokes_prepare": (c_int32, [c_void_p, c_int32, c_void_p]),
+    "mw_stokes_transfer": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
+    "mw_stokes_level_shape": (c_int32, [c_void_p, c_int32, c_int32, ctypes.POINTER(c_int32),
+                                        ctypes.POINTER(c_int32)]),
     "mw_stokes_ensemble_create": (c_int32, [c_void_p] * 5 + [c_int32, c_void_p]),
     "mw_stokes_ensemble_solve": (c_int32, [c_void_p, MwSolveParams, c_void_p]),
     "mw_stokes_ensemble_destroy": (c_int32, [c_void_p]),
@@ -104,6 +107,26 @@ class StokesSolver:
         Chebyshev intervals, the coarsest inverse) on the current stream; a solve does this itself,
         an ensemble solve (StokesEnsembleSolve) needs it done per model first."""
         call("mw_stokes_prepare", self.h, PREC[precision], stream_ptr())
+
+    def level_shape(self, level, precision="f64"):
+        """(nx, nz) elements of multigrid level `level` (0: the mesh)."""
+        nx, nz = c_int32(), c_int32()
+        call("mw_stokes_level_shape", self.h, PREC[precision], int(level), ctypes.byref(nx), ctypes.byref(nz))
+        return nx.value, nz.value
+
+    def restrict(self, level, r_fine, precision="f64"):
+        """P^T r from level `level` to level + 1 (fixed coarse dofs zero)."""
+        nx, nz = self.level_shape(level + 1, precision)
+        out = torch.zeros(2 * (2 * nx + 1) * (2 * nz + 1), dtype=r_fine.dtype, device="cuda")
+        call("mw_stokes_transfer", self.h, PREC[precision], int(level), 1, ptr(r_fine), ptr(out), stream_ptr())
+        return out
+
+    def prolong(self, level, x_coarse, precision="f64"):
+        """P x_c from level `level` + 1 to level `level` (zero on the fixed fine dofs)."""
+        nx, nz = self.level_shape(level, precision)
+        out = torch.zeros(2 * (2 * nx + 1) * (2 * nz + 1), dtype=x_coarse.dtype, device="cuda")
+        call("mw_stokes_transfer", self.h, PREC[precision], int(level), 0, ptr(x_coarse), ptr(out), stream_ptr())
+        return out
 
     def apply(self, u=None, p=None, yV=None, yP=None, precision="f64"):
         dt = torch.float32 if precision == "f32" else torch.float64

@@ -7,8 +7,9 @@ model's own solver.
   residual 1e-8 (checked independently with mw_stokes_residual) with outer iteration counts
   within 2 of each other; the solutions agree to 1e-6 relative (two solutions each within the
   tolerance; the dot products are summed in another order).
-* Step level: three steps of a BatchedEnsemble (recorded as one CUDA graph) against the same
-  models stepped alone: vrms and Nu within 1e-6 relative, positions within 1e-9.
+* Step level: three steps of a BatchedEnsemble (each model's phases before and after the solve
+  replayed from its own recorded graphs; with a size limit, the larger models' whole steps) against
+  the same models stepped alone: vrms and Nu within 1e-6 relative, positions within 1e-9.
 """
 import numpy as np
 import pytest
@@ -65,18 +66,22 @@ def test_cluster_solve_matches_per_model_solver(ns):
         assert dv < 1e-6, (m.cfg.name, dv)
 
 
-def test_batched_ensemble_steps_match_models_alone():
+@pytest.mark.parametrize("cluster_max_nel", [None, 900])
+def test_batched_ensemble_steps_match_models_alone(cluster_max_nel):
+    """cluster_max_nel=900: the larger models step alone (whole-step graphs) beside the cluster solve."""
     from meeuuw_b200.ensemble import BatchedEnsemble, sample_configs
     from meeuuw_b200.timestep import GPUModel
     cfgs = sample_configs(4, seed=3, n_range=(16, 48), Ra_range=(1e4, 1e6), contrast_range=(1.0, 1e3))
-    ens = BatchedEnsemble(cfgs)
+    ens = BatchedEnsemble(cfgs, cluster_max_nel=cluster_max_nel)
+    if cluster_max_nel is not None:
+        assert ens.batched and ens.alone, [c.nel for c in cfgs]
     for _ in range(3):
         ens.step()
     ens.synchronize()
     ens.check()
     got = ens.diagnostics()
     xs = [m.x.cpu().numpy() for m in ens.models]
-    assert ens.graph is not None and not ens.retired
+    assert len(ens.graphs) == len(cfgs) and not ens.retired
     for cfg, d, x in zip(cfgs, got, xs):
         assert d["istep"] == 4 and d["stokes"]["converged"] == 1, (cfg.name, d)
         m = GPUModel(cfg, stokes="mixed")

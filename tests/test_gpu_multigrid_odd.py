@@ -1,0 +1,90 @@
+"""Multigrid on meshes whose element counts are odd somewhere down the hierarchy.
+
+An odd element count n coarsens onto a uniform grid of ceil(n/2) elements over the same box, not
+nested in the fine one; the transfers are Q2 interpolation (prolongation) and its transpose.
+* the hierarchy: 90 x 54 elements go 90/54 -> 45/27 -> 23/14 -> 12/7 -> 6/4;
+* prolongation reproduces every quadratic field exactly (coarse nodal values of x^2, xz, z^2, ...
+  interpolate to the fine nodal values), on nested and non-nested level pairs alike;
+* restriction is the exact transpose: <R r, x_c> = <r, P x_c> to rounding (r and x_c zero on the
+  fixed dofs);
+* multigrid-PCG on a 90 x 90 free-slip box at viscosity contrast 1e4 (a random per-element field)
+  converges with the non-nested levels in at least three times fewer iterations than when the
+  hierarchy stops at the first odd count (45 x 45 smoothed as the coarsest level): 124 against 520
+  to 1e-9 in FP64 (measured).
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(nelx, nelz, Lx=1.0, free_slip=True, contrast=1e4, seed=4, **kw):
+    from meeuuw_b200 import _lib
+    from meeuuw_b200.stokes import StokesSolver
+    box = _lib.box_of(nelx, nelz, Lx, 1.0)
+    nnx, nnz = 2 * nelx + 1, 2 * nelz + 1
+    X, Z = np.meshgrid(np.arange(nnx), np.arange(nnz))
+    fix = np.zeros((nnx * nnz, 2), dtype=bool)
+    if free_slip:
+        fix[:, 0] = ((X == 0) | (X == nnx - 1)).ravel()
+        fix[:, 1] = ((Z == 0) | (Z == nnz - 1)).ravel()
+    rng = np.random.default_rng(seed)
+    etaq = np.exp(np.repeat(rng.uniform(-0.5, 0.5, nelx * nelz) * np.log(contrast), 9).reshape(-1, 9))
+    S = StokesSolver(box, torch.as_tensor(fix.ravel()).cuda(), eta_ref=1.0, L_ref=1.0, **kw)
+    S.set_viscosity(torch.as_tensor(etaq).cuda(), torch.as_tensor(etaq[:, 0]).cuda())
+    S.prepare("f64")
+    return S, fix.ravel()
+
+
+def _nodes(nx, nz, Lx):
+    x = np.tile(np.arange(2 * nx + 1) * Lx / (2 * nx), 2 * nz + 1)
+    z = np.repeat(np.arange(2 * nz + 1) / (2 * nz), 2 * nx + 1)
+    return x, z
+
+
+def test_hierarchy_of_odd_counts():
+    S, _ = _solver(90, 54, free_slip=False)
+    shapes = [S.level_shape(l) for l in range(S.levels("f64"))]
+    assert shapes == [(90, 54), (45, 27), (23, 14), (12, 7), (6, 4)], shapes
+    S0, _ = _solver(90, 54, free_slip=False, coarsen_odd=0)
+    assert [S0.level_shape(l) for l in range(S0.levels("f64"))] == [(90, 54), (45, 27)]
+
+
+def test_prolongation_reproduces_quadratics_and_restriction_is_its_transpose():
+    Lx = 1.3
+    S, _ = _solver(90, 54, Lx=Lx, free_slip=False)
+    rng = np.random.default_rng(7)
+    for l in range(S.levels("f64") - 1):
+        (fx, fz), (cx, cz) = S.level_shape(l), S.level_shape(l + 1)
+        xf, zf = _nodes(fx, fz, Lx)
+        xc, zc = _nodes(cx, cz, Lx)
+        for q in (lambda x, z: x * x, lambda x, z: x * z, lambda x, z: z * z - 0.3 * x + 2.0):
+            vc = np.stack([q(xc, zc), -q(xc, zc)], 1).ravel()
+            got = S.prolong(l, torch.as_tensor(vc).cuda()).cpu().numpy()
+            want = np.stack([q(xf, zf), -q(xf, zf)], 1).ravel()
+            assert np.abs(got - want).max() < 1e-12 * max(1.0, np.abs(want).max()), (l, np.abs(got - want).max())
+        r = rng.standard_normal(2 * (2 * fx + 1) * (2 * fz + 1))
+        xc_ = rng.standard_normal(2 * (2 * cx + 1) * (2 * cz + 1))
+        Rr = S.restrict(l, torch.as_tensor(r).cuda()).cpu().numpy()
+        Px = S.prolong(l, torch.as_tensor(xc_).cuda()).cpu().numpy()
+        lhs, rhs = float(Rr @ xc_), float(r @ Px)
+        assert abs(lhs - rhs) <= 1e-12 * (np.abs(Rr).sum() * np.abs(xc_).max() + 1.0), (l, lhs, rhs)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_multigrid_pcg_with_non_nested_levels(precision):
+    its = {}
+    for odd in (1, 0):
+        S, fix = _solver(90, 90, coarsen_odd=odd)
+        rng = np.random.default_rng(2)
+        b = rng.standard_normal(S.nv)
+        b[fix] = 0.0
+        bt = torch.as_tensor(b).cuda()
+        x, it, rr = S.solve_K(bt, precision=precision, rtol=1e-4 if precision == "f32" else 1e-9, maxit=600)
+        yV, _ = S.apply(x, torch.zeros(S.np, dtype=torch.float64, device="cuda"))
+        res = float((bt - yV).norm() / bt.norm())
+        if odd:
+            assert res < (2e-3 if precision == "f32" else 1e-8), (odd, it, res)
+        its[odd] = it
+    assert its[1] * 3 <= its[0] and its[1] < (200 if precision == "f64" else 60), its

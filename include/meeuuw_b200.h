@@ -342,6 +342,9 @@ typedef struct {
   int32_t coarsen_odd;    /* 1: an odd element count coarsens to ceil(n/2) elements over the same box
                              (a grid not nested in the fine one, Q2 interpolation as the transfer);
                              0: coarsening stops at the first odd count                           */
+  int32_t coarse_dense_max; /* keep coarsening below coarse_min (down to 2 elements a side) while the
+                             coarsest level has more unknowns than this (0: off); 168 fits the
+                             one-CTA shared-memory inverse                                          */
 } mw_stokes_params;
 
 typedef struct {

@@ -1739,6 +1739,12 @@ static void plan_levels(Hierarchy<R>& H, const LevelGeo& fine, const mw_stokes_p
     const int cz = (g.nz % 2 == 0) ? g.nz / 2 : (odd_ok ? (g.nz + 1) / 2 : 0);
     bool can = cx > 0 && cz > 0 && cx < g.nx && cz < g.nz && cx >= prm.coarse_min && cz >= prm.coarse_min &&
                H.nlev < MAXLEV && (l.nel > (int64_t)prm.coarse_min * prm.coarse_min);
+    // below coarse_min, down to 2 elements a side, while this level has more unknowns than the
+    // one-CTA shared-memory inverse takes (coarse_dense_max): a 6 x 6 coarsest level (338
+    // unknowns) inverted through global memory took most of a small model's step
+    if (!can && prm.coarse_dense_max > 0 && l.ndof > prm.coarse_dense_max && cx >= 2 && cz >= 2 && cx < g.nx &&
+        cz < g.nz && H.nlev < MAXLEV)
+      can = true;
     if (!can) break;
     LevelGeo c = g;
     c.nx = cx; c.nz = cz; c.nnx = 2 * c.nx + 1; c.nnz = 2 * c.nz + 1;
@@ -3089,6 +3095,7 @@ void mw_stokes_default_params(mw_stokes_params* p) {
   p->power_iters_warm = 3;
   p->tail_nel = 0;
   p->coarsen_odd = 1;
+  p->coarse_dense_max = 168;
 }
 
 void mw_solve_default_params(mw_solve_params* p) {

@@ -257,12 +257,13 @@ class BatchedEnsemble:
             st.wait_stream(main)
             with torch.cuda.stream(st):
                 self.models[i].step()
+        for i in self.batched:                    # fork every model from main first, ...
+            self.streams[i].wait_stream(main)
         for i in self.batched:
-            st = self.streams[i]
-            st.wait_stream(main)
-            with torch.cuda.stream(st):
+            with torch.cuda.stream(self.streams[i]):
                 rec[i][0].replay()
-            main.wait_stream(st)
+        for i in self.batched:                    # ... then join them all (a join inside the fork
+            main.wait_stream(self.streams[i])     # loop would chain the models one after another)
         if self.batched:
             m0 = self.models[self.batched[0]]
             kw = m0.stokes_solve_kw()
@@ -270,9 +271,9 @@ class BatchedEnsemble:
             with torch.cuda.stream(main):
                 self.solve.solve(use_guess=True, **kw)
         for i in self.batched:
-            st = self.streams[i]
-            st.wait_stream(main)
-            with torch.cuda.stream(st):
+            self.streams[i].wait_stream(main)
+        for i in self.batched:
+            with torch.cuda.stream(self.streams[i]):
                 rec[i][1].replay()
             m = self.models[i]
             m._replayed = True                    # outcomes are on the device

@@ -16,7 +16,8 @@ class MwStokesParams(ctypes.Structure):
     _fields_ = [("eta_ref", c_double), ("L_ref", c_double), ("precisions", c_int32), ("coarse_min", c_int32),
                 ("dense_max", c_int32), ("cheb_degree", c_int32), ("cheb_ratio", c_double),
                 ("cheb_safety", c_double), ("power_iters", c_int32), ("power_iters_warm", c_int32),
-                ("tail_nel", c_int32), ("cheb_degree_coarse", c_int32), ("coarsen_odd", c_int32)]
+                ("tail_nel", c_int32), ("cheb_degree_coarse", c_int32), ("coarsen_odd", c_int32),
+                ("coarse_dense_max", c_int32)]
 
 
 class MwSolveParams(ctypes.Structure):

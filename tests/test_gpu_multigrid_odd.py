@@ -2,7 +2,8 @@
 
 An odd element count n coarsens onto a uniform grid of ceil(n/2) elements over the same box, not
 nested in the fine one; the transfers are Q2 interpolation (prolongation) and its transpose.
-* the hierarchy: 90 x 54 elements go 90/54 -> 45/27 -> 23/14 -> 12/7 -> 6/4;
+* the hierarchy: 90 x 54 elements go 90/54 -> 45/27 -> 23/14 -> 12/7 -> 6/4 -> 3/2 (below
+  coarse_min while the coarsest level is too large for the shared-memory inverse);
 * prolongation reproduces every quadratic field exactly (coarse nodal values of x^2, xz, z^2, ...
   interpolate to the fine nodal values), on nested and non-nested level pairs alike;
 * restriction is the exact transpose: <R r, x_c> = <r, P x_c> to rounding (r and x_c zero on the
@@ -46,7 +47,7 @@ def _nodes(nx, nz, Lx):
 def test_hierarchy_of_odd_counts():
     S, _ = _solver(90, 54, free_slip=False)
     shapes = [S.level_shape(l) for l in range(S.levels("f64"))]
-    assert shapes == [(90, 54), (45, 27), (23, 14), (12, 7), (6, 4)], shapes
+    assert shapes == [(90, 54), (45, 27), (23, 14), (12, 7), (6, 4), (3, 2)], shapes
     S0, _ = _solver(90, 54, free_slip=False, coarsen_odd=0)
     assert [S0.level_shape(l) for l in range(S0.levels("f64"))] == [(90, 54), (45, 27)]
 

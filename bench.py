@@ -52,6 +52,9 @@ def parse():
                     help="solver loops driven from the host (same kernels; lets a kernel profiler list every launch)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="instead of the 512x512 model: an uneven ensemble of this many models (64..192 squared)")
+    ap.add_argument("--ensemble-batched-only", action="store_true",
+                    help="with --ensemble: time only the mode with every Stokes solve in one cluster launch, skip "
+                         "the other modes and the accuracy runs (for kernel profiles)")
     return ap.parse_args()
 
 
@@ -692,6 +695,14 @@ def run_ensemble(args):
         ms = replicas.max_over_ranks(s.elapsed_time(e), device="cuda")
         return ms, replicas.sum_over_ranks(ens.steps_done - done0, device="cuda")
 
+    if args.ensemble_batched_only:       # the cluster-solve mode alone, no accuracy runs (kernel profiles)
+        ens = BatchedEnsemble(cfgs)
+        ms, n = timed(ens)
+        if rank == 0:
+            print(json.dumps({"mode": "batched", "models": len(all_cfgs), "model_steps_per_s": n / (ms / 1000.0),
+                              "ms_per_step": ms / args.steps}), flush=True)
+        replicas.finalize()
+        return
     modes = {}
     with ClockSampler(dev) as clk:
         ens = Ensemble(cfgs, stokes="mixed")

@@ -449,7 +449,7 @@ struct ApplySmem {
 // shared memory sm.  A CTA that runs several tiles one after another separates them with a
 // __syncthreads() (the next tile's staging overwrites what this one's epilogue reads).
 template <typename R, int MODE>
-MW_D void apply_tile(const LevelGeo g, const ApplyArgs<R> a, int bx, int bz, ApplySmem<R, MODE>& sm) {
+MW_D void apply_tile(const LevelGeo& g, const ApplyArgs<R>& a, int bx, int bz, ApplySmem<R, MODE>& sm) {
   typedef typename Vec2<R>::T R2;
   constexpr bool CHEB = ApplySmem<R, MODE>::CHEB;
   constexpr bool PRO = ApplySmem<R, MODE>::PRO;
@@ -842,9 +842,9 @@ MW_D void apply_tile(const LevelGeo g, const ApplyArgs<R> a, int bx, int bz, App
 
 template <typename R, int MODE>
 __global__ void __launch_bounds__(APPLY_THREADS, sizeof(R) == 4 ? MW_APPLY_MINB : 1)
-k_apply(LevelGeo g, ApplyArgs<R> a) {
+k_apply(const __grid_constant__ LevelGeo g, const __grid_constant__ ApplyArgs<R> a) {
   pdl_entry();
-  __shared__ ApplySmem<R, MODE> sm;
+  __shared__ ApplySmem<R, MODE> sm;     // (the parameters stay in the constant bank: apply_tile takes references)
   apply_tile<R, MODE>(g, a, blockIdx.x, blockIdx.y, sm);
 }
 

@@ -750,8 +750,8 @@ def run_ensemble(args):
     # FP64 runs of the same models for the same number of steps: at the benchmark's 1e-8 and at 1e-10
     # (the reference both are measured against; FP64 at 1e-8 against it is the floor the tolerance
     # itself sets)
-    def fp64_run(tol):
-        ref = Ensemble(cfgs, stokes="f64", graphs=True, tol=tol)
+    def fp64_run(tol, stokes="f64"):
+        ref = Ensemble(cfgs, stokes=stokes, graphs=True, tol=tol)
         for _ in range(nsteps_done - 1):
             ref.step()
         ref.synchronize()
@@ -773,6 +773,9 @@ def run_ensemble(args):
             "pcg_iters_zero": sum(cold_zero[i]["inner_iters"] for i in sel)}
     fp64, act64 = fp64_run(1e-8)
     tight, act_t = fp64_run(1e-10)
+    # the mixed arm at the reference's own tolerance: what the mixed precision alone costs
+    mixed_tight, act_mt = fp64_run(1e-10, stokes="mixed")
+    err_matched = [abs(mixed_tight[i] - tight[i]) / abs(tight[i]) for i in range(len(cfgs)) if act_mt[i] and act_t[i]]
     best = max(modes, key=lambda k: modes[k]["model_steps_per_s"])
     # the accuracy figures below are the fastest recorded mode's (the thread pool's models are
     # the graphs mode's, stepped from host threads)
@@ -788,12 +791,15 @@ def run_ensemble(args):
     if world > 1:                            # gather the per-model figures on rank 0
         import torch.distributed as dist
         got = [None] * world
-        dist.all_gather_object(got, (err, retired, converged, floor))
+        dist.all_gather_object(got, (err, retired, converged, floor, err_matched))
         err = [x for g in got for x in g[0]]
         retired = {k: v for g in got for k, v in g[1].items()}
         converged = sum(g[2] for g in got)
         floor = sorted(x for g in got for x in g[3])
+        err_matched = [x for g in got for x in g[4]]
     err = sorted(err)
+    em = sorted(err_matched)
+    matched = {"models": len(em), "max": em[-1] if em else None, "median": em[len(em) // 2] if em else None}
     line = {"metric": "aggregate model-timesteps/s, uneven ensemble (64..192 squared, 16 particles/element)",
             "value": modes[best]["model_steps_per_s"], "unit": "model-timesteps/s",
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": modes[best]["ms_per_step"],
@@ -810,6 +816,7 @@ def run_ensemble(args):
                                            "median": err[len(err) // 2] if err else None,
                                            "p90": err[int(0.9 * (len(err) - 1))] if err else None},
             "vrms_rel_err_by_mode": err_modes,
+            "vrms_rel_err_mixed_1e-10_vs_fp64_1e-10": matched,
             "vrms_floor_fp64_1e-8_vs_1e-10": {"max": floor[-1] if floor else None,
                                               "median": floor[len(floor) // 2] if floor else None,
                                               "p90": floor[int(0.9 * (len(floor) - 1))] if floor else None},

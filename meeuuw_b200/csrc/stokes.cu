@@ -445,24 +445,41 @@ struct ApplySmem {
   __align__(16) R2 scx[PRO ? CLZ * CLX : 1];         // AM_CHEB_P: the coarse correction tile
 };
 
+// Where one tile's shared arrays are: the static arrays of k_apply, or an ApplySmem carved from
+// the dynamic shared memory of a kernel that runs several layouts.
+template <typename R>
+struct ApplyPtrs {
+  typedef typename Vec2<R>::T R2;
+  R* su;
+  R2 *spre, *sspare;
+  R *sp, *sye;
+  uchar2* sfix;
+  R2* scx;
+};
+
+template <typename R, int MODE>
+MW_D ApplyPtrs<R> apply_ptrs(ApplySmem<R, MODE>& sm) {
+  return ApplyPtrs<R>{sm.su, sm.spre, sm.sspare, sm.sp, sm.sye, sm.sfix, sm.scx};
+}
+
 // One operator apply over element tile (bx, bz) by the APPLY_THREADS threads of a CTA, in the
-// shared memory sm.  A CTA that runs several tiles one after another separates them with a
+// shared arrays sm.  A CTA that runs several tiles one after another separates them with a
 // __syncthreads() (the next tile's staging overwrites what this one's epilogue reads).
 template <typename R, int MODE>
-MW_D void apply_tile(const LevelGeo& g, const ApplyArgs<R>& a, int bx, int bz, ApplySmem<R, MODE>& sm) {
+MW_D void apply_tile(const LevelGeo& g, const ApplyArgs<R>& a, int bx, int bz, const ApplyPtrs<R>& sm) {
   typedef typename Vec2<R>::T R2;
   constexpr bool CHEB = ApplySmem<R, MODE>::CHEB;
   constexpr bool PRO = ApplySmem<R, MODE>::PRO;
   constexpr int NPRE = ApplySmem<R, MODE>::NPRE;
   constexpr int NJ = ApplySmem<R, MODE>::NJ;
   static_assert(2 * TZ + 1 + 2 * TX <= 2 * NJ, "the spare threads take at most two boundary nodes each");
-  auto& su = sm.su;
-  auto& spre = sm.spre;
-  auto& sspare = sm.sspare;
-  auto& sp = sm.sp;
-  auto& sye = sm.sye;
-  auto& sfix = sm.sfix;
-  auto& scx = sm.scx;
+  R* const su = sm.su;
+  R2* const spre = sm.spre;
+  R2* const sspare = sm.sspare;
+  R* const sp = sm.sp;
+  R* const sye = sm.sye;
+  uchar2* const sfix = sm.sfix;
+  R2* const scx = sm.scx;
   const int ex0 = bx * TX, ez0 = bz * TZ;
   const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
   const int tid = threadIdx.x;
@@ -840,12 +857,407 @@ MW_D void apply_tile(const LevelGeo& g, const ApplyArgs<R>& a, int bx, int bz, A
   }
 }
 
+// The operator apply as a kernel, one tile per CTA.  It repeats apply_tile's arithmetic with its
+// body inline and its own static shared arrays: compiled through apply_tile (parameters by value or
+// by reference), the FP64 Chebyshev mode ran 43 % slower and the plain FP64 512x512 step took 106
+// instead of 93 ms (FP32 the same), measured on one GPU; apply_tile serves the kernels that run
+// several tiles per CTA (the ensemble's cluster solve), and its GPU tests check the two against
+// each other through the solves.
 template <typename R, int MODE>
 __global__ void __launch_bounds__(APPLY_THREADS, sizeof(R) == 4 ? MW_APPLY_MINB : 1)
-k_apply(const __grid_constant__ LevelGeo g, const __grid_constant__ ApplyArgs<R> a) {
+k_apply(LevelGeo g, ApplyArgs<R> a) {
   pdl_entry();
-  __shared__ ApplySmem<R, MODE> sm;     // (the parameters stay in the constant bank: apply_tile takes references)
-  apply_tile<R, MODE>(g, a, blockIdx.x, blockIdx.y, sm);
+  typedef typename Vec2<R>::T R2;
+  // node vectors the epilogue reads for the four nodes each owned element emits (b; b, diag, d),
+  // fetched asynchronously while the element products run (FP32; the FP64 kernel's shared memory
+  // is already at the 48 KB static limit)
+  constexpr bool CHEB = MODE == AM_CHEB || MODE == AM_CHEB_Z || MODE == AM_CHEB_P;
+  constexpr bool PRO = MODE == AM_CHEB_P;
+  constexpr int NPRE = sizeof(R) == 8 ? 0 : (CHEB ? 3 : (MODE == AM_RESID ? 1 : 0));
+  __shared__ __align__(16) R su[LZ * LX * 2];
+  __shared__ __align__(16) R2 spre[(NPRE ? NPRE : 1) * 4 * TX * TZ];
+  constexpr int NJ = APPLY_THREADS - TX * TZ;         // spare threads: right column and top row nodes
+  static_assert(2 * TZ + 1 + 2 * TX <= 2 * NJ, "the spare threads take at most two boundary nodes each");
+  __shared__ __align__(16) R2 sspare[(NPRE ? NPRE : 1) * 2 * NJ];
+  __shared__ R sp[PZ * PX];
+  __shared__ R sye[NEL_T * 22];
+  __shared__ uchar2 sfix[LZ * LX];          // Dirichlet flags of the staged nodes
+  __shared__ __align__(16) R2 scx[PRO ? CLZ * CLX : 1];   // AM_CHEB_P: the coarse correction tile
+  const int ex0 = blockIdx.x * TX, ez0 = blockIdx.y * TZ;
+  const int lx0 = 2 * ex0 - 2, lz0 = 2 * ez0 - 2;      // lattice origin of the staged nodes
+  const int tid = threadIdx.x;
+  const bool use_u = a.u != nullptr, use_p = a.p != nullptr;
+  // Chebyshev coefficients, read now so that no epilogue load waits on them
+  const double c1 = CHEB ? a.cheb[0] : 0.0;
+  const R c2 = CHEB ? R(a.cheb[1]) : R(0);
+  const R cz = MODE == AM_CHEB_Z ? R(a.cheb0[1]) : R(0);
+  // ---- prefetch: the epilogue's node vectors (owned elements), the element viscosities ----
+  // slot j of an owned element: 0 centre (2ex+1, 2ez+1), 1 bottom midpoint (2ex+1, 2ez),
+  // 2 left midpoint (2ex, 2ez+1), 3 corner (2ex, 2ez)
+  if (NPRE && a.yV && tid < TX * TZ) {
+    const int ex = ex0 + tid % TX, ez = ez0 + tid / TX;
+    if (ex < g.nx && ez < g.nz) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int ix = 2 * ex + (j < 2 ? 1 : 0), iz = 2 * ez + ((j & 1) ? 0 : 1);
+        const int64_t n = (int64_t)iz * g.nnx + ix;
+        cp_async_pair<R>(&spre[j * TX * TZ + tid], a.bV + 2 * n);
+        if (NPRE == 3) {
+          cp_async_pair<R>(&spre[(4 + j) * TX * TZ + tid], a.diag + 2 * n);
+          if (MODE == AM_CHEB) cp_async_pair<R>(&spre[(8 + j) * TX * TZ + tid], a.d + 2 * n);
+        }
+      }
+    }
+  }
+  // the spare threads' boundary nodes (at most 2 TZ + 1 + 2 TX = 49, two per spare thread)
+  const bool lastx = ex0 + TX >= g.nx, lastz = ez0 + TZ >= g.nz;
+  const int oz1 = lastz ? 2 * g.nz + 1 : 2 * (ez0 + TZ);
+  const int ncol_v = lastx ? oz1 - 2 * ez0 : 0;
+  const int nrow_v = lastz ? (lastx ? 2 * (g.nx - ex0) : 2 * TX) : 0;
+  if (NPRE && a.yV && tid >= TX * TZ && (lastx || lastz)) {
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+      const int j = tid - TX * TZ + it * NJ;
+      if (j < ncol_v + nrow_v) {
+        const int ix = j < ncol_v ? 2 * g.nx : 2 * ex0 + (j - ncol_v);
+        const int iz = j < ncol_v ? 2 * ez0 + j : 2 * g.nz;
+        const int64_t n = (int64_t)iz * g.nnx + ix;
+        const int q = tid - TX * TZ;
+        cp_async_pair<R>(&sspare[it * NJ + q], a.bV + 2 * n);
+        if (NPRE == 3) {
+          cp_async_pair<R>(&sspare[(2 + it) * NJ + q], a.diag + 2 * n);
+          if (MODE == AM_CHEB) cp_async_pair<R>(&sspare[(4 + it) * NJ + q], a.d + 2 * n);
+        }
+      }
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  R eq[9];
+  if (tid < NEL_T) {
+    const int ex = ex0 - 1 + tid % EX, ez = ez0 - 1 + tid / EX;
+    if (ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz) {
+      const R* eg = a.eta + ((int64_t)ez * g.nx + ex) * 9;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) eq[q] = eg[q];
+    }
+  }
+  // ---- AM_CHEB_P: the coarse correction tile (loaded now, stored after the fine loads) ----
+  constexpr int NCT = PRO ? (CLZ * CLX + APPLY_THREADS - 1) / APPLY_THREADS : 1;
+  R2 cv[NCT];
+  const int cx0 = ex0 - 2, cz0 = ez0 - 2;
+  if constexpr (PRO) {
+#pragma unroll
+    for (int k = 0; k < NCT; ++k) {
+      const int i = tid + k * APPLY_THREADS;
+      const int jz = i / CLX, jx = i - jz * CLX;
+      const int cx = cx0 + jx, cz = cz0 + jz;
+      cv[k].x = 0; cv[k].y = 0;
+      if (i < CLZ * CLX && cx >= 0 && cx < a.gc.nnx && cz >= 0 && cz < a.gc.nnz)
+        cv[k] = reinterpret_cast<const R2*>(a.xc)[(int64_t)cz * a.gc.nnx + cx];
+    }
+  }
+  // x + P x_c on the free dofs of fine node (ix, iz) (the arithmetic of k_prolong_add)
+  auto corrected = [&](int ix, int iz, R2 x, uchar2 ff) -> R2 {
+    double s0, s1;
+    prolong_taps(ix, iz, [&](int jz, int jx) { return scx[(jz - cz0) * CLX + (jx - cx0)]; }, &s0, &s1);
+    if (!ff.x) x.x += (R)s0;
+    if (!ff.y) x.y += (R)s1;
+    return x;
+  };
+  // ---- stage velocity (masked; one vector load per node), pressure ----
+  // A fixed number of nodes per thread, all loads issued before any shared-memory store, so the
+  // staging costs one memory round trip rather than one per node.
+  const R2* u2 = reinterpret_cast<const R2*>(a.u);
+  const uchar2* f2 = reinterpret_cast<const uchar2*>(a.fix);
+  R2* su2 = reinterpret_cast<R2*>(su);
+  constexpr int NST = (LZ * LX + APPLY_THREADS - 1) / APPLY_THREADS;
+  constexpr int NSP = (PZ * PX + APPLY_THREADS - 1) / APPLY_THREADS;
+  R2 sv[NST];
+  uchar2 sf[NST];
+  R spv[NSP];
+  if constexpr (sizeof(R) == 8) {                    // FP64: one node at a time (fewer live registers)
+    if constexpr (PRO) {
+#pragma unroll
+      for (int k = 0; k < NCT; ++k)
+        if (tid + k * APPLY_THREADS < CLZ * CLX) scx[tid + k * APPLY_THREADS] = cv[k];
+      __syncthreads();
+    }
+    for (int i = tid; i < LZ * LX; i += APPLY_THREADS) {
+      const int lz = i / LX, lx = i - lz * LX;
+      const int ix = lx0 + lx, iz = lz0 + lz;
+      R2 v;
+      v.x = 0; v.y = 0;
+      uchar2 ff = make_uchar2(0, 0);
+      if (ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
+        const int64_t n = (int64_t)iz * g.nnx + ix;
+        ff = f2[n];
+        if (use_u) {
+          R2 uu = u2[n];
+          if constexpr (PRO) uu = corrected(ix, iz, uu, ff);
+          v.x = ff.x ? R(0) : uu.x;
+          v.y = ff.y ? R(0) : uu.y;
+        }
+      }
+      su2[i] = v;
+      sfix[i] = ff;
+    }
+    if (use_p)
+      for (int i = tid; i < PZ * PX; i += APPLY_THREADS) {
+        int jz = i / PX, jx = i % PX;
+        int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
+        sp[i] = (px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz) ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+      }
+  } else {
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    const int lz = i / LX, lx = i - lz * LX;
+    const int ix = lx0 + lx, iz = lz0 + lz;
+    sv[k].x = 0; sv[k].y = 0;
+    sf[k] = make_uchar2(0, 0);
+    if (i < LZ * LX && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) {
+      const int64_t n = (int64_t)iz * g.nnx + ix;
+      sf[k] = f2[n];
+      if (MODE == AM_CHEB_Z) {                       // x0 = (1/theta) D^-1 b
+        const R2 bb = reinterpret_cast<const R2*>(a.bV)[n], dg = reinterpret_cast<const R2*>(a.diag)[n];
+        sv[k].x = cz * bb.x / dg.x;
+        sv[k].y = cz * bb.y / dg.y;
+      } else if (use_u) {
+        sv[k] = u2[n];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NSP; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    const int jz = i / PX, jx = i % PX;
+    const int px = ex0 - 1 + jx, pz = ez0 - 1 + jz;
+    spv[k] = (use_p && i < PZ * PX && px >= 0 && px <= g.nx && pz >= 0 && pz <= g.nz)
+                 ? a.p[(int64_t)pz * (g.nx + 1) + px] : R(0);
+  }
+  if constexpr (PRO) {
+#pragma unroll
+    for (int k = 0; k < NCT; ++k)
+      if (tid + k * APPLY_THREADS < CLZ * CLX) scx[tid + k * APPLY_THREADS] = cv[k];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NST; ++k) {
+      const int i = tid + k * APPLY_THREADS;
+      const int lz = i / LX, lx = i - lz * LX;
+      const int ix = lx0 + lx, iz = lz0 + lz;
+      if (i < LZ * LX && ix >= 0 && ix < g.nnx && iz >= 0 && iz < g.nnz) sv[k] = corrected(ix, iz, sv[k], sf[k]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NST; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    if (i < LZ * LX) {
+      R2 v;
+      v.x = sf[k].x ? R(0) : sv[k].x;
+      v.y = sf[k].y ? R(0) : sv[k].y;
+      su2[i] = v;
+      sfix[i] = sf[k];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NSP; ++k) {
+    const int i = tid + k * APPLY_THREADS;
+    if (use_p && i < PZ * PX) sp[i] = spv[k];
+  }
+  }
+  __syncthreads();
+  // ---- element products ----
+  if (tid < NEL_T) {
+    int lex = tid % EX, lez = tid / EX;
+    int ex = ex0 - 1 + lex, ez = ez0 - 1 + lez;
+    if (ex >= 0 && ex < g.nx && ez >= 0 && ez < g.nz) {
+      __align__(16) R ue[18];
+      R pe[4], ye[18], ype[4];
+      const int bx = 2 * lex, bz = 2 * lez;          // staged lattice coords of local node 0
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        int li = (bz + q2_dz(k)) * LX + bx + q2_dx(k);
+        ue[2 * k] = su[2 * li]; ue[2 * k + 1] = su[2 * li + 1];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pe[k] = use_p ? sp[(lez + q1_dz(k)) * PX + lex + q1_dx(k)] : R(0);
+      const R sxe = R(2.0 / g.hx), sze = R(2.0 / g.hz), jace = R(g.hx * g.hz / 4.0), se = R(g.s);
+      if (!use_u)                                   // G p only (the Schur iteration's G d, f - G P)
+        element_apply<R, false, true>(sxe, sze, jace, se, ue, pe, eq, ye, ype, use_p);
+      else if (!a.yV)                               // G^T u only
+        element_apply<R, true, false>(sxe, sze, jace, se, ue, pe, eq, ye, ype, use_p);
+      else
+        element_apply<R>(sxe, sze, jace, se, ue, pe, eq, ye, ype, use_p);
+#pragma unroll
+      for (int k = 0; k < 18; ++k) sye[tid * 22 + k] = ye[k];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sye[tid * 22 + 18 + k] = ype[k];
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  // ---- owned nodes: sums over the incident elements in ascending element order ----
+  // Each owned element's thread takes the four nodes of its lower-left quadrant (centre, bottom
+  // and left edge midpoints, lower-left corner) and its lower-left pressure node, with the element
+  // local indices known at compile time; the spare threads take the nodes on the right and top
+  // mesh boundary, which belong to no element's lower-left quadrant.
+  // prefetched value of array k (0 b, 1 diag, 2 d): slots 0-3 are an owned element's nodes,
+  // slots 4-5 a spare thread's two boundary nodes
+  auto pre_at = [&](int k, int slot) -> R2 {
+    return slot < 4 ? spre[(4 * k + slot) * TX * TZ + tid] : sspare[(2 * k + slot - 4) * NJ + (tid - TX * TZ)];
+  };
+  // velocity node epilogue: Dirichlet rows, then the mode's output.  slot >= 0: b, diag, d were
+  // prefetched; slot < 0: read them here.
+  auto emit = [&](int ix, int iz, R y0, R y1, int slot) {
+    const int64_t n = (int64_t)iz * g.nnx + ix;
+    const int li = (iz - lz0) * LX + (ix - lx0);
+    const uchar2 ff = sfix[li];
+    const bool fixed = (ff.x | ff.y) && use_u;       // calls without a velocity (G p only) pass no diagonal
+    const bool pre = NPRE && slot >= 0;
+    // every load first, none depending on another
+    R2 uu = su2[li];                                 // the staged velocity: exact on free dofs
+    R2 dg{R(0), R(0)}, bb{R(0), R(0)}, dd{R(0), R(0)};
+    if (CHEB) dg = pre ? pre_at(1, slot) : reinterpret_cast<const R2*>(a.diag)[n];
+    else if (fixed) dg = reinterpret_cast<const R2*>(a.diag)[n];
+    if (fixed && MODE != AM_CHEB_Z) {                // the fixed components' values (staged as 0);
+      const R2 raw = reinterpret_cast<const R2*>(a.u)[n];   // a free one keeps its staged value,
+      if (ff.x) uu.x = raw.x;                        // which under AM_CHEB_P carries P x_c
+      if (ff.y) uu.y = raw.y;
+    }
+    if (MODE != AM_APPLY) bb = pre ? pre_at(0, slot) : reinterpret_cast<const R2*>(a.bV)[n];
+    if (MODE == AM_CHEB && c1 != 0.0)                // restart steps never read the old direction
+      dd = pre ? pre_at(2, slot) : reinterpret_cast<const R2*>(a.d)[n];
+    if (MODE == AM_CHEB_Z) {                         // the first step's x and d, both x0
+      const R2 x0{cz * bb.x / dg.x, cz * bb.y / dg.y};
+      if (fixed) uu = x0;
+      dd = x0;
+    }
+    R2 y;
+    y.x = y0;
+    y.y = y1;
+    if (ff.x | ff.y) {                               // eliminated rows act as K_ii u_i
+      const R2 fy = fixed ? R2{dg.x * uu.x, dg.y * uu.y} : R2{R(0), R(0)};
+      if (ff.x) y.x = fy.x;
+      if (ff.y) y.y = fy.y;
+    }
+    if (MODE == AM_APPLY) {
+      reinterpret_cast<R2*>(a.yV)[n] = y;
+    } else if (MODE == AM_RESID) {
+      reinterpret_cast<R2*>(a.yV)[n] = R2{bb.x - y.x, bb.y - y.y};
+    } else {   // Chebyshev step: d = c1 d + c2 D^-1 (b - y); x_out = u + d
+      R2 dn{c2 * (bb.x - y.x) / dg.x, c2 * (bb.y - y.y) / dg.y};
+      if (c1 != 0.0) {
+        dn.x += R(c1) * dd.x;
+        dn.y += R(c1) * dd.y;
+      }
+      reinterpret_cast<R2*>(a.d)[n] = dn;
+      reinterpret_cast<R2*>(a.xo)[n] = R2{uu.x + dn.x, uu.y + dn.y};
+    }
+  };
+  // any velocity node of the tile (incident elements found from the node's parity)
+  auto node_generic = [&](int ix, int iz, int slot) {
+    const bool xo = ix & 1, zo = iz & 1;
+    const int xa = xo ? (ix >> 1) : (ix >> 1) - 1, xb = (ix >> 1);
+    const int za = zo ? (iz >> 1) : (iz >> 1) - 1, zb = (iz >> 1);
+    const bool vxa = xa >= 0, vxb = !xo && xb < g.nx;
+    const bool vza = za >= 0, vzb = !zo && zb < g.nz;
+    const int dxa = xo ? 1 : 2, dza = zo ? 1 : 2;   // offsets inside element xa / za; 0 inside xb / zb
+    R y0 = 0, y1 = 0;
+    if (vza) {
+      const int lez = za - (ez0 - 1);
+      if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, dza);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+      if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, dza);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+    }
+    if (vzb) {
+      const int lez = zb - (ez0 - 1);
+      if (vxa) { const R* ye = sye + (lez * EX + xa - (ex0 - 1)) * 22; int k = q2_local_idx(dxa, 0);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+      if (vxb) { const R* ye = sye + (lez * EX + xb - (ex0 - 1)) * 22; int k = q2_local_idx(0, 0);
+                 y0 += ye[2 * k]; y1 += ye[2 * k + 1]; }
+    }
+    emit(ix, iz, y0, y1, slot);
+  };
+  // any pressure node of the tile
+  auto pnode_generic = [&](int px, int pz) {
+    // incident elements (pz-1, px-1) k=2, (pz-1, px) k=3, (pz, px-1) k=1, (pz, px) k=0
+    const bool l = px >= 1, rr = px < g.nx, bo = pz >= 1, to = pz < g.nz;
+    const int lx = px - ex0, lz = pz - ez0;          // tile-local index of element (px, pz) is (lx+1, lz+1)
+    R y = 0;
+    if (bo && l) y += sye[((lz) * EX + lx) * 22 + 18 + 2];
+    if (bo && rr) y += sye[((lz) * EX + lx + 1) * 22 + 18 + 3];
+    if (to && l) y += sye[((lz + 1) * EX + lx) * 22 + 18 + 1];
+    if (to && rr) y += sye[((lz + 1) * EX + lx + 1) * 22 + 18 + 0];
+    const int64_t n = (int64_t)pz * (g.nx + 1) + px;
+    a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
+  };
+  if (tid < TX * TZ) {
+    const int lx = tid % TX, lz = tid / TX;          // TX is a power of two
+    const int ex = ex0 + lx, ez = ez0 + lz;
+    if (ex < g.nx && ez < g.nz) {
+      const R* e00 = sye + ((lz + 1) * EX + lx + 1) * 22;   // element (ex, ez)
+      const R* eL = e00 - 22;                                 // (ex-1, ez)
+      const R* eB = e00 - EX * 22;                            // (ex, ez-1)
+      const R* eBL = eB - 22;                                 // (ex-1, ez-1)
+      const bool hasL = ex > 0, hasB = ez > 0;
+      if (a.yV) {
+        emit(2 * ex + 1, 2 * ez + 1, e00[16], e00[17], 0);   // centre: local node 8
+        {                                                     // bottom edge midpoint: 6 of (ex,ez-1), 4
+          R y0 = 0, y1 = 0;
+          if (hasB) { y0 += eB[12]; y1 += eB[13]; }
+          y0 += e00[8]; y1 += e00[9];
+          emit(2 * ex + 1, 2 * ez, y0, y1, 1);
+        }
+        {                                                     // left edge midpoint: 5 of (ex-1,ez), 7
+          R y0 = 0, y1 = 0;
+          if (hasL) { y0 += eL[10]; y1 += eL[11]; }
+          y0 += e00[14]; y1 += e00[15];
+          emit(2 * ex, 2 * ez + 1, y0, y1, 2);
+        }
+        {                                                     // lower-left corner: 2, 3, 1, 0
+          R y0 = 0, y1 = 0;
+          if (hasB && hasL) { y0 += eBL[4]; y1 += eBL[5]; }
+          if (hasB) { y0 += eB[6]; y1 += eB[7]; }
+          if (hasL) { y0 += eL[2]; y1 += eL[3]; }
+          y0 += e00[0]; y1 += e00[1];
+          emit(2 * ex, 2 * ez, y0, y1, 3);
+        }
+      }
+      if (a.yP) {                                             // pressure node (ex, ez): 2, 3, 1, 0
+        R y = 0;
+        if (hasB && hasL) y += eBL[18 + 2];
+        if (hasB) y += eB[18 + 3];
+        if (hasL) y += eL[18 + 1];
+        y += e00[18 + 0];
+        const int64_t n = (int64_t)ez * (g.nx + 1) + ex;
+        a.yP[n] = (MODE == AM_RESID) ? a.bP[n] - y : y;
+      }
+    }
+  } else if (lastx || lastz) {
+    // right column ix = 2 nx (rows of this tile) and top row iz = 2 nz (columns of this tile,
+    // the corner taken by the column)
+    const int j0 = tid - TX * TZ, nj = NJ;
+    if (a.yV) {
+#pragma unroll
+      for (int it = 0; it < 2; ++it) {                // the nodes whose vectors were prefetched
+        const int j = j0 + it * nj;
+        if (j < ncol_v + nrow_v) {
+          if (j < ncol_v) node_generic(2 * g.nx, 2 * ez0 + j, 4 + it);
+          else node_generic(2 * ex0 + (j - ncol_v), 2 * g.nz, 4 + it);
+        }
+      }
+    }
+    if (a.yP) {
+      const int pz1 = lastz ? g.nz + 1 : ez0 + TZ;
+      const int ncol = lastx ? pz1 - ez0 : 0;
+      const int nrow = lastz ? (lastx ? g.nx - ex0 : TX) : 0;
+      for (int j = j0; j < ncol + nrow; j += nj) {
+        if (j < ncol) pnode_generic(g.nx, ez0 + j);
+        else pnode_generic(ex0 + (j - ncol), g.nz);
+      }
+    }
+  }
 }
 
 // diag(K): sum over incident elements of the element diagonal, ascending element order.

@@ -102,7 +102,7 @@ MW_D void ens_sum(EnsCtx& c, double (&v)[NV]) {
 template <typename R, int MODE>
 MW_D void ens_apply(EnsCtx& c, const LevelGeo& g, const ApplyArgs<R>& a) {
   const int ntx = (g.nx + TX - 1) / TX, ntz = (g.nz + TZ - 1) / TZ;
-  auto& sm = *reinterpret_cast<ApplySmem<R, MODE>*>(c.tile);
+  const ApplyPtrs<R> sm = apply_ptrs(*reinterpret_cast<ApplySmem<R, MODE>*>(c.tile));
   for (int t = c.rank; t < ntx * ntz; t += ENS_CLUSTER) {
     __syncthreads();
     apply_tile<R, MODE>(g, a, t % ntx, t / ntx, sm);

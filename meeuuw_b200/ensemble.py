@@ -363,3 +363,72 @@ class Autotuner:
         except OSError:
             pass
         return rec
+
+
+def default_modes(guess=None, tol=1e-8):
+    """The ensemble's execution strategies, by name: builders cfgs -> ensemble."""
+    return {
+        "graphs": lambda cfgs: Ensemble(cfgs, stokes="mixed", tol=tol, graphs=True, guess=guess),
+        "threads": lambda cfgs: Ensemble(cfgs, stokes="mixed", tol=tol, threads=32, guess=guess),
+        "batched": lambda cfgs: BatchedEnsemble(cfgs, tol=tol, guess=guess),
+        "batched_le6000": lambda cfgs: BatchedEnsemble(cfgs, tol=tol, guess=guess, cluster_max_nel=6000),
+    }
+
+
+class ModeTuner:
+    """Picks an ensemble's execution strategy -- one recorded step per model, the thread pool, every
+    Stokes solve in one cluster launch, or that launch for the smaller models only -- by building
+    each candidate on the given models and timing a few steps after one settling step; the fastest
+    is kept (its ensemble is returned, the others released).  The choice is cached in a JSON file
+    keyed by GPU name and the ensemble's element counts, so later runs build only the chosen one.
+    Timing with several candidates changes nothing but the state of the returned ensemble's models,
+    which have taken the settling and timed steps."""
+
+    def __init__(self, cache_path=None, modes=None):
+        self.cache_path = cache_path or os.path.join(os.path.expanduser("~"), ".cache", "meeuuw_b200_modes.json")
+        self.modes = modes if modes is not None else default_modes()
+
+    @staticmethod
+    def _key(cfgs):
+        name = torch.cuda.get_device_name()
+        sizes = sorted(c.nel for c in cfgs)
+        return f"{name}|{len(sizes)}|{sum(sizes)}|{sizes[0]}|{sizes[-1]}"
+
+    def _load(self):
+        try:
+            with open(self.cache_path) as f:
+                return json.load(f)
+        except Exception:
+            return {}
+
+    def tune(self, cfgs, steps=2, use_cache=True):
+        """(mode name, its ensemble, seconds per step of every candidate timed)."""
+        key = self._key(cfgs)
+        cache = self._load()
+        if use_cache and key in cache and cache[key]["mode"] in self.modes:
+            name = cache[key]["mode"]
+            return name, self.modes[name](cfgs), cache[key]["seconds_per_step"]
+        timings, best, best_ens = {}, None, None
+        for name, build in self.modes.items():
+            ens = build(cfgs)
+            ens.step()                            # settle: recording, workspaces
+            ens.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(steps):
+                ens.step()
+            ens.synchronize()
+            timings[name] = (time.perf_counter() - t0) / steps
+            if best is None or timings[name] < timings[best]:
+                if best_ens is not None and hasattr(best_ens, "close"):
+                    best_ens.close()
+                best, best_ens = name, ens
+            elif hasattr(ens, "close"):
+                ens.close()
+        cache[key] = {"mode": best, "seconds_per_step": timings}
+        try:
+            os.makedirs(os.path.dirname(self.cache_path), exist_ok=True)
+            with open(self.cache_path, "w") as f:
+                json.dump(cache, f, indent=1)
+        except OSError:
+            pass
+        return best, best_ens, timings

@@ -53,3 +53,42 @@ def test_autotuner_picks_fastest_and_caches(tmp_path, monkeypatch):
     ens2 = _FakeEnsemble()
     rec2 = Autotuner(cache_path=str(path)).tune(ens2)
     assert rec2["threads"] == 4 and ens2.threads == 4        # from the cache, without timing
+
+
+class _FakeModeEnsemble:
+    """An ensemble whose step takes `dt` seconds."""
+
+    def __init__(self, dt):
+        self.dt, self.closed = dt, False
+
+    def step(self):
+        time.sleep(self.dt)
+
+    def synchronize(self):
+        pass
+
+    def close(self):
+        self.closed = True
+
+
+def test_mode_tuner_picks_fastest_strategy_and_caches(tmp_path, monkeypatch):
+    from meeuuw_b200.ensemble import ModeTuner
+    monkeypatch.setattr(torch.cuda, "get_device_name", lambda *a: "fake-gpu")
+    built = []
+
+    def mode(dt):
+        def build(cfgs):
+            e = _FakeModeEnsemble(dt)
+            built.append(e)
+            return e
+        return build
+    modes = {"graphs": mode(0.004), "threads": mode(0.012), "batched": mode(0.020)}
+    cfgs = sample_configs(4, seed=1)
+    path = tmp_path / "modes.json"
+    name, ens, t = ModeTuner(cache_path=str(path), modes=modes).tune(cfgs, steps=2)
+    assert name == "graphs" and ens is built[0] and set(t) == set(modes)
+    assert t["graphs"] < t["threads"] < t["batched"]
+    assert not built[0].closed and built[1].closed and built[2].closed   # the others released
+    built.clear()
+    name2, ens2, _ = ModeTuner(cache_path=str(path), modes=modes).tune(cfgs)
+    assert name2 == "graphs" and len(built) == 1                        # from the cache: one build

@@ -91,3 +91,16 @@ def test_batched_ensemble_steps_match_models_alone(cluster_max_nel):
         assert abs(d["vrms"] / r["vrms"] - 1) < 1e-6, (cfg.name, d["vrms"], r["vrms"])
         assert abs(d["Nu"] / r["Nu"] - 1) < 1e-6, (cfg.name, d["Nu"], r["Nu"])
         assert np.max(np.abs(x - m.x.cpu().numpy())) < 1e-9, cfg.name
+
+
+def test_mode_tuner_on_device(tmp_path):
+    """The strategy tuner builds and times real ensembles and returns a working one."""
+    from meeuuw_b200.ensemble import ModeTuner, default_modes, sample_configs
+    cfgs = sample_configs(3, seed=5, n_range=(16, 32), Ra_range=(1e4, 1e5), contrast_range=(1.0, 1e2))
+    modes = {k: v for k, v in default_modes().items() if k in ("graphs", "batched")}
+    name, ens, t = ModeTuner(cache_path=str(tmp_path / "m.json"), modes=modes).tune(cfgs, steps=1)
+    assert name in modes and set(t) == set(modes) and min(t.values()) == t[name]
+    ens.step()
+    ens.synchronize()
+    ens.check()
+    assert all(d["stokes"]["converged"] == 1 for d in ens.diagnostics())

@@ -453,7 +453,8 @@ int mw_stokes_solve(mw_stokes* S, const double* f, const double* h, double* solV
  * right-hand sides f, h and solutions V, P (device arrays that stay in place; V 16-byte aligned);
  * before each ensemble solve, every model's viscosity is set (mw_stokes_set_viscosity) and its
  * hierarchy prepared (mw_stokes_prepare, on a stream ordered before the solve).  The solve takes
- * precision MW_F32 and no history; each model's outcome is read with mw_stokes_device_info.
+ * precision MW_F32 and no history (MW_ERR_BAD_ARG otherwise, and while any model's viscosity was set
+ * after its last mw_stokes_prepare); each model's outcome is read with mw_stokes_device_info.
  * Replaces, for an ensemble, the per-model mw_stokes_solve calls (one per model and step). */
 typedef struct mw_stokes_ensemble mw_stokes_ensemble;
 int mw_stokes_prepare(mw_stokes* S, int32_t precision, void* stream);

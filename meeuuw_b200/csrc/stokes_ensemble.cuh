@@ -482,6 +482,7 @@ k_ens_stokes(const EnsMember* __restrict__ members, const int* __restrict__ orde
 // ---------------------------------------------------------------- C ABI
 struct mw_stokes_ensemble {
   int n = 0;
+  std::vector<mw_stokes*> solvers;   // to refuse a solve while a model's hierarchy is out of date
   mw::EnsMember* d_members = nullptr;
   int* d_order = nullptr;
   ~mw_stokes_ensemble() {
@@ -525,6 +526,7 @@ int mw_stokes_ensemble_create(mw_stokes* const* S, const double* const* f, const
   for (int i = 0; i < n; ++i) order[i] = size[i].second;
   auto* E = new mw_stokes_ensemble();
   E->n = n;
+  E->solvers.assign(S, S + n);
   if (cudaMalloc(&E->d_members, sizeof(EnsMember) * n) != cudaSuccess ||
       cudaMalloc(&E->d_order, sizeof(int) * n) != cudaSuccess ||
       cudaMemcpy(E->d_members, mem.data(), sizeof(EnsMember) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -550,6 +552,8 @@ int mw_stokes_prepare(mw_stokes* S, int32_t precision, void* stream) {
 int mw_stokes_ensemble_solve(mw_stokes_ensemble* E, mw_solve_params sp, void* stream) {
   using namespace mw;
   if (!E || sp.precision != MW_F32 || sp.history) return MW_ERR_BAD_ARG;
+  for (const mw_stokes* s : E->solvers)            // viscosity set but hierarchy not prepared
+    if (s->dirty32) return MW_ERR_BAD_ARG;
   EnsParams p;
   p.tol = sp.tol; p.inner_rtol = sp.inner_rtol; p.sweep_reduction = sp.sweep_reduction; p.sweep_target = sp.sweep_target;
   p.max_inner = sp.max_inner; p.max_outer = sp.max_outer; p.max_refine = sp.max_refine;

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -2872,15 +2873,19 @@ static int setup_hierarchy(mw_stokes* S, Hierarchy<R>& H, cudaStream_t s) {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // the attribute is set once per device and size (so that a setup recorded into a CUDA graph
-    // issues no attribute call)
-    static size_t smem_set[64] = {0};
-    bool smem_ok = dev >= 0 && dev < 64 && smem <= smem_set[dev];
-    if (!smem_ok && smem <= (size_t)optin &&
-        cudaFuncSetAttribute(k_gauss_jordan_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
-            cudaSuccess) {
-      smem_ok = true;
-      if (dev >= 0 && dev < 64) smem_set[dev] = smem;
+    // the kernel's shared-memory limit is raised once per device, to the device's maximum and under
+    // a lock: solvers set up from several host threads never call it again (nor lower it under
+    // another thread's launch, which setting it per size allowed), and a setup recorded into a CUDA
+    // graph issues no attribute call after the first set-up
+    static std::mutex attr_mu;
+    static bool attr_set[64] = {false};
+    bool smem_ok = false;
+    if (smem <= (size_t)optin && dev >= 0 && dev < 64) {
+      std::lock_guard<std::mutex> lock(attr_mu);
+      if (!attr_set[dev])
+        attr_set[dev] = cudaFuncSetAttribute(k_gauss_jordan_smem, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             optin) == cudaSuccess;
+      smem_ok = attr_set[dev];
     }
     if (smem_ok)
       pdl_launch(k_gauss_jordan_smem, 1, 1024, smem, ds, H.nd, H.Ainv);

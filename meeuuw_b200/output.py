@@ -153,7 +153,11 @@ class OutputStream:
         self.z_V = j.ravel() * model.box.hz / 2
         self.side = torch.cuda.Stream()
         self.slots = [self._slot(), self._slot()]
-        self.busy = [None, None]                                 # the event that frees each slot
+        # a slot is reused once the writer thread is done with its host buffers (waiting only for its
+        # copy to the host let a new snapshot overwrite a file's data while the file was written)
+        self.free = [threading.Event(), threading.Event()]
+        for f in self.free:
+            f.set()
         self.next = 0
         self.pvd_sol = Pvd(os.path.join(folder, "solution.pvd"))
         self.pvd_swarm = Pvd(os.path.join(folder, "swarm.pvd"))
@@ -187,8 +191,8 @@ class OutputStream:
             return
         k = self.next
         self.next ^= 1
-        if self.busy[k] is not None:
-            self.busy[k].synchronize()                            # the slot's previous copy to host
+        self.free[k].wait()                                       # the slot's previous files are written
+        self.free[k].clear()
         dev, host = self.slots[k]
         cur = torch.cuda.current_stream()
         for name, v in self._sources().items():                   # device snapshot, on the step's stream
@@ -201,18 +205,20 @@ class OutputStream:
                 host[name].copy_(dev[name], non_blocking=True)
             done = torch.cuda.Event()
             done.record(self.side)
-        self.busy[k] = done
-        self.q.put((istep, time, sol, sw, host, done))
+        self.q.put((k, istep, time, sol, sw, host, done))
 
     def _writer(self):
         while True:
             item = self.q.get()
             if item is None:
                 return
+            k = item[0]
             try:
-                self._write(*item)
+                self._write(*item[1:])
             except Exception as ex:                               # reported by the next submit / close
                 self.error = ex
+            finally:
+                self.free[k].set()
 
     def _write(self, istep, time, sol, sw, host, done):
         done.synchronize()
